@@ -1,0 +1,165 @@
+/*
+ * lesgpu.h -- C ABI of the B200 LES time-step library (liblesgpu.so).
+ *
+ * Drop-in boundary for the Fortran module entry points of the reference
+ * pseudo-spectral ABL LES (fmargairaz/new-repo, src/).  The reference's
+ * operators are Fortran subroutines that read and write module-global arrays
+ * (system.f90:21-43); here the same arrays live in HBM inside an opaque
+ * les_state and every entry point acts on them.  Fields are addressed by
+ * les_field ids and moved with les_upload / les_download in the Fortran
+ * layout (nx, ny, 0:nz+1), x fastest, as real(8).
+ *
+ * Every function returns 0 on success or a nonzero status that mirrors the
+ * reference's decomp_2d_abort codes (1 invalid option, 3 out of memory,
+ * 9 numerical failure, 22 I/O); les_last_error() gives the message.  Calls
+ * on one state are not re-entrant; each state owns one CUDA stream.
+ */
+#ifndef LESGPU_H
+#define LESGPU_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (decomp_2d_abort codes of the reference). */
+#define LES_OK 0
+#define LES_ERR_INVALID 1
+#define LES_ERR_NOMEM 3
+#define LES_ERR_NUMERICAL 9
+#define LES_ERR_IO 22
+
+/* sgs_model (compute_sgs.f90:124-175) */
+#define LES_SGS_CST_SMAG 0
+#define LES_SGS_DYN_SMAG 1
+#define LES_SGS_LASD 2
+/* wall_model (compute_wall_law.f90:119-151) */
+#define LES_WALL_FILTER 0
+#define LES_WALL_INST 1
+#define LES_WALL_HOMOG 2
+/* dealiasing build option (src/Makefile:16-26) */
+#define LES_DEALIAS_PADD 0
+#define LES_DEALIAS_TRUNC 1
+/* halo of the Lagrangian interpolation */
+#define LES_HALO_REFERENCE_1X1 0
+#define LES_HALO_PERIODIC 1
+/* precision */
+#define LES_FP64 0
+#define LES_MIXED 1
+
+/* Non-dimensional run parameters, as parameters_IO.f90:238-277 leaves them
+ * after read_parameters (lengths divided by zi, lx/ly already times pi). */
+typedef struct les_params {
+  int nx, ny, nz;
+  double dt;
+  double lx, ly, lz;
+  double z0;        /* lbc_dz0 / zi (set_bc_surface) */
+  double pfx, pfy;  /* mean pressure-gradient forcing */
+  double cs0;       /* constant Smagorinsky coefficient */
+  int sgs_model;
+  int cs_count, dyn_init;
+  int wall_law;     /* lbc_special == 'wall_law' */
+  int wall_model;
+  int dealias;
+  int lag_halo;
+  int precision;
+  int device;
+} les_params;
+
+/* Field ids: the global arrays of system.f90:21-43 and the SGS module state
+ * (compute_sgs.f90:31, compute_LagScaleDep.f90:33-36).  All are stored as
+ * (nx, ny, 0:nz+1); arrays the reference dimensions (nx,ny,nz) or
+ * (nx,ny,nz+1) use levels 1..nz or 1..nz+1 of that storage. */
+typedef enum les_field {
+  LES_U = 0, LES_V, LES_W,
+  LES_DUDX, LES_DUDY, LES_DUDZ, LES_DVDX, LES_DVDY, LES_DVDZ, LES_DWDX, LES_DWDY, LES_DWDZ,
+  LES_P, LES_DPDX, LES_DPDY, LES_DPDZ,
+  LES_RHSX, LES_RHSY, LES_RHSZ, LES_RHSX_F, LES_RHSY_F, LES_RHSZ_F,
+  LES_TXX, LES_TXY, LES_TXZ, LES_TYY, LES_TYZ, LES_TZZ,
+  LES_CS_OPT2, LES_NU_T,
+  LES_F_LM, LES_F_MM, LES_F_QN, LES_F_NN, LES_BETA,
+  LES_U_LAG, LES_V_LAG, LES_W_LAG,
+  LES_NFIELDS
+} les_field;
+
+/* Plane ids (nx, ny): boundary values, pressure-BC layers, roughness, u*. */
+typedef enum les_plane {
+  LES_LBC_U = 0, LES_LBC_V, LES_LBC_W, LES_UBC_U, LES_UBC_V, LES_UBC_W,
+  LES_BOTTOM_WK_PRESS, LES_TOP_WK_PRESS, LES_LBC_Z0, LES_U_STAR_AVG,
+  LES_NPLANES
+} les_plane;
+
+typedef struct les_state les_state;
+
+/* --- lifetime (replaces create_system system.f90:66, the *_init routines
+ *     LES_engine.f90:130-153 and clean_system system.f90:214) ----------- */
+int les_create(const les_params* p, les_state** out);
+int les_destroy(les_state* s);
+const char* les_last_error(void);
+
+/* --- data movement: host pointers are borrowed for the call ------------ */
+/* levels k0..k1 (inclusive) of field id, host array (nx, ny, k1-k0+1) */
+int les_upload(les_state* s, int field, const double* host, int k0, int k1);
+int les_download(les_state* s, int field, double* host, int k0, int k1);
+int les_upload_plane(les_state* s, int plane, const double* host);
+int les_download_plane(les_state* s, int plane, double* host);
+/* Initial state: the ic_type='files' path (initial_conditions.f90:130-212):
+ * u, v, w as (nx, ny, nz) arrays, then the initial boundary conditions. */
+int les_set_initial_conditions(les_state* s, const double* u, const double* v, const double* w);
+/* Boundary-condition types of set_bc (0 none, 1 'drc', 2 'neu') for u,v,w. */
+int les_set_bc_types(les_state* s, const int lbc_typ[3], const int ubc_typ[3]);
+/* Flags of the Lagrangian model: F_coeff_init and Lagran_init
+ * (compute_LagScaleDep.f90:31,66,288). */
+int les_set_lagrangian_init(les_state* s, int f_coeff_init);
+int les_get_lagrangian_init(les_state* s, int* f_coeff_init);
+
+/* --- module entry points ------------------------------------------------ */
+/* compute_derivatives.f90:94-137 grad_velocity_filt(f, dfdx, dfdy) */
+int les_grad_velocity_filt(les_state* s, int f, int dfdx, int dfdy);
+/* compute_derivatives.f90:375-400 ddz_uv(dfdz, f) */
+int les_ddz_uv(les_state* s, int dfdz, int f);
+/* compute_derivatives.f90:413-441 ddz_w(dfdz, f) */
+int les_ddz_w(les_state* s, int dfdz, int f);
+/* compute_derivatives.f90:464-577 div_stress(rhs, tx, ty, tz, stag[, bottom, top]);
+ * with stag == 0 the bottom_wk_press/top_wk_press planes are written. */
+int les_div_stress(les_state* s, int rhs, int tx, int ty, int tz, int stag);
+/* compute_convective_padd.f90:115-262 / compute_convective_trunc.f90:115-235
+ * compute_dealias_convec(cx, cy, cz) */
+int les_compute_dealias_convec(les_state* s, int cx, int cy, int cz);
+/* compute_pressure.f90:116-242 press_stag_array(tadv1) */
+int les_press_stag_array(les_state* s, double tadv1);
+/* compute_wall_law.f90:198-254 obukhov(u_star_avg, wall_model) */
+int les_obukhov(les_state* s);
+/* compute_wall_law.f90:107-185 wallstress(lbc_u, lbc_v, wall_model) */
+int les_wallstress(les_state* s);
+/* compute_sgs.f90:105-247 sgs_stress(jt, jtt) */
+int les_sgs_stress(les_state* s, int jt, int jtt);
+/* testfilter.f90:144-184 test_filter(f, G) on levels 1..nz+1;
+ * which = 2 for G_test (2 Delta), 4 for G_test_test (4 Delta). */
+int les_test_filter(les_state* s, int f, int which);
+/* boundary_condition_mpi.f90:33-63 set_bc for u, v, w at bottom and top */
+int les_set_bc(les_state* s);
+/* LES_engine.f90:449-498 compute_vel_grad() */
+int les_compute_vel_grad(les_state* s);
+/* LES_engine.f90:509-572 compute_RHS_adv() */
+int les_compute_rhs_adv(les_state* s);
+/* LES_engine.f90:262-283 Adams-Bashforth advance and w(0)=w(nz+1)=0 */
+int les_ab2_advance(les_state* s, double tadv1, double tadv2);
+/* LES_engine.f90:300-331 projection, rhs update, w(1)=w(nz+1)=0 */
+int les_projection(les_state* s, double tadv1);
+/* LES_engine.f90:189-360: one whole time step (wall law .. BCs and the
+ * running diagnostics).  jt is the loop counter, jt_total the global step. */
+int les_step(les_state* s, int jt, int jt_total);
+/* running_diagnostics.f90:80-136 of the last step: cfl, mke, u_star, rms div u
+ * (FP64, compensated sums). */
+int les_diagnostics(les_state* s, double out[4]);
+/* Sticky device status bits (NaN seen, zero pivot, ...); cleared on read. */
+int les_get_status(les_state* s, unsigned* bits);
+/* Synchronise the state's stream. */
+int les_sync(les_state* s);
+/* Device time of the kernels of the last les_step, per reference profiling
+ * bucket (LES_engine.f90:100-107): grad, stress, rhs, press, loop (ms). */
+int les_timers(les_state* s, double out[5]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LESGPU_H */

@@ -1,0 +1,10 @@
+"""B200-native LES time step (pseudo-spectral ABL LES of fmargairaz/new-repo).
+
+The operators run as hand-written sm_100a CUDA kernels in ``liblesgpu.so``
+behind the C ABI of ``include/lesgpu.h``; ``LES`` mirrors the reference's
+module entry points on top of it.
+"""
+from .capi import FIELDS, PLANES, LesError, load  # noqa: F401
+from .les import LES, RunParams, log_law_noise, read_namelist  # noqa: F401
+
+__all__ = ["LES", "RunParams", "LesError", "read_namelist", "log_law_noise", "FIELDS", "PLANES", "load"]

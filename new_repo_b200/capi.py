@@ -1,0 +1,108 @@
+"""ctypes binding of liblesgpu.so (the C ABI declared in include/lesgpu.h).
+
+The shared library is built in-tree by ``new_repo_b200/build.py``.  Loading
+fails loudly when it is missing: there is no CPU fallback for any operator.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "liblesgpu.so"
+
+LES_OK, LES_ERR_INVALID, LES_ERR_NOMEM, LES_ERR_NUMERICAL, LES_ERR_IO = 0, 1, 3, 9, 22
+SGS_MODELS = {"cst_Smag": 0, "dyn_Smag": 1, "dyn_LagScaleDep": 2}
+WALL_MODELS = {"wall_filter": 0, "wall_inst": 1, "wall_homog": 2}
+DEALIAS = {"padd": 0, "trunc": 1}
+LAG_HALO = {"reference1x1": 0, "periodic": 1}
+PRECISION = {"fp64": 0, "mixed": 1}
+
+FIELDS = ("u", "v", "w", "dudx", "dudy", "dudz", "dvdx", "dvdy", "dvdz", "dwdx", "dwdy", "dwdz",
+          "p", "dpdx", "dpdy", "dpdz", "rhsx", "rhsy", "rhsz", "rhsx_f", "rhsy_f", "rhsz_f",
+          "txx", "txy", "txz", "tyy", "tyz", "tzz", "cs_opt2", "nu_t",
+          "F_LM", "F_MM", "F_QN", "F_NN", "beta", "u_lag", "v_lag", "w_lag")
+FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
+PLANES = ("lbc_u", "lbc_v", "lbc_w", "ubc_u", "ubc_v", "ubc_w", "bottom_wk_press", "top_wk_press",
+          "lbc_z0", "u_star_avg")
+PLANE_ID = {n: i for i, n in enumerate(PLANES)}
+
+
+class LesParams(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("dt", C.c_double),
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double), ("z0", C.c_double),
+                ("pfx", C.c_double), ("pfy", C.c_double), ("cs0", C.c_double),
+                ("sgs_model", C.c_int), ("cs_count", C.c_int), ("dyn_init", C.c_int),
+                ("wall_law", C.c_int), ("wall_model", C.c_int), ("dealias", C.c_int),
+                ("lag_halo", C.c_int), ("precision", C.c_int), ("device", C.c_int)]
+
+
+class LesError(RuntimeError):
+    """A nonzero status from the library; ``code`` mirrors decomp_2d_abort codes."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+# (name, argtypes) of every exported entry point
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_I = C.c_int
+PROTOTYPES = {
+    "les_create": [C.POINTER(LesParams), C.POINTER(_P)],
+    "les_destroy": [_P],
+    "les_upload": [_P, _I, _D, _I, _I],
+    "les_download": [_P, _I, _D, _I, _I],
+    "les_upload_plane": [_P, _I, _D],
+    "les_download_plane": [_P, _I, _D],
+    "les_set_initial_conditions": [_P, _D, _D, _D],
+    "les_set_bc_types": [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "les_set_lagrangian_init": [_P, _I],
+    "les_get_lagrangian_init": [_P, C.POINTER(C.c_int)],
+    "les_grad_velocity_filt": [_P, _I, _I, _I],
+    "les_ddz_uv": [_P, _I, _I],
+    "les_ddz_w": [_P, _I, _I],
+    "les_div_stress": [_P, _I, _I, _I, _I, _I],
+    "les_compute_dealias_convec": [_P, _I, _I, _I],
+    "les_press_stag_array": [_P, C.c_double],
+    "les_obukhov": [_P],
+    "les_wallstress": [_P],
+    "les_sgs_stress": [_P, _I, _I],
+    "les_test_filter": [_P, _I, _I],
+    "les_set_bc": [_P],
+    "les_compute_vel_grad": [_P],
+    "les_compute_rhs_adv": [_P],
+    "les_ab2_advance": [_P, C.c_double, C.c_double],
+    "les_projection": [_P, C.c_double],
+    "les_step": [_P, _I, _I],
+    "les_diagnostics": [_P, _D],
+    "les_get_status": [_P, C.POINTER(C.c_uint)],
+    "les_sync": [_P],
+    "les_timers": [_P, _D],
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load liblesgpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: run new_repo_b200/build.py (or __graft_entry__.build())")
+        lib = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | getattr(os, "RTLD_GLOBAL", 0))
+        for name, argt in PROTOTYPES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = argt
+            fn.restype = C.c_int
+        lib.les_last_error.argtypes = []
+        lib.les_last_error.restype = C.c_char_p
+        _lib = lib
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != LES_OK:
+        msg = load().les_last_error().decode(errors="replace")
+        raise LesError(rc, msg)

@@ -1,0 +1,206 @@
+// extern "C" boundary of liblesgpu.so (declared in include/lesgpu.h).
+#include <cstring>
+#include <string>
+
+#include "../../include/lesgpu.h"
+#include "solver.cuh"
+
+struct les_state {
+  les::SolverBase* s = nullptr;
+};
+
+namespace {
+thread_local std::string g_last_error;
+
+template <typename F>
+int guard(F&& f) {
+  try {
+    f();
+    return LES_OK;
+  } catch (const les::CudaError& e) {
+    g_last_error = e.what();
+    return e.code ? e.code : LES_ERR_INVALID;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return LES_ERR_INVALID;
+  }
+}
+
+int bad_state() {
+  g_last_error = "null les_state";
+  return LES_ERR_INVALID;
+}
+}  // namespace
+
+#define STATE_OR_FAIL(s) \
+  if (!(s) || !(s)->s) return bad_state()
+
+extern "C" {
+
+const char* les_last_error(void) { return g_last_error.c_str(); }
+
+int les_create(const les_params* p, les_state** out) {
+  if (!p || !out) {
+    g_last_error = "null argument";
+    return LES_ERR_INVALID;
+  }
+  *out = nullptr;
+  return guard([&] {
+    if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0 || p->dt <= 0 || p->cs_count <= 0)
+      throw les::CudaError(LES_ERR_INVALID, "invalid grid, dt or cs_count");
+    if (p->sgs_model < LES_SGS_CST_SMAG || p->sgs_model > LES_SGS_LASD)
+      throw les::CudaError(LES_ERR_INVALID, "Invalid SGS model");
+    if (p->wall_model < LES_WALL_FILTER || p->wall_model > LES_WALL_HOMOG)
+      throw les::CudaError(LES_ERR_INVALID, "Invalid wall law type");
+    auto* st = new les_state;
+    try {
+      st->s = les::make_solver(*p);
+    } catch (...) {
+      delete st;
+      throw;
+    }
+    *out = st;
+  });
+}
+
+int les_destroy(les_state* s) {
+  if (!s) return LES_OK;
+  int rc = guard([&] { delete s->s; });
+  delete s;
+  return rc;
+}
+
+int les_upload(les_state* s, int field, const double* h, int k0, int k1) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->upload(field, h, k0, k1); });
+}
+int les_download(les_state* s, int field, double* h, int k0, int k1) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->download(field, h, k0, k1); });
+}
+int les_upload_plane(les_state* s, int plane, const double* h) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->upload_plane(plane, h); });
+}
+int les_download_plane(les_state* s, int plane, double* h) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->download_plane(plane, h); });
+}
+int les_set_initial_conditions(les_state* s, const double* u, const double* v, const double* w) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->set_initial_conditions(u, v, w); });
+}
+int les_set_bc_types(les_state* s, const int lbc[3], const int ubc[3]) {
+  STATE_OR_FAIL(s);
+  for (int i = 0; i < 3; ++i) {
+    if (lbc[i] < 0 || lbc[i] > 2 || ubc[i] < 0 || ubc[i] > 2) {
+      g_last_error = "bc type must be 0 (none), 1 (drc) or 2 (neu)";
+      return LES_ERR_INVALID;
+    }
+    s->s->lbc_t[i] = lbc[i];
+    s->s->ubc_t[i] = ubc[i];
+  }
+  return LES_OK;
+}
+int les_set_lagrangian_init(les_state* s, int f) {
+  STATE_OR_FAIL(s);
+  s->s->f_coeff_init = f != 0;
+  s->s->lagran_init = f != 0;
+  return LES_OK;
+}
+int les_get_lagrangian_init(les_state* s, int* f) {
+  STATE_OR_FAIL(s);
+  *f = s->s->f_coeff_init ? 1 : 0;
+  return LES_OK;
+}
+
+int les_grad_velocity_filt(les_state* s, int f, int dfdx, int dfdy) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->grad_velocity_filt(f, dfdx, dfdy); });
+}
+int les_ddz_uv(les_state* s, int dfdz, int f) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->ddz_uv(dfdz, f); });
+}
+int les_ddz_w(les_state* s, int dfdz, int f) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->ddz_w(dfdz, f); });
+}
+int les_div_stress(les_state* s, int rhs, int tx, int ty, int tz, int stag) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->div_stress(rhs, tx, ty, tz, stag); });
+}
+int les_compute_dealias_convec(les_state* s, int cx, int cy, int cz) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->dealias_convec(cx, cy, cz); });
+}
+int les_press_stag_array(les_state* s, double tadv1) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->press_stag_array(tadv1); });
+}
+int les_obukhov(les_state* s) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->obukhov(); });
+}
+int les_wallstress(les_state* s) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->wallstress(); });
+}
+int les_sgs_stress(les_state* s, int jt, int jtt) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->sgs_stress(jt, jtt); });
+}
+int les_test_filter(les_state* s, int f, int which) {
+  STATE_OR_FAIL(s);
+  if (which != 2 && which != 4) {
+    g_last_error = "test filter width must be 2 or 4";
+    return LES_ERR_INVALID;
+  }
+  return guard([&] { s->s->test_filter(f, which); });
+}
+int les_set_bc(les_state* s) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->set_bc(); });
+}
+int les_compute_vel_grad(les_state* s) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->compute_vel_grad(); });
+}
+int les_compute_rhs_adv(les_state* s) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->compute_rhs_adv(); });
+}
+int les_ab2_advance(les_state* s, double t1, double t2) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->ab2(t1, t2); });
+}
+int les_projection(les_state* s, double t1) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->projection(t1); });
+}
+int les_step(les_state* s, int jt, int jtt) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->step(jt, jtt); });
+}
+int les_diagnostics(les_state* s, double out[4]) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->diagnostics(out); });
+}
+int les_get_status(les_state* s, unsigned* bits) {
+  STATE_OR_FAIL(s);
+  return guard([&] { *bits = s->s->status(); });
+}
+int les_sync(les_state* s) {
+  STATE_OR_FAIL(s);
+  return guard([&] { LES_CUDA(cudaStreamSynchronize(s->s->st)); });
+}
+int les_timers(les_state* s, double out[5]) {
+  STATE_OR_FAIL(s);
+  return guard([&] {
+    LES_CUDA(cudaStreamSynchronize(s->s->st));
+    s->s->read_timers();
+    for (int i = 0; i < 5; ++i) out[i] = s->s->timers_ms[i];
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,67 @@
+// Common definitions for the B200 LES library: complex type, field layout,
+// error handling and the device status word.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <stdexcept>
+
+namespace les {
+
+// Sentinel used by the reference for undefined nodes (parameters_IO.f90:49).
+constexpr double BOGUS = -1.23456789e20;
+constexpr double KVONK = 0.4;
+
+template <typename T>
+struct __align__(2 * sizeof(T)) cplx {
+  T x, y;
+};
+
+template <typename T>
+__device__ __forceinline__ cplx<T> cmul(cplx<T> a, cplx<T> b) {
+  return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <typename T>
+__device__ __forceinline__ cplx<T> cmulc(cplx<T> a, cplx<T> b) {  // a * conj(b)
+  return {a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y};
+}
+template <typename T>
+__device__ __forceinline__ cplx<T> cadd(cplx<T> a, cplx<T> b) { return {a.x + b.x, a.y + b.y}; }
+template <typename T>
+__device__ __forceinline__ cplx<T> csub(cplx<T> a, cplx<T> b) { return {a.x - b.x, a.y - b.y}; }
+template <typename T>
+__device__ __forceinline__ cplx<T> cscale(cplx<T> a, T s) { return {a.x * s, a.y * s}; }
+// i * k * a, written as (0 + i k) * (ax + i ay) the way the reference's
+// eye*kkx*f_hat evaluates it.
+template <typename T>
+__device__ __forceinline__ cplx<T> ik_mul(T k, cplx<T> a) {
+  return {T(0) * a.x - k * a.y, T(0) * a.y + k * a.x};
+}
+
+// Device status bits (read back by les_get_status).
+enum StatusBits : unsigned {
+  ST_NAN = 1u << 0,          // NaN in the velocity (LES_engine.f90:583-616)
+  ST_PIVOT = 1u << 1,        // zero pivot in the tridiagonal solve (compute_pressure.f90:411-418)
+  ST_MLP_RANGE = 1u << 2,    // learned closure saw inputs outside its training range
+  ST_BAD_ARG = 1u << 3,      // kernel argument check failed
+};
+
+struct CudaError : std::runtime_error {
+  int code;
+  CudaError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define LES_CUDA(call)                                                              \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess) {                                                        \
+      throw ::les::CudaError(3, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    }                                                                               \
+  } while (0)
+
+#define LES_CHECK_LAUNCH() LES_CUDA(cudaGetLastError())
+
+inline int ceil_div(long a, long b) { return int((a + b - 1) / b); }
+
+}  // namespace les

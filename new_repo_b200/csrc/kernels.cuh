@@ -1,0 +1,564 @@
+// Pointwise, vertical and reduction kernels of the LES step.
+#pragma once
+#include "common.cuh"
+
+namespace les {
+
+// ---------------------------------------------------------------------------
+// boundary conditions (boundary_condition_mpi.f90:33-63); types 0/1/2 =
+// none/'drc'/'neu'.  u, v are staggered (uvp nodes), w is not.
+template <typename T>
+__global__ void k_set_bc(T* u, T* v, T* w, const T* lu, const T* lv, const T* lw, const T* tu, const T* tv,
+                         const T* tw, int4 lt, int4 ut, long plane, int nz, T dz) {
+  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < plane; p += (long)gridDim.x * blockDim.x) {
+    const long b0 = p, b1 = plane + p, t0 = (long)nz * plane + p, t1 = (long)(nz + 1) * plane + p;
+    if (lt.x == 1) u[b0] = T(2) * lu[p] - u[b1];
+    else if (lt.x == 2) u[b0] = u[b1] - lu[p] * dz;
+    if (lt.y == 1) v[b0] = T(2) * lv[p] - v[b1];
+    else if (lt.y == 2) v[b0] = v[b1] - lv[p] * dz;
+    if (lt.z == 1) w[b1] = lw[p];
+    if (ut.x == 1) u[t1] = T(2) * tu[p] - u[t0];
+    else if (ut.x == 2) u[t1] = u[t0] + tu[p] * dz;
+    if (ut.y == 1) v[t1] = T(2) * tv[p] - v[t0];
+    else if (ut.y == 2) v[t1] = v[t0] + tv[p] * dz;
+    if (ut.z == 1) w[t1] = tw[p];
+  }
+}
+
+// ddz_uv (uvp -> w, k = 1..nz+1) for u, v and ddz_w (w -> uvp, k = 1..nz,
+// top level zero) for w (compute_derivatives.f90:375-441).
+template <typename T>
+__global__ void k_ddz_vel(const T* u, const T* v, const T* w, T* dudz, T* dvdz, T* dwdz, long plane, int nz,
+                          T rdz) {
+  const long n = (long)(nz + 1) * plane;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long o = plane + q;  // levels 1..nz+1
+    const int k = int(o / plane);
+    dudz[o] = rdz * (u[o] - u[o - plane]);
+    dvdz[o] = rdz * (v[o] - v[o - plane]);
+    dwdz[o] = (k <= nz) ? rdz * (w[o + plane] - w[o]) : T(0);
+  }
+}
+
+template <typename T>
+__global__ void k_ddz(T* out, const T* f, long plane, int nz, T rdz, int w_to_uvp) {
+  const long n = (long)(nz + 1) * plane;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long o = plane + q;
+    const int k = int(o / plane);
+    if (w_to_uvp) out[o] = (k <= nz) ? rdz * (f[o + plane] - f[o]) : T(0);
+    else out[o] = rdz * (f[o] - f[o - plane]);
+  }
+}
+
+template <typename T>
+__global__ void k_fill(T* f, long n, T val) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) f[q] = val;
+}
+
+template <typename T>
+__global__ void k_scale(T* f, long n, T c) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) f[q] = c * f[q];
+}
+
+template <typename T>
+__global__ void k_copy(T* dst, const T* src, long n) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) dst[q] = src[q];
+}
+
+// ---------------------------------------------------------------------------
+// SGS stress (compute_sgs.f90:105-335)
+template <typename T>
+struct SgsArgs {
+  const T* d[9];  // dudx dudy dudz dvdx dvdy dvdz dwdx dwdy dwdz
+  const T* cs;
+  const double* l2;  // mixing length squared per level
+  T *nu, *txx, *txy, *txz, *tyy, *tyz, *tzz;
+  T* sij[6];  // optional: s11 s12 s13 s22 s23 s33
+  T* smag;    // optional: |S|
+  int write_sij;
+  int wall;
+  long plane;
+  int nz;
+};
+
+template <typename T>
+__device__ __forceinline__ void sij_at(const SgsArgs<T>& a, long o, int k, T s[6]) {
+  const long pl = a.plane;
+  T ux, uy, uz, vx, vy, vz, wx, wy, wz;
+  if (k == 1) {
+    ux = a.d[0][o];
+    uy = a.d[1][o];
+    if (a.wall) {
+      uz = a.d[2][o];
+      vz = a.d[5][o];
+    } else {
+      uz = T(0.5) * (a.d[2][o] + a.d[2][o + pl]);
+      vz = T(0.5) * (a.d[5][o] + a.d[5][o + pl]);
+    }
+    vx = a.d[3][o];
+    vy = a.d[4][o];
+    wx = T(0.5) * (a.d[6][o] + a.d[6][o + pl]);
+    wy = T(0.5) * (a.d[7][o] + a.d[7][o + pl]);
+    wz = a.d[8][o];
+  } else {
+    ux = T(0.5) * (a.d[0][o] + a.d[0][o - pl]);
+    uy = T(0.5) * (a.d[1][o] + a.d[1][o - pl]);
+    uz = a.d[2][o];
+    vx = T(0.5) * (a.d[3][o] + a.d[3][o - pl]);
+    vy = T(0.5) * (a.d[4][o] + a.d[4][o - pl]);
+    vz = a.d[5][o];
+    wx = a.d[6][o];
+    wy = a.d[7][o];
+    wz = T(0.5) * (a.d[8][o] + a.d[8][o - pl]);
+  }
+  s[0] = ux;
+  s[1] = T(0.5) * (uy + vx);
+  s[2] = T(0.5) * (uz + wx);
+  s[3] = vy;
+  s[4] = T(0.5) * (vz + wy);
+  s[5] = wz;
+}
+
+template <typename T>
+__device__ __forceinline__ T strain_norm(const T s[6]) {
+  return sqrt(T(2) * (s[0] * s[0] + s[3] * s[3] + s[5] * s[5] + T(2) * (s[1] * s[1] + s[2] * s[2] + s[4] * s[4])));
+}
+
+// S_ij and |S| on levels 1..nz+1 (written for the dynamic procedure).
+template <typename T>
+__global__ void k_sij(const SgsArgs<T> a) {
+  const long n = (long)(a.nz + 1) * a.plane;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long o = a.plane + q;
+    const int k = int(o / a.plane);
+    T s[6];
+    sij_at(a, o, k, s);
+#pragma unroll
+    for (int t = 0; t < 6; ++t) a.sij[t][o] = s[t];
+    a.smag[o] = strain_norm(s);
+  }
+}
+
+// nu_t = |S| Cs^2 l^2 and tau_ij (compute_sgs.f90:177-242).
+template <typename T>
+__global__ void k_sgs_tau(const SgsArgs<T> a) {
+  const long pl = a.plane;
+  const long n = (long)(a.nz + 1) * pl;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long o = pl + q;
+    const int k = int(o / pl);
+    T s[6];
+    sij_at(a, o, k, s);
+    const T nuk = strain_norm(s) * a.cs[o] * T(a.l2[k]);
+    a.nu[o] = nuk;
+    if (k == 1) {
+      const T tz = T(2) * nuk * a.d[8][o];
+      a.txx[o] = T(2) * nuk * a.d[0][o];
+      a.txy[o] = T(2) * nuk * T(0.5) * (a.d[1][o] + a.d[3][o]);
+      a.tyy[o] = T(2) * nuk * a.d[4][o];
+      a.tzz[o] = tz;
+      a.tzz[o - pl] = tz;  // tzz(0) = tzz(1)
+    } else {
+      if (k <= a.nz) {
+        T s2[6];
+        sij_at(a, o + pl, k + 1, s2);
+        const T nukp = strain_norm(s2) * a.cs[o + pl] * T(a.l2[k + 1]);
+        const T c = T(0.5) * (nuk + nukp);
+        a.txx[o] = T(2) * c * a.d[0][o];
+        a.txy[o] = T(2) * c * T(0.5) * (a.d[1][o] + a.d[3][o]);
+        a.tyy[o] = T(2) * c * a.d[4][o];
+        a.tzz[o] = T(2) * c * a.d[8][o];
+      }
+      a.txz[o] = T(2) * nuk * s[2];
+      a.tyz[o] = T(2) * nuk * s[4];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Lagrangian scale-dependent dynamic model (compute_LagScaleDep.f90)
+template <typename T>
+__global__ void k_lag_accum(T* ul, T* vl, T* wl, const T* u, const T* v, const T* w, long n) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    ul[q] = ul[q] + u[q];
+    vl[q] = vl[q] + v[q];
+    wl[q] = wl[q] + w[q];
+  }
+}
+
+struct LagGeom {
+  int nx, ny, nz;
+  long plane;
+  int mode;  // 0 reference 1x1 halo, 1 periodic
+  double dt, dx, dy, dz, cs;
+};
+
+// FF(i, j, k) of compute_interpolag_coeff (1-based i, j; level k in 0..nz+2)
+// as update_halo3 (decomp_2d_custom.f90:902-1024) and the overrides of
+// compute_LagScaleDep.f90:441-452 leave it.
+template <typename T>
+__device__ __forceinline__ T ff_at(const T* F, int i, int j, int k, const LagGeom& g) {
+  if (k == 0) k = 1;
+  const bool inner = (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny);
+  int ii = (i == 0) ? g.nx : ((i == g.nx + 1) ? 1 : i);
+  int jj;
+  if (k >= g.nz + 1) {
+    if (inner) return F[(long)(g.nz + 1) * g.plane + (long)(j - 1) * g.nx + (i - 1)];
+    if (g.mode == 1) {
+      jj = (j == 0) ? g.ny : ((j == g.ny + 1) ? 1 : j);
+      return F[(long)(g.nz + 1) * g.plane + (long)(jj - 1) * g.nx + (ii - 1)];
+    }
+    k -= 2;  // self-message halo: levels nz+1, nz+2 hold copies of nz-1, nz
+  }
+  if (g.mode == 1) jj = (j == 0) ? g.ny : ((j == g.ny + 1) ? 1 : j);
+  else jj = (j == 0) ? 2 : ((j == g.ny + 1) ? g.ny - 1 : j);
+  return F[(long)k * g.plane + (long)(jj - 1) * g.nx + (ii - 1)];
+}
+
+// compute_interpolag_weight (:309-411) + compute_interpolag_coeff (:427-474)
+// for the four F fields at once; writes the interpolated fields to Fn.
+template <typename T>
+__global__ void k_lag_interp(const T* ul, const T* vl, const T* wl, const T* F0, const T* F1, const T* F2,
+                             const T* F3, T* N0, T* N1, T* N2, T* N3, LagGeom g) {
+  const long pl = g.plane;
+  const long n = (long)(g.nz + 1) * pl;
+  const T cs = T(g.cs);
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long o = pl + q;
+    const int k = int(o / pl);
+    const int jj = int((o % pl) / g.nx);
+    const int i = int(o % g.nx) + 1;
+    const int j = jj + 1;
+    T uu, vv;
+    if (k == 1) {
+      uu = ul[o] / cs;
+      vv = vl[o] / cs;
+    } else {
+      uu = T(0.5) * (ul[o] / cs + ul[o - pl] / cs);
+      vv = T(0.5) * (vl[o] / cs + vl[o - pl] / cs);
+    }
+    const T xp = -uu * T(g.dt) * cs / T(g.dx);
+    const T yp = -vv * T(g.dt) * cs / T(g.dy);
+    T zp;
+    if (k <= 2) {
+      const long o2 = 2 * pl + (o % pl);
+      const T w2 = wl[o2] / cs;
+      T z2 = -w2 * T(g.dt) * cs / T(g.dz);
+      z2 = z2 + fmin(z2, T(0));
+      z2 = fmin(T(1), z2);
+      z2 = fmax(T(-1), z2);
+      zp = z2;
+    } else {
+      const T ww = wl[o] / cs;
+      zp = -ww * T(g.dt) * cs / T(g.dz);
+    }
+    const int ax = i + (signbit(xp) ? -1 : 1);
+    const int ay = j + (signbit(yp) ? -1 : 1);
+    const int az = k + (signbit(zp) ? -1 : 1);
+    const T cx = fabs(xp), cy = fabs(yp), cz = fabs(zp);
+    const T fx = T(1) - cx, fy = T(1) - cy, fz = T(1) - cz;
+    const T* Fs[4] = {F0, F1, F2, F3};
+    T* Ns[4] = {N0, N1, N2, N3};
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const T* F = Fs[t];
+      Ns[t][o] = fx * fy * (ff_at(F, i, j, k, g) * fz + ff_at(F, i, j, az, g) * cz) +
+                 fx * cy * (ff_at(F, i, ay, k, g) * fz + ff_at(F, i, ay, az, g) * cz) +
+                 cx * fy * (ff_at(F, ax, j, k, g) * fz + ff_at(F, ax, j, az, g) * cz) +
+                 cx * cy * (ff_at(F, ax, ay, k, g) * fz + ff_at(F, ax, ay, az, g) * cz);
+    }
+  }
+}
+
+__device__ __forceinline__ double f32max_tiny(double x) {
+  return double(fmaxf(1e-24f, float(x)));
+}
+
+// update_interpolag_coeff x2 (:607-640) and compute_dynamic_coeff (:651-707),
+// including the default-REAL (float) casts of the reference's max() clips.
+template <typename T>
+__global__ void k_lasd_update(T* FLM, T* FMM, T* FQN, T* FNN, const T* LM, const T* MM, const T* QN, const T* NN,
+                              T* cs, T* beta, int init, long plane, int nz, double opftdelta, double lagran_dt,
+                              double beta_pow) {
+  const long n = (long)(nz + 1) * plane;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long o = plane + q;
+    const int k = int(o / plane);
+    double flm, fmm, fqn, fnn;
+    const double lm = LM[o], mm = MM[o], qn = QN[o], nn = NN[o];
+    if (init) {
+      fmm = mm;
+      flm = 0.03 * mm;
+      fnn = nn;
+      fqn = 0.03 * nn;
+    } else {
+      flm = FLM[o];
+      fmm = FMM[o];
+      fqn = FQN[o];
+      fnn = FNN[o];
+    }
+    // 2 Delta pair
+    {
+      double tmp = double(fmaxf(float(flm * fmm), 1e-24f));
+      tmp = opftdelta * pow(tmp, -0.125);
+      tmp = f32max_tiny(tmp);
+      const double dumfac = lagran_dt / tmp;
+      const double epsi = dumfac / (1.0 + dumfac);
+      flm = epsi * lm + (1.0 - epsi) * flm;
+      fmm = epsi * mm + (1.0 - epsi) * fmm;
+      flm = f32max_tiny(flm);
+    }
+    // 4 Delta pair
+    {
+      double tmp = double(fmaxf(float(fqn * fnn), 1e-24f));
+      tmp = opftdelta * pow(tmp, -0.125);
+      tmp = f32max_tiny(tmp);
+      const double dumfac = lagran_dt / tmp;
+      const double epsi = dumfac / (1.0 + dumfac);
+      fqn = epsi * qn + (1.0 - epsi) * fqn;
+      fnn = epsi * nn + (1.0 - epsi) * fnn;
+      fqn = f32max_tiny(fqn);
+    }
+    FLM[o] = T(flm);
+    FMM[o] = T(fmm);
+    FQN[o] = T(fqn);
+    FNN[o] = T(fnn);
+    // coefficient: use the stored values, as the reference's arrays hold them
+    const double c2 = f32max_tiny(double(T(flm)) / double(T(fmm)));
+    const double c4 = f32max_tiny(double(T(fqn)) / double(T(fnn)));
+    double b = (beta_pow == 1.0) ? (c4 / c2) : pow(c4 / c2, beta_pow);
+    b = double(fmaxf(float(b), 0.125f));
+    if (k == nz + 1) b = 1.0;
+    beta[o] = T(b);
+    cs[o] = T(f32max_tiny(c2 / b));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// time advancement (LES_engine.f90:253-331)
+template <typename T>
+__global__ void k_ab2(T* u, T* v, T* w, const T* rx, const T* ry, const T* rz, const T* fx, const T* fy,
+                      const T* fz, long plane, int nz, T dt, T t1, T t2) {
+  const long n = (long)(nz + 2) * plane;
+  for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n; o += (long)gridDim.x * blockDim.x) {
+    const int k = int(o / plane);
+    if (k >= 1 && k <= nz) {
+      u[o] = u[o] + dt * (t1 * rx[o] + t2 * fx[o]);
+      v[o] = v[o] + dt * (t1 * ry[o] + t2 * fy[o]);
+      w[o] = w[o] + dt * (t1 * rz[o] + t2 * fz[o]);
+    } else {
+      w[o] = T(0);  // w(0) = w(nz+1) = 0
+    }
+  }
+}
+
+// projection and rhs update (LES_engine.f90:303-331), w(1) = w(nz+1) = 0.
+template <typename T>
+__global__ void k_projection(T* u, T* v, T* w, T* rx, T* ry, T* rz, const T* dpdx, const T* dpdy, const T* dpdz,
+                             long plane, int nz, T dtt) {
+  const long n = (long)(nz + 2) * plane;
+  for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n; o += (long)gridDim.x * blockDim.x) {
+    const int k = int(o / plane);
+    if (k >= 1 && k <= nz) {
+      const T dz_ = dpdz[o];
+      u[o] = u[o] - dtt * dpdx[o];
+      v[o] = v[o] - dtt * dpdy[o];
+      w[o] = (k == 1) ? T(0) : w[o] - dtt * dz_;
+      rx[o] = rx[o] - dpdx[o];
+      ry[o] = ry[o] - dpdy[o];
+      rz[o] = rz[o] - dz_;
+    } else if (k == nz + 1) {
+      w[o] = T(0);
+    }
+  }
+}
+
+// p = fluctuation + FP64 mean profile (mixed precision only), p(nz+1) = BOGUS
+template <typename T>
+__global__ void k_p_finish(T* p, const double* pmean, long plane, int nz) {
+  const long n = (long)(nz + 2) * plane;
+  for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n; o += (long)gridDim.x * blockDim.x) {
+    const int k = int(o / plane);
+    if (k == nz + 1) p[o] = T(BOGUS);
+    else if (pmean) p[o] = T(double(p[o]) + pmean[k]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pressure: one Thomas solve per (kx, ky) (compute_pressure.f90:256-305,
+// 448-493, matrix of build_matrix :544-619), always in FP64.
+template <typename T>
+__global__ void k_tridiag(const cplx<T>* Hx, const cplx<T>* Hy, const cplx<T>* Hz, const cplx<T>* bot,
+                          const cplx<T>* top, const double* kkx, const double* kky, cplx<T>* phat,
+                          cplx<double>* xs, double* gam, double* pmean, unsigned* status, int lhx, int ny, int nz,
+                          double dz, int drop_mean) {
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ky = blockIdx.y;
+  if (kx >= lhx) return;
+  const long col = (long)ky * lhx + kx;
+  const long sp = (long)ny * lhx;
+  if (kx == lhx - 1 || ky == ny / 2) {
+    for (int l = 0; l <= nz + 1; ++l) phat[l * sp + col] = cplx<T>{T(0), T(0)};
+    return;
+  }
+  const bool mean = (kx == 0 && ky == 0);
+  const double a_in = 1.0 / (dz * dz);
+  const double kxv = kkx[col], kyv = kky[col];
+  const double b_in = -((kxv * kxv + kyv * kyv) + 2.0 / (dz * dz));
+  // row 1: bottom Neumann closure (p1 - p0 = dz * bottom layer) or p0 = 0
+  cplx<double> r;
+  if (mean) r = {0.0, 0.0};
+  else r = {double(bot[col].x) * dz, double(bot[col].y) * dz};
+  double bet = mean ? 1.0 : -1.0;
+  double cprev = mean ? 0.0 : 1.0;
+  cplx<double> x = {r.x / bet, r.y / bet};
+  xs[col] = x;
+  bool bad = false;
+  for (int k = 1; k <= nz; ++k) {
+    const long o = k * sp + col;
+    const cplx<T> hx = Hx[o], hy = Hy[o], hz = Hz[o];
+    const cplx<T> hzp = (k < nz) ? Hz[o + sp] : cplx<T>{T(0), T(0)};
+    const double sx = kxv * double(hx.x) + kyv * double(hy.x);
+    const double sy = kxv * double(hx.y) + kyv * double(hy.y);
+    r = {-sy + (double(hzp.x) - double(hz.x)) / dz, sx + (double(hzp.y) - double(hz.y)) / dz};
+    const double g = cprev / bet;
+    bet = b_in - a_in * g;
+    bad |= (bet == 0.0);
+    x = {(r.x - a_in * x.x) / bet, (r.y - a_in * x.y) / bet};
+    gam[o] = g;
+    xs[o] = x;
+    cprev = a_in;
+  }
+  {  // top row: -p(nz) + p(nz+1) = dz * top layer
+    const long o = (long)(nz + 1) * sp + col;
+    r = {double(top[col].x) * dz, double(top[col].y) * dz};
+    const double g = cprev / bet;
+    bet = 1.0 - (-1.0) * g;
+    bad |= (bet == 0.0);
+    x = {(r.x - (-1.0) * x.x) / bet, (r.y - (-1.0) * x.y) / bet};
+    gam[o] = g;
+  }
+  if (bad) atomicOr(status, ST_PIVOT);
+  phat[(long)(nz + 1) * sp + col] = cplx<T>{T(0), T(0)};
+  for (int k = nz; k >= 0; --k) {
+    const long o = k * sp + col;
+    const cplx<double> xk = xs[o];
+    const double g = gam[o + sp];
+    x = {xk.x - g * x.x, xk.y - g * x.y};
+    if (mean && pmean) pmean[k] = x.x;
+    phat[o] = (mean && drop_mean) ? cplx<T>{T(0), T(0)} : cplx<T>{T(x.x), T(x.y)};
+  }
+  if (mean && pmean) pmean[nz + 1] = 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// running diagnostics (running_diagnostics.f90:148-305) with Neumaier sums
+struct Neu {
+  double s = 0.0, c = 0.0;
+  __device__ __forceinline__ void add(double x) {
+    const double t = s + x;
+    if (fabs(s) >= fabs(x)) c += (s - t) + x;
+    else c += (x - t) + s;
+    s = t;
+  }
+  __device__ __forceinline__ double val() const { return s + c; }
+};
+
+constexpr int DIAG_BLOCKS = 296;
+constexpr int DIAG_NV = 8;  // umax vmax wmax | usum vsum wsum divsum | nan
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_diag_partial(const T* u, const T* v, const T* w, const T* dudx,
+                                                      const T* dvdy, const T* dwdz, long plane, int nz,
+                                                      double* part) {
+  double mx[3] = {-1234567890.0, -1234567890.0, -1234567890.0};
+  Neu su, sv, sw, sd;
+  int nan = 0;
+  const long n = (long)nz * plane;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long o = plane + q;
+    const double uu = u[o], vv = v[o], ww = w[o];
+    nan |= (uu != uu) | (vv != vv) | (ww != ww);
+    mx[0] = fmax(mx[0], fabs(uu));
+    mx[1] = fmax(mx[1], fabs(vv));
+    mx[2] = fmax(mx[2], fabs(ww));
+    su.add(uu);
+    sv.add(vv);
+    sw.add(0.5 * (ww + double(w[o + plane])));
+    const double dv = double(dudx[o]) + double(dvdy[o]) + double(dwdz[o]);
+    sd.add(dv * dv);
+  }
+  __shared__ double sm[DIAG_NV + 4][256];
+  const int t = threadIdx.x;
+  sm[0][t] = mx[0];
+  sm[1][t] = mx[1];
+  sm[2][t] = mx[2];
+  sm[3][t] = su.s;
+  sm[4][t] = sv.s;
+  sm[5][t] = sw.s;
+  sm[6][t] = sd.s;
+  sm[7][t] = nan;
+  sm[8][t] = su.c;
+  sm[9][t] = sv.c;
+  sm[10][t] = sw.c;
+  sm[11][t] = sd.c;
+  __syncthreads();
+  if (t == 0) {
+    double m0 = sm[0][0], m1 = sm[1][0], m2 = sm[2][0], fl = 0;
+    Neu a[4];
+    for (int i = 0; i < 256; ++i) {
+      m0 = fmax(m0, sm[0][i]);
+      m1 = fmax(m1, sm[1][i]);
+      m2 = fmax(m2, sm[2][i]);
+      for (int q = 0; q < 4; ++q) {
+        a[q].add(sm[3 + q][i]);
+        a[q].add(sm[8 + q][i]);
+      }
+      fl = fmax(fl, sm[7][i]);
+    }
+    double* out = part + (long)blockIdx.x * DIAG_NV;
+    out[0] = m0;
+    out[1] = m1;
+    out[2] = m2;
+    for (int q = 0; q < 4; ++q) out[3 + q] = a[q].val();
+    out[7] = fl;
+  }
+}
+
+template <typename T>
+__global__ void k_diag_final(const double* part, int nblocks, const T* ustar, long plane, double dt, double dx,
+                             double dy, double dz, double npts, double* out, unsigned* status) {
+  __shared__ double sm[2][256];
+  Neu su;
+  for (long p = threadIdx.x; p < plane; p += blockDim.x) su.add(double(ustar[p]));
+  sm[0][threadIdx.x] = su.s;
+  sm[1][threadIdx.x] = su.c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Neu us;
+    for (int i = 0; i < blockDim.x; ++i) {
+      us.add(sm[0][i]);
+      us.add(sm[1][i]);
+    }
+    double m0 = part[0], m1 = part[1], m2 = part[2], fl = 0;
+    Neu a[4];
+    for (int b = 0; b < nblocks; ++b) {
+      const double* q = part + (long)b * DIAG_NV;
+      m0 = fmax(m0, q[0]);
+      m1 = fmax(m1, q[1]);
+      m2 = fmax(m2, q[2]);
+      for (int t = 0; t < 4; ++t) a[t].add(q[3 + t]);
+      fl = fmax(fl, q[7]);
+    }
+    const double cfl = dt * (m0 / dx + m1 / dy + m2 / dz);
+    const double um = a[0].val() / npts, vm = a[1].val() / npts, wm = a[2].val() / npts;
+    out[0] = cfl;
+    out[1] = 0.5 * (um * um + vm * vm + wm * wm);
+    out[2] = us.val() / double(plane);
+    out[3] = sqrt(a[3].val() / npts);
+    if (fl != 0.0) atomicOr(status, ST_NAN);
+  }
+}
+
+}  // namespace les

@@ -1,0 +1,1039 @@
+// Device-resident LES state and the operator sequence of one time step
+// (LES_engine.f90:189-360), for FP64 and mixed (FP32 fields) precision.
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "kernels.cuh"
+#include "launch.cuh"
+#include "solver.cuh"
+
+namespace les {
+
+namespace {
+constexpr double PI = 3.1415926535897932384626433;  // parameters_IO.f90:42
+constexpr int NSPEC = 21;
+
+int grid_for(long n, int bs = 256) {
+  long g = (n + bs - 1) / bs;
+  if (g > 148L * 32) g = 148L * 32;
+  if (g < 1) g = 1;
+  return int(g);
+}
+
+template <typename T>
+T* dalloc(size_t n) {
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(T) + 256);
+  if (e != cudaSuccess) throw CudaError(3, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  LES_CUDA(cudaMemset(p, 0, n * sizeof(T) + 256));
+  return reinterpret_cast<T*>(p);
+}
+}  // namespace
+
+template <typename T>
+class Solver final : public SolverBase {
+ public:
+  T* F[LES_NFIELDS] = {};
+  T* PL[LES_NPLANES] = {};
+  // tables
+  T *kkx = nullptr, *kky = nullptr, *gt = nullptr, *gtt = nullptr;
+  double *kkxd = nullptr, *kkyd = nullptr, *l2 = nullptr;
+  std::map<int, cplx<T>*> tw;
+  int nk2 = 1, nk4 = 1;  // kx columns with a nonzero 2Delta / 4Delta filter
+  int ky2 = 0, ky4 = 0;
+  double delta = 0, beta_pow = 1;
+  // workspace
+  cplx<T>* spec[NSPEC] = {};
+  cplx<T>* spec4[NSPEC] = {};
+  T* fine[6] = {};
+  T* sc[15] = {};  // S, s11..s33, LM, MM, QN, NN, Fn x4
+  cplx<double>* xs = nullptr;
+  double* gam = nullptr;
+  double* pmean = nullptr;
+  double* part = nullptr;
+  double* dout = nullptr;
+  unsigned* dstatus = nullptr;
+  std::vector<void*> allocs;
+  cudaEvent_t ev[6] = {};
+
+  explicit Solver(const les_params& p) {
+    P = p;
+    g.nx = p.nx;
+    g.ny = p.ny;
+    g.nz = p.nz;
+    g.L = p.nz + 2;
+    g.lhx = p.nx / 2 + 1;
+    g.lhy = p.ny / 2 + 1;
+    g.nx2 = 3 * p.nx / 2;
+    g.ny2 = 3 * p.ny / 2;
+    if (!supported_length(p.nx) || !supported_length(p.ny) || !supported_length(g.nx2) ||
+        !supported_length(g.ny2) || p.nz < 2)
+      throw CudaError(1, "grid size not supported (nx, ny in {16,32,64,128,256,512}, nz >= 2)");
+    LES_CUDA(cudaSetDevice(p.device));
+    LES_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (auto& e : ev) LES_CUDA(cudaEventCreate(&e));
+    static bool attrs = false;
+    if (!attrs) {
+      init_spectral_attributes();
+      attrs = true;
+    }
+    const long nf = g.field();
+    for (int i = 0; i < LES_NFIELDS; ++i) F[i] = track(dalloc<T>(nf));
+    for (int i = 0; i < LES_NPLANES; ++i) PL[i] = track(dalloc<T>(g.plane()));
+    build_tables();
+    const long se = (long)g.L * std::max((long)g.ny * g.lhx, (long)g.ny2 * (g.nx / 2));
+    for (int i = 0; i < NSPEC; ++i) spec[i] = track(dalloc<cplx<T>>(se));
+    for (int i = 0; i < NSPEC; ++i) spec4[i] = track(dalloc<cplx<T>>((long)g.L * g.ny * nk4));
+    const long fe = (long)g.L * g.ny2 * g.nx2;
+    for (auto& f : fine) f = track(dalloc<T>(fe));
+    for (auto& f : sc) f = track(dalloc<T>(nf));
+    xs = track(dalloc<cplx<double>>((long)g.L * g.ny * g.lhx));
+    gam = track(dalloc<double>((long)g.L * g.ny * g.lhx));
+    pmean = track(dalloc<double>(g.L));
+    part = track(dalloc<double>(DIAG_BLOCKS * DIAG_NV));
+    dout = track(dalloc<double>(8));
+    dstatus = track(dalloc<unsigned>(4));
+    // system.f90:196-198 and set_bc_surface (boundary_condition_mpi.f90:124-129)
+    fill(F[LES_W], 0, 0, T(BOGUS));
+    fill_plane(PL[LES_LBC_Z0], T(p.z0));
+    LES_CUDA(cudaStreamSynchronize(st));
+  }
+
+  ~Solver() override {
+    if (st) cudaStreamSynchronize(st);
+    for (void* q : allocs) cudaFree(q);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (st) cudaStreamDestroy(st);
+  }
+
+  template <typename U>
+  U* track(U* q) {
+    allocs.push_back(q);
+    return q;
+  }
+
+  // ------------------------------------------------------------ tables ----
+  void build_tables() {
+    const int nx = g.nx, ny = g.ny, lhx = g.lhx, lhy = g.lhy;
+    const double lx = P.lx, ly = P.ly;
+    std::vector<double> hkx((long)ny * lhx), hky((long)ny * lhx), hk2((long)ny * lhx);
+    // fft_engine.f90:127-143
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < lhx; ++i) {
+        double kx = double(i);
+        double ky = double(((j + ny / 2) % ny) - ny / 2);
+        if (i == lhx - 1 || j == lhy - 1) {
+          kx = 0.0;
+          ky = 0.0;
+        }
+        kx = 2.0 * PI / lx * kx;
+        ky = 2.0 * PI / ly * ky;
+        hkx[(long)j * lhx + i] = kx;
+        hky[(long)j * lhx + i] = ky;
+        hk2[(long)j * lhx + i] = kx * kx + ky * ky;
+      }
+    const double dx = P.lx / double(nx), dy = P.ly / double(ny), dz = P.lz / double(g.nz);
+    // testfilter.f90:101-131 (cutoff compared in default REAL)
+    auto make_g = [&](double alpha, int& nkc, int& kyc) {
+      std::vector<T> G((long)ny * lhx);
+      const double del = alpha * std::sqrt(dx * dy);
+      const double q = PI / del;
+      const double kc2 = q * q;
+      nkc = 1;
+      kyc = 0;
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < lhx; ++i) {
+          double v = 1.0 / double(nx * ny);
+          if (double(float(hk2[(long)j * lhx + i])) >= kc2) v = 0.0;
+          if (i == lhx - 1 || j == ny / 2) v = 0.0;
+          G[(long)j * lhx + i] = T(v);
+          if (v != 0.0) {
+            nkc = std::max(nkc, i + 1);
+            kyc = std::max(kyc, std::min(j, ny - j));
+          }
+        }
+      return G;
+    };
+    auto G2 = make_g(2.0, nk2, ky2);
+    auto G4 = make_g(4.0, nk4, ky4);
+    std::vector<T> tkx(hkx.size()), tky(hky.size());
+    for (size_t i = 0; i < hkx.size(); ++i) {
+      tkx[i] = T(hkx[i]);
+      tky[i] = T(hky[i]);
+    }
+    kkx = up(tkx);
+    kky = up(tky);
+    kkxd = up(hkx);
+    kkyd = up(hky);
+    gt = up(G2);
+    gtt = up(G4);
+    delta = std::pow(dx * dy * dz, 1.0 / 3.0);  // compute_sgs.f90:144
+    beta_pow = std::log(2.0) / (std::log(4.0) - std::log(2.0));
+    set_mixing_length();
+    for (int n : {g.nx, g.ny, g.nx2, g.ny2}) twiddles(n);
+  }
+
+  void set_mixing_length() {
+    // compute_sgs.f90:143-168: l = Delta, or the wall-damped cst_Smag length
+    std::vector<double> l2h(g.L, delta * delta);
+    const double dz = P.lz / double(g.nz);
+    if (P.sgs_model == LES_SGS_CST_SMAG) {
+      const double n = 2.0;
+      for (int k = 1; k <= g.nz + 1; ++k) {
+        const double z = (k == 1) ? 0.5 * dz : (1 + k - 2.0) * dz;
+        const double l = std::pow(std::pow(P.cs0, n) * std::pow(KVONK * z, -n) + std::pow(delta, -n), -1.0 / n);
+        l2h[k] = l * l;
+      }
+    }
+    if (!l2) l2 = track(dalloc<double>(g.L));
+    LES_CUDA(cudaMemcpy(l2, l2h.data(), sizeof(double) * g.L, cudaMemcpyHostToDevice));
+  }
+
+  template <typename U>
+  U* up(const std::vector<U>& h) {
+    U* d = track(dalloc<U>(h.size()));
+    LES_CUDA(cudaMemcpy(d, h.data(), sizeof(U) * h.size(), cudaMemcpyHostToDevice));
+    return d;
+  }
+
+  const cplx<T>* twiddles(int n) {
+    auto it = tw.find(n);
+    if (it != tw.end()) return it->second;
+    std::vector<cplx<T>> h(n);
+    for (int m = 0; m < n; ++m) {
+      const long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)n;
+      h[m] = cplx<T>{T(std::cos(a)), T(std::sin(a))};
+    }
+    cplx<T>* d = up(h);
+    tw[n] = d;
+    return d;
+  }
+
+  // ----------------------------------------------------------- helpers ----
+  T* lev(T* f, int k) const { return f + (long)k * g.plane(); }
+  void fill(T* f, int k0, int k1, T v) {
+    const long n = (long)(k1 - k0 + 1) * g.plane();
+    k_fill<T><<<grid_for(n), 256, 0, st>>>(lev(f, k0), n, v);
+    LES_CHECK_LAUNCH();
+  }
+  void fill_plane(T* f, T v) {
+    k_fill<T><<<grid_for(g.plane()), 256, 0, st>>>(f, g.plane(), v);
+    LES_CHECK_LAUNCH();
+  }
+
+  XFArgs<T> xf(int op, int nf, int plane0, int nplanes, int NX, int rows_pp, int nk) {
+    XFArgs<T> a;
+    std::memset(&a, 0, sizeof(a));
+    a.op = op;
+    a.nf = nf;
+    a.plane0 = plane0;
+    a.rows_pp = rows_pp;
+    a.nrows = (long)nplanes * rows_pp;
+    a.nk = nk;
+    a.nz = g.nz;
+    a.wall = P.wall_law;
+    a.in_pstride = (long)rows_pp * NX;
+    a.out_pstride = (long)rows_pp * nk;
+    a.tw = twiddles(NX);
+    return a;
+  }
+  YPArgs<T> yp(int op, int nin, int nout, int ncols, int nk_in, int NY, int nk_out, int NYO, int plane0) {
+    YPArgs<T> a;
+    std::memset(&a, 0, sizeof(a));
+    a.op = op;
+    a.nin = nin;
+    a.nout = nout;
+    a.ncols = ncols;
+    a.nk_in = nk_in;
+    a.nk_out = nk_out;
+    a.in_pstride = (long)NY * nk_in;
+    a.out_pstride = (long)NYO * nk_out;
+    a.plane0 = plane0;
+    a.nxh = g.nx / 2;
+    a.lhx = g.lhx;
+    a.kkx = kkx;
+    a.kky = kky;
+    a.tw_in = twiddles(NY);
+    a.tw_out = twiddles(NYO);
+    return a;
+  }
+  XIArgs<T> xi(int op, int nin, int plane0, int nplanes, int NX, int rows_pp, int nk) {
+    XIArgs<T> a;
+    std::memset(&a, 0, sizeof(a));
+    a.op = op;
+    a.nin = nin;
+    a.plane0 = plane0;
+    a.rows_pp = rows_pp;
+    a.nrows = (long)nplanes * rows_pp;
+    a.nk = nk;
+    a.nz = g.nz;
+    a.in_pstride = (long)rows_pp * nk;
+    a.out_pstride = (long)rows_pp * NX;
+    a.tw = twiddles(NX);
+    return a;
+  }
+
+  // ------------------------------------------------------ data movement ----
+  void upload(int field, const double* h, int k0, int k1) override {
+    check_field(field, k0, k1);
+    const long n = (long)(k1 - k0 + 1) * g.plane();
+    std::vector<T> tmp(n);
+    for (long i = 0; i < n; ++i) tmp[i] = T(h[i]);
+    LES_CUDA(cudaMemcpyAsync(lev(F[field], k0), tmp.data(), n * sizeof(T), cudaMemcpyHostToDevice, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+  }
+  void download(int field, double* h, int k0, int k1) override {
+    check_field(field, k0, k1);
+    const long n = (long)(k1 - k0 + 1) * g.plane();
+    std::vector<T> tmp(n);
+    LES_CUDA(cudaMemcpyAsync(tmp.data(), lev(F[field], k0), n * sizeof(T), cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+    for (long i = 0; i < n; ++i) h[i] = double(tmp[i]);
+  }
+  void upload_plane(int plane, const double* h) override {
+    if (plane < 0 || plane >= LES_NPLANES) throw CudaError(1, "invalid plane id");
+    std::vector<T> tmp(g.plane());
+    for (long i = 0; i < g.plane(); ++i) tmp[i] = T(h[i]);
+    LES_CUDA(cudaMemcpyAsync(PL[plane], tmp.data(), g.plane() * sizeof(T), cudaMemcpyHostToDevice, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+  }
+  void download_plane(int plane, double* h) override {
+    if (plane < 0 || plane >= LES_NPLANES) throw CudaError(1, "invalid plane id");
+    std::vector<T> tmp(g.plane());
+    LES_CUDA(cudaMemcpyAsync(tmp.data(), PL[plane], g.plane() * sizeof(T), cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+    for (long i = 0; i < g.plane(); ++i) h[i] = double(tmp[i]);
+  }
+  void check_field(int field, int k0, int k1) const {
+    if (field < 0 || field >= LES_NFIELDS) throw CudaError(1, "invalid field id");
+    if (k0 < 0 || k1 > g.nz + 1 || k1 < k0) throw CudaError(1, "invalid level range");
+  }
+
+  void set_initial_conditions(const double* u, const double* v, const double* w) override {
+    upload(LES_U, u, 1, g.nz);
+    upload(LES_V, v, 1, g.nz);
+    upload(LES_W, w, 1, g.nz);
+    // initial BCs with the namelist defaults: lbc 'drc' 0, ubc u,v 'neu' 0, w 'drc' 0
+    const int4 lt = make_int4(1, 1, 1, 0), ut = make_int4(2, 2, 1, 0);
+    for (int pl : {LES_LBC_U, LES_LBC_V, LES_LBC_W, LES_UBC_U, LES_UBC_V, LES_UBC_W}) fill_plane(PL[pl], T(0));
+    launch_bc(lt, ut);
+    fill(F[LES_W], 0, 0, T(BOGUS));
+    if (P.wall_law) {  // LES_engine.f90:168-171
+      lbc_t[0] = 2;
+      lbc_t[1] = 2;
+    }
+    LES_CUDA(cudaStreamSynchronize(st));
+  }
+
+  void launch_bc(int4 lt, int4 ut) {
+    k_set_bc<T><<<grid_for(g.plane()), 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], PL[LES_LBC_U], PL[LES_LBC_V],
+                                                    PL[LES_LBC_W], PL[LES_UBC_U], PL[LES_UBC_V], PL[LES_UBC_W],
+                                                    lt, ut, g.plane(), g.nz, T(P.lz / double(g.nz)));
+    LES_CHECK_LAUNCH();
+  }
+  void set_bc() override {
+    launch_bc(make_int4(lbc_t[0], lbc_t[1], lbc_t[2], 0), make_int4(ubc_t[0], ubc_t[1], ubc_t[2], 0));
+  }
+
+  double dz() const { return P.lz / double(g.nz); }
+
+  // ------------------------------------------------ compute_derivatives ----
+  // grad_velocity_filt for up to three fields at once
+  void grad_fields(const int* f, const int* dx, const int* dy, int nfld) {
+    const int L = g.L;
+    auto a = xf(XF_SCALE, nfld, 0, L, g.nx, g.ny, g.lhx);
+    a.c0 = 1.0 / double(g.nx * g.ny);
+    for (int q = 0; q < nfld; ++q) {
+      a.in[q] = F[f[q]];
+      a.out[q] = spec[q];
+    }
+    launch_xfwd<T>(g.nx, a, st);
+    auto b = yp(YP_GRAD, 1, 3, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 0);
+    for (int q = 0; q < nfld; ++q) {
+      b.in[q] = spec[q];
+      b.out[3 * q + 0] = spec[q];
+      b.out[3 * q + 1] = spec[3 + 2 * q];
+      b.out[3 * q + 2] = spec[4 + 2 * q];
+    }
+    launch_ypass<T>(g.ny, g.ny, b, L, nfld, st);
+    auto c = xi(XI_STORE, 3 * nfld, 0, L, g.nx, g.ny, g.lhx);
+    for (int q = 0; q < nfld; ++q) {
+      c.in[3 * q + 0] = spec[q];
+      c.in[3 * q + 1] = spec[3 + 2 * q];
+      c.in[3 * q + 2] = spec[4 + 2 * q];
+      c.out[3 * q + 0] = F[f[q]];
+      c.out[3 * q + 1] = F[dx[q]];
+      c.out[3 * q + 2] = F[dy[q]];
+    }
+    for (int q = 0; q < 3 * nfld; ++q) {
+      c.lo[q] = 0;
+      c.hi[q] = g.nz + 1;
+    }
+    launch_xinv<T>(g.nx, c, st);
+  }
+  void grad_velocity_filt(int f, int dfdx, int dfdy) override { grad_fields(&f, &dfdx, &dfdy, 1); }
+
+  void ddz_uv(int dfdz, int f) override {
+    k_ddz<T><<<grid_for((long)(g.nz + 1) * g.plane()), 256, 0, st>>>(F[dfdz], F[f], g.plane(), g.nz, T(1.0 / dz()), 0);
+    LES_CHECK_LAUNCH();
+  }
+  void ddz_w(int dfdz, int f) override {
+    k_ddz<T><<<grid_for((long)(g.nz + 1) * g.plane()), 256, 0, st>>>(F[dfdz], F[f], g.plane(), g.nz, T(1.0 / dz()), 1);
+    LES_CHECK_LAUNCH();
+  }
+
+  void compute_vel_grad() override {
+    const int f[3] = {LES_U, LES_V, LES_W};
+    const int dx[3] = {LES_DUDX, LES_DVDX, LES_DWDX};
+    const int dy[3] = {LES_DUDY, LES_DVDY, LES_DWDY};
+    grad_fields(f, dx, dy, 3);
+    set_bc();
+    k_ddz_vel<T><<<grid_for((long)(g.nz + 1) * g.plane()), 256, 0, st>>>(
+        F[LES_U], F[LES_V], F[LES_W], F[LES_DUDZ], F[LES_DVDZ], F[LES_DWDZ], g.plane(), g.nz, T(1.0 / dz()));
+    LES_CHECK_LAUNCH();
+  }
+
+  // stress divergence of up to three equations (compute_derivatives.f90:464-577)
+  struct DivEq {
+    int rhs, tx, ty, tz, stag;
+    double pf;
+  };
+  void div_eqs(const DivEq* e, int neq, bool layers) {
+    // forward transforms of the distinct tx, ty fields
+    int ids[6];
+    int nid = 0;
+    auto slot = [&](int fid) {
+      for (int q = 0; q < nid; ++q)
+        if (ids[q] == fid) return q;
+      ids[nid] = fid;
+      return nid++;
+    };
+    int sx[3], sy[3];
+    for (int q = 0; q < neq; ++q) {
+      sx[q] = slot(e[q].tx);
+      sy[q] = slot(e[q].ty);
+    }
+    auto a = xf(XF_SCALE, nid, 1, g.nz + 1, g.nx, g.ny, g.lhx);
+    a.c0 = 1.0 / double(g.nx * g.ny);
+    for (int q = 0; q < nid; ++q) {
+      a.in[q] = F[ids[q]];
+      a.out[q] = spec[q];
+    }
+    launch_xfwd<T>(g.nx, a, st);
+    auto b = yp(YP_DIV2, 2, 1, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 1);
+    for (int q = 0; q < neq; ++q) {
+      b.in[2 * q] = spec[sx[q]];
+      b.in[2 * q + 1] = spec[sy[q]];
+      b.out[q] = spec[6 + q];
+    }
+    launch_ypass<T>(g.ny, g.ny, b, g.nz + 1, neq, st);
+    auto c = xi(XI_DIV, neq, 1, g.nz + 1, g.nx, g.ny, g.lhx);
+    c.c0 = 1.0 / dz();
+    for (int q = 0; q < neq; ++q) {
+      c.in[q] = spec[6 + q];
+      c.out[q] = F[e[q].rhs];
+      c.aux[q] = F[e[q].tz];
+      c.lo[q] = e[q].stag;
+      c.pf[q] = e[q].pf;
+    }
+    c.out[8] = layers ? PL[LES_BOTTOM_WK_PRESS] : nullptr;
+    c.out[9] = layers ? PL[LES_TOP_WK_PRESS] : nullptr;
+    launch_xinv<T>(g.nx, c, st);
+  }
+  void div_stress(int rhs, int tx, int ty, int tz, int stag) override {
+    DivEq e{rhs, tx, ty, tz, stag, 0.0};
+    div_eqs(&e, 1, !stag);
+    if (stag) {
+      // optional layers are BOGUS for the staggered call (compute_derivatives.f90:560-574)
+    }
+  }
+
+  // -------------------------------------------- compute_convective_padd ----
+  void dealias_convec(int cx, int cy, int cz) override {
+    const int nz = g.nz;
+    const bool padd = (P.dealias == LES_DEALIAS_PADD);
+    const int nkin = padd ? g.nx / 2 : int(std::ceil(double(float(g.nx)) / 3.0)) - 1;
+    const int FNX = padd ? g.nx2 : g.nx;
+    const int FNY = padd ? g.ny2 : g.ny;
+    // 1. transforms of -c u, -c v, -c w and the vorticity (levels 1..nz+1)
+    auto a = xf(XF_CONV_IN, 6, 1, nz + 1, g.nx, g.ny, nkin);
+    a.c0 = 1.0 / double(g.nx * g.ny);
+    const int ins[9] = {LES_U, LES_V, LES_W, LES_DWDY, LES_DVDZ, LES_DUDZ, LES_DWDX, LES_DVDX, LES_DUDY};
+    for (int q = 0; q < 9; ++q) a.in[q] = F[ins[q]];
+    for (int q = 0; q < 6; ++q) a.out[q] = spec[q];
+    launch_xfwd<T>(g.nx, a, st);
+    // 2. y: pad to 3ny/2 (or 2/3-rule mask)
+    if (padd) {
+      auto b = yp(YP_PAD, 1, 1, nkin, nkin, g.ny, nkin, g.ny2, 1);
+      for (int q = 0; q < 6; ++q) {
+        b.in[q] = spec[q];
+        b.out[q] = spec[6 + q];
+      }
+      launch_ypass<T>(g.ny, g.ny2, b, nz + 1, 6, st);
+    } else {
+      auto b = yp(YP_MASK, 1, 1, nkin, nkin, g.ny, nkin, g.ny, 1);
+      b.tt = int(std::ceil(double(float(g.ny)) / 3.0)) - 2;
+      for (int q = 0; q < 6; ++q) {
+        b.in[q] = spec[q];
+        b.out[q] = spec[6 + q];
+      }
+      launch_ypass<T>(g.ny, g.ny, b, nz + 1, 6, st);
+    }
+    // 3. x: c2r on the fine (or base) grid
+    auto c = xi(XI_STORE, 6, 1, nz + 1, FNX, FNY, nkin);
+    for (int q = 0; q < 6; ++q) {
+      c.in[q] = spec[6 + q];
+      c.out[q] = fine[q];
+      c.lo[q] = 0;
+      c.hi[q] = nz + 1;
+    }
+    launch_xinv<T>(FNX, c, st);
+    // 4. products on the fine grid, transformed back (levels 1..nz)
+    const int nkout = padd ? g.nx / 2 : int(std::ceil(double(float(2 * g.lhx)) / 3.0)) - 1;
+    auto d = xf(XF_PROD, 3, 1, nz, FNX, FNY, nkout);
+    d.c0 = padd ? 1.0 / double(g.nx2 * g.ny2) : 1.0 / double(g.nx * g.ny);
+    for (int q = 0; q < 6; ++q) d.in[q] = fine[q];
+    for (int q = 0; q < 3; ++q) d.out[q] = spec[q];
+    launch_xfwd<T>(FNX, d, st);
+    if (padd) {
+      auto e = yp(YP_TRUNC, 1, 1, nkout, nkout, g.ny2, nkout, g.ny, 1);
+      for (int q = 0; q < 3; ++q) {
+        e.in[q] = spec[q];
+        e.out[q] = spec[3 + q];
+      }
+      launch_ypass<T>(g.ny2, g.ny, e, nz, 3, st);
+    } else {
+      auto e = yp(YP_MASK, 1, 1, nkout, nkout, g.ny, nkout, g.ny, 1);
+      e.tt = int(std::ceil(double(float(2 * g.lhy)) / 3.0)) - 2;
+      for (int q = 0; q < 3; ++q) {
+        e.in[q] = spec[q];
+        e.out[q] = spec[3 + q];
+      }
+      launch_ypass<T>(g.ny, g.ny, e, nz, 3, st);
+    }
+    const bool is_rhs = (cx == LES_RHSX && cy == LES_RHSY && cz == LES_RHSZ);
+    auto h = xi(is_rhs ? XI_CONV : XI_STORE, 3, 1, nz, g.nx, g.ny, nkout);
+    const int outs[3] = {cx, cy, cz};
+    for (int q = 0; q < 3; ++q) {
+      h.in[q] = spec[3 + q];
+      h.out[q] = F[outs[q]];
+      h.lo[q] = 1;
+      h.hi[q] = nz;
+    }
+    if (is_rhs) {
+      h.out[3] = F[LES_RHSX_F];
+      h.out[4] = F[LES_RHSY_F];
+      h.out[5] = F[LES_RHSZ_F];
+    }
+    launch_xinv<T>(g.nx, h, st);
+    // ghost levels of the outputs (compute_convective_padd.f90:251-259)
+    for (int q = 0; q < 3; ++q) {
+      if (padd) {
+        fill(F[outs[q]], 0, 0, T(BOGUS));
+        fill(F[outs[q]], nz + 1, nz + 1, T(BOGUS));
+      }
+    }
+    if (!padd) trunc_ghosts(outs);
+  }
+
+  // compute_convective_trunc leaves its vorticity scratch in the ghost levels
+  void trunc_ghosts(const int* outs) {
+    // level 0: wall rows zeroed for cx, cy; level nz+1 and cz level 0 hold
+    // c*(vorticity) of that level
+    scratch_vort_level(outs, 0);
+    scratch_vort_level(outs, g.nz + 1);
+  }
+  void scratch_vort_level(const int* outs, int k);
+
+  // ---------------------------------------------------- compute_pressure ----
+  void press_stag_array(double tadv1) override {
+    const int nz = g.nz;
+    const double c = 1.0 / double(g.nx * g.ny);
+    // bottom/top layers (compute_pressure.f90:151-165, 196-203)
+    k_scale<T><<<grid_for(g.plane()), 256, 0, st>>>(PL[LES_BOTTOM_WK_PRESS], g.plane(), T(c));
+    LES_CHECK_LAUNCH();
+    cplx<T>* bot = spec[0] + (long)(g.L - 1) * g.ny * g.lhx;  // last plane of spec[0] is unused
+    cplx<T>* top = spec[1] + (long)(g.L - 1) * g.ny * g.lhx;
+    {
+      auto a = xf(XF_SCALE, 1, 0, 1, g.nx, g.ny, g.lhx);
+      a.c0 = 1.0;
+      a.in[0] = PL[LES_BOTTOM_WK_PRESS];
+      a.out[0] = bot;
+      launch_xfwd<T>(g.nx, a, st);
+      a.c0 = c;
+      a.in[0] = PL[LES_TOP_WK_PRESS];
+      a.out[0] = top;
+      launch_xfwd<T>(g.nx, a, st);
+      auto b = yp(YP_FWDKILL, 1, 1, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 0);
+      b.in[0] = bot;
+      b.out[0] = bot;
+      b.in[1] = top;
+      b.out[1] = top;
+      launch_ypass<T>(g.ny, g.ny, b, 1, 2, st);
+    }
+    // H = FFT(u / (dt tadv1 nx ny)), Nyquist killed (levels 1..nz)
+    auto a = xf(XF_PRESS, 3, 1, nz, g.nx, g.ny, g.lhx);
+    a.c0 = c / tadv1;
+    a.c1 = P.dt;
+    const int uvw[3] = {LES_U, LES_V, LES_W};
+    for (int q = 0; q < 3; ++q) {
+      a.in[q] = F[uvw[q]];
+      a.out[q] = spec[2 + q];
+    }
+    launch_xfwd<T>(g.nx, a, st);
+    auto b = yp(YP_FWDKILL, 1, 1, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 1);
+    for (int q = 0; q < 3; ++q) {
+      b.in[q] = spec[2 + q];
+      b.out[q] = spec[2 + q];
+    }
+    launch_ypass<T>(g.ny, g.ny, b, nz, 3, st);
+    // tridiagonal solve per (kx, ky) -> p^ in spec[5], levels 0..nz+1
+    const bool mixed = (P.precision == LES_MIXED);
+    dim3 tg(ceil_div(g.lhx, 64), g.ny);
+    k_tridiag<T><<<tg, 64, 0, st>>>(spec[2], spec[3], spec[4], bot, top, kkxd, kkyd, spec[5], xs, gam,
+                                   mixed ? pmean : nullptr, dstatus, g.lhx, g.ny, nz, dz(), mixed ? 1 : 0);
+    LES_CHECK_LAUNCH();
+    // compute_press_grad: i kx p^, i ky p^, p^ -> dpdx, dpdy (1..nz), p (0..nz+1)
+    auto e = yp(YP_PGRAD, 1, 3, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 0);
+    e.in[0] = spec[5];
+    e.out[0] = spec[6];
+    e.out[1] = spec[7];
+    e.out[2] = spec[5];
+    launch_ypass<T>(g.ny, g.ny, e, g.L, 1, st);
+    auto h = xi(XI_STORE, 3, 0, g.L, g.nx, g.ny, g.lhx);
+    h.in[0] = spec[6];
+    h.in[1] = spec[7];
+    h.in[2] = spec[5];
+    h.out[0] = F[LES_DPDX];
+    h.out[1] = F[LES_DPDY];
+    h.out[2] = F[LES_P];
+    h.lo[0] = 1;
+    h.hi[0] = nz;
+    h.lo[1] = 1;
+    h.hi[1] = nz;
+    h.lo[2] = 0;
+    h.hi[2] = nz + 1;
+    launch_xinv<T>(g.nx, h, st);
+    // dpdz (compute_pressure.f90:359-369), then p(nz+1) = BOGUS (:353-357)
+    dpdz_only();
+    k_p_finish<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_P], mixed ? pmean : nullptr, g.plane(), nz);
+    LES_CHECK_LAUNCH();
+  }
+  void dpdz_only();
+
+  // ---------------------------------------------------- compute_wall_law ----
+  void wall_layer() {
+    if (P.wall_model == LES_WALL_FILTER) {
+      // get_layer_filter (utility_tools.f90:261-307) + test_filter_layer
+      cplx<T>* s0 = spec[0];
+      cplx<T>* s1 = spec[1];
+      auto a = xf(XF_SCALE, 2, 0, 1, g.nx, g.ny, nk2);
+      a.c0 = 1.0;
+      a.in[0] = lev(F[LES_U], 1);
+      a.in[1] = lev(F[LES_V], 1);
+      a.out[0] = s0;
+      a.out[1] = s1;
+      launch_xfwd<T>(g.nx, a, st);
+      auto b = yp(YP_FILTER1, 1, 1, nk2, nk2, g.ny, nk2, g.ny, 0);
+      b.G0 = gt;
+      b.in[0] = s0;
+      b.out[0] = s0;
+      b.in[1] = s1;
+      b.out[1] = s1;
+      launch_ypass<T>(g.ny, g.ny, b, 1, 2, st);
+      auto c = xi(XI_WALL, 2, 0, 1, g.nx, g.ny, nk2);
+      c.in[0] = s0;
+      c.in[1] = s1;
+      c.c0 = dz();
+      c.out_pstride = g.plane();
+      c.aux[0] = PL[LES_LBC_Z0];
+      c.out[0] = PL[LES_U_STAR_AVG];
+      c.out[1] = PL[LES_LBC_U];
+      c.out[2] = PL[LES_LBC_V];
+      c.out[3] = F[LES_TXZ];
+      c.out[4] = F[LES_TYZ];
+      c.out[5] = F[LES_DUDZ];
+      c.out[6] = F[LES_DVDZ];
+      launch_xinv<T>(g.nx, c, st);
+    } else {
+      wall_plain();
+    }
+  }
+  void wall_plain();
+  void obukhov() override { wall_layer(); }
+  void wallstress() override { wall_layer(); }
+
+  // -------------------------------------------------------- compute_sgs ----
+  SgsArgs<T> sgs_args() {
+    SgsArgs<T> a;
+    std::memset(&a, 0, sizeof(a));
+    const int d[9] = {LES_DUDX, LES_DUDY, LES_DUDZ, LES_DVDX, LES_DVDY, LES_DVDZ, LES_DWDX, LES_DWDY, LES_DWDZ};
+    for (int q = 0; q < 9; ++q) a.d[q] = F[d[q]];
+    a.cs = F[LES_CS_OPT2];
+    a.l2 = l2;
+    a.nu = F[LES_NU_T];
+    a.txx = F[LES_TXX];
+    a.txy = F[LES_TXY];
+    a.txz = F[LES_TXZ];
+    a.tyy = F[LES_TYY];
+    a.tyz = F[LES_TYZ];
+    a.tzz = F[LES_TZZ];
+    for (int q = 0; q < 6; ++q) a.sij[q] = sc[1 + q];
+    a.smag = sc[0];
+    a.wall = P.wall_law;
+    a.plane = g.plane();
+    a.nz = g.nz;
+    return a;
+  }
+
+  void sgs_stress(int jt, int jtt) override {
+    const long n1 = (long)(g.nz + 1) * g.plane();
+    auto a = sgs_args();
+    if (P.sgs_model == LES_SGS_CST_SMAG) {
+      fill(F[LES_CS_OPT2], 1, g.nz + 1, T(P.cs0 * P.cs0));
+    } else if (P.sgs_model == LES_SGS_LASD) {
+      lasd(a, jtt);
+    } else if (P.sgs_model == LES_SGS_DYN_SMAG) {
+      dynsmag(a, jt, jtt);
+    } else {
+      throw CudaError(1, "Invalid SGS model");
+    }
+    k_sgs_tau<T><<<grid_for(n1), 256, 0, st>>>(a);
+    LES_CHECK_LAUNCH();
+  }
+
+  // dynamic-procedure contractions at both test scales (compute_dynamic_mum x2)
+  void dynamic_mum(SgsArgs<T>& a, bool both) {
+    const long n1 = (long)(g.nz + 1) * g.plane();
+    k_sij<T><<<grid_for(n1), 256, 0, st>>>(a);
+    LES_CHECK_LAUNCH();
+    auto x = xf(XF_LASD, 21, 1, g.nz + 1, g.nx, g.ny, nk2);
+    x.in[0] = F[LES_U];
+    x.in[1] = F[LES_V];
+    x.in[2] = F[LES_W];
+    for (int q = 0; q < 6; ++q) x.in[3 + q] = sc[1 + q];
+    x.in[9] = sc[0];
+    for (int q = 0; q < 21; ++q) x.out[q] = spec[q];
+    launch_xfwd<T>(g.nx, x, st);
+    auto y = yp(both ? YP_FILTER2 : YP_FILTER1, 1, both ? 2 : 1, nk2, nk2, g.ny, nk2, g.ny, 1);
+    y.G0 = gt;
+    y.G1 = gtt;
+    y.ncols1 = nk4;
+    y.nk_out1 = nk4;
+    y.out_pstride1 = (long)g.ny * nk4;
+    for (int q = 0; q < 21; ++q) {
+      y.in[q] = spec[q];
+      y.out[(both ? 2 : 1) * q] = spec[q];
+      if (both) y.out[2 * q + 1] = spec4[q];
+    }
+    launch_ypass<T>(g.ny, g.ny, y, g.nz + 1, 21, st);
+    const double cst = 2.0 * delta * delta;
+    for (int sc_i = 0; sc_i < (both ? 2 : 1); ++sc_i) {
+      const int nk = sc_i == 0 ? nk2 : nk4;
+      auto z = xi(XI_LASD, 21, 1, g.nz + 1, g.nx, g.ny, nk);
+      z.c0 = cst;
+      z.c1 = sc_i == 0 ? 4.0 : 16.0;
+      for (int q = 0; q < 21; ++q) z.in[q] = sc_i == 0 ? spec[q] : spec4[q];
+      z.out[0] = sc[7 + 2 * sc_i];
+      z.out[1] = sc[8 + 2 * sc_i];
+      launch_xinv<T>(g.nx, z, st);
+    }
+  }
+
+  void lasd(SgsArgs<T>& a, int jtt) {
+    const int nz = g.nz;
+    if (jtt >= P.dyn_init) {
+      k_lag_accum<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_U_LAG], F[LES_V_LAG], F[LES_W_LAG], F[LES_U],
+                                                         F[LES_V], F[LES_W], g.field());
+      LES_CHECK_LAUNCH();
+    }
+    if (jtt < P.dyn_init) {
+      fill(F[LES_CS_OPT2], 1, nz + 1, T(0.03));
+      return;
+    }
+    if (jtt % P.cs_count != 0) return;
+    dynamic_mum(a, true);
+    const long n1 = (long)(nz + 1) * g.plane();
+    if (f_coeff_init) {
+      LagGeom geo{g.nx, g.ny, nz, g.plane(), P.lag_halo, P.dt, P.lx / double(g.nx), P.ly / double(g.ny), dz(),
+                  double(P.cs_count)};
+      k_lag_interp<T><<<grid_for(n1), 256, 0, st>>>(F[LES_U_LAG], F[LES_V_LAG], F[LES_W_LAG], F[LES_F_LM],
+                                                   F[LES_F_MM], F[LES_F_QN], F[LES_F_NN], sc[11], sc[12], sc[13],
+                                                   sc[14], geo);
+      LES_CHECK_LAUNCH();
+      std::swap(F[LES_F_LM], sc[11]);
+      std::swap(F[LES_F_MM], sc[12]);
+      std::swap(F[LES_F_QN], sc[13]);
+      std::swap(F[LES_F_NN], sc[14]);
+    }
+    k_lasd_update<T><<<grid_for(n1), 256, 0, st>>>(F[LES_F_LM], F[LES_F_MM], F[LES_F_QN], F[LES_F_NN], sc[7],
+                                                  sc[8], sc[9], sc[10], F[LES_CS_OPT2], F[LES_BETA],
+                                                  f_coeff_init ? 0 : 1, g.plane(), nz, 1.5 * delta,
+                                                  P.dt * double(P.cs_count), beta_pow);
+    LES_CHECK_LAUNCH();
+    f_coeff_init = true;
+    lagran_init = true;
+    for (int q : {LES_U_LAG, LES_V_LAG, LES_W_LAG}) fill(F[q], 0, nz + 1, T(0));
+  }
+
+  void dynsmag(SgsArgs<T>& a, int jt, int jtt);
+
+  void test_filter(int f, int which) override {
+    const int nk = which == 4 ? nk4 : nk2;
+    auto a = xf(XF_SCALE, 1, 1, g.nz + 1, g.nx, g.ny, nk);
+    a.c0 = 1.0;
+    a.in[0] = F[f];
+    a.out[0] = spec[0];
+    launch_xfwd<T>(g.nx, a, st);
+    auto b = yp(YP_FILTER1, 1, 1, nk, nk, g.ny, nk, g.ny, 1);
+    b.G0 = which == 4 ? gtt : gt;
+    b.in[0] = spec[0];
+    b.out[0] = spec[0];
+    launch_ypass<T>(g.ny, g.ny, b, g.nz + 1, 1, st);
+    auto c = xi(XI_STORE, 1, 1, g.nz + 1, g.nx, g.ny, nk);
+    c.in[0] = spec[0];
+    c.out[0] = F[f];
+    c.lo[0] = 1;
+    c.hi[0] = g.nz + 1;
+    launch_xinv<T>(g.nx, c, st);
+  }
+
+  // -------------------------------------------------------- LES_engine ----
+  void compute_rhs_adv() override {
+    // rhs_f = rhs ; rhs = convective term (fused in the convective store)
+    dealias_convec(LES_RHSX, LES_RHSY, LES_RHSZ);
+    DivEq e[3] = {{LES_RHSX, LES_TXX, LES_TXY, LES_TXZ, 1, P.pfx},
+                  {LES_RHSY, LES_TXY, LES_TYY, LES_TYZ, 1, P.pfy},
+                  {LES_RHSZ, LES_TXZ, LES_TYZ, LES_TZZ, 0, 0.0}};
+    div_eqs(e, 3, true);
+  }
+
+  void ab2(double tadv1, double tadv2) override {
+    k_ab2<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], F[LES_RHSX], F[LES_RHSY],
+                                                 F[LES_RHSZ], F[LES_RHSX_F], F[LES_RHSY_F], F[LES_RHSZ_F],
+                                                 g.plane(), g.nz, T(P.dt), T(tadv1), T(tadv2));
+    LES_CHECK_LAUNCH();
+  }
+
+  void projection(double tadv1) override {
+    // dpdz was formed by press_stag_array; this applies LES_engine.f90:303-331
+    k_projection<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], F[LES_RHSX], F[LES_RHSY],
+                                                        F[LES_RHSZ], F[LES_DPDX], F[LES_DPDY], F[LES_DPDZ],
+                                                        g.plane(), g.nz, T(P.dt * tadv1));
+    LES_CHECK_LAUNCH();
+  }
+
+  void step(int jt, int jtt) override {
+    LES_CUDA(cudaEventRecord(ev[0], st));
+    if (P.wall_law) wall_layer();  // obukhov + wallstress (same filtered layer)
+    compute_vel_grad();
+    LES_CUDA(cudaEventRecord(ev[1], st));
+    sgs_stress(jt, jtt);
+    LES_CUDA(cudaEventRecord(ev[2], st));
+    compute_rhs_adv();
+    LES_CUDA(cudaEventRecord(ev[3], st));
+    double t1, t2;
+    if (jtt == 1) {
+      t1 = 1.0;
+      t2 = 0.0;
+    } else {
+      t1 = 1.5;
+      t2 = 1.0 - t1;
+    }
+    ab2(t1, t2);
+    press_stag_array(t1);
+    LES_CUDA(cudaEventRecord(ev[4], st));
+    projection(t1);
+    set_bc();
+    diagnostics_launch();
+    LES_CUDA(cudaEventRecord(ev[5], st));
+    timed = true;
+  }
+  bool timed = false;
+
+  void diagnostics_launch() {
+    k_diag_partial<T><<<DIAG_BLOCKS, 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], F[LES_DUDX], F[LES_DVDY],
+                                                  F[LES_DWDZ], g.plane(), g.nz, part);
+    LES_CHECK_LAUNCH();
+    k_diag_final<T><<<1, 256, 0, st>>>(part, DIAG_BLOCKS, PL[LES_U_STAR_AVG], g.plane(), P.dt,
+                                      P.lx / double(g.nx), P.ly / double(g.ny), dz(),
+                                      double(g.nx) * double(g.ny) * double(g.nz), dout, dstatus);
+    LES_CHECK_LAUNCH();
+  }
+  void diagnostics(double out[4]) override {
+    diagnostics_launch();
+    LES_CUDA(cudaMemcpyAsync(out, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+  }
+  unsigned status() override {
+    unsigned h = 0;
+    LES_CUDA(cudaMemcpyAsync(&h, dstatus, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaMemsetAsync(dstatus, 0, sizeof(unsigned), st));
+    LES_CUDA(cudaStreamSynchronize(st));
+    return h;
+  }
+  void read_timers() override {
+    if (!timed) return;
+    LES_CUDA(cudaEventSynchronize(ev[5]));
+    float ms[5];
+    LES_CUDA(cudaEventElapsedTime(&ms[0], ev[0], ev[1]));
+    LES_CUDA(cudaEventElapsedTime(&ms[1], ev[1], ev[2]));
+    LES_CUDA(cudaEventElapsedTime(&ms[2], ev[2], ev[3]));
+    LES_CUDA(cudaEventElapsedTime(&ms[3], ev[3], ev[4]));
+    LES_CUDA(cudaEventElapsedTime(&ms[4], ev[0], ev[5]));
+    for (int i = 0; i < 5; ++i) timers_ms[i] = ms[i];
+  }
+};
+
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_dpdz(T* dpdz, const T* p, long plane, int nz, T rdz, const double* pmean) {
+  const long n = (long)nz * plane;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long o = plane + q;
+    const int k = int(o / plane);
+    if (pmean) {
+      // p holds the fluctuation only (mean mode dropped from the FP32
+      // transform); the mean-mode difference is taken in FP64
+      dpdz[o] = T(double(rdz * (p[o] - p[o - plane])) + double(rdz) * (pmean[k] - pmean[k - 1]));
+    } else {
+      dpdz[o] = rdz * (p[o] - p[o - plane]);
+    }
+  }
+}
+
+template <typename T>
+void Solver<T>::dpdz_only() {
+  const bool mixed = (P.precision == LES_MIXED);
+  k_dpdz<T><<<grid_for((long)g.nz * g.plane()), 256, 0, st>>>(F[LES_DPDZ], F[LES_P], g.plane(), g.nz,
+                                                             T(1.0 / dz()), mixed ? pmean : nullptr);
+  LES_CHECK_LAUNCH();
+}
+
+template <typename T>
+__global__ void k_vort_level(T* cx, T* cy, T* cz, const T* dwdy, const T* dvdz, const T* dudz, const T* dwdx,
+                             const T* dvdx, const T* dudy, long plane, int k, T c, int wall) {
+  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < plane; p += (long)gridDim.x * blockDim.x) {
+    const long o = (long)k * plane + p;
+    if (wall && k == 0) {
+      cx[o] = T(0);
+      cy[o] = T(0);
+    } else {
+      cx[o] = c * (dwdy[o] - dvdz[o]);
+      cy[o] = c * (dudz[o] - dwdx[o]);
+    }
+    cz[o] = c * (dvdx[o] - dudy[o]);
+  }
+}
+
+template <typename T>
+void Solver<T>::scratch_vort_level(const int* outs, int k) {
+  k_vort_level<T><<<grid_for(g.plane()), 256, 0, st>>>(
+      F[outs[0]], F[outs[1]], F[outs[2]], F[LES_DWDY], F[LES_DVDZ], F[LES_DUDZ], F[LES_DWDX], F[LES_DVDX],
+      F[LES_DUDY], g.plane(), k, T(1.0 / double(g.nx * g.ny)), P.wall_law);
+  LES_CHECK_LAUNCH();
+}
+
+// wall_inst / wall_homog (compute_wall_law.f90:119-138, 210-228)
+template <typename T>
+__global__ void k_wall_plain(const T* u1, const T* v1, double um, double vm, int homog, const T* z0, T* ustar,
+                             T* lbu, T* lbv, T* txz1, T* tyz1, T* dudz1, T* dvdz1, long plane, double dz) {
+  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < plane; p += (long)gridDim.x * blockDim.x) {
+    const double uu = homog ? um : double(u1[p]);
+    const double vv = homog ? vm : double(v1[p]);
+    const double uavg = sqrt(uu * uu + vv * vv);
+    const double us = KVONK * uavg / log((0.5 * dz) / double(z0[p]));
+    double bu = 0, bv = 0, tx = 0, ty = 0;
+    if (uavg != 0.0) {
+      bu = us / (0.5 * dz * KVONK) * uu / uavg;
+      bv = us / (0.5 * dz * KVONK) * vv / uavg;
+      tx = (us * us) * uu / uavg;
+      ty = (us * us) * vv / uavg;
+    }
+    ustar[p] = T(us);
+    lbu[p] = T(bu);
+    lbv[p] = T(bv);
+    txz1[p] = T(tx);
+    tyz1[p] = T(ty);
+    dudz1[p] = T(bu);
+    dvdz1[p] = T(bv);
+  }
+}
+
+template <typename T>
+void Solver<T>::wall_plain() {
+  double um = 0, vm = 0;
+  const int homog = (P.wall_model == LES_WALL_HOMOG);
+  if (homog) {
+    std::vector<double> h(g.plane());
+    download(LES_U, h.data(), 1, 1);
+    double s = 0;
+    for (double x : h) s += x;
+    um = (1.0 / double(g.nx * g.ny)) * s;
+    download(LES_V, h.data(), 1, 1);
+    s = 0;
+    for (double x : h) s += x;
+    vm = (1.0 / double(g.nx * g.ny)) * s;
+  }
+  k_wall_plain<T><<<grid_for(g.plane()), 256, 0, st>>>(lev(F[LES_U], 1), lev(F[LES_V], 1), um, vm, homog,
+                                                       PL[LES_LBC_Z0], PL[LES_U_STAR_AVG], PL[LES_LBC_U],
+                                                       PL[LES_LBC_V], lev(F[LES_TXZ], 1), lev(F[LES_TYZ], 1),
+                                                       lev(F[LES_DUDZ], 1), lev(F[LES_DVDZ], 1), g.plane(), dz());
+  LES_CHECK_LAUNCH();
+}
+
+// plane-averaged dynamic Smagorinsky (compute_DynSmag.f90:61-245)
+template <typename T>
+__global__ void k_plane_ratio(const T* LM, const T* MM, T* cs, long plane, int nz) {
+  // one block per level k = 1..nz+1; Neumaier sums in FP64
+  const int k = blockIdx.x + 1;
+  __shared__ double s[4][256];
+  Neu a, b;
+  for (long p = threadIdx.x; p < plane; p += blockDim.x) {
+    a.add(double(LM[(long)k * plane + p]));
+    b.add(double(MM[(long)k * plane + p]));
+  }
+  s[0][threadIdx.x] = a.s;
+  s[1][threadIdx.x] = a.c;
+  s[2][threadIdx.x] = b.s;
+  s[3][threadIdx.x] = b.c;
+  __syncthreads();
+  __shared__ double res;
+  if (threadIdx.x == 0) {
+    Neu x, y;
+    for (int i = 0; i < blockDim.x; ++i) {
+      x.add(s[0][i]);
+      x.add(s[1][i]);
+      y.add(s[2][i]);
+      y.add(s[3][i]);
+    }
+    const double num = x.val() / double(plane), den = y.val() / double(plane);
+    double c = (den != 0.0) ? num / den : 0.0;
+    res = fmax(0.0, c);
+  }
+  __syncthreads();
+  for (long p = threadIdx.x; p < plane; p += blockDim.x) cs[(long)k * plane + p] = T(res);
+}
+
+template <typename T>
+void Solver<T>::dynsmag(SgsArgs<T>& a, int jt, int jtt) {
+  if (jtt < P.dyn_init) {
+    fill(F[LES_CS_OPT2], 1, g.nz + 1, T(0.03));
+    return;
+  }
+  if (jt % P.cs_count != 0) return;
+  dynamic_mum(a, false);
+  k_plane_ratio<T><<<g.nz + 1, 256, 0, st>>>(sc[7], sc[8], F[LES_CS_OPT2], g.plane(), g.nz);
+  LES_CHECK_LAUNCH();
+}
+
+SolverBase* make_solver(const les_params& p) {
+  if (p.precision == LES_MIXED) return new Solver<float>(p);
+  return new Solver<double>(p);
+}
+
+}  // namespace les

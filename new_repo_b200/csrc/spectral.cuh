@@ -1,0 +1,524 @@
+// Batched horizontal 2-D real FFT passes with fused prologues/epilogues.
+//
+// A 2-D r2c/c2r of the reference (decomp_2d_fft_2d.f90:498-577: x r2c,
+// transpose X->Y, y c2c) becomes three kernel families that work on every
+// level of a field in one launch:
+//
+//   xfwd  : physical rows (length NX) -> half-spectrum rows, first nk modes.
+//           The load step computes the transformed quantity on the fly
+//           (scaling, vorticity, fine-grid products, SGS test-filter inputs).
+//   ypass : columns of a spectral buffer -> y FFT (length NY) -> spectral op
+//           (i*k multiply, Nyquist kill, filter, 3/2 pad or truncate) ->
+//           inverse y FFT (length NYO) -> spectral buffer.  This is where the
+//           2DECOMP X<->Y pencil transpose happens: columns are staged through
+//           shared memory, no global transpose is ever written.
+//   xinv  : half-spectrum rows -> c2r (length NX) -> fused store op
+//           (plain store, rhs accumulation, stress divergence with its dz
+//           term and pressure-BC layers, SGS dynamic-procedure contraction).
+//
+// Spectral buffers are [level][ky row][kx] with kx fastest, so the x passes
+// read and write whole contiguous rows and the y pass reads C consecutive kx
+// columns per row (128-byte segments).
+#pragma once
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace les {
+
+constexpr int MAXIN = 24;
+constexpr int MAXOUT = 48;
+
+// ---------------------------------------------------------------- xfwd ----
+enum XFOp : int {
+  XF_SCALE = 0,   // field f = c0 * in[f]
+  XF_CONV_IN = 1, // u,v,w scaled by -c0 and the three vorticity components (c0 scaled)
+  XF_PROD = 2,    // fine-grid u x omega products (inputs on the padded grid)
+  XF_LASD = 3,    // the 21 test-filter inputs of the dynamic procedure
+  XF_PRESS = 4,   // field f = c0 * (in[f] / c1)   (compute_pressure.f90:138-140)
+};
+
+template <typename T>
+struct XFArgs {
+  int op, nf, R;
+  long nrows;      // rows to process = nplanes * rows_pp
+  int rows_pp;     // rows per plane of the input grid
+  int plane0;      // first level
+  int nk;          // modes stored per output row
+  int nz;
+  int wall;        // wall-law special rows at k=1
+  long in_pstride; // elements per plane of the input grid
+  long in_rstride; // elements per row of the input grid (== NX)
+  double c0, c1;
+  const T* in[12];
+  cplx<T>* out[MAXIN];
+  long out_pstride;  // rows_pp * nk
+  const cplx<T>* tw; // exp(-2 pi i m / NX), m < NX
+};
+
+// Values of every field at level l, row j, column i (input grid), written to
+// v[f * vs] (shared memory).
+template <typename T>
+__device__ __forceinline__ void xf_load_point(const XFArgs<T>& a, int l, int j, int i, T* v, int vs) {
+  const long off = (long)l * a.in_pstride + (long)j * a.in_rstride + i;
+  switch (a.op) {
+    case XF_SCALE: {
+      for (int f = 0; f < a.nf; ++f) v[f * vs] = T(a.c0) * a.in[f][off];
+      break;
+    }
+    case XF_PRESS: {
+      for (int f = 0; f < a.nf; ++f) v[f * vs] = T(a.c0) * (a.in[f][off] / T(a.c1));
+      break;
+    }
+    case XF_CONV_IN: {
+      // compute_convective_padd.f90:133-165
+      const T c = T(a.c0);
+      v[0 * vs] = -c * a.in[0][off];
+      v[1 * vs] = -c * a.in[1][off];
+      v[2 * vs] = -c * a.in[2][off];
+      const T* dwdy = a.in[3];
+      const T* dvdz = a.in[4];
+      const T* dudz = a.in[5];
+      const T* dwdx = a.in[6];
+      const T* dvdx = a.in[7];
+      const T* dudy = a.in[8];
+      if (a.wall && l == 0) {
+        v[3 * vs] = T(0);
+        v[4 * vs] = T(0);
+      } else if (a.wall && l == 1) {
+        const long up = off + a.in_pstride;
+        v[3 * vs] = c * (T(0.5) * (dwdy[off] + dwdy[up]) - dvdz[off]);
+        v[4 * vs] = c * (dudz[off] - T(0.5) * (dwdx[off] + dwdx[up]));
+      } else {
+        v[3 * vs] = c * (dwdy[off] - dvdz[off]);
+        v[4 * vs] = c * (dudz[off] - dwdx[off]);
+      }
+      v[5 * vs] = c * (dvdx[off] - dudy[off]);
+      break;
+    }
+    case XF_PROD: {
+      // compute_convective_padd.f90:180-249 on the fine grid; inputs are
+      // ub, vb, wb, o1, o2, o3 (padded -c*u, -c*v, -c*w and vorticity).
+      const T c = T(a.c0);
+      const T* ub = a.in[0];
+      const T* vb = a.in[1];
+      const T* wb = a.in[2];
+      const T* o1 = a.in[3];
+      const T* o2 = a.in[4];
+      const T* o3 = a.in[5];
+      const long up = off + a.in_pstride;
+      const long dn = off - a.in_pstride;
+      if (l == 1) {
+        v[0 * vs] = c * (-vb[off] * o3[off] + T(0.5) * wb[up] * o2[up]);
+        v[1 * vs] = c * (ub[off] * o3[off] + T(0.5) * wb[up] * (-o1[up]));
+        v[2 * vs] = T(0);
+      } else {
+        v[0 * vs] = c * (-vb[off] * o3[off] + T(0.5) * (wb[up] * o2[up] + wb[off] * o2[off]));
+        v[1 * vs] = c * (ub[off] * o3[off] + T(0.5) * (wb[off] * (-o1[off]) + wb[up] * (-o1[up])));
+        v[2 * vs] = c * T(0.5) * ((ub[off] + ub[dn]) * (-o2[off]) + (vb[off] + vb[dn]) * (o1[off]));
+      }
+      break;
+    }
+    case XF_LASD: {
+      // compute_LagScaleDep.f90:501-584: u_ft, A_ij, S_ij, |S| S_ij
+      const T* u = a.in[0];
+      const T* vv = a.in[1];
+      const T* w = a.in[2];
+      T uf, vf, wf;
+      if (l == 1) {
+        uf = u[off];
+        vf = vv[off];
+        wf = T(0.25) * w[off + a.in_pstride];
+      } else {
+        const long dn = off - a.in_pstride;
+        uf = T(0.5) * (u[off] + u[dn]);
+        vf = T(0.5) * (vv[off] + vv[dn]);
+        wf = w[off];
+      }
+      v[0 * vs] = uf;
+      v[1 * vs] = vf;
+      v[2 * vs] = wf;
+      v[3 * vs] = uf * uf;  // A11
+      v[4 * vs] = uf * vf;  // A12
+      v[5 * vs] = uf * wf;  // A13
+      v[6 * vs] = vf * vf;  // A22
+      v[7 * vs] = vf * wf;  // A23
+      v[8 * vs] = wf * wf;  // A33
+      const T S = a.in[9][off];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {  // s11 s12 s13 s22 s23 s33
+        const T s = a.in[3 + q][off];
+        v[(9 + q) * vs] = s;
+        v[(15 + q) * vs] = S * s;
+      }
+      break;
+    }
+  }
+}
+
+template <typename T, int NX>
+__global__ void __launch_bounds__(256) k_xfwd(const XFArgs<T> a) {
+  constexpr int M = NX / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* b0 = tw + NX;
+  const int nseq = a.R * a.nf;
+  cplx<T>* b1 = b0 + nseq * M;
+  for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
+  const long g0 = (long)blockIdx.x * a.R;
+  // load: one thread per point; sequence s = r*nf + f holds the packed row
+  // z_m = x_{2m} + i x_{2m+1}, i.e. the real row itself viewed as complex.
+  T* xr = reinterpret_cast<T*>(b0);
+  for (int idx = threadIdx.x; idx < a.R * NX; idx += blockDim.x) {
+    const int r = idx / NX;
+    const int i = idx - r * NX;
+    const long g = g0 + r;
+    T* dst = xr + (long)(r * a.nf) * NX + i;
+    if (g < a.nrows) {
+      const int l = a.plane0 + int(g / a.rows_pp);
+      const int j = int(g % a.rows_pp);
+      xf_load_point(a, l, j, i, dst, NX);
+    } else {
+      for (int f = 0; f < a.nf; ++f) dst[f * NX] = T(0);
+    }
+  }
+  __syncthreads();
+  cplx<T>* Z = fft_batch<T, M, false, 2>(b0, b1, nseq, M, tw);
+  // r2c post-processing: X_k = E_k + W^k O_k for k < nk
+  for (int idx = threadIdx.x; idx < nseq * a.nk; idx += blockDim.x) {
+    const int s = idx / a.nk;
+    const int k = idx - s * a.nk;
+    const int r = s / a.nf;
+    const int f = s - r * a.nf;
+    const long g = g0 + r;
+    if (g >= a.nrows) continue;
+    const cplx<T> zk = Z[s * M + (k == M ? 0 : k)];
+    const cplx<T> zm = Z[s * M + ((M - k) % M)];
+    const cplx<T> e = {T(0.5) * (zk.x + zm.x), T(0.5) * (zk.y - zm.y)};
+    // o = (zk - conj(zm)) / (2i)
+    const cplx<T> o = {T(0.5) * (zk.y + zm.y), T(-0.5) * (zk.x - zm.x)};
+    const cplx<T> w = tw[k];
+    const cplx<T> X = cadd(e, cmul(o, w));
+    const int l = a.plane0 + int(g / a.rows_pp);
+    const int j = int(g % a.rows_pp);
+    a.out[f][(long)l * a.out_pstride + (long)j * a.nk + k] = X;
+  }
+}
+
+// --------------------------------------------------------------- ypass ----
+enum YPOp : int {
+  YP_GRAD = 0,     // f -> f, i kx f, i ky f           (Nyquist killed)
+  YP_DIV2 = 1,     // (fx, fy) -> i kx fx + i ky fy     (Nyquist killed)
+  YP_FWDKILL = 2,  // f -> f, no inverse y transform    (Nyquist killed)
+  YP_PGRAD = 3,    // p^ (already y-spectral) -> i kx p, i ky p, p
+  YP_FILTER2 = 4,  // f -> G0 f, G1 f
+  YP_PAD = 5,      // ny -> 3ny/2 zero padding (ky Nyquist dropped)
+  YP_TRUNC = 6,    // 3ny/2 -> ny truncation (ky Nyquist zeroed)
+  YP_MASK = 7,     // keep |ky| <= tt (2/3-rule truncation)
+  YP_FILTER1 = 8,  // f -> G0 f
+};
+
+template <typename T>
+struct YPArgs {
+  int op, nin, nout, C, lc;  // C = 1 << lc columns per CTA
+  int ncols;           // columns processed
+  int ncols1;          // columns stored for the second FILTER2 output
+  int nk_in, nk_out, nk_out1;
+  int plane0;
+  long in_pstride, out_pstride, out_pstride1;
+  int nxh, lhx;        // base-grid Nyquist column and row length of kkx/kky/G
+  int tt;              // YP_MASK: largest |ky| kept
+  const cplx<T>* in[MAXIN];
+  cplx<T>* out[MAXOUT];
+  const T* kkx;        // [ny][lhx]
+  const T* kky;
+  const T* G0;         // [ny][lhx] filter kernels (include 1/(nx ny))
+  const T* G1;
+  const cplx<T>* tw_in;   // length NY table
+  const cplx<T>* tw_out;  // length NYO table
+};
+
+template <typename T, int NY, int NYO>
+__global__ void __launch_bounds__(256) k_ypass(const YPArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* twi = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* two = twi + NY;
+  cplx<T>* bufA = two + NYO;
+  constexpr int SI = NY + 1;
+  constexpr int SO = NYO + 1;
+  const int C = a.C;
+  const int nmax = max(a.nin * SI, a.nout * SO);
+  cplx<T>* bufB = bufA + C * nmax;
+  for (int i = threadIdx.x; i < NY; i += blockDim.x) twi[i] = a.tw_in[i];
+  for (int i = threadIdx.x; i < NYO; i += blockDim.x) two[i] = a.tw_out[i];
+  const int col0 = blockIdx.x * C;
+  const int l = a.plane0 + blockIdx.y;
+  const int grp = blockIdx.z;
+  // load C columns of every input field
+  for (int idx = threadIdx.x; idx < a.nin * NY * C; idx += blockDim.x) {
+    const int c = idx & (C - 1);
+    const int t = idx >> a.lc;
+    const int ky = t % NY;
+    const int q = t / NY;
+    const int kx = col0 + c;
+    cplx<T> v = {T(0), T(0)};
+    if (kx < a.ncols) v = a.in[grp * a.nin + q][(long)l * a.in_pstride + (long)ky * a.nk_in + kx];
+    bufA[(q * C + c) * SI + ky] = v;
+  }
+  __syncthreads();
+  cplx<T>* F = bufA;
+  if (a.op != YP_PGRAD) F = fft_batch<T, NY, false>(bufA, bufB, a.nin * C, SI, twi);
+  cplx<T>* D = (F == bufA) ? bufB : bufA;
+  cplx<T>* E = (F == bufA) ? bufA : bufB;
+  // spectral op -> D (nout * C sequences of length NYO)
+  for (int idx = threadIdx.x; idx < a.nout * NYO * C; idx += blockDim.x) {
+    const int c = idx & (C - 1);
+    const int t = idx >> a.lc;
+    const int ky = t % NYO;
+    const int q = t / NYO;
+    const int kx = col0 + c;
+    cplx<T> r = {T(0), T(0)};
+    if (kx < a.ncols) {
+      switch (a.op) {
+        case YP_GRAD: {
+          const bool kill = (ky == NY / 2) || (kx == a.nxh);
+          const cplx<T> f = kill ? cplx<T>{T(0), T(0)} : F[c * SI + ky];
+          if (q == 0) r = f;
+          else if (q == 1) r = ik_mul(a.kkx[ky * a.lhx + kx], f);
+          else r = ik_mul(a.kky[ky * a.lhx + kx], f);
+          break;
+        }
+        case YP_DIV2: {
+          const bool kill = (ky == NY / 2) || (kx == a.nxh);
+          if (!kill) {
+            const cplx<T> fx = F[c * SI + ky];
+            const cplx<T> fy = F[(C + c) * SI + ky];
+            r = cadd(ik_mul(a.kkx[ky * a.lhx + kx], fx), ik_mul(a.kky[ky * a.lhx + kx], fy));
+          }
+          break;
+        }
+        case YP_FWDKILL: {
+          const bool kill = (ky == NY / 2) || (kx == a.nxh);
+          if (!kill) r = F[(q * C + c) * SI + ky];
+          break;
+        }
+        case YP_PGRAD: {
+          const cplx<T> f = F[c * SI + ky];
+          if (q == 0) r = ik_mul(a.kkx[ky * a.lhx + kx], f);
+          else if (q == 1) r = ik_mul(a.kky[ky * a.lhx + kx], f);
+          else r = f;
+          break;
+        }
+        case YP_FILTER1:
+        case YP_FILTER2: {
+          const cplx<T> f = F[c * SI + ky];
+          const T g = (q == 0 ? a.G0 : a.G1)[ky * a.lhx + kx];
+          r = cplx<T>{f.x * g, f.y * g};
+          break;
+        }
+        case YP_PAD: {
+          // NYO = 3 NY / 2: modes 0..NY/2-1 and -(NY/2-1)..-1 kept
+          if (ky < NY / 2) r = F[c * SI + ky];
+          else if (ky > NYO - NY / 2) r = F[c * SI + ky - (NYO - NY)];
+          break;
+        }
+        case YP_TRUNC: {
+          // NY = 3 NYO / 2
+          if (ky < NYO / 2) r = F[c * SI + ky];
+          else if (ky > NYO / 2) r = F[c * SI + ky + (NY - NYO)];
+          break;
+        }
+        case YP_MASK: {
+          if (ky <= a.tt || ky >= NY - a.tt) r = F[(q * C + c) * SI + ky];
+          break;
+        }
+      }
+    }
+    D[(q * C + c) * SO + ky] = r;
+  }
+  __syncthreads();
+  cplx<T>* Y = D;
+  if (a.op != YP_FWDKILL) Y = fft_batch<T, NYO, true>(D, E, a.nout * C, SO, two);
+  for (int idx = threadIdx.x; idx < a.nout * NYO * C; idx += blockDim.x) {
+    const int c = idx & (C - 1);
+    const int t = idx >> a.lc;
+    const int ky = t % NYO;
+    const int q = t / NYO;
+    const int kx = col0 + c;
+    if (a.op == YP_FILTER2 && q == 1) {
+      if (kx < a.ncols1)
+        a.out[grp * a.nout + q][(long)l * a.out_pstride1 + (long)ky * a.nk_out1 + kx] = Y[(q * C + c) * SO + ky];
+    } else if (kx < a.ncols) {
+      a.out[grp * a.nout + q][(long)l * a.out_pstride + (long)ky * a.nk_out + kx] = Y[(q * C + c) * SO + ky];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- xinv ----
+enum XIOp : int {
+  XI_STORE = 0,  // out[f](l) = x_f for lo[f] <= l <= hi[f]
+  XI_CONV = 1,   // rhs_f = rhs ; rhs = x   (levels 1..nz)
+  XI_DIV = 2,    // rhs += x + dz(tz) + pf ; pressure-BC layers of the w equation
+  XI_LASD = 3,   // 21 filtered fields -> L:M and M:M
+  XI_WALL = 4,   // filtered u1, v1 -> u*, Neumann ghost value, wall stress
+};
+
+template <typename T>
+struct XIArgs {
+  int op, nin, R;
+  long nrows;
+  int rows_pp;
+  int plane0;
+  int nk;          // modes present in the input rows (rest zero)
+  int nz;
+  long in_pstride;
+  long out_pstride;  // elements per plane of the output grid
+  double c0, c1, c2, c3;
+  double pf[4];
+  int lo[MAXIN], hi[MAXIN];
+  const cplx<T>* in[MAXIN];
+  T* out[16];
+  const T* aux[8];
+  const cplx<T>* tw;  // exp(-2 pi i m / NX), m < NX
+};
+
+template <typename T, int NX>
+__global__ void __launch_bounds__(256) k_xinv(const XIArgs<T> a) {
+  constexpr int M = NX / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* b0 = tw + NX;
+  const int nseq = a.R * a.nin;
+  cplx<T>* b1 = b0 + nseq * M;
+  for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
+  __syncthreads();
+  const long g0 = (long)blockIdx.x * a.R;
+  // c2r pre-processing: Z_k = (X_k + conj X_{M-k}) + i W^{-k} (X_k - conj X_{M-k})
+  for (int idx = threadIdx.x; idx < nseq * M; idx += blockDim.x) {
+    const int s = idx / M;
+    const int k = idx - s * M;
+    const int r = s / a.nin;
+    const int f = s - r * a.nin;
+    const long g = g0 + r;
+    cplx<T> z = {T(0), T(0)};
+    if (g < a.nrows) {
+      const int l = a.plane0 + int(g / a.rows_pp);
+      const int j = int(g % a.rows_pp);
+      const cplx<T>* row = a.in[f] + (long)l * a.in_pstride + (long)j * a.nk;
+      cplx<T> xk = (k < a.nk) ? row[k] : cplx<T>{T(0), T(0)};
+      cplx<T> xm = (M - k < a.nk) ? row[M - k] : cplx<T>{T(0), T(0)};
+      if (k == 0) {  // DC and Nyquist bins: imaginary parts ignored (c2r)
+        xk.y = T(0);
+        xm.y = T(0);
+      }
+      const cplx<T> s1 = {xk.x + xm.x, xk.y - xm.y};  // X_k + conj(X_{M-k})
+      const cplx<T> d1 = {xk.x - xm.x, xk.y + xm.y};  // X_k - conj(X_{M-k})
+      const cplx<T> w = tw[k];                        // W^{k}; need W^{-k} = conj
+      const cplx<T> t = cmulc(d1, w);                 // d1 * W^{-k}
+      z = {s1.x - t.y, s1.y + t.x};                   // s1 + i t
+    }
+    b0[s * M + k] = z;
+  }
+  __syncthreads();
+  const cplx<T>* Zr = fft_batch<T, M, true, 2>(b0, b1, nseq, M, tw);
+  const T* xs = reinterpret_cast<const T*>(Zr);  // x_i of sequence s at xs[s*NX + i]
+  for (int idx = threadIdx.x; idx < a.R * NX; idx += blockDim.x) {
+    const int r = idx / NX;
+    const int i = idx - r * NX;
+    const long g = g0 + r;
+    if (g >= a.nrows) continue;
+    const int l = a.plane0 + int(g / a.rows_pp);
+    const int j = int(g % a.rows_pp);
+    const long off = (long)l * a.out_pstride + (long)j * NX + i;
+    const T* x = xs + (long)(r * a.nin) * NX + i;  // field f at x[f*NX]
+    switch (a.op) {
+      case XI_STORE: {
+        for (int f = 0; f < a.nin; ++f)
+          if (l >= a.lo[f] && l <= a.hi[f]) a.out[f][off] = x[f * NX];
+        break;
+      }
+      case XI_CONV: {
+        // LES_engine.f90:516-533: rhs_f = rhs ; rhs = convective term
+        if (l >= 1 && l <= a.nz) {
+          for (int f = 0; f < 3; ++f) {
+            a.out[3 + f][off] = a.out[f][off];
+            a.out[f][off] = x[f * NX];
+          }
+        }
+        break;
+      }
+      case XI_DIV: {
+        // compute_derivatives.f90:544-574 + LES_engine.f90:546-551, one
+        // equation per input: out[q] = rhs, aux[q] = tz, lo[q] = stag,
+        // pf[q] = forcing; out[8]/out[9] = bottom/top pressure-BC layers of
+        // the non-staggered (w) equation.  c0 = 1/dz.
+        const T rdz = T(a.c0);
+        const long pl = a.out_pstride;
+        const long p2 = (long)j * NX + i;
+        for (int q = 0; q < a.nin; ++q) {
+          const T* tz = a.aux[q];
+          const T xq = x[q * NX];
+          if (l >= 1 && l <= a.nz) {
+            const T dzq = a.lo[q] ? rdz * (tz[off + pl] - tz[off])   // ddz_w
+                                  : rdz * (tz[off] - tz[off - pl]);  // ddz_uv
+            a.out[q][off] = (a.out[q][off] + xq) + dzq + T(a.pf[q]);
+            if (!a.lo[q] && l == 1 && a.out[8]) a.out[8][p2] = xq + dzq;
+          }
+          if (!a.lo[q] && l == a.nz + 1 && a.out[9]) a.out[9][p2] = xq;
+        }
+        break;
+      }
+      case XI_LASD: {
+        // compute_LagScaleDep.f90:541-594; c0 = 2 delta^2, c1 = alpha^2
+        const T uf = x[0], vf = x[NX], wf = x[2 * NX];
+        const T a11 = x[3 * NX] - uf * uf;
+        const T a12 = x[4 * NX] - uf * vf;
+        const T a13 = x[5 * NX] - uf * wf;
+        const T a22 = x[6 * NX] - vf * vf;
+        const T a23 = x[7 * NX] - vf * wf;
+        const T a33 = x[8 * NX] - wf * wf;
+        const T s11 = x[9 * NX], s12 = x[10 * NX], s13 = x[11 * NX];
+        const T s22 = x[12 * NX], s23 = x[13 * NX], s33 = x[14 * NX];
+        const T sft = sqrt(T(2) * (s11 * s11 + s22 * s22 + s33 * s33 +
+                                   T(2) * (s12 * s12 + s13 * s13 + s23 * s23)));
+        const T cst = T(a.c0), tf2 = T(a.c1);
+        const T b11 = cst * (x[15 * NX] - tf2 * sft * s11);
+        const T b12 = cst * (x[16 * NX] - tf2 * sft * s12);
+        const T b13 = cst * (x[17 * NX] - tf2 * sft * s13);
+        const T b22 = cst * (x[18 * NX] - tf2 * sft * s22);
+        const T b23 = cst * (x[19 * NX] - tf2 * sft * s23);
+        const T b33 = cst * (x[20 * NX] - tf2 * sft * s33);
+        a.out[0][off] = a11 * b11 + a22 * b22 + a33 * b33 + T(2) * (a12 * b12 + a13 * b13 + a23 * b23);
+        a.out[1][off] = b11 * b11 + b22 * b22 + b33 * b33 + T(2) * (b12 * b12 + b13 * b13 + b23 * b23);
+        break;
+      }
+      case XI_WALL: {
+        // compute_wall_law.f90:143-183, 247-251 on the filtered first level.
+        // c0 = dz, c1 = 1/log-free constant unused; aux[0] = z0 plane.
+        // out: u_star_avg, lbc_u, lbc_v, txz(1), tyz(1), dudz(1), dvdz(1)
+        const long p2 = (long)j * NX + i;
+        const double u1 = double(x[0]), v1 = double(x[NX]);
+        const double uavg = sqrt(u1 * u1 + v1 * v1);
+        const double dz = a.c0;
+        const double ustar = KVONK * uavg / log((0.5 * dz) / double(a.aux[0][p2]));
+        double bu = 0.0, bv = 0.0, tx = 0.0, ty = 0.0;
+        if (uavg != 0.0) {
+          bu = ustar / (0.5 * dz * KVONK) * u1 / uavg;
+          bv = ustar / (0.5 * dz * KVONK) * v1 / uavg;
+          tx = (ustar * ustar) * u1 / uavg;
+          ty = (ustar * ustar) * v1 / uavg;
+        }
+        a.out[0][p2] = T(ustar);
+        a.out[1][p2] = T(bu);
+        a.out[2][p2] = T(bv);
+        const long o1 = a.out_pstride + p2;  // level 1 of a field
+        a.out[3][o1] = T(tx);
+        a.out[4][o1] = T(ty);
+        a.out[5][o1] = T(bu);
+        a.out[6][o1] = T(bv);
+        break;
+      }
+    }
+  }
+}
+
+}  // namespace les

@@ -1,0 +1,364 @@
+"""Host-side mirror of the reference's LES module interface, driving the
+B200 library through its C ABI.
+
+The Fortran reference exposes module subroutines that act on module-global
+arrays (``src/system.f90:21-43``); ``LES`` keeps those arrays in HBM and
+offers the same entry points under the same names:
+
+=====================================  ==========================================
+reference (file:line)                  here
+=====================================  ==========================================
+read_parameters  parameters_IO.f90:128 ``RunParams`` / ``read_namelist``
+create_system + *_init                 ``LES(params)``
+set_initial_conditions ('files')       ``LES.set_initial_conditions``
+initial_conditions.f90:130-212
+grad_velocity_filt                     ``LES.grad_velocity_filt``
+compute_derivatives.f90:94
+ddz_uv / ddz_w  :375 / :413            ``LES.ddz_uv`` / ``LES.ddz_w``
+div_stress  :464                       ``LES.div_stress``
+compute_dealias_convec                 ``LES.compute_dealias_convec``
+compute_convective_padd.f90:115
+press_stag_array compute_pressure:116  ``LES.press_stag_array``
+obukhov / wallstress                   ``LES.obukhov`` / ``LES.wallstress``
+compute_wall_law.f90:198 / :107
+sgs_stress compute_sgs.f90:105         ``LES.sgs_stress``
+test_filter testfilter.f90:144         ``LES.test_filter``
+set_bc boundary_condition_mpi.f90:33   ``LES.set_bc``
+compute_vel_grad LES_engine.f90:449    ``LES.compute_vel_grad``
+compute_RHS_adv LES_engine.f90:509     ``LES.compute_RHS_adv``
+time loop body LES_engine.f90:189-360  ``LES.step``
+compute_running_diagnistics            ``LES.diagnostics``
+running_diagnostics.f90:80
+=====================================  ==========================================
+
+Errors: the reference aborts through ``decomp_2d_abort(code, msg)``; here a
+nonzero library status raises ``LesError`` carrying the same code
+(1 invalid option, 3 out of memory, 9 numerical failure, 22 I/O).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import re
+from dataclasses import dataclass, field, replace
+from pathlib import Path
+
+import numpy as np
+
+from . import capi
+from .capi import FIELD_ID, PLANE_ID, LesError, LesParams, check
+
+PI = 3.1415926535897932384626433  # parameters_IO.f90:42
+KVONK = 0.4
+
+
+@dataclass
+class RunParams:
+    """Namelist parameters (parameters_IO.f90:151-166) and the derived sizes of
+    read_parameters (:238-277)."""
+
+    nx: int = 32
+    ny: int = 32
+    nz: int = 32
+    dt: float = 2e-4
+    dim_dt_flag: bool = False
+    xy_pi: bool = True
+    lx_in: float = 2.0
+    ly_in: float = 2.0
+    lz_in: float = 1.0
+    zi: float = 1.0
+    u_scale: float = 1.0
+    lbc_dz0: float = 1e-4
+    pfx: float = 1.0
+    pfy: float = 0.0
+    cs0: float = 0.16
+    sgs_model: str = "dyn_LagScaleDep"
+    cs_count: int = 5
+    dyn_init: int = 5
+    lbc_special: str = "wall_law"
+    wall_model: str = "wall_filter"
+    dealias: str = "padd"
+    lag_halo: str = "reference1x1"
+
+    lx: float = field(init=False, default=0.0)
+    ly: float = field(init=False, default=0.0)
+    lz: float = field(init=False, default=0.0)
+    dx: float = field(init=False, default=0.0)
+    dy: float = field(init=False, default=0.0)
+    dz: float = field(init=False, default=0.0)
+    z0: float = field(init=False, default=0.0)
+    dt_nd: float = field(init=False, default=0.0)
+
+    def __post_init__(self):
+        self.derive()
+
+    def derive(self) -> "RunParams":
+        lx, ly, lz = self.lx_in, self.ly_in, self.lz_in
+        if self.xy_pi:
+            lx = lx * PI
+            ly = ly * PI
+        self.lx, self.ly, self.lz = lx / self.zi, ly / self.zi, lz / self.zi
+        self.dt_nd = self.dt * self.u_scale / self.zi if self.dim_dt_flag else self.dt
+        self.dx = self.lx / float(self.nx)
+        self.dy = self.ly / float(self.ny)
+        self.dz = self.lz / float(self.nz)
+        self.z0 = self.lbc_dz0 / self.zi
+        return self
+
+    def with_(self, **kw) -> "RunParams":
+        return replace(self, **kw).derive()
+
+    def to_c(self, precision: str = "fp64", device: int = 0) -> LesParams:
+        for name, table, val in (("sgs_model", capi.SGS_MODELS, self.sgs_model),
+                                 ("wall_model", capi.WALL_MODELS, self.wall_model),
+                                 ("dealias", capi.DEALIAS, self.dealias),
+                                 ("lag_halo", capi.LAG_HALO, self.lag_halo),
+                                 ("precision", capi.PRECISION, precision)):
+            if val not in table:
+                raise LesError(capi.LES_ERR_INVALID, f"Invalid {name}: {val!r}")
+        return LesParams(self.nx, self.ny, self.nz, self.dt_nd, self.lx, self.ly, self.lz, self.z0,
+                         self.pfx, self.pfy, self.cs0, capi.SGS_MODELS[self.sgs_model], self.cs_count,
+                         self.dyn_init, 1 if self.lbc_special == "wall_law" else 0,
+                         capi.WALL_MODELS[self.wall_model], capi.DEALIAS[self.dealias],
+                         capi.LAG_HALO[self.lag_halo], capi.PRECISION[precision], device)
+
+
+_NML_KEYS = {"p_on_y", "p_on_z", "nx", "ny", "nz", "nt", "dt", "dim_dt_flag", "restart_flag", "xy_pi", "lx",
+             "ly", "lz", "u_scale", "zi", "lbc_dz0", "re", "pfx", "pfy", "cs0", "sgs_model", "cs_count",
+             "dyn_init", "lbc_special", "wall_model"}
+
+
+def read_namelist(path: str | Path) -> tuple[RunParams, dict]:
+    """Parse a ``parameters.nlst`` (parameters_IO.f90:151-234) into RunParams.
+
+    Returns (params, raw) where raw holds every key=value found.  Raises
+    LesError(22) when the file cannot be read, like the reference's
+    MPI_Abort(22) (parameters_IO.f90:173-234)."""
+    try:
+        text = Path(path).read_text()
+    except OSError as e:
+        raise LesError(capi.LES_ERR_IO, f"Could not open {path} for reading ({e})") from e
+    raw = {}
+    for m in re.finditer(r"(\w+)\s*=\s*('[^']*'|\"[^\"]*\"|[^\s,/]+)", text):
+        key, val = m.group(1).lower(), m.group(2).strip()
+        if val[0] in "'\"":
+            v = val[1:-1]
+        elif val.lower() in (".true.", "t", ".t."):
+            v = True
+        elif val.lower() in (".false.", "f", ".f."):
+            v = False
+        else:
+            try:
+                v = int(val)
+            except ValueError:
+                v = float(val.lower().replace("d", "e"))
+        raw[key] = v
+    kw = dict(nx=raw.get("nx", 32), ny=raw.get("ny", 32), nz=raw.get("nz", 32), dt=float(raw.get("dt", 2e-4)),
+              dim_dt_flag=bool(raw.get("dim_dt_flag", False)), xy_pi=bool(raw.get("xy_pi", True)),
+              lx_in=float(raw.get("lx", 2.0)), ly_in=float(raw.get("ly", 2.0)), lz_in=float(raw.get("lz", 1.0)),
+              zi=float(raw.get("zi", 1.0)), u_scale=float(raw.get("u_scale", 1.0)),
+              lbc_dz0=float(raw.get("lbc_dz0", 1e-4)), pfx=float(raw.get("pfx", 1.0)),
+              pfy=float(raw.get("pfy", 0.0)), cs0=float(raw.get("cs0", 0.16)),
+              sgs_model=str(raw.get("sgs_model", "cst_Smag")), cs_count=int(raw.get("cs_count", 5)),
+              dyn_init=int(raw.get("dyn_init", 1500)), lbc_special=str(raw.get("lbc_special", "std")),
+              wall_model=str(raw.get("wall_model", "wall_filter")))
+    return RunParams(**kw), raw
+
+
+def log_law_noise(p: RunParams, seed: int = 0, amp: float = 0.1):
+    """Synthetic initial velocity (nz, ny, nx): u = ln(z/z0)/kappa at uvp heights
+    z = (k-1/2) dz (initial_conditions.f90:101-117 with u_star = 1) plus
+    uniform noise in [-amp, amp) from a counter-based hash of
+    (seed, field, index) (splitmix64).  The reference's own ran3 noise is not
+    reproduced; fields are handed over through the ic_type='files' path."""
+    z = (np.arange(1, p.nz + 1) - 0.5) * p.dz
+    arg = (1.0 / KVONK) * np.log(z / p.z0)
+    shape = (p.nz, p.ny, p.nx)
+    u = np.broadcast_to(arg[:, None, None], shape).copy()
+    v = np.zeros(shape)
+    w = np.zeros(shape)
+    for fid, a in enumerate((u, v, w)):
+        a += amp * _hash_uniform(seed, fid, shape)
+    return u, v, w
+
+
+def _hash_uniform(seed: int, fid: int, shape):
+    n = int(np.prod(shape))
+    x = np.arange(n, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        x = x + np.uint64((seed * 1000003 + fid * 7919 + 1) & 0xFFFFFFFFFFFFFFFF) * np.uint64(0x9E3779B97F4A7C15)
+        z = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    u01 = (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    return (2.0 * u01 - 1.0).reshape(shape)
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class LES:
+    """One device-resident LES state on one GPU."""
+
+    def __init__(self, params: RunParams, precision: str = "fp64", device: int = 0):
+        self.lib = capi.load()
+        self.params = params
+        self.precision = precision
+        self._cp = params.to_c(precision, device)
+        h = C.c_void_p()
+        check(self.lib.les_create(C.byref(self._cp), C.byref(h)))
+        self._h = h
+        self.jt_total = 0
+        self.jt = 0
+
+    # ------------------------------------------------------------- lifetime
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.les_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ------------------------------------------------------- data movement
+    @property
+    def shape(self):
+        p = self.params
+        return (p.nz + 2, p.ny, p.nx)
+
+    def _fid(self, f) -> int:
+        if isinstance(f, str):
+            if f not in FIELD_ID:
+                raise LesError(capi.LES_ERR_INVALID, f"unknown field {f!r}")
+            return FIELD_ID[f]
+        return int(f)
+
+    def upload(self, name, arr, k0: int = 0, k1: int | None = None):
+        k1 = self.params.nz + 1 if k1 is None else k1
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.size != (k1 - k0 + 1) * self.params.ny * self.params.nx:
+            raise LesError(capi.LES_ERR_INVALID, "array size does not match the level range")
+        check(self.lib.les_upload(self._h, self._fid(name), _dptr(a), k0, k1))
+
+    def download(self, name, k0: int = 0, k1: int | None = None) -> np.ndarray:
+        k1 = self.params.nz + 1 if k1 is None else k1
+        out = np.empty((k1 - k0 + 1, self.params.ny, self.params.nx))
+        check(self.lib.les_download(self._h, self._fid(name), _dptr(out), k0, k1))
+        return out
+
+    def upload_plane(self, name, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        check(self.lib.les_upload_plane(self._h, PLANE_ID[name], _dptr(a)))
+
+    def download_plane(self, name) -> np.ndarray:
+        out = np.empty((self.params.ny, self.params.nx))
+        check(self.lib.les_download_plane(self._h, PLANE_ID[name], _dptr(out)))
+        return out
+
+    def set_initial_conditions(self, u, v, w):
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (u, v, w)]
+        check(self.lib.les_set_initial_conditions(self._h, *map(_dptr, a)))
+
+    def set_bc_types(self, lbc=(2, 2, 1), ubc=(2, 2, 1)):
+        la = (C.c_int * 3)(*lbc)
+        ua = (C.c_int * 3)(*ubc)
+        check(self.lib.les_set_bc_types(self._h, la, ua))
+
+    @property
+    def f_coeff_init(self) -> bool:
+        v = C.c_int()
+        check(self.lib.les_get_lagrangian_init(self._h, C.byref(v)))
+        return bool(v.value)
+
+    @f_coeff_init.setter
+    def f_coeff_init(self, val: bool):
+        check(self.lib.les_set_lagrangian_init(self._h, 1 if val else 0))
+
+    # -------------------------------------------------- module entry points
+    def grad_velocity_filt(self, f, dfdx, dfdy):
+        check(self.lib.les_grad_velocity_filt(self._h, self._fid(f), self._fid(dfdx), self._fid(dfdy)))
+
+    def ddz_uv(self, dfdz, f):
+        check(self.lib.les_ddz_uv(self._h, self._fid(dfdz), self._fid(f)))
+
+    def ddz_w(self, dfdz, f):
+        check(self.lib.les_ddz_w(self._h, self._fid(dfdz), self._fid(f)))
+
+    def div_stress(self, rhs, tx, ty, tz, stag: bool):
+        check(self.lib.les_div_stress(self._h, *(self._fid(x) for x in (rhs, tx, ty, tz)), 1 if stag else 0))
+
+    def compute_dealias_convec(self, cx="rhsx", cy="rhsy", cz="rhsz"):
+        check(self.lib.les_compute_dealias_convec(self._h, self._fid(cx), self._fid(cy), self._fid(cz)))
+
+    def press_stag_array(self, tadv1: float):
+        check(self.lib.les_press_stag_array(self._h, float(tadv1)))
+
+    def obukhov(self):
+        check(self.lib.les_obukhov(self._h))
+
+    def wallstress(self):
+        check(self.lib.les_wallstress(self._h))
+
+    def sgs_stress(self, jt: int, jtt: int):
+        check(self.lib.les_sgs_stress(self._h, int(jt), int(jtt)))
+
+    def test_filter(self, f, alpha: int = 2):
+        check(self.lib.les_test_filter(self._h, self._fid(f), int(alpha)))
+
+    def set_bc(self):
+        check(self.lib.les_set_bc(self._h))
+
+    def compute_vel_grad(self):
+        check(self.lib.les_compute_vel_grad(self._h))
+
+    def compute_RHS_adv(self):
+        check(self.lib.les_compute_rhs_adv(self._h))
+
+    def ab2_advance(self, tadv1: float, tadv2: float):
+        check(self.lib.les_ab2_advance(self._h, float(tadv1), float(tadv2)))
+
+    def projection(self, tadv1: float):
+        check(self.lib.les_projection(self._h, float(tadv1)))
+
+    def step(self, n: int = 1):
+        """Advance n time steps (the LES_engine.f90:189-360 loop body)."""
+        for _ in range(n):
+            self.jt += 1
+            self.jt_total += 1
+            check(self.lib.les_step(self._h, self.jt, self.jt_total))
+
+    def diagnostics(self) -> tuple:
+        """(cfl, mke, u_star, rms div u) of running_diagnostics.f90:148-305."""
+        out = np.zeros(4)
+        check(self.lib.les_diagnostics(self._h, _dptr(out)))
+        return tuple(float(x) for x in out)
+
+    def status(self) -> int:
+        v = C.c_uint()
+        check(self.lib.les_get_status(self._h, C.byref(v)))
+        return int(v.value)
+
+    def sync(self):
+        check(self.lib.les_sync(self._h))
+
+    def timers(self) -> dict:
+        out = np.zeros(5)
+        check(self.lib.les_timers(self._h, _dptr(out)))
+        return dict(zip(("grad", "stress", "rhs", "press", "loop"), out.tolist()))
+
+    def state_dict(self, names=None) -> dict:
+        names = capi.FIELDS if names is None else names
+        d = {n: self.download(n) for n in names}
+        for pn in capi.PLANES:
+            d[pn] = self.download_plane(pn)
+        return d
