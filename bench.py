@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""Throughput of the LES time step on B200: Mpts*steps/s at 256^3.
+
+Headline arm: the mixed-precision step (FP32 fields, FFTs, convection and
+SGS; FP64 tridiagonal pressure solve, mean mode and compensated diagnostics)
+with the Lagrangian scale-dependent dynamic SGS model, beside the plain FP64
+GPU step of the same seed (its throughput and the velocity error between the
+two runs are part of the JSON line).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (one 256^3 domain per GPU, no data-path
+collective): weak scaling.  The reference arm (--impl reference) times the
+CPU FP64 restatement of the reference algorithm on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mpts*steps/s at 256^3 (LES time step, FP32 + dynamic SGS closure vs plain FP64 GPU)"
+UNIT = "Mpts*steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="grid nx = ny (= nz unless --nz)")
+    ap.add_argument("--nz", type=int, default=None, help="vertical levels (default: --n)")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- helpers
+def peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text()), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            parts = [x.strip() for x in l.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return None, 0, 0, 1
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    backend = "nccl" if args.impl == "ours" else "gloo"
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600),
+                            **({"device_id": torch.device("cuda", local)} if backend == "nccl" else {}))
+    return dist, rank, local, ws
+
+
+def max_over_ranks(dist, x: float, local: int) -> float:
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, local):
+    if dist is not None:
+        import torch
+
+        if dist.get_backend() == "nccl":
+            dist.barrier(device_ids=[local])
+        else:
+            dist.barrier()
+
+
+def run_params(n: int, nz: int | None = None):
+    from new_repo_b200 import RunParams
+
+    # 2pi x 2pi x 1 channel, log-law wall (z0 = 1e-4), dp/dx = -1, LASD SGS
+    # (cs_count = 5; the dynamic procedure starts at step 5), 3/2 dealiasing
+    return RunParams(nx=n, ny=n, nz=nz or n, dt=1e-4, lbc_dz0=1e-4, pfx=1.0, sgs_model="dyn_LagScaleDep",
+                     cs_count=5, dyn_init=5, lbc_special="wall_law", wall_model="wall_filter", dealias="padd")
+
+
+# --------------------------------------------------------------- our arm
+def timed_steps(les, k: int) -> float:
+    les.sync()
+    les.event_record(0)
+    les.step(k)
+    les.event_record(1)
+    return les.event_elapsed(0, 1)
+
+
+def run_ours(args, dist, rank, local, ws):
+    import numpy as np
+
+    from new_repo_b200 import LES, log_law_noise
+
+    p = run_params(args.n, args.nz)
+    npts = p.nx * p.ny * p.nz
+    K, W = args.steps, max(args.warmup, 3)
+    u0, v0, w0 = log_law_noise(p, seed=rank)
+    out = {}
+
+    # ---- headline: mixed precision ----
+    les = LES(p, precision="mixed", device=local)
+    les.set_initial_conditions(u0, v0, w0)
+    les.step(W)
+    les.sync()
+    barrier(dist, local)
+    les.profile(True)
+    n0 = les.launch_count()
+    with ClockSampler(local) as clk:
+        ms = timed_steps(les, K)
+    n1 = les.launch_count()
+    prof = les.profile_report()
+    les.profile(False)
+    barrier(dist, local)
+    ms = max_over_ranks(dist, ms, local)
+    value = npts * K * ws / (ms / 1e3) / 1e6
+    mixed_u = [les.download(n, 1, p.nz) for n in ("u", "v", "w")] if not args.no_fp64 else None
+    status = les.status()
+
+    # ---- roofline of the dominant kernel (live events of the timed region) ----
+    top = max(prof.items(), key=lambda kv: kv[1]["ms"])
+    label, rec = top
+    avg_ms = rec["ms"] / rec["launches"]
+    achieved = rec["bytes_per_launch"] / (avg_ms / 1e3) / 1e9
+    pk, pk_kind = peaks()
+    roof = {"kernel": label, "bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
+            "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4), "peak_source": pk_kind,
+            "traffic": ncu_traffic(label), "avg_launch_ms": round(avg_ms, 4),
+            "algorithmic_bytes_per_launch": rec["bytes_per_launch"], "share_of_step": round(rec["ms"] / ms, 4)}
+    # step-level: algorithmic bytes per step (105 F + 28 F / cs_count, F = N * 4 B)
+    F = npts * 4.0
+    step_bytes = (105.0 + 28.0 / p.cs_count) * F
+    step_roof = {"algorithmic_bytes_per_step": step_bytes,
+                 "achieved_gbs": round(step_bytes / (ms / K / 1e3) / 1e9, 1),
+                 "frac": round(step_bytes / (ms / K / 1e3) / 1e9 / pk["hbm_gbs"], 4)}
+
+    # ---- end to end through the public API with pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(les, p, min(K, 20), local)
+    les.close()
+
+    # ---- plain FP64 GPU step, same seed ----
+    fp64 = None
+    if not args.no_fp64:
+        l64 = LES(p, precision="fp64", device=local)
+        l64.set_initial_conditions(u0, v0, w0)
+        l64.step(W)
+        l64.sync()
+        ms64 = timed_steps(l64, K)
+        ref_u = [l64.download(n, 1, p.nz) for n in ("u", "v", "w")]
+        l64.close()
+        ms64 = max_over_ranks(dist, ms64, local)
+        num = sum(float(((a - b) ** 2).sum()) for a, b in zip(mixed_u, ref_u))
+        den = sum(float((b ** 2).sum()) for b in ref_u)
+        prof_m = mixed_u[0].mean(axis=(1, 2))
+        prof_r = ref_u[0].mean(axis=(1, 2))
+        fp64 = {"value": round(npts * K * ws / (ms64 / 1e3) / 1e6, 2), "ms_per_step": round(ms64 / K, 4),
+                "speedup_of_headline": round(ms64 / ms, 3),
+                "velocity_rms_rel_error": float(math.sqrt(num / den)),
+                "mean_profile_drift": float(np.abs(prof_m - prof_r).max() / np.abs(prof_r).max()),
+                "after_steps": W + K}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_sample(args.n)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+            "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (fields, FFTs, convection, SGS) + f64 (pressure solve, mean mode, diagnostics)",
+            "data": "synthetic: log-law profile + seeded uniform +-0.1 noise (counter-based hash)",
+            "config": {"workload": f"LES time step {p.nx}x{p.ny}x{p.nz}, 3/2 dealiasing, LASD SGS "
+                                   f"(cs_count 5, dynamic update every 5th step), log-law wall, FP32+FP64-pressure",
+                       "grid": [p.nx, p.ny, p.nz], "dt": p.dt_nd, "sgs_model": p.sgs_model,
+                       "precision": "mixed", "parallelism": f"replicas x{ws}",
+                       "l2": "inputs larger than L2 (>= 9 GB of fields per step)"},
+            "roofline": roof, "step_roofline": step_roof,
+            "e2e": e2e, "gpu_launches": n1 - n0, "fp64_gpu": fp64, "cpu_baseline": cpu,
+            "clocks": clk.summary(), "status_bits": status,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def ncu_traffic(label: str):
+    """dram bytes per launch of the dominant kernel from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / "traffic.json"
+    try:
+        d = json.loads(f.read_text())
+        return d.get(label)
+    except Exception:
+        return None
+
+
+def run_e2e(les, p, K: int, local: int):
+    """K steps through the public API with the velocity state held in
+    page-locked host memory (the drop-in boundary: the host arrays stay
+    authoritative): per step H2D u,v,w -> les_step -> D2H u,v,w + diagnostics."""
+    import torch
+
+    L = p.nz + 2
+    shape = (L, p.ny, p.nx)
+    host = [torch.empty(shape, dtype=torch.float64, pin_memory=True) for _ in range(3)]
+    diag = torch.empty(4, dtype=torch.float64, pin_memory=True)
+    names = ("u", "v", "w")
+    for h, n in zip(host, names):
+        les.download_async(n, h.data_ptr())
+    les.sync()
+    les.event_record(2)
+    t0 = time.perf_counter()
+    for _ in range(K):
+        for h, n in zip(host, names):
+            les.upload_async(n, h.data_ptr())
+        les.step(1)
+        les.diagnostics_async(diag.data_ptr())
+        for h, n in zip(host, names):
+            les.download_async(n, h.data_ptr())
+    les.event_record(3)
+    les.sync()
+    wall = time.perf_counter() - t0
+    ms = les.event_elapsed(2, 3)
+    npts = p.nx * p.ny * p.nz
+    bytes_io = 3 * L * p.ny * p.nx * 8
+    return {"value": round(npts * K / (ms / 1e3) / 1e6, 2), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
+            "d2h_bytes_per_step": bytes_io + 32, "steps": K, "ms_per_step": round(ms / K, 4),
+            "host_wall_ms_per_step": round(wall * 1e3 / K, 4)}
+
+
+# --------------------------------------------------------- CPU baseline
+def cpu_sample(n: int):
+    """The FP64 oracle on the host cores: one plain step and one dynamic-update
+    step of an n x n x 32 slab of the workload, amortised over cs_count = 5."""
+    from oracle import les_oracle as O
+
+    cores = os.cpu_count() or 1
+    O.set_workers(cores)
+    p = O.Params(nx=n, ny=n, nz=32, dt=1e-4, dyn_init=1, cs_count=2)
+    ops = O.Ops(p)
+    st = O.make_state(p)
+    t = []
+    for _ in range(4):  # plain, F-initialising update, plain, interpolating update
+        t0 = time.perf_counter()
+        O.les_step(ops, st)
+        t.append(time.perf_counter() - t0)
+    t_plain = 0.5 * (t[0] + t[2])
+    t_upd = t[3]
+    per_step = (4 * t_plain + t_upd) / 5.0
+    pts = p.nx * p.ny * p.nz
+    return {"value": round(pts / per_step / 1e6, 4), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"numpy/scipy FP64 oracle, {n}x{n}x32 slab: plain step {t_plain:.2f} s, "
+                      f"dynamic-update step {t_upd:.2f} s, amortised 4:1 (cs_count 5)"}
+
+
+# -------------------------------------------------------- reference arm
+def run_reference(args, dist, rank, ws):
+    if rank != 0:
+        return
+    from oracle import les_oracle as O
+
+    cores = os.cpu_count() or 1
+    O.set_workers(cores)
+    n = args.n
+    nz = 8
+    p = O.Params(nx=n, ny=n, nz=nz, dt=1e-4, dyn_init=5, cs_count=5)
+    ops = O.Ops(p)
+    st = O.make_state(p)
+    W, K = max(args.warmup, 3), args.steps
+    for _ in range(W):
+        O.les_step(ops, st)
+    t0 = time.perf_counter()
+    for _ in range(K):
+        O.les_step(ops, st)
+    dt = time.perf_counter() - t0
+    pts = p.nx * p.ny * p.nz
+    v = pts * K / dt / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": ws,
+            "steps": K, "warmup": W, "ms_per_step": round(dt * 1e3 / K, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"LES time step, {n}x{n}x{nz} slab of the {n}^3 workload per sample step",
+                       "grid": [n, n, nz]},
+            "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"one full time step of a {n}x{n}x{nz} slab per step (FP64 oracle, "
+                                       f"scipy pocketfft with {cores} workers); the Fortran reference cannot "
+                                       "be built here (no Fortran compiler, MPI, FFTW or 2DECOMP&FFT)"},
+            "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    dist, rank, local, ws = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist, rank, ws)
+        else:
+            run_ours(args, dist, rank, local, ws)
+    finally:
+        if dist is not None:
+            barrier(dist, local)
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -159,6 +159,27 @@ int les_sync(les_state* s);
  * bucket (LES_engine.f90:100-107): grad, stress, rhs, press, loop (ms). */
 int les_timers(les_state* s, double out[5]);
 
+/* --- measurement (replaces the mpi_wtime timers of LES_engine.f90:100-107,
+ *     428-435 with device-side events) ------------------------------------ */
+/* Per-launch profiling: with enable != 0 every kernel launch is bracketed by
+ * CUDA events on the state's stream.  les_profile_report writes a JSON object
+ * {"<operator>/<kernel>": {"launches", "ms", "bytes_per_launch"}, ...} where
+ * bytes_per_launch is the launch's algorithmic traffic (inputs read once,
+ * outputs written once). */
+int les_profile(les_state* s, int enable);
+int les_profile_report(les_state* s, char* buf, int buflen);
+/* Number of kernels launched on this state since creation. */
+int les_launch_count(les_state* s, long long* n);
+/* Record timing event slot (0..15) on the state's stream / elapsed ms b - a. */
+int les_event_record(les_state* s, int slot);
+int les_event_elapsed(les_state* s, int a, int b, double* ms);
+/* Asynchronous FP64 transfers from/to page-locked host memory on the state's
+ * stream (converted on the device in mixed precision); les_sync completes
+ * them. */
+int les_upload_async(les_state* s, int field, const double* pinned, int k0, int k1);
+int les_download_async(les_state* s, int field, double* pinned, int k0, int k1);
+int les_diagnostics_async(les_state* s, double* pinned_out4);
+
 #ifdef __cplusplus
 }
 #endif

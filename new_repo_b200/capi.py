@@ -80,6 +80,14 @@ PROTOTYPES = {
     "les_get_status": [_P, C.POINTER(C.c_uint)],
     "les_sync": [_P],
     "les_timers": [_P, _D],
+    "les_profile": [_P, _I],
+    "les_profile_report": [_P, C.c_char_p, _I],
+    "les_launch_count": [_P, C.POINTER(C.c_longlong)],
+    "les_event_record": [_P, _I],
+    "les_event_elapsed": [_P, _I, _I, _D],
+    "les_upload_async": [_P, _I, C.c_void_p, _I, _I],
+    "les_download_async": [_P, _I, C.c_void_p, _I, _I],
+    "les_diagnostics_async": [_P, C.c_void_p],
 }
 
 _lib = None

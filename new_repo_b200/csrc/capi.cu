@@ -32,8 +32,9 @@ int bad_state() {
 }
 }  // namespace
 
-#define STATE_OR_FAIL(s) \
-  if (!(s) || !(s)->s) return bad_state()
+#define STATE_OR_FAIL(s)            \
+  if (!(s) || !(s)->s) return bad_state(); \
+  les::g_hook = (s)->s
 
 extern "C" {
 
@@ -45,6 +46,7 @@ int les_create(const les_params* p, les_state** out) {
     return LES_ERR_INVALID;
   }
   *out = nullptr;
+  les::g_hook = nullptr;  // never observe launches through a previous state
   return guard([&] {
     if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0 || p->dt <= 0 || p->cs_count <= 0)
       throw les::CudaError(LES_ERR_INVALID, "invalid grid, dt or cs_count");
@@ -65,6 +67,7 @@ int les_create(const les_params* p, les_state** out) {
 
 int les_destroy(les_state* s) {
   if (!s) return LES_OK;
+  if (les::g_hook == s->s) les::g_hook = nullptr;
   int rc = guard([&] { delete s->s; });
   delete s;
   return rc;
@@ -194,6 +197,51 @@ int les_sync(les_state* s) {
   STATE_OR_FAIL(s);
   return guard([&] { LES_CUDA(cudaStreamSynchronize(s->s->st)); });
 }
+int les_profile(les_state* s, int enable) {
+  STATE_OR_FAIL(s);
+  return guard([&] {
+    LES_CUDA(cudaStreamSynchronize(s->s->st));
+    s->s->profile(enable != 0);
+  });
+}
+int les_profile_report(les_state* s, char* buf, int buflen) {
+  STATE_OR_FAIL(s);
+  return guard([&] {
+    const std::string r = s->s->profile_report();
+    if ((int)r.size() + 1 > buflen) throw les::CudaError(LES_ERR_INVALID, "profile report buffer too small");
+    std::memcpy(buf, r.c_str(), r.size() + 1);
+  });
+}
+int les_launch_count(les_state* s, long long* n) {
+  STATE_OR_FAIL(s);
+  *n = s->s->launches;
+  return LES_OK;
+}
+int les_event_record(les_state* s, int slot) {
+  STATE_OR_FAIL(s);
+  if (slot < 0 || slot >= 16) {
+    g_last_error = "event slot must be in 0..15";
+    return LES_ERR_INVALID;
+  }
+  return guard([&] { s->s->record_event(slot); });
+}
+int les_event_elapsed(les_state* s, int a, int b, double* ms) {
+  STATE_OR_FAIL(s);
+  return guard([&] { *ms = s->s->elapsed(a, b); });
+}
+int les_upload_async(les_state* s, int field, const double* pinned, int k0, int k1) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->upload_async(field, pinned, k0, k1); });
+}
+int les_download_async(les_state* s, int field, double* pinned, int k0, int k1) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->download_async(field, pinned, k0, k1); });
+}
+int les_diagnostics_async(les_state* s, double* pinned_out4) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->diagnostics_async(pinned_out4); });
+}
+
 int les_timers(les_state* s, double out[5]) {
   STATE_OR_FAIL(s);
   return guard([&] {

@@ -61,6 +61,12 @@ __global__ void k_scale(T* f, long n, T c) {
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) f[q] = c * f[q];
 }
 
+template <typename D, typename S>
+__global__ void k_convert(D* dst, const S* src, long n) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+    dst[q] = D(src[q]);
+}
+
 template <typename T>
 __global__ void k_copy(T* dst, const T* src, long n) {
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) dst[q] = src[q];

@@ -2,7 +2,27 @@
 #pragma once
 #include "spectral.cuh"
 
+#include <string>
+
 namespace les {
+
+// Observer of every kernel launch: the solver counts launches and, when
+// profiling, brackets each one with CUDA events on its stream.  bytes is the
+// launch's compulsory (algorithmic) HBM traffic: each input read once, each
+// output written once.
+struct LaunchHook {
+  virtual void before(const char* kind, double bytes) = 0;
+  virtual void after() = 0;
+  virtual ~LaunchHook() = default;
+};
+extern thread_local LaunchHook* g_hook;
+
+inline void hook_before(const char* kind, double bytes) {
+  if (g_hook) g_hook->before(kind, bytes);
+}
+inline void hook_after() {
+  if (g_hook) g_hook->after();
+}
 
 bool supported_length(int n);
 void init_spectral_attributes();

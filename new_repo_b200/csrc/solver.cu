@@ -5,12 +5,22 @@
 #include <map>
 #include <memory>
 #include <vector>
+#include <type_traits>
 
 #include "kernels.cuh"
 #include "launch.cuh"
 #include "solver.cuh"
 
 namespace les {
+
+// launch a pointwise kernel under the launch hook (count + optional events)
+#define KL(kind, bytes, ...)   \
+  do {                         \
+    hook_before(kind, bytes);  \
+    __VA_ARGS__;               \
+    LES_CHECK_LAUNCH();        \
+    hook_after();              \
+  } while (0)
 
 namespace {
 constexpr double PI = 3.1415926535897932384626433;  // parameters_IO.f90:42
@@ -50,6 +60,11 @@ class Solver final : public SolverBase {
   cplx<T>* spec4[NSPEC] = {};
   T* fine[6] = {};
   T* sc[15] = {};  // S, s11..s33, LM, MM, QN, NN, Fn x4
+  T* refbuf[MAXIN] = {};  // per-level reference values (mixed precision)
+  // FP64 spectral workspace of the pressure path in mixed precision
+  cplx<double>* pspec[8] = {};
+  std::map<int, cplx<double>*> twd;
+  double *kkx64 = nullptr, *kky64 = nullptr;
   cplx<double>* xs = nullptr;
   double* gam = nullptr;
   double* pmean = nullptr;
@@ -90,6 +105,9 @@ class Solver final : public SolverBase {
     const long fe = (long)g.L * g.ny2 * g.nx2;
     for (auto& f : fine) f = track(dalloc<T>(fe));
     for (auto& f : sc) f = track(dalloc<T>(nf));
+    for (auto& f : refbuf) f = track(dalloc<T>(g.L));
+    if (mixed())
+      for (auto& f : pspec) f = track(dalloc<cplx<double>>((long)g.L * g.ny * g.lhx));
     xs = track(dalloc<cplx<double>>((long)g.L * g.ny * g.lhx));
     gam = track(dalloc<double>((long)g.L * g.ny * g.lhx));
     pmean = track(dalloc<double>(g.L));
@@ -169,6 +187,8 @@ class Solver final : public SolverBase {
     kky = up(tky);
     kkxd = up(hkx);
     kkyd = up(hky);
+    kkx64 = kkxd;
+    kky64 = kkyd;
     gt = up(G2);
     gtt = up(G4);
     delta = std::pow(dx * dy * dz, 1.0 / 3.0);  // compute_sgs.f90:144
@@ -200,6 +220,19 @@ class Solver final : public SolverBase {
     return d;
   }
 
+  const cplx<double>* twiddles64(int n) {
+    auto it = twd.find(n);
+    if (it != twd.end()) return it->second;
+    std::vector<cplx<double>> h(n);
+    for (int m = 0; m < n; ++m) {
+      const long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)n;
+      h[m] = cplx<double>{double(std::cos(a)), double(std::sin(a))};
+    }
+    cplx<double>* d = up(h);
+    twd[n] = d;
+    return d;
+  }
+
   const cplx<T>* twiddles(int n) {
     auto it = tw.find(n);
     if (it != tw.end()) return it->second;
@@ -217,12 +250,10 @@ class Solver final : public SolverBase {
   T* lev(T* f, int k) const { return f + (long)k * g.plane(); }
   void fill(T* f, int k0, int k1, T v) {
     const long n = (long)(k1 - k0 + 1) * g.plane();
-    k_fill<T><<<grid_for(n), 256, 0, st>>>(lev(f, k0), n, v);
-    LES_CHECK_LAUNCH();
+    KL("k_fill", double(n) * sizeof(T), k_fill<T><<<grid_for(n), 256, 0, st>>>(lev(f, k0), n, v));
   }
   void fill_plane(T* f, T v) {
-    k_fill<T><<<grid_for(g.plane()), 256, 0, st>>>(f, g.plane(), v);
-    LES_CHECK_LAUNCH();
+    KL("k_fill", double(g.plane()) * sizeof(T), k_fill<T><<<grid_for(g.plane()), 256, 0, st>>>(f, g.plane(), v));
   }
 
   XFArgs<T> xf(int op, int nf, int plane0, int nplanes, int NX, int rows_pp, int nk) {
@@ -313,6 +344,34 @@ class Solver final : public SolverBase {
     if (k0 < 0 || k1 > g.nz + 1 || k1 < k0) throw CudaError(1, "invalid level range");
   }
 
+  double* staging = nullptr;  // FP64 device staging field (mixed precision transfers)
+  void upload_async(int field, const double* h, int k0, int k1) override {
+    check_field(field, k0, k1);
+    const long n = (long)(k1 - k0 + 1) * g.plane();
+    if constexpr (std::is_same<T, double>::value) {
+      LES_CUDA(cudaMemcpyAsync(lev(F[field], k0), h, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    } else {
+      if (!staging) staging = track(dalloc<double>(g.field()));
+      LES_CUDA(cudaMemcpyAsync(staging, h, n * sizeof(double), cudaMemcpyHostToDevice, st));
+      KL("k_convert", 12.0 * n, k_convert<T, double><<<grid_for(n), 256, 0, st>>>(lev(F[field], k0), staging, n));
+    }
+  }
+  void download_async(int field, double* h, int k0, int k1) override {
+    check_field(field, k0, k1);
+    const long n = (long)(k1 - k0 + 1) * g.plane();
+    if constexpr (std::is_same<T, double>::value) {
+      LES_CUDA(cudaMemcpyAsync(h, lev(F[field], k0), n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    } else {
+      if (!staging) staging = track(dalloc<double>(g.field()));
+      KL("k_convert", 12.0 * n, k_convert<double, T><<<grid_for(n), 256, 0, st>>>(staging, lev(F[field], k0), n));
+      LES_CUDA(cudaMemcpyAsync(h, staging, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+  }
+  void diagnostics_async(double* h) override {
+    diagnostics_launch();
+    LES_CUDA(cudaMemcpyAsync(h, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+
   void set_initial_conditions(const double* u, const double* v, const double* w) override {
     upload(LES_U, u, 1, g.nz);
     upload(LES_V, v, 1, g.nz);
@@ -330,20 +389,30 @@ class Solver final : public SolverBase {
   }
 
   void launch_bc(int4 lt, int4 ut) {
-    k_set_bc<T><<<grid_for(g.plane()), 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], PL[LES_LBC_U], PL[LES_LBC_V],
+    KL("k_set_bc", 8.0 * g.plane() * sizeof(T), k_set_bc<T><<<grid_for(g.plane()), 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], PL[LES_LBC_U], PL[LES_LBC_V],
                                                     PL[LES_LBC_W], PL[LES_UBC_U], PL[LES_UBC_V], PL[LES_UBC_W],
-                                                    lt, ut, g.plane(), g.nz, T(P.lz / double(g.nz)));
-    LES_CHECK_LAUNCH();
+                                                    lt, ut, g.plane(), g.nz, T(P.lz / double(g.nz))));
   }
   void set_bc() override {
+    Tag tag_(this, "bc");
     launch_bc(make_int4(lbc_t[0], lbc_t[1], lbc_t[2], 0), make_int4(ubc_t[0], ubc_t[1], ubc_t[2], 0));
   }
 
   double dz() const { return P.lz / double(g.nz); }
+  bool mixed() const { return P.precision == LES_MIXED; }
+  // Mixed precision: transform each field minus its value at (0,0) of the
+  // level; refout[q] receives the value the inverse transform adds back.
+  void use_refs(XFArgs<T>& a, int nf) {
+    if (!mixed()) return;
+    a.use_ref = 1;
+    a.ref_mul = 1.0 / a.c0;
+    for (int q = 0; q < nf; ++q) a.refout[q] = refbuf[q];
+  }
 
   // ------------------------------------------------ compute_derivatives ----
   // grad_velocity_filt for up to three fields at once
   void grad_fields(const int* f, const int* dx, const int* dy, int nfld) {
+    Tag tag_(this, "grad");
     const int L = g.L;
     auto a = xf(XF_SCALE, nfld, 0, L, g.nx, g.ny, g.lhx);
     a.c0 = 1.0 / double(g.nx * g.ny);
@@ -351,6 +420,7 @@ class Solver final : public SolverBase {
       a.in[q] = F[f[q]];
       a.out[q] = spec[q];
     }
+    use_refs(a, nfld);
     launch_xfwd<T>(g.nx, a, st);
     auto b = yp(YP_GRAD, 1, 3, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 0);
     for (int q = 0; q < nfld; ++q) {
@@ -373,17 +443,17 @@ class Solver final : public SolverBase {
       c.lo[q] = 0;
       c.hi[q] = g.nz + 1;
     }
+    if (mixed())
+      for (int q = 0; q < nfld; ++q) c.refin[3 * q] = refbuf[q];  // the filtered field itself
     launch_xinv<T>(g.nx, c, st);
   }
   void grad_velocity_filt(int f, int dfdx, int dfdy) override { grad_fields(&f, &dfdx, &dfdy, 1); }
 
   void ddz_uv(int dfdz, int f) override {
-    k_ddz<T><<<grid_for((long)(g.nz + 1) * g.plane()), 256, 0, st>>>(F[dfdz], F[f], g.plane(), g.nz, T(1.0 / dz()), 0);
-    LES_CHECK_LAUNCH();
+    KL("k_ddz", 2.0 * (g.nz + 1) * g.plane() * sizeof(T), k_ddz<T><<<grid_for((long)(g.nz + 1) * g.plane()), 256, 0, st>>>(F[dfdz], F[f], g.plane(), g.nz, T(1.0 / dz()), 0));
   }
   void ddz_w(int dfdz, int f) override {
-    k_ddz<T><<<grid_for((long)(g.nz + 1) * g.plane()), 256, 0, st>>>(F[dfdz], F[f], g.plane(), g.nz, T(1.0 / dz()), 1);
-    LES_CHECK_LAUNCH();
+    KL("k_ddz", 2.0 * (g.nz + 1) * g.plane() * sizeof(T), k_ddz<T><<<grid_for((long)(g.nz + 1) * g.plane()), 256, 0, st>>>(F[dfdz], F[f], g.plane(), g.nz, T(1.0 / dz()), 1));
   }
 
   void compute_vel_grad() override {
@@ -392,9 +462,9 @@ class Solver final : public SolverBase {
     const int dy[3] = {LES_DUDY, LES_DVDY, LES_DWDY};
     grad_fields(f, dx, dy, 3);
     set_bc();
-    k_ddz_vel<T><<<grid_for((long)(g.nz + 1) * g.plane()), 256, 0, st>>>(
-        F[LES_U], F[LES_V], F[LES_W], F[LES_DUDZ], F[LES_DVDZ], F[LES_DWDZ], g.plane(), g.nz, T(1.0 / dz()));
-    LES_CHECK_LAUNCH();
+    Tag tag_(this, "grad");
+    KL("k_ddz_vel", 6.0 * (g.nz + 1) * g.plane() * sizeof(T), k_ddz_vel<T><<<grid_for((long)(g.nz + 1) * g.plane()), 256, 0, st>>>(
+        F[LES_U], F[LES_V], F[LES_W], F[LES_DUDZ], F[LES_DVDZ], F[LES_DWDZ], g.plane(), g.nz, T(1.0 / dz())));
   }
 
   // stress divergence of up to three equations (compute_derivatives.f90:464-577)
@@ -403,6 +473,7 @@ class Solver final : public SolverBase {
     double pf;
   };
   void div_eqs(const DivEq* e, int neq, bool layers) {
+    Tag tag_(this, "divstress");
     // forward transforms of the distinct tx, ty fields
     int ids[6];
     int nid = 0;
@@ -423,6 +494,7 @@ class Solver final : public SolverBase {
       a.in[q] = F[ids[q]];
       a.out[q] = spec[q];
     }
+    use_refs(a, nid);  // derivatives of the per-level constants vanish
     launch_xfwd<T>(g.nx, a, st);
     auto b = yp(YP_DIV2, 2, 1, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 1);
     for (int q = 0; q < neq; ++q) {
@@ -454,6 +526,7 @@ class Solver final : public SolverBase {
 
   // -------------------------------------------- compute_convective_padd ----
   void dealias_convec(int cx, int cy, int cz) override {
+    Tag tag_(this, "convec");
     const int nz = g.nz;
     const bool padd = (P.dealias == LES_DEALIAS_PADD);
     const int nkin = padd ? g.nx / 2 : int(std::ceil(double(float(g.nx)) / 3.0)) - 1;
@@ -465,6 +538,7 @@ class Solver final : public SolverBase {
     const int ins[9] = {LES_U, LES_V, LES_W, LES_DWDY, LES_DVDZ, LES_DUDZ, LES_DWDX, LES_DVDX, LES_DUDY};
     for (int q = 0; q < 9; ++q) a.in[q] = F[ins[q]];
     for (int q = 0; q < 6; ++q) a.out[q] = spec[q];
+    use_refs(a, 6);
     launch_xfwd<T>(g.nx, a, st);
     // 2. y: pad to 3ny/2 (or 2/3-rule mask)
     if (padd) {
@@ -490,6 +564,7 @@ class Solver final : public SolverBase {
       c.out[q] = fine[q];
       c.lo[q] = 0;
       c.hi[q] = nz + 1;
+      if (mixed()) c.refin[q] = refbuf[q];
     }
     launch_xinv<T>(FNX, c, st);
     // 4. products on the fine grid, transformed back (levels 1..nz)
@@ -498,6 +573,11 @@ class Solver final : public SolverBase {
     d.c0 = padd ? 1.0 / double(g.nx2 * g.ny2) : 1.0 / double(g.nx * g.ny);
     for (int q = 0; q < 6; ++q) d.in[q] = fine[q];
     for (int q = 0; q < 3; ++q) d.out[q] = spec[q];
+    if (mixed()) {
+      d.use_ref = 1;
+      d.ref_mul = 1.0 / d.c0;
+      for (int q = 0; q < 3; ++q) d.refout[q] = refbuf[6 + q];
+    }
     launch_xfwd<T>(FNX, d, st);
     if (padd) {
       auto e = yp(YP_TRUNC, 1, 1, nkout, nkout, g.ny2, nkout, g.ny, 1);
@@ -523,6 +603,7 @@ class Solver final : public SolverBase {
       h.out[q] = F[outs[q]];
       h.lo[q] = 1;
       h.hi[q] = nz;
+      if (mixed()) h.refin[q] = refbuf[6 + q];
     }
     if (is_rhs) {
       h.out[3] = F[LES_RHSX_F];
@@ -550,83 +631,165 @@ class Solver final : public SolverBase {
   void scratch_vort_level(const int* outs, int k);
 
   // ---------------------------------------------------- compute_pressure ----
+  // The pressure path transforms in S = FP64 in both precisions: its RHS
+  // (div u*) is a small difference of large terms.
+  template <typename S>
+  XFArgs<S> xf_s(int op, int nf, int plane0, int nplanes, int nk) {
+    XFArgs<S> a;
+    std::memset(&a, 0, sizeof(a));
+    a.op = op;
+    a.nf = nf;
+    a.plane0 = plane0;
+    a.rows_pp = g.ny;
+    a.nrows = (long)nplanes * g.ny;
+    a.nk = nk;
+    a.nz = g.nz;
+    a.in_pstride = (long)g.ny * g.nx;
+    a.out_pstride = (long)g.ny * nk;
+    a.tw = twiddles64(g.nx);
+    return a;
+  }
+  template <typename S>
+  YPArgs<S> yp_s(int op, int nin, int nout, int plane0) {
+    YPArgs<S> a;
+    std::memset(&a, 0, sizeof(a));
+    a.op = op;
+    a.nin = nin;
+    a.nout = nout;
+    a.ncols = g.lhx;
+    a.nk_in = g.lhx;
+    a.nk_out = g.lhx;
+    a.in_pstride = (long)g.ny * g.lhx;
+    a.out_pstride = (long)g.ny * g.lhx;
+    a.plane0 = plane0;
+    a.nxh = g.nx / 2;
+    a.lhx = g.lhx;
+    a.kkx = kkx64;
+    a.kky = kky64;
+    a.tw_in = twiddles64(g.ny);
+    a.tw_out = twiddles64(g.ny);
+    return a;
+  }
+  template <typename S>
+  XIArgs<S> xi_s(int op, int nin, int plane0, int nplanes) {
+    XIArgs<S> a;
+    std::memset(&a, 0, sizeof(a));
+    a.op = op;
+    a.nin = nin;
+    a.plane0 = plane0;
+    a.rows_pp = g.ny;
+    a.nrows = (long)nplanes * g.ny;
+    a.nk = g.lhx;
+    a.nz = g.nz;
+    a.in_pstride = (long)g.ny * g.lhx;
+    a.out_pstride = (long)g.ny * g.nx;
+    a.tw = twiddles64(g.nx);
+    return a;
+  }
+  template <typename S>
+  static void set_in(XFArgs<S>& a, int q, T* f) {
+    if constexpr (std::is_same<T, float>::value && std::is_same<S, double>::value) {
+      a.inf[q] = f;
+      a.in_f32 = 1;
+    } else {
+      a.in[q] = reinterpret_cast<const S*>(f);
+    }
+  }
+  template <typename S>
+  static void set_out(XIArgs<S>& a, int q, T* f) {
+    if constexpr (std::is_same<T, float>::value && std::is_same<S, double>::value) {
+      a.outf[q] = f;
+      a.out_f32 = 1;
+    } else {
+      a.out[q] = reinterpret_cast<S*>(f);
+    }
+  }
+
   void press_stag_array(double tadv1) override {
+    Tag tag_(this, "press");
+    press_tadv1_ = tadv1;
+    if (mixed()) press_impl<double>(pspec);
+    else press_impl<double>(reinterpret_cast<cplx<double>**>(spec));
+  }
+
+  template <typename S>
+  void press_impl(cplx<S>** sp) {
+    const double tadv1 = press_tadv1_;
     const int nz = g.nz;
     const double c = 1.0 / double(g.nx * g.ny);
     // bottom/top layers (compute_pressure.f90:151-165, 196-203)
-    k_scale<T><<<grid_for(g.plane()), 256, 0, st>>>(PL[LES_BOTTOM_WK_PRESS], g.plane(), T(c));
-    LES_CHECK_LAUNCH();
-    cplx<T>* bot = spec[0] + (long)(g.L - 1) * g.ny * g.lhx;  // last plane of spec[0] is unused
-    cplx<T>* top = spec[1] + (long)(g.L - 1) * g.ny * g.lhx;
+    KL("k_scale", 2.0 * g.plane() * sizeof(T), k_scale<T><<<grid_for(g.plane()), 256, 0, st>>>(PL[LES_BOTTOM_WK_PRESS], g.plane(), T(c)));
+    cplx<S>* bot = sp[0];  // plane 0 of sp[0] / sp[1]
+    cplx<S>* top = sp[1];
     {
-      auto a = xf(XF_SCALE, 1, 0, 1, g.nx, g.ny, g.lhx);
+      auto a = xf_s<S>(XF_SCALE, 1, 0, 1, g.lhx);
       a.c0 = 1.0;
-      a.in[0] = PL[LES_BOTTOM_WK_PRESS];
+      set_in(a, 0, PL[LES_BOTTOM_WK_PRESS]);
       a.out[0] = bot;
-      launch_xfwd<T>(g.nx, a, st);
+      launch_xfwd<S>(g.nx, a, st);
       a.c0 = c;
-      a.in[0] = PL[LES_TOP_WK_PRESS];
+      set_in(a, 0, PL[LES_TOP_WK_PRESS]);
       a.out[0] = top;
-      launch_xfwd<T>(g.nx, a, st);
-      auto b = yp(YP_FWDKILL, 1, 1, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 0);
+      launch_xfwd<S>(g.nx, a, st);
+      auto b = yp_s<S>(YP_FWDKILL, 1, 1, 0);
       b.in[0] = bot;
       b.out[0] = bot;
       b.in[1] = top;
       b.out[1] = top;
-      launch_ypass<T>(g.ny, g.ny, b, 1, 2, st);
+      launch_ypass<S>(g.ny, g.ny, b, 1, 2, st);
     }
     // H = FFT(u / (dt tadv1 nx ny)), Nyquist killed (levels 1..nz)
-    auto a = xf(XF_PRESS, 3, 1, nz, g.nx, g.ny, g.lhx);
+    auto a = xf_s<S>(XF_PRESS, 3, 1, nz, g.lhx);
     a.c0 = c / tadv1;
     a.c1 = P.dt;
     const int uvw[3] = {LES_U, LES_V, LES_W};
     for (int q = 0; q < 3; ++q) {
-      a.in[q] = F[uvw[q]];
-      a.out[q] = spec[2 + q];
+      set_in(a, q, F[uvw[q]]);
+      a.out[q] = sp[2 + q];
     }
-    launch_xfwd<T>(g.nx, a, st);
-    auto b = yp(YP_FWDKILL, 1, 1, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 1);
+    launch_xfwd<S>(g.nx, a, st);
+    auto b = yp_s<S>(YP_FWDKILL, 1, 1, 1);
     for (int q = 0; q < 3; ++q) {
-      b.in[q] = spec[2 + q];
-      b.out[q] = spec[2 + q];
+      b.in[q] = sp[2 + q];
+      b.out[q] = sp[2 + q];
     }
-    launch_ypass<T>(g.ny, g.ny, b, nz, 3, st);
-    // tridiagonal solve per (kx, ky) -> p^ in spec[5], levels 0..nz+1
-    const bool mixed = (P.precision == LES_MIXED);
+    launch_ypass<S>(g.ny, g.ny, b, nz, 3, st);
+    // tridiagonal solve per (kx, ky) -> p^ in sp[5], levels 0..nz+1; in
+    // mixed precision the mean mode is kept apart in FP64 (pmean)
     dim3 tg(ceil_div(g.lhx, 64), g.ny);
-    k_tridiag<T><<<tg, 64, 0, st>>>(spec[2], spec[3], spec[4], bot, top, kkxd, kkyd, spec[5], xs, gam,
-                                   mixed ? pmean : nullptr, dstatus, g.lhx, g.ny, nz, dz(), mixed ? 1 : 0);
-    LES_CHECK_LAUNCH();
+    KL("k_tridiag", 112.0 * double(g.L) * g.ny * g.lhx, k_tridiag<S><<<tg, 64, 0, st>>>(sp[2], sp[3], sp[4], bot, top, kkxd, kkyd, sp[5], xs, gam,
+                                   mixed() ? pmean : nullptr, dstatus, g.lhx, g.ny, nz, dz(), mixed() ? 1 : 0));
     // compute_press_grad: i kx p^, i ky p^, p^ -> dpdx, dpdy (1..nz), p (0..nz+1)
-    auto e = yp(YP_PGRAD, 1, 3, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 0);
-    e.in[0] = spec[5];
-    e.out[0] = spec[6];
-    e.out[1] = spec[7];
-    e.out[2] = spec[5];
-    launch_ypass<T>(g.ny, g.ny, e, g.L, 1, st);
-    auto h = xi(XI_STORE, 3, 0, g.L, g.nx, g.ny, g.lhx);
-    h.in[0] = spec[6];
-    h.in[1] = spec[7];
-    h.in[2] = spec[5];
-    h.out[0] = F[LES_DPDX];
-    h.out[1] = F[LES_DPDY];
-    h.out[2] = F[LES_P];
+    auto e = yp_s<S>(YP_PGRAD, 1, 3, 0);
+    e.in[0] = sp[5];
+    e.out[0] = sp[6];
+    e.out[1] = sp[7];
+    e.out[2] = sp[5];
+    launch_ypass<S>(g.ny, g.ny, e, g.L, 1, st);
+    auto h = xi_s<S>(XI_STORE, 3, 0, g.L);
+    h.in[0] = sp[6];
+    h.in[1] = sp[7];
+    h.in[2] = sp[5];
+    set_out(h, 0, F[LES_DPDX]);
+    set_out(h, 1, F[LES_DPDY]);
+    set_out(h, 2, F[LES_P]);
     h.lo[0] = 1;
     h.hi[0] = nz;
     h.lo[1] = 1;
     h.hi[1] = nz;
     h.lo[2] = 0;
     h.hi[2] = nz + 1;
-    launch_xinv<T>(g.nx, h, st);
+    launch_xinv<S>(g.nx, h, st);
     // dpdz (compute_pressure.f90:359-369), then p(nz+1) = BOGUS (:353-357)
     dpdz_only();
-    k_p_finish<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_P], mixed ? pmean : nullptr, g.plane(), nz);
-    LES_CHECK_LAUNCH();
+    KL("k_p_finish", (mixed() ? 2.0 * g.field() : double(g.plane())) * sizeof(T), k_p_finish<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_P], mixed() ? pmean : nullptr, g.plane(), nz));
   }
+  double press_tadv1_ = 1.0;
   void dpdz_only();
 
   // ---------------------------------------------------- compute_wall_law ----
   void wall_layer() {
+    Tag tag_(this, "wall");
     if (P.wall_model == LES_WALL_FILTER) {
       // get_layer_filter (utility_tools.f90:261-307) + test_filter_layer
       cplx<T>* s0 = spec[0];
@@ -637,6 +800,7 @@ class Solver final : public SolverBase {
       a.in[1] = lev(F[LES_V], 1);
       a.out[0] = s0;
       a.out[1] = s1;
+      use_refs(a, 2);
       launch_xfwd<T>(g.nx, a, st);
       auto b = yp(YP_FILTER1, 1, 1, nk2, nk2, g.ny, nk2, g.ny, 0);
       b.G0 = gt;
@@ -648,6 +812,10 @@ class Solver final : public SolverBase {
       auto c = xi(XI_WALL, 2, 0, 1, g.nx, g.ny, nk2);
       c.in[0] = s0;
       c.in[1] = s1;
+      if (mixed()) {
+        c.refin[0] = refbuf[0];
+        c.refin[1] = refbuf[1];
+      }
       c.c0 = dz();
       c.out_pstride = g.plane();
       c.aux[0] = PL[LES_LBC_Z0];
@@ -691,6 +859,7 @@ class Solver final : public SolverBase {
   }
 
   void sgs_stress(int jt, int jtt) override {
+    Tag tag_(this, "sgs");
     const long n1 = (long)(g.nz + 1) * g.plane();
     auto a = sgs_args();
     if (P.sgs_model == LES_SGS_CST_SMAG) {
@@ -702,15 +871,13 @@ class Solver final : public SolverBase {
     } else {
       throw CudaError(1, "Invalid SGS model");
     }
-    k_sgs_tau<T><<<grid_for(n1), 256, 0, st>>>(a);
-    LES_CHECK_LAUNCH();
+    KL("k_sgs_tau", 17.0 * (g.nz + 1) * g.plane() * sizeof(T), k_sgs_tau<T><<<grid_for(n1), 256, 0, st>>>(a));
   }
 
   // dynamic-procedure contractions at both test scales (compute_dynamic_mum x2)
   void dynamic_mum(SgsArgs<T>& a, bool both) {
     const long n1 = (long)(g.nz + 1) * g.plane();
-    k_sij<T><<<grid_for(n1), 256, 0, st>>>(a);
-    LES_CHECK_LAUNCH();
+    KL("k_sij", 16.0 * (g.nz + 1) * g.plane() * sizeof(T), k_sij<T><<<grid_for(n1), 256, 0, st>>>(a));
     auto x = xf(XF_LASD, 21, 1, g.nz + 1, g.nx, g.ny, nk2);
     x.in[0] = F[LES_U];
     x.in[1] = F[LES_V];
@@ -718,6 +885,7 @@ class Solver final : public SolverBase {
     for (int q = 0; q < 6; ++q) x.in[3 + q] = sc[1 + q];
     x.in[9] = sc[0];
     for (int q = 0; q < 21; ++q) x.out[q] = spec[q];
+    x.fluct = mixed() ? 1 : 0;
     launch_xfwd<T>(g.nx, x, st);
     auto y = yp(both ? YP_FILTER2 : YP_FILTER1, 1, both ? 2 : 1, nk2, nk2, g.ny, nk2, g.ny, 1);
     y.G0 = gt;
@@ -745,11 +913,11 @@ class Solver final : public SolverBase {
   }
 
   void lasd(SgsArgs<T>& a, int jtt) {
+    Tag tag_(this, "lasd");
     const int nz = g.nz;
     if (jtt >= P.dyn_init) {
-      k_lag_accum<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_U_LAG], F[LES_V_LAG], F[LES_W_LAG], F[LES_U],
-                                                         F[LES_V], F[LES_W], g.field());
-      LES_CHECK_LAUNCH();
+      KL("k_lag_accum", 9.0 * g.field() * sizeof(T), k_lag_accum<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_U_LAG], F[LES_V_LAG], F[LES_W_LAG], F[LES_U],
+                                                         F[LES_V], F[LES_W], g.field()));
     }
     if (jtt < P.dyn_init) {
       fill(F[LES_CS_OPT2], 1, nz + 1, T(0.03));
@@ -761,20 +929,18 @@ class Solver final : public SolverBase {
     if (f_coeff_init) {
       LagGeom geo{g.nx, g.ny, nz, g.plane(), P.lag_halo, P.dt, P.lx / double(g.nx), P.ly / double(g.ny), dz(),
                   double(P.cs_count)};
-      k_lag_interp<T><<<grid_for(n1), 256, 0, st>>>(F[LES_U_LAG], F[LES_V_LAG], F[LES_W_LAG], F[LES_F_LM],
+      KL("k_lag_interp", 11.0 * (g.nz + 1) * g.plane() * sizeof(T), k_lag_interp<T><<<grid_for(n1), 256, 0, st>>>(F[LES_U_LAG], F[LES_V_LAG], F[LES_W_LAG], F[LES_F_LM],
                                                    F[LES_F_MM], F[LES_F_QN], F[LES_F_NN], sc[11], sc[12], sc[13],
-                                                   sc[14], geo);
-      LES_CHECK_LAUNCH();
+                                                   sc[14], geo));
       std::swap(F[LES_F_LM], sc[11]);
       std::swap(F[LES_F_MM], sc[12]);
       std::swap(F[LES_F_QN], sc[13]);
       std::swap(F[LES_F_NN], sc[14]);
     }
-    k_lasd_update<T><<<grid_for(n1), 256, 0, st>>>(F[LES_F_LM], F[LES_F_MM], F[LES_F_QN], F[LES_F_NN], sc[7],
+    KL("k_lasd_update", 14.0 * (g.nz + 1) * g.plane() * sizeof(T), k_lasd_update<T><<<grid_for(n1), 256, 0, st>>>(F[LES_F_LM], F[LES_F_MM], F[LES_F_QN], F[LES_F_NN], sc[7],
                                                   sc[8], sc[9], sc[10], F[LES_CS_OPT2], F[LES_BETA],
                                                   f_coeff_init ? 0 : 1, g.plane(), nz, 1.5 * delta,
-                                                  P.dt * double(P.cs_count), beta_pow);
-    LES_CHECK_LAUNCH();
+                                                  P.dt * double(P.cs_count), beta_pow));
     f_coeff_init = true;
     lagran_init = true;
     for (int q : {LES_U_LAG, LES_V_LAG, LES_W_LAG}) fill(F[q], 0, nz + 1, T(0));
@@ -783,11 +949,13 @@ class Solver final : public SolverBase {
   void dynsmag(SgsArgs<T>& a, int jt, int jtt);
 
   void test_filter(int f, int which) override {
+    Tag tag_(this, "testfilter");
     const int nk = which == 4 ? nk4 : nk2;
     auto a = xf(XF_SCALE, 1, 1, g.nz + 1, g.nx, g.ny, nk);
     a.c0 = 1.0;
     a.in[0] = F[f];
     a.out[0] = spec[0];
+    use_refs(a, 1);
     launch_xfwd<T>(g.nx, a, st);
     auto b = yp(YP_FILTER1, 1, 1, nk, nk, g.ny, nk, g.ny, 1);
     b.G0 = which == 4 ? gtt : gt;
@@ -799,6 +967,7 @@ class Solver final : public SolverBase {
     c.out[0] = F[f];
     c.lo[0] = 1;
     c.hi[0] = g.nz + 1;
+    if (mixed()) c.refin[0] = refbuf[0];
     launch_xinv<T>(g.nx, c, st);
   }
 
@@ -813,18 +982,18 @@ class Solver final : public SolverBase {
   }
 
   void ab2(double tadv1, double tadv2) override {
-    k_ab2<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], F[LES_RHSX], F[LES_RHSY],
+    Tag tag_(this, "ab2");
+    KL("k_ab2", 12.0 * g.nz * g.plane() * sizeof(T), k_ab2<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], F[LES_RHSX], F[LES_RHSY],
                                                  F[LES_RHSZ], F[LES_RHSX_F], F[LES_RHSY_F], F[LES_RHSZ_F],
-                                                 g.plane(), g.nz, T(P.dt), T(tadv1), T(tadv2));
-    LES_CHECK_LAUNCH();
+                                                 g.plane(), g.nz, T(P.dt), T(tadv1), T(tadv2)));
   }
 
   void projection(double tadv1) override {
+    Tag tag_(this, "projection");
     // dpdz was formed by press_stag_array; this applies LES_engine.f90:303-331
-    k_projection<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], F[LES_RHSX], F[LES_RHSY],
+    KL("k_projection", 15.0 * g.nz * g.plane() * sizeof(T), k_projection<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], F[LES_RHSX], F[LES_RHSY],
                                                         F[LES_RHSZ], F[LES_DPDX], F[LES_DPDY], F[LES_DPDZ],
-                                                        g.plane(), g.nz, T(P.dt * tadv1));
-    LES_CHECK_LAUNCH();
+                                                        g.plane(), g.nz, T(P.dt * tadv1)));
   }
 
   void step(int jt, int jtt) override {
@@ -856,13 +1025,12 @@ class Solver final : public SolverBase {
   bool timed = false;
 
   void diagnostics_launch() {
-    k_diag_partial<T><<<DIAG_BLOCKS, 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], F[LES_DUDX], F[LES_DVDY],
-                                                  F[LES_DWDZ], g.plane(), g.nz, part);
-    LES_CHECK_LAUNCH();
-    k_diag_final<T><<<1, 256, 0, st>>>(part, DIAG_BLOCKS, PL[LES_U_STAR_AVG], g.plane(), P.dt,
+    Tag tag_(this, "diag");
+    KL("k_diag_partial", 6.0 * g.nz * g.plane() * sizeof(T), k_diag_partial<T><<<DIAG_BLOCKS, 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], F[LES_DUDX], F[LES_DVDY],
+                                                  F[LES_DWDZ], g.plane(), g.nz, part));
+    KL("k_diag_final", double(g.plane()) * sizeof(T), k_diag_final<T><<<1, 256, 0, st>>>(part, DIAG_BLOCKS, PL[LES_U_STAR_AVG], g.plane(), P.dt,
                                       P.lx / double(g.nx), P.ly / double(g.ny), dz(),
-                                      double(g.nx) * double(g.ny) * double(g.nz), dout, dstatus);
-    LES_CHECK_LAUNCH();
+                                      double(g.nx) * double(g.ny) * double(g.nz), dout, dstatus));
   }
   void diagnostics(double out[4]) override {
     diagnostics_launch();
@@ -909,9 +1077,8 @@ __global__ void k_dpdz(T* dpdz, const T* p, long plane, int nz, T rdz, const dou
 template <typename T>
 void Solver<T>::dpdz_only() {
   const bool mixed = (P.precision == LES_MIXED);
-  k_dpdz<T><<<grid_for((long)g.nz * g.plane()), 256, 0, st>>>(F[LES_DPDZ], F[LES_P], g.plane(), g.nz,
-                                                             T(1.0 / dz()), mixed ? pmean : nullptr);
-  LES_CHECK_LAUNCH();
+  KL("k_dpdz", 2.0 * g.nz * g.plane() * sizeof(T), k_dpdz<T><<<grid_for((long)g.nz * g.plane()), 256, 0, st>>>(F[LES_DPDZ], F[LES_P], g.plane(), g.nz,
+                                                             T(1.0 / dz()), mixed ? pmean : nullptr));
 }
 
 template <typename T>
@@ -932,10 +1099,9 @@ __global__ void k_vort_level(T* cx, T* cy, T* cz, const T* dwdy, const T* dvdz, 
 
 template <typename T>
 void Solver<T>::scratch_vort_level(const int* outs, int k) {
-  k_vort_level<T><<<grid_for(g.plane()), 256, 0, st>>>(
+  KL("k_vort_level", 9.0 * g.plane() * sizeof(T), k_vort_level<T><<<grid_for(g.plane()), 256, 0, st>>>(
       F[outs[0]], F[outs[1]], F[outs[2]], F[LES_DWDY], F[LES_DVDZ], F[LES_DUDZ], F[LES_DWDX], F[LES_DVDX],
-      F[LES_DUDY], g.plane(), k, T(1.0 / double(g.nx * g.ny)), P.wall_law);
-  LES_CHECK_LAUNCH();
+      F[LES_DUDY], g.plane(), k, T(1.0 / double(g.nx * g.ny)), P.wall_law));
 }
 
 // wall_inst / wall_homog (compute_wall_law.f90:119-138, 210-228)
@@ -979,11 +1145,10 @@ void Solver<T>::wall_plain() {
     for (double x : h) s += x;
     vm = (1.0 / double(g.nx * g.ny)) * s;
   }
-  k_wall_plain<T><<<grid_for(g.plane()), 256, 0, st>>>(lev(F[LES_U], 1), lev(F[LES_V], 1), um, vm, homog,
+  KL("k_wall_plain", 10.0 * g.plane() * sizeof(T), k_wall_plain<T><<<grid_for(g.plane()), 256, 0, st>>>(lev(F[LES_U], 1), lev(F[LES_V], 1), um, vm, homog,
                                                        PL[LES_LBC_Z0], PL[LES_U_STAR_AVG], PL[LES_LBC_U],
                                                        PL[LES_LBC_V], lev(F[LES_TXZ], 1), lev(F[LES_TYZ], 1),
-                                                       lev(F[LES_DUDZ], 1), lev(F[LES_DVDZ], 1), g.plane(), dz());
-  LES_CHECK_LAUNCH();
+                                                       lev(F[LES_DUDZ], 1), lev(F[LES_DVDZ], 1), g.plane(), dz()));
 }
 
 // plane-averaged dynamic Smagorinsky (compute_DynSmag.f90:61-245)
@@ -1027,8 +1192,34 @@ void Solver<T>::dynsmag(SgsArgs<T>& a, int jt, int jtt) {
   }
   if (jt % P.cs_count != 0) return;
   dynamic_mum(a, false);
-  k_plane_ratio<T><<<g.nz + 1, 256, 0, st>>>(sc[7], sc[8], F[LES_CS_OPT2], g.plane(), g.nz);
-  LES_CHECK_LAUNCH();
+  KL("k_plane_ratio", 3.0 * (g.nz + 1) * g.plane() * sizeof(T), k_plane_ratio<T><<<g.nz + 1, 256, 0, st>>>(sc[7], sc[8], F[LES_CS_OPT2], g.plane(), g.nz));
+}
+
+std::string SolverBase::profile_report() {
+  LES_CUDA(cudaStreamSynchronize(st));
+  struct Acc {
+    long n = 0;
+    double ms = 0, bytes = 0;
+  };
+  std::map<std::string, Acc> acc;
+  for (const auto& r : recs) {
+    float ms = 0;
+    LES_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+    auto& x = acc[r.label];
+    x.n += 1;
+    x.ms += ms;
+    x.bytes += r.bytes;
+  }
+  std::string out = "{";
+  bool first = true;
+  char buf[512];
+  for (const auto& kv : acc) {
+    std::snprintf(buf, sizeof(buf), "%s\"%s\": {\"launches\": %ld, \"ms\": %.6f, \"bytes_per_launch\": %.1f}",
+                  first ? "" : ", ", kv.first.c_str(), kv.second.n, kv.second.ms, kv.second.bytes / kv.second.n);
+    out += buf;
+    first = false;
+  }
+  return out + "}";
 }
 
 SolverBase* make_solver(const les_params& p) {

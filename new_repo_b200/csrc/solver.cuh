@@ -1,10 +1,13 @@
 // Device-resident LES state and the operators of one time step.
 #pragma once
 #include <map>
+#include <cstdio>
 #include <vector>
 #include "../../include/lesgpu.h"
 #include "common.cuh"
 #include "spectral.cuh"
+#include "launch.cuh"
+#include <string>
 
 namespace les {
 
@@ -14,17 +17,73 @@ struct Grid {
   long field() const { return plane() * L; }
 };
 
-// Per-precision interface so the C ABI can hold either instantiation.
-struct SolverBase {
+// Per-precision interface so the C ABI can hold either instantiation.  It
+// observes every kernel launch (LaunchHook): a launch counter, and with
+// profiling on, CUDA events on the state's stream around each launch,
+// labelled "<operator>/<kernel>" with the launch's algorithmic bytes.
+struct SolverBase : LaunchHook {
   les_params P{};
   Grid g{};
   cudaStream_t st = nullptr;
+  long launches = 0;
+  std::string tag = "op";
+  bool prof_on = false;
+  struct Rec {
+    std::string label;
+    double bytes;
+    cudaEvent_t a, b;
+  };
+  std::vector<cudaEvent_t> pool;
+  size_t pool_next = 0;
+  std::vector<Rec> recs;
+  Rec pending;
+  cudaEvent_t next_event() {
+    if (pool_next >= pool.size()) {
+      cudaEvent_t e;
+      LES_CUDA(cudaEventCreate(&e));
+      pool.push_back(e);
+    }
+    return pool[pool_next++];
+  }
+  void before(const char* kind, double bytes) override {
+    ++launches;
+    if (!prof_on) return;
+    pending.label = tag + "/" + kind;
+    pending.bytes = bytes;
+    pending.a = next_event();
+    LES_CUDA(cudaEventRecord(pending.a, st));
+  }
+  void after() override {
+    if (!prof_on) return;
+    pending.b = next_event();
+    LES_CUDA(cudaEventRecord(pending.b, st));
+    recs.push_back(pending);
+  }
+  void profile(bool on) {
+    prof_on = on;
+    recs.clear();
+    pool_next = 0;
+  }
+  // per label: launches, total ms, bytes per launch (JSON object)
+  std::string profile_report();
+  // RAII operator tag
+  struct Tag {
+    SolverBase* s;
+    std::string old;
+    Tag(SolverBase* s_, const char* t) : s(s_), old(s_->tag) { s->tag = t; }
+    ~Tag() { s->tag = old; }
+  };
   bool f_coeff_init = false;
   bool lagran_init = false;
   int lbc_t[3] = {1, 1, 1};  // 'drc' until the wall law switches u,v to 'neu'
   int ubc_t[3] = {2, 2, 1};
   float timers_ms[5] = {0, 0, 0, 0, 0};
-  virtual ~SolverBase() = default;
+  ~SolverBase() override {
+    if (g_hook == this) g_hook = nullptr;
+    for (auto e : pool) cudaEventDestroy(e);
+    for (auto e : slots)
+      if (e) cudaEventDestroy(e);
+  }
   virtual void upload(int field, const double* h, int k0, int k1) = 0;
   virtual void download(int field, double* h, int k0, int k1) = 0;
   virtual void upload_plane(int plane, const double* h) = 0;
@@ -49,6 +108,24 @@ struct SolverBase {
   virtual void diagnostics(double out[4]) = 0;
   virtual unsigned status() = 0;
   virtual void read_timers() = 0;
+  // pinned-host FP64 transfers on the state's stream (converted on device in
+  // mixed precision); the caller synchronises
+  virtual void upload_async(int field, const double* pinned, int k0, int k1) = 0;
+  virtual void download_async(int field, double* pinned, int k0, int k1) = 0;
+  virtual void diagnostics_async(double* pinned4) = 0;
+  // timing events on the state's stream
+  cudaEvent_t slots[16] = {};
+  void record_event(int i) {
+    if (!slots[i]) LES_CUDA(cudaEventCreate(&slots[i]));
+    LES_CUDA(cudaEventRecord(slots[i], st));
+  }
+  double elapsed(int a, int b) {
+    if (a < 0 || b < 0 || a >= 16 || b >= 16 || !slots[a] || !slots[b]) throw CudaError(1, "event slot not recorded");
+    LES_CUDA(cudaEventSynchronize(slots[b]));
+    float ms = 0;
+    LES_CUDA(cudaEventElapsedTime(&ms, slots[a], slots[b]));
+    return ms;
+  }
 };
 
 SolverBase* make_solver(const les_params& p);

@@ -46,10 +46,16 @@ struct XFArgs {
   int nk;          // modes stored per output row
   int nz;
   int wall;        // wall-law special rows at k=1
+  int use_ref;     // subtract each field's value at (i,j)=(0,0) of the level
+  int fluct;       // XF_LASD: form products of u, v, w minus their (0,0) values
+  double ref_mul;  // refout = ref * ref_mul (the value the inverse adds back)
+  T* refout[MAXIN];
   long in_pstride; // elements per plane of the input grid
   long in_rstride; // elements per row of the input grid (== NX)
   double c0, c1;
   const T* in[12];
+  const float* inf[12];  // FP32 inputs of an FP64 transform (in_f32 = 1)
+  int in_f32;
   cplx<T>* out[MAXIN];
   long out_pstride;  // rows_pp * nk
   const cplx<T>* tw; // exp(-2 pi i m / NX), m < NX
@@ -62,11 +68,12 @@ __device__ __forceinline__ void xf_load_point(const XFArgs<T>& a, int l, int j, 
   const long off = (long)l * a.in_pstride + (long)j * a.in_rstride + i;
   switch (a.op) {
     case XF_SCALE: {
-      for (int f = 0; f < a.nf; ++f) v[f * vs] = T(a.c0) * a.in[f][off];
+      for (int f = 0; f < a.nf; ++f) v[f * vs] = T(a.c0) * (a.in_f32 ? T(a.inf[f][off]) : a.in[f][off]);
       break;
     }
     case XF_PRESS: {
-      for (int f = 0; f < a.nf; ++f) v[f * vs] = T(a.c0) * (a.in[f][off] / T(a.c1));
+      for (int f = 0; f < a.nf; ++f)
+        v[f * vs] = T(a.c0) * ((a.in_f32 ? T(a.inf[f][off]) : a.in[f][off]) / T(a.c1));
       break;
     }
     case XF_CONV_IN: {
@@ -134,6 +141,20 @@ __device__ __forceinline__ void xf_load_point(const XFArgs<T>& a, int l, int j, 
         vf = T(0.5) * (vv[off] + vv[dn]);
         wf = w[off];
       }
+      if (a.fluct) {
+        // L_ij = filt(u_i u_j) - filt(u_i) filt(u_j) is unchanged when a
+        // per-level constant is removed from u_i; FP32 keeps the fluctuation.
+        const long o0 = (long)l * a.in_pstride;
+        if (l == 1) {
+          uf -= u[o0];
+          vf -= vv[o0];
+          wf -= T(0.25) * w[o0 + a.in_pstride];
+        } else {
+          uf -= T(0.5) * (u[o0] + u[o0 - a.in_pstride]);
+          vf -= T(0.5) * (vv[o0] + vv[o0 - a.in_pstride]);
+          wf -= w[o0];
+        }
+      }
       v[0 * vs] = uf;
       v[1 * vs] = vf;
       v[2 * vs] = wf;
@@ -165,6 +186,21 @@ __global__ void __launch_bounds__(256) k_xfwd(const XFArgs<T> a) {
   cplx<T>* b1 = b0 + nseq * M;
   for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
   const long g0 = (long)blockIdx.x * a.R;
+  T* refs = reinterpret_cast<T*>(b1 + nseq * M);  // R * nf per-row references
+  if (a.use_ref) {
+    for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
+      const long g = g0 + r;
+      if (g >= a.nrows) continue;
+      const int l = a.plane0 + int(g / a.rows_pp);
+      const int j = int(g % a.rows_pp);
+      xf_load_point(a, l, 0, 0, refs + r * a.nf, 1);
+      for (int f = 0; f < a.nf; ++f) {
+        if (!a.refout[f]) refs[r * a.nf + f] = T(0);
+        else if (j == 0) a.refout[f][l] = T(double(refs[r * a.nf + f]) * a.ref_mul);
+      }
+    }
+    __syncthreads();
+  }
   // load: one thread per point; sequence s = r*nf + f holds the packed row
   // z_m = x_{2m} + i x_{2m+1}, i.e. the real row itself viewed as complex.
   T* xr = reinterpret_cast<T*>(b0);
@@ -177,6 +213,8 @@ __global__ void __launch_bounds__(256) k_xfwd(const XFArgs<T> a) {
       const int l = a.plane0 + int(g / a.rows_pp);
       const int j = int(g % a.rows_pp);
       xf_load_point(a, l, j, i, dst, NX);
+      if (a.use_ref)
+        for (int f = 0; f < a.nf; ++f) dst[f * NX] -= refs[r * a.nf + f];
     } else {
       for (int f = 0; f < a.nf; ++f) dst[f * NX] = T(0);
     }
@@ -376,7 +414,10 @@ struct XIArgs {
   double pf[4];
   int lo[MAXIN], hi[MAXIN];
   const cplx<T>* in[MAXIN];
+  const T* refin[MAXIN];  // per-level values added back to input field f
   T* out[16];
+  float* outf[16];  // FP32 outputs of an FP64 transform (out_f32 = 1, XI_STORE)
+  int out_f32;
   const T* aux[8];
   const cplx<T>* tw;  // exp(-2 pi i m / NX), m < NX
 };
@@ -429,11 +470,17 @@ __global__ void __launch_bounds__(256) k_xinv(const XIArgs<T> a) {
     const int l = a.plane0 + int(g / a.rows_pp);
     const int j = int(g % a.rows_pp);
     const long off = (long)l * a.out_pstride + (long)j * NX + i;
-    const T* x = xs + (long)(r * a.nin) * NX + i;  // field f at x[f*NX]
+    T* xw = const_cast<T*>(xs) + (long)(r * a.nin) * NX + i;
+    for (int f = 0; f < a.nin; ++f)  // this thread alone touches (r, i)
+      if (a.refin[f]) xw[f * NX] += a.refin[f][l];
+    const T* x = xw;  // field f at x[f*NX]
     switch (a.op) {
       case XI_STORE: {
         for (int f = 0; f < a.nin; ++f)
-          if (l >= a.lo[f] && l <= a.hi[f]) a.out[f][off] = x[f * NX];
+          if (l >= a.lo[f] && l <= a.hi[f]) {
+            if (a.out_f32) a.outf[f][off] = float(x[f * NX]);
+            else a.out[f][off] = x[f * NX];
+          }
         break;
       }
       case XI_CONV: {

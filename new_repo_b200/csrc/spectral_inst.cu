@@ -5,6 +5,8 @@
 
 namespace les {
 
+thread_local LaunchHook* g_hook = nullptr;
+
 namespace {
 constexpr int SMEM_CAP = 200 * 1024;
 
@@ -36,10 +38,14 @@ void launch_xfwd(int NX, XFArgs<T> a, cudaStream_t st) {
   const int M = NX / 2;
   a.R = rows_per_cta<T>(a.nf, M);
   a.in_rstride = NX;
-  const size_t smem = sizeof(cplx<T>) * (NX + 2 * (size_t)a.R * a.nf * M);
+  const size_t smem = sizeof(cplx<T>) * (NX + 2 * (size_t)a.R * a.nf * M) + sizeof(T) * a.R * a.nf;
   if (smem > SMEM_CAP) throw CudaError(1, "xfwd: shared memory request too large");
   const int grid = ceil_div(a.nrows, a.R);
   if (grid == 0) return;
+  static const int nin_of_op[] = {0, 9, 6, 10, 0};
+  const int nin = (a.op == XF_SCALE || a.op == XF_PRESS) ? a.nf : nin_of_op[a.op];
+  const size_t isz = (a.in_f32 ? sizeof(float) : sizeof(T));
+  hook_before("xfwd", double(a.nrows) * NX * nin * isz + double(a.nrows) * a.nf * a.nk * sizeof(cplx<T>));
   switch (NX) {
 #define XF_CASE(N) \
   case N: k_xfwd<T, N><<<grid, 256, smem, st>>>(a); break;
@@ -49,6 +55,7 @@ void launch_xfwd(int NX, XFArgs<T> a, cudaStream_t st) {
       throw CudaError(1, "xfwd: unsupported transform length " + std::to_string(NX));
   }
   LES_CHECK_LAUNCH();
+  hook_after();
 }
 
 template <typename T>
@@ -59,6 +66,15 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
   if (smem > SMEM_CAP) throw CudaError(1, "xinv: shared memory request too large");
   const int grid = ceil_div(a.nrows, a.R);
   if (grid == 0) return;
+  {
+    const size_t osz = (a.out_f32 ? sizeof(float) : sizeof(T));
+    int nout = a.nin, rmw = 0;
+    if (a.op == XI_CONV) { nout = 6; rmw = 3; }
+    else if (a.op == XI_DIV) { nout = a.nin; rmw = 2 * a.nin; }
+    else if (a.op == XI_LASD) nout = 2;
+    else if (a.op == XI_WALL) nout = 7;
+    hook_before("xinv", double(a.nrows) * a.nin * a.nk * sizeof(cplx<T>) + double(a.nrows) * NX * (nout + rmw) * osz);
+  }
   switch (NX) {
 #define XI_CASE(N) \
   case N: k_xinv<T, N><<<grid, 256, smem, st>>>(a); break;
@@ -68,6 +84,7 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
       throw CudaError(1, "xinv: unsupported transform length " + std::to_string(NX));
   }
   LES_CHECK_LAUNCH();
+  hook_after();
 }
 
 template <typename T>
@@ -83,6 +100,8 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
   dim3 grid(ceil_div(a.ncols, a.C), nplanes, ngroups);
   if (grid.x == 0 || nplanes == 0 || ngroups == 0) return;
   const int key = NY * 10000 + NYO;
+  hook_before("ypass", double(nplanes) * ngroups * a.ncols * sizeof(cplx<T>) *
+                           (double(a.op == YP_PGRAD ? 1 : a.nin) * NY + double(a.nout) * NYO));
   switch (key) {
 #define YP_CASE(A, B) \
   case A * 10000 + B: k_ypass<T, A, B><<<grid, 256, smem, st>>>(a); break;
@@ -94,6 +113,7 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
       throw CudaError(1, "ypass: unsupported length pair " + std::to_string(NY) + "->" + std::to_string(NYO));
   }
   LES_CHECK_LAUNCH();
+  hook_after();
 }
 
 template <typename T>

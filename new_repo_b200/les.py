@@ -356,6 +356,42 @@ class LES:
         check(self.lib.les_timers(self._h, _dptr(out)))
         return dict(zip(("grad", "stress", "rhs", "press", "loop"), out.tolist()))
 
+    # ------------------------------------------------------------ measurement
+    def profile(self, enable: bool = True):
+        check(self.lib.les_profile(self._h, 1 if enable else 0))
+
+    def profile_report(self) -> dict:
+        import json
+
+        buf = C.create_string_buffer(1 << 20)
+        check(self.lib.les_profile_report(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
+    def launch_count(self) -> int:
+        v = C.c_longlong()
+        check(self.lib.les_launch_count(self._h, C.byref(v)))
+        return int(v.value)
+
+    def event_record(self, slot: int):
+        check(self.lib.les_event_record(self._h, int(slot)))
+
+    def event_elapsed(self, a: int, b: int) -> float:
+        v = C.c_double()
+        check(self.lib.les_event_elapsed(self._h, int(a), int(b), C.byref(v)))
+        return float(v.value)
+
+    def upload_async(self, name, pinned_ptr: int, k0: int = 0, k1: int | None = None):
+        """Copy levels k0..k1 of a field from page-locked host memory (address)."""
+        k1 = self.params.nz + 1 if k1 is None else k1
+        check(self.lib.les_upload_async(self._h, self._fid(name), C.c_void_p(pinned_ptr), k0, k1))
+
+    def download_async(self, name, pinned_ptr: int, k0: int = 0, k1: int | None = None):
+        k1 = self.params.nz + 1 if k1 is None else k1
+        check(self.lib.les_download_async(self._h, self._fid(name), C.c_void_p(pinned_ptr), k0, k1))
+
+    def diagnostics_async(self, pinned_ptr: int):
+        check(self.lib.les_diagnostics_async(self._h, C.c_void_p(pinned_ptr)))
+
     def state_dict(self, names=None) -> dict:
         names = capi.FIELDS if names is None else names
         d = {n: self.download(n) for n in names}

