@@ -210,6 +210,9 @@ def run_ours(args, dist, rank, local, ws):
     # step-level: algorithmic bytes per step (105 F + 28 F / cs_count, F = N * 4 B)
     F = npts * 4.0
     step_bytes = (105.0 + 28.0 / p.cs_count) * F
+    prof_top = sorted(({"kernel": k, "ms_per_step": round(v["ms"] / K, 4), "launches_per_step": v["launches"] / K,
+                        "gbs": round(v["bytes_per_launch"] * v["launches"] / (v["ms"] / 1e3) / 1e9, 1)}
+                       for k, v in prof.items()), key=lambda d: -d["ms_per_step"])[:12]
     step_roof = {"algorithmic_bytes_per_step": step_bytes,
                  "achieved_gbs": round(step_bytes / (ms / K / 1e3) / 1e9, 1),
                  "frac": round(step_bytes / (ms / K / 1e3) / 1e9 / pk["hbm_gbs"], 4)}
@@ -256,7 +259,7 @@ def run_ours(args, dist, rank, local, ws):
                        "grid": [p.nx, p.ny, p.nz], "dt": p.dt_nd, "sgs_model": p.sgs_model,
                        "precision": "mixed", "parallelism": f"replicas x{ws}",
                        "l2": "inputs larger than L2 (>= 9 GB of fields per step)"},
-            "roofline": roof, "step_roofline": step_roof,
+            "roofline": roof, "step_roofline": step_roof, "profile_top": prof_top,
             "e2e": e2e, "gpu_launches": n1 - n0, "fp64_gpu": fp64, "cpu_baseline": cpu,
             "clocks": clk.summary(), "status_bits": status,
         }

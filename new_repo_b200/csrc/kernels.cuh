@@ -471,16 +471,18 @@ struct Neu {
   __device__ __forceinline__ double val() const { return s + c; }
 };
 
-constexpr int DIAG_BLOCKS = 296;
-constexpr int DIAG_NV = 8;  // umax vmax wmax | usum vsum wsum divsum | nan
+constexpr int DIAG_BLOCKS = 1184;
+constexpr int DIAG_NV = 9;  // umax vmax wmax | usum vsum wsum divsum | nan | u* sum
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_diag_partial(const T* u, const T* v, const T* w, const T* dudx,
-                                                      const T* dvdy, const T* dwdz, long plane, int nz,
-                                                      double* part) {
+                                                      const T* dvdy, const T* dwdz, const T* ustar, long plane,
+                                                      int nz, double* part) {
   double mx[3] = {-1234567890.0, -1234567890.0, -1234567890.0};
-  Neu su, sv, sw, sd;
+  Neu su, sv, sw, sd, sus;
   int nan = 0;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < plane; q += (long)gridDim.x * blockDim.x)
+    sus.add(double(ustar[q]));
   const long n = (long)nz * plane;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const long o = plane + q;
@@ -495,8 +497,10 @@ __global__ void __launch_bounds__(256) k_diag_partial(const T* u, const T* v, co
     const double dv = double(dudx[o]) + double(dvdy[o]) + double(dwdz[o]);
     sd.add(dv * dv);
   }
-  __shared__ double sm[DIAG_NV + 4][256];
+  __shared__ double sm[DIAG_NV + 6][256];
   const int t = threadIdx.x;
+  sm[DIAG_NV + 4][t] = sus.s;
+  sm[DIAG_NV + 5][t] = sus.c;
   sm[0][t] = mx[0];
   sm[1][t] = mx[1];
   sm[2][t] = mx[2];
@@ -512,8 +516,10 @@ __global__ void __launch_bounds__(256) k_diag_partial(const T* u, const T* v, co
   __syncthreads();
   if (t == 0) {
     double m0 = sm[0][0], m1 = sm[1][0], m2 = sm[2][0], fl = 0;
-    Neu a[4];
+    Neu a[4], us;
     for (int i = 0; i < 256; ++i) {
+      us.add(sm[DIAG_NV + 4][i]);
+      us.add(sm[DIAG_NV + 5][i]);
       m0 = fmax(m0, sm[0][i]);
       m1 = fmax(m1, sm[1][i]);
       m2 = fmax(m2, sm[2][i]);
@@ -529,41 +535,56 @@ __global__ void __launch_bounds__(256) k_diag_partial(const T* u, const T* v, co
     out[2] = m2;
     for (int q = 0; q < 4; ++q) out[3 + q] = a[q].val();
     out[7] = fl;
+    out[8] = us.val();
   }
 }
 
-template <typename T>
-__global__ void k_diag_final(const double* part, int nblocks, const T* ustar, long plane, double dt, double dx,
-                             double dy, double dz, double npts, double* out, unsigned* status) {
-  __shared__ double sm[2][256];
-  Neu su;
-  for (long p = threadIdx.x; p < plane; p += blockDim.x) su.add(double(ustar[p]));
-  sm[0][threadIdx.x] = su.s;
-  sm[1][threadIdx.x] = su.c;
+__global__ void k_diag_final(const double* part, int nblocks, long plane, double dt, double dx, double dy,
+                             double dz, double npts, double* out, unsigned* status) {
+  // fixed-order combination of the block partials (deterministic)
+  __shared__ double sm[9][256];
+  __shared__ double cm[6][256];
+  const int t = threadIdx.x;
+  double m0 = -1e300, m1 = -1e300, m2 = -1e300, fl = 0;
+  Neu a[5];
+  for (int b = t; b < nblocks; b += blockDim.x) {
+    const double* q = part + (long)b * DIAG_NV;
+    m0 = fmax(m0, q[0]);
+    m1 = fmax(m1, q[1]);
+    m2 = fmax(m2, q[2]);
+    for (int i = 0; i < 4; ++i) a[i].add(q[3 + i]);
+    a[4].add(q[8]);
+    fl = fmax(fl, q[7]);
+  }
+  sm[0][t] = m0;
+  sm[1][t] = m1;
+  sm[2][t] = m2;
+  sm[3][t] = fl;
+  for (int i = 0; i < 5; ++i) {
+    sm[4 + i][t] = a[i].s;
+    if (i < 5) cm[i][t] = a[i].c;
+  }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    Neu us;
+  if (t == 0) {
+    double x0 = sm[0][0], x1 = sm[1][0], x2 = sm[2][0], f = 0;
+    Neu s[5];
     for (int i = 0; i < blockDim.x; ++i) {
-      us.add(sm[0][i]);
-      us.add(sm[1][i]);
+      x0 = fmax(x0, sm[0][i]);
+      x1 = fmax(x1, sm[1][i]);
+      x2 = fmax(x2, sm[2][i]);
+      f = fmax(f, sm[3][i]);
+      for (int q = 0; q < 5; ++q) {
+        s[q].add(sm[4 + q][i]);
+        s[q].add(cm[q][i]);
+      }
     }
-    double m0 = part[0], m1 = part[1], m2 = part[2], fl = 0;
-    Neu a[4];
-    for (int b = 0; b < nblocks; ++b) {
-      const double* q = part + (long)b * DIAG_NV;
-      m0 = fmax(m0, q[0]);
-      m1 = fmax(m1, q[1]);
-      m2 = fmax(m2, q[2]);
-      for (int t = 0; t < 4; ++t) a[t].add(q[3 + t]);
-      fl = fmax(fl, q[7]);
-    }
-    const double cfl = dt * (m0 / dx + m1 / dy + m2 / dz);
-    const double um = a[0].val() / npts, vm = a[1].val() / npts, wm = a[2].val() / npts;
+    const double cfl = dt * (x0 / dx + x1 / dy + x2 / dz);
+    const double um = s[0].val() / npts, vm = s[1].val() / npts, wm = s[2].val() / npts;
     out[0] = cfl;
     out[1] = 0.5 * (um * um + vm * vm + wm * wm);
-    out[2] = us.val() / double(plane);
-    out[3] = sqrt(a[3].val() / npts);
-    if (fl != 0.0) atomicOr(status, ST_NAN);
+    out[2] = s[4].val() / double(plane);
+    out[3] = sqrt(s[3].val() / npts);
+    if (f != 0.0) atomicOr(status, ST_NAN);
   }
 }
 

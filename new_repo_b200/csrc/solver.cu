@@ -1026,11 +1026,12 @@ class Solver final : public SolverBase {
 
   void diagnostics_launch() {
     Tag tag_(this, "diag");
-    KL("k_diag_partial", 6.0 * g.nz * g.plane() * sizeof(T), k_diag_partial<T><<<DIAG_BLOCKS, 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], F[LES_DUDX], F[LES_DVDY],
-                                                  F[LES_DWDZ], g.plane(), g.nz, part));
-    KL("k_diag_final", double(g.plane()) * sizeof(T), k_diag_final<T><<<1, 256, 0, st>>>(part, DIAG_BLOCKS, PL[LES_U_STAR_AVG], g.plane(), P.dt,
-                                      P.lx / double(g.nx), P.ly / double(g.ny), dz(),
-                                      double(g.nx) * double(g.ny) * double(g.nz), dout, dstatus));
+    KL("k_diag_partial", 6.0 * g.nz * g.plane() * sizeof(T),
+       k_diag_partial<T><<<DIAG_BLOCKS, 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], F[LES_DUDX], F[LES_DVDY],
+                                                     F[LES_DWDZ], PL[LES_U_STAR_AVG], g.plane(), g.nz, part));
+    KL("k_diag_final", double(DIAG_BLOCKS) * DIAG_NV * 8.0,
+       k_diag_final<<<1, 256, 0, st>>>(part, DIAG_BLOCKS, g.plane(), P.dt, P.lx / double(g.nx), P.ly / double(g.ny),
+                                      dz(), double(g.nx) * double(g.ny) * double(g.nz), dout, dstatus));
   }
   void diagnostics(double out[4]) override {
     diagnostics_launch();

@@ -21,7 +21,7 @@
 // columns per row (128-byte segments).
 #pragma once
 #include "common.cuh"
-#include "fft.cuh"
+#include "fft2.cuh"
 
 namespace les {
 
@@ -176,17 +176,36 @@ __device__ __forceinline__ void xf_load_point(const XFArgs<T>& a, int l, int j, 
   }
 }
 
+// number of sequence slots in an x pass: rounded up to whole warps
+template <int M>
+__host__ __device__ constexpr int seq_pad(int nseq) {
+  constexpr int spw = 32 / Geo<M>::T;  // sequences per warp
+  return ((nseq + spw - 1) / spw) * spw;
+}
+
 template <typename T, int NX>
-__global__ void __launch_bounds__(256) k_xfwd(const XFArgs<T> a) {
+__global__ void __launch_bounds__(256, 2) k_xfwd(const XFArgs<T> a) {
   constexpr int M = NX / 2;
+  constexpr int TL = Geo<M>::T;
+  constexpr int E = Geo<M>::E;
+  constexpr int RI = Layout<M, false>::in;
+  constexpr int RO = Layout<M, false>::out;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
-  cplx<T>* b0 = tw + NX;
+  cplx<T>* buf = tw + NX;
   const int nseq = a.R * a.nf;
-  cplx<T>* b1 = b0 + nseq * M;
+  const int npad = seq_pad<M>(nseq);
+  T* refs = reinterpret_cast<T*>(buf + (long)npad * M);  // R * nf per-row references
+  int* rowl = reinterpret_cast<int*>(refs + a.R * a.nf);  // level of row r (-1: beyond the grid)
+  int* rowj = rowl + a.R;
   for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
   const long g0 = (long)blockIdx.x * a.R;
-  T* refs = reinterpret_cast<T*>(b1 + nseq * M);  // R * nf per-row references
+  for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
+    const long g = g0 + r;
+    rowl[r] = (g < a.nrows) ? a.plane0 + int(g / a.rows_pp) : -1;
+    rowj[r] = (g < a.nrows) ? int(g % a.rows_pp) : 0;
+  }
+  __syncthreads();
   if (a.use_ref) {
     for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
       const long g = g0 + r;
@@ -203,15 +222,14 @@ __global__ void __launch_bounds__(256) k_xfwd(const XFArgs<T> a) {
   }
   // load: one thread per point; sequence s = r*nf + f holds the packed row
   // z_m = x_{2m} + i x_{2m+1}, i.e. the real row itself viewed as complex.
-  T* xr = reinterpret_cast<T*>(b0);
+  T* xr = reinterpret_cast<T*>(buf);
   for (int idx = threadIdx.x; idx < a.R * NX; idx += blockDim.x) {
     const int r = idx / NX;
     const int i = idx - r * NX;
-    const long g = g0 + r;
     T* dst = xr + (long)(r * a.nf) * NX + i;
-    if (g < a.nrows) {
-      const int l = a.plane0 + int(g / a.rows_pp);
-      const int j = int(g % a.rows_pp);
+    const int l = rowl[r];
+    if (l >= 0) {
+      const int j = rowj[r];
       xf_load_point(a, l, j, i, dst, NX);
       if (a.use_ref)
         for (int f = 0; f < a.nf; ++f) dst[f * NX] -= refs[r * a.nf + f];
@@ -219,26 +237,43 @@ __global__ void __launch_bounds__(256) k_xfwd(const XFArgs<T> a) {
       for (int f = 0; f < a.nf; ++f) dst[f * NX] = T(0);
     }
   }
+  for (int idx = nseq * M + threadIdx.x; idx < npad * M; idx += blockDim.x) buf[idx] = cplx<T>{T(0), T(0)};
   __syncthreads();
-  cplx<T>* Z = fft_batch<T, M, false, 2>(b0, b1, nseq, M, tw);
-  // r2c post-processing: X_k = E_k + W^k O_k for k < nk
-  for (int idx = threadIdx.x; idx < nseq * a.nk; idx += blockDim.x) {
-    const int s = idx / a.nk;
-    const int k = idx - s * a.nk;
-    const int r = s / a.nf;
-    const int f = s - r * a.nf;
-    const long g = g0 + r;
-    if (g >= a.nrows) continue;
-    const cplx<T> zk = Z[s * M + (k == M ? 0 : k)];
-    const cplx<T> zm = Z[s * M + ((M - k) % M)];
-    const cplx<T> e = {T(0.5) * (zk.x + zm.x), T(0.5) * (zk.y - zm.y)};
-    // o = (zk - conj(zm)) / (2i)
-    const cplx<T> o = {T(0.5) * (zk.y + zm.y), T(-0.5) * (zk.x - zm.x)};
-    const cplx<T> w = tw[k];
-    const cplx<T> X = cadd(e, cmul(o, w));
-    const int l = a.plane0 + int(g / a.rows_pp);
-    const int j = int(g % a.rows_pp);
-    a.out[f][(long)l * a.out_pstride + (long)j * a.nk + k] = X;
+  // complex FFT of length M per sequence in registers, then the r2c split
+  const int lane_t = threadIdx.x % TL;
+  for (int base = 0; base < npad; base += blockDim.x / TL) {
+    const int s = base + threadIdx.x / TL;
+    if (base + (threadIdx.x / 32) * (32 / TL) >= npad) break;  // whole warp beyond the slots
+    cplx<T>* seq = buf + (long)s * M;
+    cplx<T> v[E];
+#pragma unroll
+    for (int g = 0; g < E / RI; ++g)
+#pragma unroll
+      for (int r = 0; r < RI; ++r) v[g * RI + r] = seq[lane_t + TL * g + r * (M / RI)];
+    reg_fft<T, M, false, 2>(v, seq, lane_t, tw);
+    __syncwarp();
+#pragma unroll
+    for (int g = 0; g < E / RO; ++g)
+#pragma unroll
+      for (int r = 0; r < RO; ++r) seq[lane_t + TL * g + r * (M / RO)] = v[g * RO + r];
+    __syncwarp();
+    if (s < nseq) {
+      const int r = s / a.nf;
+      const int f = s - r * a.nf;
+      const int l = rowl[r];
+      if (l >= 0) {
+        const int j = rowj[r];
+        cplx<T>* orow = a.out[f] + (long)l * a.out_pstride + (long)j * a.nk;
+        for (int k = lane_t; k < a.nk; k += TL) {
+          // X_k = E_k + W^k O_k, E = (Z_k + conj Z_{M-k})/2, O = (Z_k - conj Z_{M-k})/(2i)
+          const cplx<T> zk = seq[k == M ? 0 : k];
+          const cplx<T> zm = seq[(M - k) % M];
+          const cplx<T> e = {T(0.5) * (zk.x + zm.x), T(0.5) * (zk.y - zm.y)};
+          const cplx<T> o = {T(0.5) * (zk.y + zm.y), T(-0.5) * (zk.x - zm.x)};
+          orow[k] = c_add(e, c_mul(o, tw[k]));
+        }
+      }
+    }
   }
 }
 
@@ -275,23 +310,67 @@ struct YPArgs {
   const cplx<T>* tw_out;  // length NYO table
 };
 
+// Elementwise spectral op at (kx, ky) for output q; F0/F1 are the forward
+// transforms of the (up to two) input fields at that point.
+template <typename T, int NY>
+__device__ __forceinline__ cplx<T> yp_op(const YPArgs<T>& a, int q, int kx, int ky, cplx<T> F0, cplx<T> F1) {
+  const cplx<T> zero = {T(0), T(0)};
+  switch (a.op) {
+    case YP_GRAD: {
+      if (ky == NY / 2 || kx == a.nxh) return zero;
+      if (q == 0) return F0;
+      if (q == 1) return ik_mul(a.kkx[ky * a.lhx + kx], F0);
+      return ik_mul(a.kky[ky * a.lhx + kx], F0);
+    }
+    case YP_DIV2: {
+      if (ky == NY / 2 || kx == a.nxh) return zero;
+      return c_add(ik_mul(a.kkx[ky * a.lhx + kx], F0), ik_mul(a.kky[ky * a.lhx + kx], F1));
+    }
+    case YP_FWDKILL:
+      return (ky == NY / 2 || kx == a.nxh) ? zero : F0;
+    case YP_PGRAD: {
+      if (q == 0) return ik_mul(a.kkx[ky * a.lhx + kx], F0);
+      if (q == 1) return ik_mul(a.kky[ky * a.lhx + kx], F0);
+      return F0;
+    }
+    case YP_FILTER1:
+    case YP_FILTER2: {
+      const T g = (q == 0 ? a.G0 : a.G1)[ky * a.lhx + kx];
+      return cplx<T>{F0.x * g, F0.y * g};
+    }
+    case YP_MASK:
+      return (ky <= a.tt || ky >= NY - a.tt) ? F0 : zero;
+    default:
+      return F0;  // YP_PAD / YP_TRUNC: position remap only
+  }
+}
+
 template <typename T, int NY, int NYO>
-__global__ void __launch_bounds__(256) k_ypass(const YPArgs<T> a) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPArgs<T> a) {
+  constexpr int TL = Geo<NY>::T;
+  static_assert(Geo<NYO>::T == TL, "pad/truncate pairs must share the lanes per sequence");
+  constexpr int EI = Geo<NY>::E;
+  constexpr int EO = Geo<NYO>::E;
+  constexpr int FI = Layout<NY, false>::in;    // forward input groups
+  constexpr int FO = Layout<NY, false>::out;   // forward output groups
+  constexpr int II = Layout<NYO, true>::in;    // inverse input groups
+  constexpr int IO = Layout<NYO, true>::out;   // inverse output groups
+  constexpr bool SAME = (NY == NYO);
+  static_assert(!SAME || FO == II, "forward output layout must feed the inverse");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* twi = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* two = twi + NY;
-  cplx<T>* bufA = two + NYO;
   constexpr int SI = NY + 1;
   constexpr int SO = NYO + 1;
   const int C = a.C;
-  const int nmax = max(a.nin * SI, a.nout * SO);
-  cplx<T>* bufB = bufA + C * nmax;
+  cplx<T>* bin = two + NYO;           // [nin][C][SI]
+  cplx<T>* bout = bin + a.nin * C * SI;  // [C][SO]
   for (int i = threadIdx.x; i < NY; i += blockDim.x) twi[i] = a.tw_in[i];
   for (int i = threadIdx.x; i < NYO; i += blockDim.x) two[i] = a.tw_out[i];
   const int col0 = blockIdx.x * C;
   const int l = a.plane0 + blockIdx.y;
   const int grp = blockIdx.z;
-  // load C columns of every input field
+  // coalesced load of C columns of every input field
   for (int idx = threadIdx.x; idx < a.nin * NY * C; idx += blockDim.x) {
     const int c = idx & (C - 1);
     const int t = idx >> a.lc;
@@ -300,94 +379,129 @@ __global__ void __launch_bounds__(256) k_ypass(const YPArgs<T> a) {
     const int kx = col0 + c;
     cplx<T> v = {T(0), T(0)};
     if (kx < a.ncols) v = a.in[grp * a.nin + q][(long)l * a.in_pstride + (long)ky * a.nk_in + kx];
-    bufA[(q * C + c) * SI + ky] = v;
+    bin[(q * C + c) * SI + ky] = v;
   }
   __syncthreads();
-  cplx<T>* F = bufA;
-  if (a.op != YP_PGRAD) F = fft_batch<T, NY, false>(bufA, bufB, a.nin * C, SI, twi);
-  cplx<T>* D = (F == bufA) ? bufB : bufA;
-  cplx<T>* E = (F == bufA) ? bufA : bufB;
-  // spectral op -> D (nout * C sequences of length NYO)
-  for (int idx = threadIdx.x; idx < a.nout * NYO * C; idx += blockDim.x) {
-    const int c = idx & (C - 1);
-    const int t = idx >> a.lc;
-    const int ky = t % NYO;
-    const int q = t / NYO;
-    const int kx = col0 + c;
-    cplx<T> r = {T(0), T(0)};
-    if (kx < a.ncols) {
-      switch (a.op) {
-        case YP_GRAD: {
-          const bool kill = (ky == NY / 2) || (kx == a.nxh);
-          const cplx<T> f = kill ? cplx<T>{T(0), T(0)} : F[c * SI + ky];
-          if (q == 0) r = f;
-          else if (q == 1) r = ik_mul(a.kkx[ky * a.lhx + kx], f);
-          else r = ik_mul(a.kky[ky * a.lhx + kx], f);
-          break;
-        }
-        case YP_DIV2: {
-          const bool kill = (ky == NY / 2) || (kx == a.nxh);
-          if (!kill) {
-            const cplx<T> fx = F[c * SI + ky];
-            const cplx<T> fy = F[(C + c) * SI + ky];
-            r = cadd(ik_mul(a.kkx[ky * a.lhx + kx], fx), ik_mul(a.kky[ky * a.lhx + kx], fy));
-          }
-          break;
-        }
-        case YP_FWDKILL: {
-          const bool kill = (ky == NY / 2) || (kx == a.nxh);
-          if (!kill) r = F[(q * C + c) * SI + ky];
-          break;
-        }
-        case YP_PGRAD: {
-          const cplx<T> f = F[c * SI + ky];
-          if (q == 0) r = ik_mul(a.kkx[ky * a.lhx + kx], f);
-          else if (q == 1) r = ik_mul(a.kky[ky * a.lhx + kx], f);
-          else r = f;
-          break;
-        }
-        case YP_FILTER1:
-        case YP_FILTER2: {
-          const cplx<T> f = F[c * SI + ky];
-          const T g = (q == 0 ? a.G0 : a.G1)[ky * a.lhx + kx];
-          r = cplx<T>{f.x * g, f.y * g};
-          break;
-        }
-        case YP_PAD: {
-          // NYO = 3 NY / 2: modes 0..NY/2-1 and -(NY/2-1)..-1 kept
-          if (ky < NY / 2) r = F[c * SI + ky];
-          else if (ky > NYO - NY / 2) r = F[c * SI + ky - (NYO - NY)];
-          break;
-        }
-        case YP_TRUNC: {
-          // NY = 3 NYO / 2
-          if (ky < NYO / 2) r = F[c * SI + ky];
-          else if (ky > NYO / 2) r = F[c * SI + ky + (NY - NYO)];
-          break;
-        }
-        case YP_MASK: {
-          if (ky <= a.tt || ky >= NY - a.tt) r = F[(q * C + c) * SI + ky];
-          break;
+  const int c = threadIdx.x / TL;
+  const int lt = threadIdx.x % TL;
+  const int kx = col0 + c;
+  // forward transform in registers; the stress divergence folds its second
+  // input into w = i kx F0 + i ky F1 before the output loop
+  cplx<T> f0[EI];
+  cplx<T> w[EO];
+  {
+    cplx<T>* seq = bin + c * SI;
+    if (a.op == YP_PGRAD) {
+      // input is already y-spectral: load it in the inverse input layout
+#pragma unroll
+      for (int g = 0; g < EI / II; ++g)
+#pragma unroll
+        for (int r = 0; r < II; ++r) f0[g * II + r] = seq[lt + TL * g + r * (NY / II)];
+    } else {
+#pragma unroll
+      for (int g = 0; g < EI / FI; ++g)
+#pragma unroll
+        for (int r = 0; r < FI; ++r) f0[g * FI + r] = seq[lt + TL * g + r * (NY / FI)];
+      reg_fft<T, NY, false>(f0, seq, lt, twi);
+      if constexpr (SAME) {
+        if (a.op == YP_DIV2) {
+          const cplx<T> zero = {T(0), T(0)};
+#pragma unroll
+          for (int g = 0; g < EI / FO; ++g)
+#pragma unroll
+            for (int r = 0; r < FO; ++r) {
+              const int ky = lt + TL * g + r * (NY / FO);
+              const bool kill = (ky == NY / 2) || (kx == a.nxh) || (kx >= a.ncols);
+              w[g * FO + r] = kill ? zero : ik_mul(a.kkx[ky * a.lhx + kx], f0[g * FO + r]);
+            }
+          cplx<T>* seq1 = bin + (C + c) * SI;
+#pragma unroll
+          for (int g = 0; g < EI / FI; ++g)
+#pragma unroll
+            for (int r = 0; r < FI; ++r) f0[g * FI + r] = seq1[lt + TL * g + r * (NY / FI)];
+          reg_fft<T, NY, false>(f0, seq1, lt, twi);
+#pragma unroll
+          for (int g = 0; g < EI / FO; ++g)
+#pragma unroll
+            for (int r = 0; r < FO; ++r) {
+              const int ky = lt + TL * g + r * (NY / FO);
+              const bool kill = (ky == NY / 2) || (kx == a.nxh) || (kx >= a.ncols);
+              if (!kill) w[g * FO + r] = c_add(w[g * FO + r], ik_mul(a.kky[ky * a.lhx + kx], f0[g * FO + r]));
+            }
         }
       }
     }
-    D[(q * C + c) * SO + ky] = r;
   }
-  __syncthreads();
-  cplx<T>* Y = D;
-  if (a.op != YP_FWDKILL) Y = fft_batch<T, NYO, true>(D, E, a.nout * C, SO, two);
-  for (int idx = threadIdx.x; idx < a.nout * NYO * C; idx += blockDim.x) {
-    const int c = idx & (C - 1);
-    const int t = idx >> a.lc;
-    const int ky = t % NYO;
-    const int q = t / NYO;
-    const int kx = col0 + c;
-    if (a.op == YP_FILTER2 && q == 1) {
-      if (kx < a.ncols1)
-        a.out[grp * a.nout + q][(long)l * a.out_pstride1 + (long)ky * a.nk_out1 + kx] = Y[(q * C + c) * SO + ky];
-    } else if (kx < a.ncols) {
-      a.out[grp * a.nout + q][(long)l * a.out_pstride + (long)ky * a.nk_out + kx] = Y[(q * C + c) * SO + ky];
+  cplx<T>* sout = bout + c * SO;
+  for (int q = 0; q < a.nout; ++q) {
+    if constexpr (SAME) {
+      // forward output layout (groups FO) == inverse input layout; the
+      // stress divergence already holds its result in w
+      if (a.op != YP_DIV2) {
+#pragma unroll
+        for (int g = 0; g < EI / FO; ++g)
+#pragma unroll
+          for (int r = 0; r < FO; ++r) {
+            const int ky = lt + TL * g + r * (NY / FO);
+            w[g * FO + r] = (kx < a.ncols) ? yp_op<T, NY>(a, q, kx, ky, f0[g * FO + r], f0[g * FO + r])
+                                           : cplx<T>{T(0), T(0)};
+          }
+      }
+    } else {
+      // 3/2 pad or truncate: remap the forward output through the slot
+      for (int i = lt; i < NYO; i += TL) sout[i] = cplx<T>{T(0), T(0)};
+      __syncwarp();
+#pragma unroll
+      for (int g = 0; g < EI / FO; ++g)
+#pragma unroll
+        for (int r = 0; r < FO; ++r) {
+          const int ky = lt + TL * g + r * (NY / FO);
+          int ko = -1;
+          if (a.op == YP_PAD) {
+            if (ky < NY / 2) ko = ky;
+            else if (ky > NY / 2) ko = ky + (NYO - NY);
+          } else {  // YP_TRUNC, NY = 3 NYO / 2
+            if (ky < NYO / 2) ko = ky;
+            else if (ky > NY - NYO / 2) ko = ky - (NY - NYO);
+          }
+          if (ko >= 0 && kx < a.ncols) sout[ko] = f0[g * FO + r];
+        }
+      __syncwarp();
+#pragma unroll
+      for (int g = 0; g < EO / II; ++g)
+#pragma unroll
+        for (int r = 0; r < II; ++r) w[g * II + r] = sout[lt + TL * g + r * (NYO / II)];
+      __syncwarp();
     }
+    if (a.op == YP_FWDKILL) {
+      // no inverse: the op output is in the forward output layout (groups FO)
+#pragma unroll
+      for (int g = 0; g < EO / FO; ++g)
+#pragma unroll
+        for (int r = 0; r < FO; ++r) sout[lt + TL * g + r * (NYO / FO)] = w[g * FO + r];
+    } else {
+      reg_fft<T, NYO, true>(w, sout, lt, two);
+      __syncwarp();
+#pragma unroll
+      for (int g = 0; g < EO / IO; ++g)
+#pragma unroll
+        for (int r = 0; r < IO; ++r) sout[lt + TL * g + r * (NYO / IO)] = w[g * IO + r];
+    }
+    __syncthreads();
+    // coalesced store of output q
+    const bool second = (a.op == YP_FILTER2 && q == 1);
+    const int lim = second ? a.ncols1 : a.ncols;
+    for (int idx = threadIdx.x; idx < NYO * C; idx += blockDim.x) {
+      const int cc = idx & (C - 1);
+      const int ky = idx >> a.lc;
+      const int kxx = col0 + cc;
+      if (kxx < lim) {
+        const cplx<T> val = bout[cc * SO + ky];
+        if (second) a.out[grp * a.nout + q][(long)l * a.out_pstride1 + (long)ky * a.nk_out1 + kxx] = val;
+        else a.out[grp * a.nout + q][(long)l * a.out_pstride + (long)ky * a.nk_out + kxx] = val;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -423,52 +537,103 @@ struct XIArgs {
 };
 
 template <typename T, int NX>
-__global__ void __launch_bounds__(256) k_xinv(const XIArgs<T> a) {
+__global__ void __launch_bounds__(256, 2) k_xinv(const XIArgs<T> a) {
   constexpr int M = NX / 2;
+  constexpr int TL = Geo<M>::T;
+  constexpr int E = Geo<M>::E;
+  constexpr int RI = Layout<M, true>::in;
+  constexpr int RO = Layout<M, true>::out;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
-  cplx<T>* b0 = tw + NX;
+  cplx<T>* buf = tw + NX;
   const int nseq = a.R * a.nin;
-  cplx<T>* b1 = b0 + nseq * M;
+  const int npad = seq_pad<M>(nseq);
+  int* rowl = reinterpret_cast<int*>(buf + (long)npad * M);  // level of row r (-1: beyond the grid)
+  int* rowj = rowl + a.R;
   for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
-  __syncthreads();
   const long g0 = (long)blockIdx.x * a.R;
-  // c2r pre-processing: Z_k = (X_k + conj X_{M-k}) + i W^{-k} (X_k - conj X_{M-k})
-  for (int idx = threadIdx.x; idx < nseq * M; idx += blockDim.x) {
-    const int s = idx / M;
-    const int k = idx - s * M;
-    const int r = s / a.nin;
-    const int f = s - r * a.nin;
+  for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
     const long g = g0 + r;
-    cplx<T> z = {T(0), T(0)};
-    if (g < a.nrows) {
-      const int l = a.plane0 + int(g / a.rows_pp);
-      const int j = int(g % a.rows_pp);
-      const cplx<T>* row = a.in[f] + (long)l * a.in_pstride + (long)j * a.nk;
-      cplx<T> xk = (k < a.nk) ? row[k] : cplx<T>{T(0), T(0)};
-      cplx<T> xm = (M - k < a.nk) ? row[M - k] : cplx<T>{T(0), T(0)};
-      if (k == 0) {  // DC and Nyquist bins: imaginary parts ignored (c2r)
-        xk.y = T(0);
-        xm.y = T(0);
-      }
-      const cplx<T> s1 = {xk.x + xm.x, xk.y - xm.y};  // X_k + conj(X_{M-k})
-      const cplx<T> d1 = {xk.x - xm.x, xk.y + xm.y};  // X_k - conj(X_{M-k})
-      const cplx<T> w = tw[k];                        // W^{k}; need W^{-k} = conj
-      const cplx<T> t = cmulc(d1, w);                 // d1 * W^{-k}
-      z = {s1.x - t.y, s1.y + t.x};                   // s1 + i t
-    }
-    b0[s * M + k] = z;
+    rowl[r] = (g < a.nrows) ? a.plane0 + int(g / a.rows_pp) : -1;
+    rowj[r] = (g < a.nrows) ? int(g % a.rows_pp) : 0;
   }
   __syncthreads();
-  const cplx<T>* Zr = fft_batch<T, M, true, 2>(b0, b1, nseq, M, tw);
-  const T* xs = reinterpret_cast<const T*>(Zr);  // x_i of sequence s at xs[s*NX + i]
+  // a plain store writes straight from registers; the other ops combine
+  // fields per point through shared memory
+  const bool direct = (a.op == XI_STORE);
+  const int lane_t = threadIdx.x % TL;
+  for (int base = 0; base < npad; base += blockDim.x / TL) {
+    const int s = base + threadIdx.x / TL;
+    if (base + (threadIdx.x / 32) * (32 / TL) >= npad) break;  // whole warp beyond the slots
+    const int r = s / a.nin;
+    const int f = s - r * a.nin;
+    const bool valid = (s < nseq) && (rowl[r < a.R ? r : 0] >= 0);
+    int l = 0, j = 0;
+    if (valid) {
+      l = rowl[r];
+      j = rowj[r];
+    }
+    cplx<T>* seq = buf + (long)s * M;
+    // c2r split: Z_m = (X_m + conj X_{M-m}) + i W^{-m} (X_m - conj X_{M-m}),
+    // imaginary parts of the DC and Nyquist bins ignored
+    cplx<T> v[E];
+    const cplx<T>* row = valid ? a.in[f] + (long)l * a.in_pstride + (long)j * a.nk : nullptr;
+#pragma unroll
+    for (int gg = 0; gg < E / RI; ++gg)
+#pragma unroll
+      for (int rr = 0; rr < RI; ++rr) {
+        const int m = lane_t + TL * gg + rr * (M / RI);
+        cplx<T> z = {T(0), T(0)};
+        if (valid) {
+          cplx<T> xk = (m < a.nk) ? row[m] : cplx<T>{T(0), T(0)};
+          cplx<T> xm = (M - m < a.nk) ? row[M - m] : cplx<T>{T(0), T(0)};
+          if (m == 0) {
+            xk.y = T(0);
+            xm.y = T(0);
+          }
+          const cplx<T> s1 = {xk.x + xm.x, xk.y - xm.y};
+          const cplx<T> d1 = {xk.x - xm.x, xk.y + xm.y};
+          const cplx<T> t = c_mulc(d1, tw[m]);
+          z = {s1.x - t.y, s1.y + t.x};
+        }
+        v[gg * RI + rr] = z;
+      }
+    reg_fft<T, M, true, 2>(v, seq, lane_t, tw);
+    if (direct) {
+      if (valid && l >= a.lo[f] && l <= a.hi[f]) {
+        const T ref = a.refin[f] ? a.refin[f][l] : T(0);
+        const long off = (long)l * a.out_pstride + (long)j * NX;
+#pragma unroll
+        for (int gg = 0; gg < E / RO; ++gg)
+#pragma unroll
+          for (int rr = 0; rr < RO; ++rr) {
+            const int m = lane_t + TL * gg + rr * (M / RO);
+            const cplx<T> z = v[gg * RO + rr];
+            if (a.out_f32) {
+              *reinterpret_cast<float2*>(a.outf[f] + off + 2 * m) = make_float2(float(z.x + ref), float(z.y + ref));
+            } else {
+              a.out[f][off + 2 * m] = z.x + ref;
+              a.out[f][off + 2 * m + 1] = z.y + ref;
+            }
+          }
+      }
+    } else {
+      __syncwarp();
+#pragma unroll
+      for (int gg = 0; gg < E / RO; ++gg)
+#pragma unroll
+        for (int rr = 0; rr < RO; ++rr) seq[lane_t + TL * gg + rr * (M / RO)] = v[gg * RO + rr];
+    }
+  }
+  if (direct) return;
+  __syncthreads();
+  const T* xs = reinterpret_cast<const T*>(buf);  // x_i of sequence s at xs[s*NX + i]
   for (int idx = threadIdx.x; idx < a.R * NX; idx += blockDim.x) {
     const int r = idx / NX;
     const int i = idx - r * NX;
-    const long g = g0 + r;
-    if (g >= a.nrows) continue;
-    const int l = a.plane0 + int(g / a.rows_pp);
-    const int j = int(g % a.rows_pp);
+    const int l = rowl[r];
+    if (l < 0) continue;
+    const int j = rowj[r];
     const long off = (long)l * a.out_pstride + (long)j * NX + i;
     T* xw = const_cast<T*>(xs) + (long)(r * a.nin) * NX + i;
     for (int f = 0; f < a.nin; ++f)  // this thread alone touches (r, i)

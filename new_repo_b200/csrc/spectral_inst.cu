@@ -12,12 +12,37 @@ constexpr int SMEM_CAP = 200 * 1024;
 
 template <typename T>
 int rows_per_cta(int nseq_per_row, int M) {
-  // keep one ping-pong buffer at ~48 KB so two CTAs fit on an SM
-  const int target = int((48 * 1024) / sizeof(cplx<T>));
+  // keep the in-place sequence buffer near 32 KB so several CTAs fit on an SM
+  const int target = int((32 * 1024) / sizeof(cplx<T>));
   int R = target / (nseq_per_row * M);
   if (R < 1) R = 1;
   if (R > 32) R = 32;
   return R;
+}
+
+// lanes per sequence of the register FFT of length n (fft2.cuh plans)
+int lanes(int n) {
+  switch (n) {
+    case 8: return Geo<8>::T;
+    case 12: return Geo<12>::T;
+    case 16: return Geo<16>::T;
+    case 24: return Geo<24>::T;
+    case 32: return Geo<32>::T;
+    case 48: return Geo<48>::T;
+    case 64: return Geo<64>::T;
+    case 96: return Geo<96>::T;
+    case 128: return Geo<128>::T;
+    case 192: return Geo<192>::T;
+    case 256: return Geo<256>::T;
+    case 384: return Geo<384>::T;
+    case 512: return Geo<512>::T;
+    case 768: return Geo<768>::T;
+    default: throw CudaError(1, "no FFT plan for length " + std::to_string(n));
+  }
+}
+int pad_seqs(int nseq, int M) {
+  const int spw = 32 / lanes(M);
+  return ((nseq + spw - 1) / spw) * spw;
 }
 }  // namespace
 
@@ -38,7 +63,8 @@ void launch_xfwd(int NX, XFArgs<T> a, cudaStream_t st) {
   const int M = NX / 2;
   a.R = rows_per_cta<T>(a.nf, M);
   a.in_rstride = NX;
-  const size_t smem = sizeof(cplx<T>) * (NX + 2 * (size_t)a.R * a.nf * M) + sizeof(T) * a.R * a.nf;
+  const size_t smem = sizeof(cplx<T>) * (NX + (size_t)pad_seqs(a.R * a.nf, M) * M) + sizeof(T) * a.R * a.nf +
+                      2 * sizeof(int) * a.R + 16;
   if (smem > SMEM_CAP) throw CudaError(1, "xfwd: shared memory request too large");
   const int grid = ceil_div(a.nrows, a.R);
   if (grid == 0) return;
@@ -62,7 +88,7 @@ template <typename T>
 void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
   const int M = NX / 2;
   a.R = rows_per_cta<T>(a.nin, M);
-  const size_t smem = sizeof(cplx<T>) * (NX + 2 * (size_t)a.R * a.nin * M);
+  const size_t smem = sizeof(cplx<T>) * (NX + (size_t)pad_seqs(a.R * a.nin, M) * M) + 2 * sizeof(int) * a.R;
   if (smem > SMEM_CAP) throw CudaError(1, "xinv: shared memory request too large");
   const int grid = ceil_div(a.nrows, a.R);
   if (grid == 0) return;
@@ -89,14 +115,17 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
 
 template <typename T>
 void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaStream_t st) {
-  const int nmax = std::max(a.nin * (NY + 1), a.nout * (NYO + 1));
-  const size_t per_col = 2 * (size_t)nmax * sizeof(cplx<T>);
-  int lc = 4;  // up to 16 columns per CTA
-  while (lc > 0 && ((size_t(1) << lc) * per_col > 96 * 1024 || (1 << lc) > 2 * a.ncols)) --lc;
+  const int TL = lanes(NY);
+  if (lanes(NYO) != TL) throw CudaError(1, "ypass: length pair with different lane counts");
+  const size_t per_col = (size_t)(a.nin * (NY + 1) + (NYO + 1)) * sizeof(cplx<T>);
+  int lc = 0;  // C = 1 << lc columns per CTA, C * TL <= 256 threads
+  while ((2 << lc) * TL <= 256 && (size_t(2) << lc) * per_col <= 96 * 1024 && (1 << lc) < a.ncols) ++lc;
+  while ((1 << lc) * TL < 32) ++lc;  // at least one full warp
   a.lc = lc;
   a.C = 1 << lc;
   const size_t smem = sizeof(cplx<T>) * (NY + NYO) + (size_t)a.C * per_col;
   if (smem > SMEM_CAP) throw CudaError(1, "ypass: shared memory request too large");
+  const int threads = a.C * TL;
   dim3 grid(ceil_div(a.ncols, a.C), nplanes, ngroups);
   if (grid.x == 0 || nplanes == 0 || ngroups == 0) return;
   const int key = NY * 10000 + NYO;
@@ -104,7 +133,7 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
                            (double(a.op == YP_PGRAD ? 1 : a.nin) * NY + double(a.nout) * NYO));
   switch (key) {
 #define YP_CASE(A, B) \
-  case A * 10000 + B: k_ypass<T, A, B><<<grid, 256, smem, st>>>(a); break;
+  case A * 10000 + B: k_ypass<T, A, B><<<grid, threads, smem, st>>>(a); break;
     YP_CASE(16, 16) YP_CASE(32, 32) YP_CASE(64, 64) YP_CASE(128, 128) YP_CASE(256, 256) YP_CASE(512, 512)
     YP_CASE(16, 24) YP_CASE(32, 48) YP_CASE(64, 96) YP_CASE(128, 192) YP_CASE(256, 384) YP_CASE(512, 768)
     YP_CASE(24, 16) YP_CASE(48, 32) YP_CASE(96, 64) YP_CASE(192, 128) YP_CASE(384, 256) YP_CASE(768, 512)
