@@ -3,9 +3,13 @@
 
 Headline arm: the mixed-precision step (FP32 fields, FFTs, convection and
 SGS; FP64 tridiagonal pressure solve, mean mode and compensated diagnostics)
-with the Lagrangian scale-dependent dynamic SGS model, beside the plain FP64
-GPU step of the same seed (its throughput and the velocity error between the
-two runs are part of the JSON line).
+with the learned SGS closure (8 invariants -> 64 -> 64 -> Cs^2 on the tcgen05
+tensor cores, trained on the GPU from Lagrangian scale-dependent dynamic
+(LASD) pairs of the first steps, untimed; LASD fallback for columns outside
+the training range and an LASD check of the closure every 10 updates).
+Beside it, the same step with the LASD closure and the plain FP64 GPU step
+(LASD) of the same seed: their throughputs and the velocity error between
+the headline and FP64 runs are part of the JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -29,7 +33,7 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "Mpts*steps/s at 256^3 (LES time step, FP32 + dynamic SGS closure vs plain FP64 GPU)"
+METRIC = "Mpts*steps/s at 256^3 (LES time step, FP32 + learned SGS closure vs plain FP64 GPU)"
 UNIT = "Mpts*steps/s"
 
 
@@ -44,6 +48,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--closure", default="mlp", choices=["mlp", "lasd"], help="SGS closure of the headline arm")
+    ap.add_argument("--train-steps", type=int, default=20, help="LASD steps that produce the training pairs")
     return ap.parse_args()
 
 
@@ -178,9 +184,11 @@ def run_ours(args, dist, rank, local, ws):
     u0, v0, w0 = log_law_noise(p, seed=rank)
     out = {}
 
-    # ---- headline: mixed precision ----
+    # ---- headline: mixed precision, learned closure trained on the GPU ----
     les = LES(p, precision="mixed", device=local)
     les.set_initial_conditions(u0, v0, w0)
+    T = args.train_steps if args.closure == "mlp" else 0
+    train = train_closure(les, p, T) if T else None
     les.step(W)
     les.sync()
     barrier(dist, local)
@@ -196,7 +204,8 @@ def run_ours(args, dist, rank, local, ws):
     value = npts * K * ws / (ms / 1e3) / 1e6
     mixed_u = [les.download(n, 1, p.nz) for n in ("u", "v", "w")] if not args.no_fp64 else None
     status = les.status()
-
+    if train is not None:
+        train.update(les.mlp_info())
     # ---- roofline of the dominant kernel (live events of the timed region) ----
     top = max(prof.items(), key=lambda kv: kv[1]["ms"])
     label, rec = top
@@ -223,12 +232,24 @@ def run_ours(args, dist, rank, local, ws):
         e2e = run_e2e(les, p, min(K, 20), local)
     les.close()
 
-    # ---- plain FP64 GPU step, same seed ----
+    # ---- the same step with the LASD closure (mixed precision) ----
+    lasd = None
+    if args.closure == "mlp" and not args.no_fp64:
+        ll = LES(p, precision="mixed", device=local)
+        ll.set_initial_conditions(u0, v0, w0)
+        ll.step(T + W)
+        ll.sync()
+        msl = max_over_ranks(dist, timed_steps(ll, K), local)
+        ll.close()
+        lasd = {"value": round(npts * K * ws / (msl / 1e3) / 1e6, 2), "ms_per_step": round(msl / K, 4),
+                "speedup_of_headline": round(msl / ms, 3)}
+
+    # ---- plain FP64 GPU step (LASD), same seed and step count ----
     fp64 = None
     if not args.no_fp64:
         l64 = LES(p, precision="fp64", device=local)
         l64.set_initial_conditions(u0, v0, w0)
-        l64.step(W)
+        l64.step(T + W)
         l64.sync()
         ms64 = timed_steps(l64, K)
         ref_u = [l64.download(n, 1, p.nz) for n in ("u", "v", "w")]
@@ -242,7 +263,7 @@ def run_ours(args, dist, rank, local, ws):
                 "speedup_of_headline": round(ms64 / ms, 3),
                 "velocity_rms_rel_error": float(math.sqrt(num / den)),
                 "mean_profile_drift": float(np.abs(prof_m - prof_r).max() / np.abs(prof_r).max()),
-                "after_steps": W + K}
+                "after_steps": T + W + K}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -254,16 +275,43 @@ def run_ours(args, dist, rank, local, ws):
             "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (fields, FFTs, convection, SGS) + f64 (pressure solve, mean mode, diagnostics)",
             "data": "synthetic: log-law profile + seeded uniform +-0.1 noise (counter-based hash)",
-            "config": {"workload": f"LES time step {p.nx}x{p.ny}x{p.nz}, 3/2 dealiasing, LASD SGS "
-                                   f"(cs_count 5, dynamic update every 5th step), log-law wall, FP32+FP64-pressure",
-                       "grid": [p.nx, p.ny, p.nz], "dt": p.dt_nd, "sgs_model": p.sgs_model,
+            "config": {"workload": f"LES time step {p.nx}x{p.ny}x{p.nz}, 3/2 dealiasing, "
+                                   + ("learned SGS closure (LASD fallback/check)" if T else "LASD SGS")
+                                   + " (cs_count 5, closure update every 5th step), log-law wall, "
+                                     "FP32+FP64-pressure",
+                       "grid": [p.nx, p.ny, p.nz], "dt": p.dt_nd, "sgs_model": "mlp" if T else p.sgs_model,
                        "precision": "mixed", "parallelism": f"replicas x{ws}",
                        "l2": "inputs larger than L2 (>= 9 GB of fields per step)"},
             "roofline": roof, "step_roofline": step_roof, "profile_top": prof_top,
-            "e2e": e2e, "gpu_launches": n1 - n0, "fp64_gpu": fp64, "cpu_baseline": cpu,
+            "e2e": e2e, "gpu_launches": n1 - n0, "fp64_gpu": fp64, "lasd_mixed": lasd, "closure_training": train,
+            "cpu_baseline": cpu,
             "clocks": clk.summary(), "status_bits": status,
         }
         print(json.dumps(line), flush=True)
+
+
+def train_closure(les, p, T: int) -> dict:
+    """Untimed: T LASD steps; the (invariants, log Cs^2) pairs of every update
+    step from step 10 on (one point in 8) train the closure on the GPU; the
+    state then continues with the learned closure."""
+    les.mlp_init(0)
+    les.mlp_reset_data(1 << 22)
+    t0 = time.perf_counter()
+    for _ in range(T):
+        les.step(1)
+        if les.jt_total >= 10 and les.jt_total % p.cs_count == 0:
+            les.mlp_collect(stride=8, seed=les.jt_total)
+    les.sync()
+    t1 = time.perf_counter()
+    ntr, nva = les.mlp_counts()
+    les.mlp_fit_stats()
+    losses, val = les.mlp_train(epochs=2, tiles_per_step=16, lr=2e-3)
+    les.sync()
+    t2 = time.perf_counter()
+    les.set_sgs_model("mlp")
+    return {"lasd_steps": T, "train_pairs": ntr, "validation_pairs": nva, "epochs": 2,
+            "batch": 16 * 128, "train_loss": [round(float(x), 4) for x in losses],
+            "validation_loss": round(val, 4), "collect_s": round(t1 - t0, 3), "train_s": round(t2 - t1, 3)}
 
 
 def ncu_traffic(label: str):

@@ -31,6 +31,9 @@ extern "C" {
 #define LES_SGS_CST_SMAG 0
 #define LES_SGS_DYN_SMAG 1
 #define LES_SGS_LASD 2
+/* learned closure: Cs^2 from the 8 -> 64 -> 64 -> 1 network (no reference
+ * counterpart; stands in for the dynamic procedure of compute_sgs.f90:171) */
+#define LES_SGS_MLP 3
 /* wall_model (compute_wall_law.f90:119-151) */
 #define LES_WALL_FILTER 0
 #define LES_WALL_INST 1
@@ -179,6 +182,48 @@ int les_event_elapsed(les_state* s, int a, int b, double* ms);
 int les_upload_async(les_state* s, int field, const double* pinned, int k0, int k1);
 int les_download_async(les_state* s, int field, double* pinned, int k0, int k1);
 int les_diagnostics_async(les_state* s, double* pinned_out4);
+
+/* ---- learned SGS closure (no reference counterpart) ---------------------
+ * Cs^2 = exp(net(invariants)) from an 8 -> 64 -> 64 -> 1 GELU network with
+ * BF16 weights and FP32 accumulation (tcgen05 tensor cores), evaluated at
+ * the dynamic-update cadence of compute_sgs.f90:171 (every cs_count steps
+ * after dyn_init).  Training data are (invariants, log Cs^2) pairs of the
+ * Lagrangian scale-dependent procedure (LASD, compute_sgs.f90:286) collected
+ * from a running state.  Columns whose invariants leave the training range
+ * fall back to the dynamic procedure; every `check_every` updates the
+ * dynamic procedure also runs on the whole domain and the RMS of
+ * log Cs^2 - log Cs^2_dyn is recorded.
+ * Parameters: float[LES_MLP_NPARAM + LES_MLP_NSTATS] = W1[8][64], b1[64],
+ * W2[64][64], b2[64], w3[64], b3, then feature mean[8], std[8],
+ * min[8], max[8] (normalised units), target mean, target std. */
+#define LES_MLP_NPARAM 4801
+#define LES_MLP_NSTATS 34
+int les_set_sgs_model(les_state* s, int model);
+int les_mlp_init(les_state* s, unsigned seed);
+int les_mlp_set_params(les_state* s, const float* params, int n);
+int les_mlp_get_params(les_state* s, float* params, int n);
+/* (re)allocate room for `cap` training and `cap` validation samples, empty */
+int les_mlp_reset_data(les_state* s, long cap);
+/* append the current state's (invariants, log cs_opt2) pairs, one point in
+ * `stride` (seeded hash), 10 % of them to the validation set */
+int les_mlp_collect(les_state* s, int stride, unsigned seed);
+int les_mlp_counts(les_state* s, long long out2[2]);
+/* feature/target statistics of the collected data; normalises it in place */
+int les_mlp_fit_stats(les_state* s);
+/* Adam on the mean squared error in normalised log Cs^2; batches of
+ * 128 * tiles_per_step samples; loss_epochs[epochs] (may be NULL) gets the
+ * last batch loss of each epoch, val_loss the validation loss (or -1) */
+int les_mlp_train(les_state* s, int epochs, int tiles_per_step, double lr, double* loss_epochs,
+                  double* val_loss);
+/* network output (normalised units) for n host feature rows x[n][8] */
+int les_mlp_forward(les_state* s, const float* x, long n, float* y);
+/* gradient of mean((y - t)^2) over n host rows into grad[LES_MLP_NPARAM] */
+int les_mlp_grad(les_state* s, const float* x, const float* t, long n, float* grad, float* loss);
+/* out4: last check's RMS log error (-1 if none), flagged columns of the last
+ * update, number of updates, weights loaded (1/0) */
+int les_mlp_info(les_state* s, double out4[4]);
+/* dynamic-procedure check every `every` closure updates (0 = never) */
+int les_mlp_set_check_every(les_state* s, int every);
 
 #ifdef __cplusplus
 }

@@ -12,7 +12,9 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "liblesgpu.so"
 
 LES_OK, LES_ERR_INVALID, LES_ERR_NOMEM, LES_ERR_NUMERICAL, LES_ERR_IO = 0, 1, 3, 9, 22
-SGS_MODELS = {"cst_Smag": 0, "dyn_Smag": 1, "dyn_LagScaleDep": 2}
+SGS_MODELS = {"cst_Smag": 0, "dyn_Smag": 1, "dyn_LagScaleDep": 2, "mlp": 3}
+MLP_NPARAM = 4801
+MLP_NSTATS = 34
 WALL_MODELS = {"wall_filter": 0, "wall_inst": 1, "wall_homog": 2}
 DEALIAS = {"padd": 0, "trunc": 1}
 LAG_HALO = {"reference1x1": 0, "periodic": 1}
@@ -49,6 +51,7 @@ class LesError(RuntimeError):
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
 _I = C.c_int
+_F = C.POINTER(C.c_float)
 PROTOTYPES = {
     "les_create": [C.POINTER(LesParams), C.POINTER(_P)],
     "les_destroy": [_P],
@@ -88,6 +91,19 @@ PROTOTYPES = {
     "les_upload_async": [_P, _I, C.c_void_p, _I, _I],
     "les_download_async": [_P, _I, C.c_void_p, _I, _I],
     "les_diagnostics_async": [_P, C.c_void_p],
+    "les_set_sgs_model": [_P, _I],
+    "les_mlp_init": [_P, C.c_uint],
+    "les_mlp_set_params": [_P, _F, _I],
+    "les_mlp_get_params": [_P, _F, _I],
+    "les_mlp_reset_data": [_P, C.c_long],
+    "les_mlp_collect": [_P, _I, C.c_uint],
+    "les_mlp_counts": [_P, C.POINTER(C.c_longlong)],
+    "les_mlp_fit_stats": [_P],
+    "les_mlp_train": [_P, _I, _I, C.c_double, _D, _D],
+    "les_mlp_forward": [_P, _F, C.c_long, _F],
+    "les_mlp_grad": [_P, _F, _F, C.c_long, _F, _F],
+    "les_mlp_info": [_P, _D],
+    "les_mlp_set_check_every": [_P, _I],
 }
 
 _lib = None

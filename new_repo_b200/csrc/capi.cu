@@ -50,7 +50,7 @@ int les_create(const les_params* p, les_state** out) {
   return guard([&] {
     if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0 || p->dt <= 0 || p->cs_count <= 0)
       throw les::CudaError(LES_ERR_INVALID, "invalid grid, dt or cs_count");
-    if (p->sgs_model < LES_SGS_CST_SMAG || p->sgs_model > LES_SGS_LASD)
+    if (p->sgs_model < LES_SGS_CST_SMAG || p->sgs_model > LES_SGS_MLP)
       throw les::CudaError(LES_ERR_INVALID, "Invalid SGS model");
     if (p->wall_model < LES_WALL_FILTER || p->wall_model > LES_WALL_HOMOG)
       throw les::CudaError(LES_ERR_INVALID, "Invalid wall law type");
@@ -240,6 +240,83 @@ int les_download_async(les_state* s, int field, double* pinned, int k0, int k1) 
 int les_diagnostics_async(les_state* s, double* pinned_out4) {
   STATE_OR_FAIL(s);
   return guard([&] { s->s->diagnostics_async(pinned_out4); });
+}
+
+int les_set_sgs_model(les_state* s, int model) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->set_sgs_model(model); });
+}
+int les_mlp_init(les_state* s, unsigned seed) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->mlp_init(seed); });
+}
+int les_mlp_set_params(les_state* s, const float* p, int n) {
+  STATE_OR_FAIL(s);
+  if (!p) return bad_state();
+  return guard([&] { s->s->mlp_set_params(p, n); });
+}
+int les_mlp_get_params(les_state* s, float* p, int n) {
+  STATE_OR_FAIL(s);
+  if (!p) return bad_state();
+  return guard([&] { s->s->mlp_get_params(p, n); });
+}
+int les_mlp_reset_data(les_state* s, long cap) {
+  STATE_OR_FAIL(s);
+  if (cap <= 0) {
+    g_last_error = "learned closure: capacity must be positive";
+    return LES_ERR_INVALID;
+  }
+  return guard([&] { s->s->mlp_reset_data(cap); });
+}
+int les_mlp_collect(les_state* s, int stride, unsigned seed) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->mlp_collect(stride, seed); });
+}
+int les_mlp_counts(les_state* s, long long out2[2]) {
+  STATE_OR_FAIL(s);
+  if (!out2) return bad_state();
+  return guard([&] { s->s->mlp_counts(out2); });
+}
+int les_mlp_fit_stats(les_state* s) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->mlp_fit_stats(); });
+}
+int les_mlp_train(les_state* s, int epochs, int tiles_per_step, double lr, double* loss_epochs, double* val_loss) {
+  STATE_OR_FAIL(s);
+  if (epochs < 0 || tiles_per_step <= 0 || !(lr > 0)) {
+    g_last_error = "learned closure: invalid training arguments";
+    return LES_ERR_INVALID;
+  }
+  return guard([&] { s->s->mlp_train(epochs, tiles_per_step, lr, loss_epochs, val_loss); });
+}
+int les_mlp_forward(les_state* s, const float* x, long n, float* y) {
+  STATE_OR_FAIL(s);
+  if (!x || !y || n <= 0) {
+    g_last_error = "learned closure: invalid forward arguments";
+    return LES_ERR_INVALID;
+  }
+  return guard([&] { s->s->mlp_forward_host(x, n, y); });
+}
+int les_mlp_grad(les_state* s, const float* x, const float* t, long n, float* grad, float* loss) {
+  STATE_OR_FAIL(s);
+  if (!x || !t || !grad || !loss || n <= 0) {
+    g_last_error = "learned closure: invalid gradient arguments";
+    return LES_ERR_INVALID;
+  }
+  return guard([&] { s->s->mlp_grad_host(x, t, n, grad, loss); });
+}
+int les_mlp_info(les_state* s, double out4[4]) {
+  STATE_OR_FAIL(s);
+  if (!out4) return bad_state();
+  return guard([&] { s->s->mlp_info(out4); });
+}
+int les_mlp_set_check_every(les_state* s, int every) {
+  STATE_OR_FAIL(s);
+  if (every < 0) {
+    g_last_error = "learned closure: check interval must be >= 0";
+    return LES_ERR_INVALID;
+  }
+  return guard([&] { s->s->mlp_set_check_every(every); });
 }
 
 int les_timers(les_state* s, double out[5]) {

@@ -1,0 +1,711 @@
+// Learned SGS closure kernels on the sm_100a tensor cores (tcgen05).
+//
+// A tile is 128 points (one tensor-core M = 128 row block); each of the 128
+// threads owns one point/row.  Layer 1 (K = 8 features padded to 16) and
+// layer 2 (K = 64) run as tcgen05.mma with BF16 operands staged in shared
+// memory and FP32 accumulators in TMEM; bias, GELU and the 64 -> 1 output
+// layer run on the CUDA cores from the TMEM rows.  The training kernel adds
+// the backward pass: the hidden-layer error g2 . W2^T is a third tcgen05
+// GEMM, the weight gradients are row reductions accumulated per thread.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "launch.cuh"
+#include "mlp.cuh"
+#include "tc05.cuh"
+
+namespace les {
+
+namespace {
+constexpr int TILE = 128;
+constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, 64);
+// byte offsets of the packed operand images inside MlpDevice::img
+constexpr int IMG_B1 = 0;           // 64 x 16  (N x K), K-major, 2 KB
+constexpr int IMG_B2 = 2048;        // 64 x 64, 8 KB: B2[n][k] = W2[k][n]
+constexpr int IMG_B2T = 2048 + 8192;  // 64 x 64, 8 KB: B2T[k][n] = W2[k][n]
+constexpr int IMG_BYTES = 2048 + 8192 + 8192;
+
+// byte offset of element (row, k) in a K-major no-swizzle tile whose 16-byte
+// K chunks are 128 B apart and whose 8-row groups are sbo bytes apart
+__host__ __device__ constexpr int kmaj_off(int row, int k, int sbo) {
+  return (row >> 3) * sbo + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
+}
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752440f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+  const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752440f));
+  const float pdf = 0.39894228040143267794f * expf(-0.5f * x * x);
+  return cdf + x * pdf;
+}
+
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+  __nv_bfloat16 h = __float2bfloat16_rn(x);
+  return *reinterpret_cast<uint16_t*>(&h);
+}
+
+// raw (transformed, not normalised) invariants at level k, offset o
+template <typename T>
+__device__ __forceinline__ void raw_features(const MlpFeatIn<T>& a, long o, int k, float* t) {
+  const long pl = a.plane;
+  float ux, uy, uz, vx, vy, vz, wx, wy, wz, uh, vh;
+  if (k == 1) {
+    ux = float(a.d[0][o]);
+    uy = float(a.d[1][o]);
+    uz = a.wall ? float(a.d[2][o]) : 0.5f * float(a.d[2][o] + a.d[2][o + pl]);
+    vx = float(a.d[3][o]);
+    vy = float(a.d[4][o]);
+    vz = a.wall ? float(a.d[5][o]) : 0.5f * float(a.d[5][o] + a.d[5][o + pl]);
+    wx = 0.5f * float(a.d[6][o] + a.d[6][o + pl]);
+    wy = 0.5f * float(a.d[7][o] + a.d[7][o + pl]);
+    wz = float(a.d[8][o]);
+    uh = float(a.u[o]);
+    vh = float(a.v[o]);
+  } else {
+    ux = 0.5f * float(a.d[0][o] + a.d[0][o - pl]);
+    uy = 0.5f * float(a.d[1][o] + a.d[1][o - pl]);
+    uz = float(a.d[2][o]);
+    vx = 0.5f * float(a.d[3][o] + a.d[3][o - pl]);
+    vy = 0.5f * float(a.d[4][o] + a.d[4][o - pl]);
+    vz = float(a.d[5][o]);
+    wx = float(a.d[6][o]);
+    wy = float(a.d[7][o]);
+    wz = 0.5f * float(a.d[8][o] + a.d[8][o - pl]);
+    uh = 0.5f * float(a.u[o] + a.u[o - pl]);
+    vh = 0.5f * float(a.v[o] + a.v[o - pl]);
+  }
+  const float s11 = ux, s22 = vy, s33 = wz;
+  const float s12 = 0.5f * (uy + vx), s13 = 0.5f * (uz + wx), s23 = 0.5f * (vz + wy);
+  const float o12 = 0.5f * (uy - vx), o13 = 0.5f * (uz - wx), o23 = 0.5f * (vz - wy);
+  const float ss = s11 * s11 + s22 * s22 + s33 * s33 + 2.0f * (s12 * s12 + s13 * s13 + s23 * s23);
+  const float smag = sqrtf(2.0f * ss);
+  const float oo = 2.0f * (o12 * o12 + o13 * o13 + o23 * o23);
+  // tr(S^3) of the symmetric strain tensor
+  const float r3 = s11 * s11 * s11 + s22 * s22 * s22 + s33 * s33 * s33 +
+                   3.0f * (s12 * s12 * (s11 + s22) + s13 * s13 * (s11 + s33) + s23 * s23 * (s22 + s33)) +
+                   6.0f * s12 * s13 * s23;
+  const float z = (k == 1) ? 0.5f * a.dz : float(k - 1) * a.dz;
+  t[0] = log1pf(smag);
+  t[1] = log1pf(ss);
+  t[2] = log1pf(oo);
+  t[3] = copysignf(log1pf(fabsf(r3)), r3);
+  t[4] = log1pf(z / a.delta);
+  t[5] = 0.0f;  // gradient Richardson number: zero without buoyancy
+  t[6] = log1pf(sqrtf(uh * uh + vh * vh));
+  t[7] = a.log_delta_z0;
+}
+
+__device__ __forceinline__ unsigned hash32(unsigned x) {
+  x ^= x >> 16;
+  x *= 0x7feb352dU;
+  x ^= x >> 15;
+  x *= 0x846ca68bU;
+  x ^= x >> 16;
+  return x;
+}
+
+// --------------------------------------------------------- collection ----
+template <typename T>
+__global__ void k_mlp_collect(const MlpFeatIn<T> a, const T* cs, MlpDevice m, int stride, unsigned seed) {
+  const long n = (long)(a.nz + 1) * a.plane;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const unsigned h = hash32(unsigned(q) * 2654435761u ^ seed);
+    if (h % unsigned(stride) != 0) continue;
+    const long o = a.plane + q;
+    const int k = int(o / a.plane);
+    float t[8];
+    raw_features(a, o, k, t);
+    const float y = fmaxf(logf(fmaxf(float(cs[o]), 1e-30f)), MLP_LOG_CS_FLOOR);
+    const int val = ((h / unsigned(stride)) % 10u) == 0u;  // 10 % held out
+    const unsigned long long idx = atomicAdd(&m.counts[val], 1ull);
+    if ((long)idx >= m.cap) continue;
+    float* x = (val ? m.vx : m.dx) + idx * MLP_IN;
+#pragma unroll
+    for (int i = 0; i < MLP_IN; ++i) x[i] = t[i];
+    (val ? m.vt : m.dt)[idx] = y;
+  }
+}
+
+// statistics (double accumulators): sum, sum of squares, min, max of the 8
+// raw features and the target, over train + validation
+__global__ void __launch_bounds__(128) k_mlp_stats(const float* x, const float* t, long n, double* acc) {
+  __shared__ double s[18][128];
+  __shared__ float mn[9][128], mx[9][128];
+  double loc[18] = {0};
+  float lmin[9], lmax[9];
+  for (int i = 0; i < 9; ++i) {
+    lmin[i] = 3.0e38f;
+    lmax[i] = -3.0e38f;
+  }
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    for (int i = 0; i < 9; ++i) {
+      const float v = (i < 8) ? x[q * 8 + i] : t[q];
+      loc[2 * i] += v;
+      loc[2 * i + 1] += double(v) * v;
+      lmin[i] = fminf(lmin[i], v);
+      lmax[i] = fmaxf(lmax[i], v);
+    }
+  }
+  for (int i = 0; i < 18; ++i) s[i][threadIdx.x] = loc[i];
+  for (int i = 0; i < 9; ++i) {
+    mn[i][threadIdx.x] = lmin[i];
+    mx[i][threadIdx.x] = lmax[i];
+  }
+  __syncthreads();
+  if (threadIdx.x < 18) {
+    double v = 0;
+    for (int j = 0; j < 128; ++j) v += s[threadIdx.x][j];
+    atomicAdd(&acc[threadIdx.x], v);
+  } else if (threadIdx.x >= 32 && threadIdx.x < 41) {
+    const int i = threadIdx.x - 32;
+    float a = 3.0e38f, b = -3.0e38f;
+    for (int j = 0; j < 128; ++j) {
+      a = fminf(a, mn[i][j]);
+      b = fmaxf(b, mx[i][j]);
+    }
+    // order-preserving float -> int for atomic min/max
+    int ia = __float_as_int(a), ib = __float_as_int(b);
+    ia = ia >= 0 ? ia : ia ^ 0x7fffffff;
+    ib = ib >= 0 ? ib : ib ^ 0x7fffffff;
+    atomicMin(reinterpret_cast<int*>(&acc[18 + i]), ia);
+    atomicMax(reinterpret_cast<int*>(&acc[27 + i]), ib);
+  }
+}
+
+__global__ void k_mlp_normalize(float* x, float* t, long n, const float* stats) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    for (int i = 0; i < 8; ++i) x[q * 8 + i] = (x[q * 8 + i] - stats[MLP_S_MU + i]) / stats[MLP_S_SD + i];
+    t[q] = (t[q] - stats[MLP_S_YMU]) / stats[MLP_S_YSD];
+  }
+}
+
+// ---------------------------------------------------------- packing ----
+__global__ void k_mlp_pack(const float* p, uint16_t* img) {
+  unsigned char* base = reinterpret_cast<unsigned char*>(img);
+  for (int i = threadIdx.x; i < 64 * 16; i += blockDim.x) {  // B1[n][k] = W1[k][n], k < 8
+    const int n = i / 16, k = i % 16;
+    const float v = (k < MLP_IN) ? p[MLP_O_W1 + k * MLP_H + n] : 0.0f;
+    *reinterpret_cast<uint16_t*>(base + IMG_B1 + kmaj_off(n, k, 256)) = bf16_bits(v);
+  }
+  for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) {
+    const int r = i / 64, c = i % 64;
+    const float w = p[MLP_O_W2 + r * MLP_H + c];  // W2[k=r][n=c]
+    *reinterpret_cast<uint16_t*>(base + IMG_B2 + kmaj_off(c, r, 1024)) = bf16_bits(w);   // B2[n][k]
+    *reinterpret_cast<uint16_t*>(base + IMG_B2T + kmaj_off(r, c, 1024)) = bf16_bits(w);  // B2T[k][n]
+  }
+}
+
+// -------------------------------------------------- shared tile layout ----
+struct __align__(1024) MlpSmem {
+  unsigned char A1[TILE * 16 * 2];   // 4 KB  features (K-major, sbo 256)
+  unsigned char A2[TILE * 64 * 2];   // 16 KB h1 (K-major, sbo 1024)
+  unsigned char G2[TILE * 64 * 2];   // 16 KB g2 (training: A of g2 . W2^T)
+  unsigned char B1[2048];
+  unsigned char B2[8192];
+  unsigned char B2T[8192];
+  float b1[64], b2[64], w3[64];
+  float stats[MLP_NS];
+  float b3;
+  uint64_t mbar;
+  uint32_t tmem;
+  int ok;
+};
+
+__device__ __forceinline__ void load_images(MlpSmem& S, const uint16_t* img, const float* p, const float* stats,
+                                            bool with_b2t) {
+  const uint4* src = reinterpret_cast<const uint4*>(img);
+  uint4* d1 = reinterpret_cast<uint4*>(S.B1);
+  for (int i = threadIdx.x; i < 2048 / 16; i += blockDim.x) d1[i] = src[i];
+  uint4* d2 = reinterpret_cast<uint4*>(S.B2);
+  for (int i = threadIdx.x; i < 8192 / 16; i += blockDim.x) d2[i] = src[2048 / 16 + i];
+  if (with_b2t) {
+    uint4* d3 = reinterpret_cast<uint4*>(S.B2T);
+    for (int i = threadIdx.x; i < 8192 / 16; i += blockDim.x) d3[i] = src[(2048 + 8192) / 16 + i];
+  }
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+    S.b1[i] = p[MLP_O_B1 + i];
+    S.b2[i] = p[MLP_O_B2 + i];
+    S.w3[i] = p[MLP_O_W3 + i];
+  }
+  for (int i = threadIdx.x; i < MLP_NS; i += blockDim.x) S.stats[i] = stats[i];
+  if (threadIdx.x == 0) S.b3 = p[MLP_O_B3];
+}
+
+// write this thread's 8 normalised features as row `row` of A1
+__device__ __forceinline__ void put_features(MlpSmem& S, int row, const float* x) {
+  uint4 c0, c1;
+  uint16_t h[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) h[i] = bf16_bits(x[i]);
+  c0.x = h[0] | (uint32_t(h[1]) << 16);
+  c0.y = h[2] | (uint32_t(h[3]) << 16);
+  c0.z = h[4] | (uint32_t(h[5]) << 16);
+  c0.w = h[6] | (uint32_t(h[7]) << 16);
+  c1 = make_uint4(0, 0, 0, 0);
+  *reinterpret_cast<uint4*>(S.A1 + kmaj_off(row, 0, 256)) = c0;
+  *reinterpret_cast<uint4*>(S.A1 + kmaj_off(row, 8, 256)) = c1;
+}
+
+// write 64 values as row `row` of a K-major (sbo 1024) BF16 tile
+__device__ __forceinline__ void put_row64(unsigned char* tile, int row, const float* v) {
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    uint4 q;
+    q.x = bf16_bits(v[8 * c + 0]) | (uint32_t(bf16_bits(v[8 * c + 1])) << 16);
+    q.y = bf16_bits(v[8 * c + 2]) | (uint32_t(bf16_bits(v[8 * c + 3])) << 16);
+    q.z = bf16_bits(v[8 * c + 4]) | (uint32_t(bf16_bits(v[8 * c + 5])) << 16);
+    q.w = bf16_bits(v[8 * c + 6]) | (uint32_t(bf16_bits(v[8 * c + 7])) << 16);
+    *reinterpret_cast<uint4*>(tile + kmaj_off(row, 8 * c, 1024)) = q;
+  }
+}
+__device__ __forceinline__ float tile_val(const unsigned char* tile, int row, int k, int sbo) {
+  const uint16_t b = *reinterpret_cast<const uint16_t*>(tile + kmaj_off(row, k, sbo));
+  return __uint_as_float(uint32_t(b) << 16);
+}
+
+// 64 TMEM columns of this thread's lane starting at column col
+__device__ __forceinline__ void tmem_row64(uint32_t tbase, int col, float* v) {
+  const uint32_t lane = uint32_t((threadIdx.x / 32) * 32) << 16;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) tc::tmem_ld16(tbase + lane + uint32_t(col + 16 * j), v + 16 * j);
+  tc::tmem_wait_ld();
+}
+
+// issue one tensor-core stage (thread 0) and wait for it (bounded);
+// returns false (and flags the status) when the wait ran out
+__device__ __forceinline__ bool tc_stage(MlpSmem& S, uint32_t& phase, unsigned* status, int which) {
+  if (threadIdx.x == 0) {
+    tc::fence_after_sync();
+    const uint32_t a1 = tc::smem_u32(S.A1), a2 = tc::smem_u32(S.A2), g2 = tc::smem_u32(S.G2);
+    const uint32_t b1 = tc::smem_u32(S.B1), b2 = tc::smem_u32(S.B2), b2t = tc::smem_u32(S.B2T);
+    if (which == 0) {  // D1 = X . W1
+      tc::mma_bf16(S.tmem + 0, tc::smem_desc(a1, 128, 256), tc::smem_desc(b1, 128, 256), IDESC, 0);
+    } else if (which == 1) {  // D2 = H1 . W2
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+        tc::mma_bf16(S.tmem + 64, tc::smem_desc(a2 + 256 * s, 128, 1024), tc::smem_desc(b2 + 256 * s, 128, 1024),
+                     IDESC, s > 0);
+    } else {  // D3 = G2 . W2^T
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+        tc::mma_bf16(S.tmem + 128, tc::smem_desc(g2 + 256 * s, 128, 1024), tc::smem_desc(b2t + 256 * s, 128, 1024),
+                     IDESC, s > 0);
+    }
+    tc::mma_commit(&S.mbar);
+    S.ok = tc::mbar_wait(&S.mbar, phase) ? 1 : 0;
+    if (!S.ok) atomicOr(status, 16u);
+  }
+  phase ^= 1u;
+  __syncthreads();
+  tc::fence_after_sync();
+  return S.ok != 0;
+}
+
+__device__ __forceinline__ void tc_setup(MlpSmem& S, uint32_t ncols) {
+  if (threadIdx.x < 32) {
+    tc::tmem_alloc(&S.tmem, ncols);
+    tc::tmem_relinquish();
+  }
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&S.mbar, 1);
+    tc::fence_mbar_init();
+  }
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+}
+__device__ __forceinline__ void tc_teardown(MlpSmem& S, uint32_t ncols, uint32_t phase) {
+  // after a timed-out stage, wait (bounded) for the MMA still in flight
+  if (threadIdx.x == 0 && !S.ok) tc::mbar_wait(&S.mbar, phase ^ 1u);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (threadIdx.x < 32) tc::tmem_dealloc(S.tmem, ncols);
+}
+
+// ------------------------------------------------------------ inference ----
+template <typename T>
+__global__ void __launch_bounds__(TILE) k_mlp_infer(const MlpFeatIn<T> a, T* cs, MlpDevice m, unsigned* status) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  MlpSmem& S = *reinterpret_cast<MlpSmem*>(smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023));
+  load_images(S, m.img, m.params, m.stats, false);
+  if (threadIdx.x == 0) S.ok = 1;
+  tc_setup(S, 128);
+  uint32_t phase = 0;
+  const long npts = (long)(a.nz + 1) * a.plane;
+  const long ntiles = (npts + TILE - 1) / TILE;
+  for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long q = tile * TILE + threadIdx.x;
+    const bool valid = q < npts;
+    float x[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long o = 0;
+    if (valid) {
+      o = a.plane + q;
+      const int k = int(o / a.plane);
+      float t[8];
+      raw_features(a, o, k, t);
+      bool out = false;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        x[i] = (t[i] - S.stats[MLP_S_MU + i]) / S.stats[MLP_S_SD + i];
+        out |= (x[i] < S.stats[MLP_S_MIN + i] - 0.25f) || (x[i] > S.stats[MLP_S_MAX + i] + 0.25f);
+      }
+      if (out) m.colflag[q % a.plane] = 1;
+    }
+    put_features(S, threadIdx.x, x);
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (!tc_stage(S, phase, status, 0)) break;
+    float h[64];
+    tmem_row64(S.tmem, 0, h);
+#pragma unroll
+    for (int i = 0; i < 64; ++i) h[i] = gelu(h[i] + S.b1[i]);
+    put_row64(S.A2, threadIdx.x, h);
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (!tc_stage(S, phase, status, 1)) break;
+    tmem_row64(S.tmem, 64, h);
+    float y = S.b3;
+#pragma unroll
+    for (int i = 0; i < 64; ++i) y += S.w3[i] * gelu(h[i] + S.b2[i]);
+    if (valid) {
+      const float lc = S.stats[MLP_S_YMU] + S.stats[MLP_S_YSD] * y;
+      cs[o] = T(fminf(fmaxf(expf(lc), 1e-24f), 1.0f));
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+  }
+  tc_teardown(S, 128, phase);
+}
+
+// ------------------------------------------------------------- training ----
+// One launch: each CTA loops over tiles of samples [tile*128, +128) < n,
+// forward + backward; per-thread gradient accumulators are added to
+// m.grad once per CTA.  Gradient of L = mean_i (y_i - t_i)^2 with inv_n = 1/n.
+struct TrainSmem {
+  MlpSmem s;
+  float red[TILE][65];  // h2, then delta1 (fp32 rows)
+  float g2f[TILE][65];  // g2 (fp32 rows)
+  float xf[TILE][8];
+  float dy[TILE];
+};
+
+__global__ void __launch_bounds__(TILE) k_mlp_train(MlpDevice m, const float* X, const float* Tg, long n,
+                                                    float inv_n, float* y_out, float* loss, unsigned* status) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  TrainSmem& TS = *reinterpret_cast<TrainSmem*>(smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023));
+  MlpSmem& S = TS.s;
+  load_images(S, m.img, m.params, m.stats, true);
+  if (threadIdx.x == 0) S.ok = 1;
+  tc_setup(S, 256);
+  const int tid = threadIdx.x;
+  // gradient ownership: dW2 entries k = tid/2, n in [32*(tid%2), +32); dW1
+  // entries f = tid/16, k in [4*(tid%16), +4); biases / w3 by tid < 64
+  float aw2[32], aw1[4];
+  for (int i = 0; i < 32; ++i) aw2[i] = 0.0f;
+  for (int i = 0; i < 4; ++i) aw1[i] = 0.0f;
+  float ab1 = 0.0f, ab2 = 0.0f, aw3 = 0.0f, ab3 = 0.0f, aloss = 0.0f;
+  uint32_t phase = 0;
+  const long ntiles = (n + TILE - 1) / TILE;
+  for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long q = tile * TILE + tid;
+    const bool valid = q < n;
+    float x[8];
+    for (int i = 0; i < 8; ++i) x[i] = valid ? X[q * 8 + i] : 0.0f;
+    const float tg = valid ? Tg[q] : 0.0f;
+    put_features(S, tid, x);
+    for (int i = 0; i < 8; ++i) TS.xf[tid][i] = tile_val(S.A1, tid, i, 256);  // bf16-rounded inputs
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (!tc_stage(S, phase, status, 0)) break;
+    float z1[64], h[64];
+    tmem_row64(S.tmem, 0, z1);
+#pragma unroll
+    for (int i = 0; i < 64; ++i) {
+      z1[i] += S.b1[i];
+      h[i] = gelu(z1[i]);
+    }
+    put_row64(S.A2, tid, h);
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (!tc_stage(S, phase, status, 1)) break;
+    tmem_row64(S.tmem, 64, h);  // z2 (without bias)
+    float y = S.b3;
+    for (int i = 0; i < 64; ++i) {
+      h[i] += S.b2[i];  // z2
+      y += S.w3[i] * gelu(h[i]);
+    }
+    if (y_out && valid) y_out[q] = y;
+    const float dy = valid ? 2.0f * (y - tg) * inv_n : 0.0f;
+    if (valid) aloss += (y - tg) * (y - tg) * inv_n;
+    TS.dy[tid] = dy;
+    float g2[64];
+    for (int i = 0; i < 64; ++i) {
+      TS.red[tid][i] = gelu(h[i]);          // h2
+      g2[i] = dy * S.w3[i] * gelu_grad(h[i]);
+      TS.g2f[tid][i] = g2[i];
+    }
+    put_row64(S.G2, tid, g2);
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    // dw3, db3, db2 (row reductions over the tile)
+    if (tid < 64) {
+      float s3 = 0.0f, s2 = 0.0f;
+      for (int r = 0; r < TILE; ++r) {
+        s3 += TS.dy[r] * TS.red[r][tid];
+        s2 += TS.g2f[r][tid];
+      }
+      aw3 += s3;
+      ab2 += s2;
+    } else if (tid == 64) {
+      float s = 0.0f;
+      for (int r = 0; r < TILE; ++r) s += TS.dy[r];
+      ab3 += s;
+    }
+    // dW2[k][n] = sum_r h1[r][k] g2[r][n] (h1 as the BF16 values layer 2 used)
+    {
+      const int kk = tid >> 1, n0 = (tid & 1) * 32;
+      for (int r = 0; r < TILE; ++r) {
+        const float hv = tile_val(S.A2, r, kk, 1024);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) aw2[i] += hv * TS.g2f[r][n0 + i];
+      }
+    }
+    if (!tc_stage(S, phase, status, 2)) break;
+    // delta1 = (g2 . W2^T) * gelu'(z1)
+    float d1[64];
+    tmem_row64(S.tmem, 128, d1);
+    for (int i = 0; i < 64; ++i) TS.red[tid][i] = d1[i] * gelu_grad(z1[i]);
+    __syncthreads();
+    if (tid < 64) {
+      float s = 0.0f;
+      for (int r = 0; r < TILE; ++r) s += TS.red[r][tid];
+      ab1 += s;
+    }
+    {
+      const int f = tid >> 4, k0 = (tid & 15) * 4;
+      for (int r = 0; r < TILE; ++r) {
+        const float xv = TS.xf[r][f];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) aw1[i] += xv * TS.red[r][k0 + i];
+      }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+  }
+  tc_teardown(S, 256, phase);
+  {
+    const int kk = tid >> 1, n0 = (tid & 1) * 32;
+    for (int i = 0; i < 32; ++i) atomicAdd(&m.grad[MLP_O_W2 + kk * MLP_H + n0 + i], aw2[i]);
+    const int f = tid >> 4, k0 = (tid & 15) * 4;
+    for (int i = 0; i < 4; ++i) atomicAdd(&m.grad[MLP_O_W1 + f * MLP_H + k0 + i], aw1[i]);
+    if (tid < 64) {
+      atomicAdd(&m.grad[MLP_O_B1 + tid], ab1);
+      atomicAdd(&m.grad[MLP_O_B2 + tid], ab2);
+      atomicAdd(&m.grad[MLP_O_W3 + tid], aw3);
+    }
+    if (tid == 64) atomicAdd(&m.grad[MLP_O_B3], ab3);
+    // loss: warp reduce then one atomic per warp
+    for (int off = 16; off > 0; off >>= 1) aloss += __shfl_down_sync(0xffffffffu, aloss, off);
+    if ((tid & 31) == 0 && loss) atomicAdd(loss, aloss);
+  }
+}
+
+__global__ void k_mlp_adam(float* p, const float* g, float* mm, float* vv, int step, float lr) {
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  const float c1 = 1.0f - powf(b1, float(step)), c2 = 1.0f - powf(b2, float(step));
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < MLP_NP; i += gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    mm[i] = b1 * mm[i] + (1.0f - b1) * gi;
+    vv[i] = b2 * vv[i] + (1.0f - b2) * gi * gi;
+    p[i] -= lr * (mm[i] / c1) / (sqrtf(vv[i] / c2) + eps);
+  }
+}
+
+__global__ void k_mlp_count_flags(const int* flag, long plane, int* out) {
+  int c = 0;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < plane; q += (long)gridDim.x * blockDim.x) c += flag[q];
+  for (int off = 16; off > 0; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+template <typename T>
+__global__ void k_mlp_blend(T* cs, const T* cs_dyn, const int* flag, long plane, int nz, double* err2, int check) {
+  const long n = (long)(nz + 1) * plane;
+  double e = 0.0;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long o = plane + q;
+    if (check) {
+      const double d = log(fmax(double(cs[o]), 1e-6)) - log(fmax(double(cs_dyn[o]), 1e-6));
+      e += d * d;
+    }
+    if (flag[q % plane]) cs[o] = cs_dyn[o];
+  }
+  if (check) {
+    for (int off = 16; off > 0; off >>= 1) e += __shfl_down_sync(0xffffffffu, e, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(err2, e);
+  }
+}
+
+size_t infer_smem() { return sizeof(MlpSmem) + 1024; }
+size_t train_smem() { return sizeof(TrainSmem) + 1024; }
+
+}  // namespace
+
+// ------------------------------------------------------------- host side ----
+template <typename T>
+void mlp_collect(const MlpFeatIn<T>& in, const T* cs, MlpDevice& m, int stride, unsigned seed, cudaStream_t st) {
+  const long n = (long)(in.nz + 1) * in.plane;
+  hook_before("k_mlp_collect", double(n) * 12 * sizeof(T));
+  k_mlp_collect<T><<<148 * 8, 256, 0, st>>>(in, cs, m, stride, seed);
+  LES_CHECK_LAUNCH();
+  hook_after();
+}
+
+template <typename T>
+void mlp_infer(const MlpFeatIn<T>& in, T* cs, MlpDevice& m, unsigned* status, cudaStream_t st) {
+  LES_CUDA(cudaMemsetAsync(m.colflag, 0, sizeof(int) * m.plane, st));
+  const long n = (long)(in.nz + 1) * in.plane;
+  const long ntiles = (n + TILE - 1) / TILE;
+  const int grid = int(std::min<long>(ntiles, 148L * 4));
+  hook_before("k_mlp_infer", double(n) * 12 * sizeof(T));
+  k_mlp_infer<T><<<grid, TILE, infer_smem(), st>>>(in, cs, m, status);
+  LES_CHECK_LAUNCH();
+  hook_after();
+}
+
+void init_mlp_attributes() {
+  LES_CUDA(cudaFuncSetAttribute(k_mlp_infer<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem()));
+  LES_CUDA(cudaFuncSetAttribute(k_mlp_infer<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem()));
+  LES_CUDA(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem()));
+}
+
+void mlp_pack(MlpDevice& m, cudaStream_t st) {
+  hook_before("k_mlp_pack", double(MLP_NP) * 4 + IMG_BYTES);
+  k_mlp_pack<<<1, 256, 0, st>>>(m.params, m.img);
+  LES_CHECK_LAUNCH();
+  hook_after();
+}
+
+void mlp_grad(MlpDevice& m, const float* x, const float* t, long n, float* y_out, float* loss_dev, unsigned* status,
+              cudaStream_t st) {
+  LES_CUDA(cudaMemsetAsync(m.grad, 0, sizeof(float) * MLP_NP, st));
+  if (loss_dev) LES_CUDA(cudaMemsetAsync(loss_dev, 0, sizeof(float), st));
+  const long ntiles = (n + TILE - 1) / TILE;
+  const int grid = int(std::max<long>(1, std::min<long>(ntiles, 148L)));
+  hook_before("k_mlp_train", double(n) * 36.0);
+  k_mlp_train<<<grid, TILE, train_smem(), st>>>(m, x, t, n, 1.0f / float(n), y_out, loss_dev, status);
+  LES_CHECK_LAUNCH();
+  hook_after();
+}
+
+void mlp_adam(MlpDevice& m, int step, float lr, cudaStream_t st) {
+  hook_before("k_mlp_adam", double(MLP_NP) * 20);
+  k_mlp_adam<<<19, 256, 0, st>>>(m.params, m.grad, m.adam_m, m.adam_v, step, lr);
+  LES_CHECK_LAUNCH();
+  hook_after();
+  mlp_pack(m, st);
+}
+
+void mlp_fit_stats(MlpDevice& m, cudaStream_t st) {
+  unsigned long long cnt[2];
+  LES_CUDA(cudaMemcpyAsync(cnt, m.counts, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+  LES_CUDA(cudaStreamSynchronize(st));
+  const long nt = std::min<long>((long)cnt[0], m.cap), nv = std::min<long>((long)cnt[1], m.cap);
+  if (nt < 2) throw CudaError(1, "learned closure: no training data collected");
+  double* acc = nullptr;
+  LES_CUDA(cudaMalloc(&acc, 36 * sizeof(double)));
+  std::vector<double> init(36, 0.0);
+  // min slots start at +max, max slots at -max (order-preserving ints)
+  for (int i = 0; i < 9; ++i) {
+    int big = 0x7f7fffff, neg = int(0xff7fffffu) ^ 0x7fffffff;
+    std::memcpy(&init[18 + i], &big, sizeof(int));
+    std::memcpy(&init[27 + i], &neg, sizeof(int));
+  }
+  LES_CUDA(cudaMemcpyAsync(acc, init.data(), 36 * sizeof(double), cudaMemcpyHostToDevice, st));
+  k_mlp_stats<<<148, 128, 0, st>>>(m.dx, m.dt, nt, acc);
+  LES_CHECK_LAUNCH();
+  std::vector<double> h(36);
+  LES_CUDA(cudaMemcpyAsync(h.data(), acc, 36 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  LES_CUDA(cudaStreamSynchronize(st));
+  cudaFree(acc);
+  float s[MLP_NS];
+  auto unorder = [](double slot) {
+    int iv;
+    std::memcpy(&iv, &slot, sizeof(int));
+    iv = iv >= 0 ? iv : iv ^ 0x7fffffff;
+    float f;
+    std::memcpy(&f, &iv, sizeof(float));
+    return f;
+  };
+  for (int i = 0; i < 9; ++i) {
+    const double mean = h[2 * i] / double(nt);
+    double var = h[2 * i + 1] / double(nt) - mean * mean;
+    double sd = var > 1e-12 ? std::sqrt(var) : 1.0;
+    const float mn = unorder(h[18 + i]), mx = unorder(h[27 + i]);
+    if (i < 8) {
+      s[MLP_S_MU + i] = float(mean);
+      s[MLP_S_SD + i] = float(sd);
+      s[MLP_S_MIN + i] = float((mn - mean) / sd);
+      s[MLP_S_MAX + i] = float((mx - mean) / sd);
+    } else {
+      s[MLP_S_YMU] = float(mean);
+      s[MLP_S_YSD] = float(sd);
+    }
+  }
+  LES_CUDA(cudaMemcpyAsync(m.stats, s, sizeof(s), cudaMemcpyHostToDevice, st));
+  k_mlp_normalize<<<148 * 4, 256, 0, st>>>(m.dx, m.dt, nt, m.stats);
+  LES_CHECK_LAUNCH();
+  if (nv > 0) {
+    k_mlp_normalize<<<148 * 4, 256, 0, st>>>(m.vx, m.vt, nv, m.stats);
+    LES_CHECK_LAUNCH();
+  }
+  LES_CUDA(cudaStreamSynchronize(st));
+}
+
+int mlp_count_flags(MlpDevice& m, int* dcount, cudaStream_t st) {
+  LES_CUDA(cudaMemsetAsync(dcount, 0, sizeof(int), st));
+  hook_before("k_mlp_count_flags", double(m.plane) * 4);
+  k_mlp_count_flags<<<148, 256, 0, st>>>(m.colflag, m.plane, dcount);
+  LES_CHECK_LAUNCH();
+  hook_after();
+  int h = 0;
+  LES_CUDA(cudaMemcpyAsync(&h, dcount, sizeof(int), cudaMemcpyDeviceToHost, st));
+  LES_CUDA(cudaStreamSynchronize(st));
+  return h;
+}
+
+template <typename T>
+double mlp_blend(T* cs, const T* cs_dyn, MlpDevice& m, int nz, bool check, double* derr, cudaStream_t st) {
+  LES_CUDA(cudaMemsetAsync(derr, 0, sizeof(double), st));
+  const long n = (long)(nz + 1) * m.plane;
+  hook_before("k_mlp_blend", double(n) * 3 * sizeof(T));
+  k_mlp_blend<T><<<148 * 4, 256, 0, st>>>(cs, cs_dyn, m.colflag, m.plane, nz, derr, check ? 1 : 0);
+  LES_CHECK_LAUNCH();
+  hook_after();
+  double h = 0;
+  if (check) {
+    LES_CUDA(cudaMemcpyAsync(&h, derr, sizeof(double), cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+    h = std::sqrt(h / double(n));
+  }
+  return h;
+}
+template double mlp_blend<float>(float*, const float*, MlpDevice&, int, bool, double*, cudaStream_t);
+template double mlp_blend<double>(double*, const double*, MlpDevice&, int, bool, double*, cudaStream_t);
+
+template void mlp_collect<float>(const MlpFeatIn<float>&, const float*, MlpDevice&, int, unsigned, cudaStream_t);
+template void mlp_collect<double>(const MlpFeatIn<double>&, const double*, MlpDevice&, int, unsigned, cudaStream_t);
+template void mlp_infer<float>(const MlpFeatIn<float>&, float*, MlpDevice&, unsigned*, cudaStream_t);
+template void mlp_infer<double>(const MlpFeatIn<double>&, double*, MlpDevice&, unsigned*, cudaStream_t);
+
+}  // namespace les

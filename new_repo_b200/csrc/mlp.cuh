@@ -1,0 +1,80 @@
+// Learned SGS closure: 8 resolved invariants -> 64 -> 64 -> Cs^2 (GELU),
+// BF16 weights with FP32 accumulation on the tcgen05 tensor cores.
+#pragma once
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace les {
+
+constexpr int MLP_IN = 8;
+constexpr int MLP_H = 64;
+// flat FP32 parameter vector: W1[8][64], b1[64], W2[64][64], b2[64], w3[64], b3
+constexpr int MLP_O_W1 = 0;
+constexpr int MLP_O_B1 = MLP_O_W1 + MLP_IN * MLP_H;
+constexpr int MLP_O_W2 = MLP_O_B1 + MLP_H;
+constexpr int MLP_O_B2 = MLP_O_W2 + MLP_H * MLP_H;
+constexpr int MLP_O_W3 = MLP_O_B2 + MLP_H;
+constexpr int MLP_O_B3 = MLP_O_W3 + MLP_H;
+constexpr int MLP_NP = MLP_O_B3 + 1;  // 4801 trainable parameters
+// statistics: feature mean[8], std[8], min[8], max[8] (normalised units),
+// target mean, target std
+constexpr int MLP_S_MU = 0, MLP_S_SD = 8, MLP_S_MIN = 16, MLP_S_MAX = 24, MLP_S_YMU = 32, MLP_S_YSD = 33;
+constexpr int MLP_NS = 34;
+constexpr float MLP_LOG_CS_FLOOR = -13.815510557964274f;  // log(1e-6): targets below are clamped
+
+// inputs of the feature function (the state's gradients and velocity)
+template <typename T>
+struct MlpFeatIn {
+  const T* d[9];  // dudx dudy dudz dvdx dvdy dvdz dwdx dwdy dwdz
+  const T* u;
+  const T* v;
+  long plane;
+  int nz;
+  int wall;
+  float dz, delta, log_delta_z0;
+};
+
+struct MlpDevice {
+  float* params = nullptr;     // MLP_NP master weights
+  float* stats = nullptr;      // MLP_NS
+  uint16_t* img = nullptr;     // packed BF16 operand images: B1 (2 KB), B2 (8 KB), B2T (8 KB)
+  float* grad = nullptr;       // MLP_NP
+  float* adam_m = nullptr;
+  float* adam_v = nullptr;
+  float* dx = nullptr;         // training features (normalised) [cap][8]
+  float* dt = nullptr;         // training targets (normalised) [cap]
+  float* vx = nullptr;         // validation features
+  float* vt = nullptr;
+  unsigned long long* counts = nullptr;  // [0] train, [1] validation
+  long cap = 0;
+  float* scratch = nullptr;    // forward outputs of the host-features path
+  int* colflag = nullptr;      // per (i,j) column: 1 = features left the training range
+  long plane = 0;
+};
+
+// feature transforms shared by inference and data collection
+template <typename T>
+void mlp_collect(const MlpFeatIn<T>& in, const T* cs, MlpDevice& m, int stride, unsigned seed, cudaStream_t st);
+template <typename T>
+void mlp_infer(const MlpFeatIn<T>& in, T* cs, MlpDevice& m, unsigned* status, cudaStream_t st);
+// statistics of the collected raw data, then normalisation in place
+void mlp_fit_stats(MlpDevice& m, cudaStream_t st);
+// opt the tensor-core kernels in to their shared-memory sizes (current device)
+void init_mlp_attributes();
+// pack the BF16 operand images from the FP32 master weights
+void mlp_pack(MlpDevice& m, cudaStream_t st);
+// one optimisation pass: gradients of the mean squared error over the
+// samples [first, first + n) of a buffer (x [n][8], t [n]) into m.grad;
+// with y_out != nullptr also writes the network outputs (normalised).
+void mlp_grad(MlpDevice& m, const float* x, const float* t, long n, float* y_out, float* loss_dev, unsigned* status,
+              cudaStream_t st);
+void mlp_adam(MlpDevice& m, int step, float lr, cudaStream_t st);
+// number of (i,j) columns flagged out of the training range by the last inference
+int mlp_count_flags(MlpDevice& m, int* dcount, cudaStream_t st);
+// replace flagged columns of cs by cs_dyn; with check, returns the RMS of
+// log(cs) - log(cs_dyn) over all points (both floored at 1e-6)
+template <typename T>
+double mlp_blend(T* cs, const T* cs_dyn, MlpDevice& m, int nz, bool check, double* derr, cudaStream_t st);
+
+}  // namespace les

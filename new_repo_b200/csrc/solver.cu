@@ -8,6 +8,9 @@
 #include <type_traits>
 
 #include "kernels.cuh"
+#include "mlp.cuh"
+#include <algorithm>
+#include <random>
 #include "launch.cuh"
 #include "solver.cuh"
 
@@ -342,6 +345,243 @@ class Solver final : public SolverBase {
   void check_field(int field, int k0, int k1) const {
     if (field < 0 || field >= LES_NFIELDS) throw CudaError(1, "invalid field id");
     if (k0 < 0 || k1 > g.nz + 1 || k1 < k0) throw CudaError(1, "invalid level range");
+  }
+
+  // ------------------------------------------------------ learned closure ----
+  MlpDevice md;
+  bool mlp_alloc = false, mlp_ready = false;
+  long mlp_updates = 0;
+  int mlp_check_every = 10;  // dynamic-procedure check every 10 updates (50 steps at cs_count 5)
+  double mlp_last_err = -1.0;
+  int mlp_last_flags = 0;
+  int* dcount = nullptr;
+  double* derr = nullptr;
+  int mlp_adam_step = 0;
+
+  void ensure_mlp() {
+    if (mlp_alloc) return;
+    md.params = track(dalloc<float>(MLP_NP));
+    md.stats = track(dalloc<float>(MLP_NS));
+    md.img = track(dalloc<uint16_t>(18432 / 2));
+    md.grad = track(dalloc<float>(MLP_NP));
+    md.adam_m = track(dalloc<float>(MLP_NP));
+    md.adam_v = track(dalloc<float>(MLP_NP));
+    md.colflag = track(dalloc<int>(g.plane()));
+    md.counts = track(dalloc<unsigned long long>(2));
+    md.plane = g.plane();
+    dcount = track(dalloc<int>(1));
+    derr = track(dalloc<double>(1));
+    init_mlp_attributes();
+    mlp_alloc = true;
+  }
+  MlpFeatIn<T> feat_in() {
+    MlpFeatIn<T> a;
+    const int d[9] = {LES_DUDX, LES_DUDY, LES_DUDZ, LES_DVDX, LES_DVDY, LES_DVDZ, LES_DWDX, LES_DWDY, LES_DWDZ};
+    for (int q = 0; q < 9; ++q) a.d[q] = F[d[q]];
+    a.u = F[LES_U];
+    a.v = F[LES_V];
+    a.plane = g.plane();
+    a.nz = g.nz;
+    a.wall = P.wall_law;
+    a.dz = float(dz());
+    a.delta = float(delta);
+    a.log_delta_z0 = float(std::log(delta / P.z0));
+    return a;
+  }
+  void set_sgs_model(int m) override {
+    if (m < LES_SGS_CST_SMAG || m > LES_SGS_MLP) throw CudaError(1, "Invalid SGS model");
+    P.sgs_model = m;
+    set_mixing_length();
+  }
+  void mlp_init(unsigned seed) override {
+    ensure_mlp();
+    std::mt19937 rng(seed);
+    std::vector<float> p(MLP_NP, 0.0f);
+    auto fill_w = [&](int off, int fin, int fout) {
+      std::normal_distribution<float> nd(0.0f, std::sqrt(2.0f / float(fin + fout)));
+      for (int i = 0; i < fin * fout; ++i) p[off + i] = nd(rng);
+    };
+    fill_w(MLP_O_W1, MLP_IN, MLP_H);
+    fill_w(MLP_O_W2, MLP_H, MLP_H);
+    fill_w(MLP_O_W3, MLP_H, 1);
+    std::vector<float> s(MLP_NS, 0.0f);
+    for (int i = 0; i < 8; ++i) {
+      s[MLP_S_SD + i] = 1.0f;
+      s[MLP_S_MIN + i] = -1e30f;
+      s[MLP_S_MAX + i] = 1e30f;
+    }
+    s[MLP_S_YMU] = std::log(0.03f);
+    s[MLP_S_YSD] = 1.0f;
+    std::vector<float> all(p);
+    all.insert(all.end(), s.begin(), s.end());
+    mlp_set_params(all.data(), MLP_NP + MLP_NS);
+    LES_CUDA(cudaMemsetAsync(md.adam_m, 0, sizeof(float) * MLP_NP, st));
+    LES_CUDA(cudaMemsetAsync(md.adam_v, 0, sizeof(float) * MLP_NP, st));
+    mlp_adam_step = 0;
+  }
+  void mlp_set_params(const float* p, int n) override {
+    if (n != MLP_NP + MLP_NS) throw CudaError(1, "learned closure: expected " + std::to_string(MLP_NP + MLP_NS) + " values");
+    ensure_mlp();
+    LES_CUDA(cudaMemcpyAsync(md.params, p, sizeof(float) * MLP_NP, cudaMemcpyHostToDevice, st));
+    LES_CUDA(cudaMemcpyAsync(md.stats, p + MLP_NP, sizeof(float) * MLP_NS, cudaMemcpyHostToDevice, st));
+    mlp_pack(md, st);
+    LES_CUDA(cudaStreamSynchronize(st));
+    mlp_ready = true;
+  }
+  void mlp_get_params(float* p, int n) override {
+    if (n != MLP_NP + MLP_NS) throw CudaError(1, "learned closure: expected " + std::to_string(MLP_NP + MLP_NS) + " values");
+    ensure_mlp();
+    LES_CUDA(cudaMemcpyAsync(p, md.params, sizeof(float) * MLP_NP, cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaMemcpyAsync(p + MLP_NP, md.stats, sizeof(float) * MLP_NS, cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+  }
+  void mlp_reset_data(long cap) override {
+    ensure_mlp();
+    if (cap != md.cap) {
+      for (float* q : {md.dx, md.dt, md.vx, md.vt})
+        if (q) {
+          cudaFree(q);
+          allocs.erase(std::remove(allocs.begin(), allocs.end(), (void*)q), allocs.end());
+        }
+      md.cap = cap;
+      md.dx = track(dalloc<float>(cap * MLP_IN));
+      md.dt = track(dalloc<float>(cap));
+      md.vx = track(dalloc<float>(cap * MLP_IN));
+      md.vt = track(dalloc<float>(cap));
+    }
+    LES_CUDA(cudaMemsetAsync(md.counts, 0, 2 * sizeof(unsigned long long), st));
+    LES_CUDA(cudaStreamSynchronize(st));
+  }
+  void mlp_collect(int stride, unsigned seed) override {
+    if (!mlp_alloc || md.cap == 0) throw CudaError(1, "learned closure: call les_mlp_reset_data first");
+    Tag tag_(this, "mlp");
+    les::mlp_collect<T>(feat_in(), F[LES_CS_OPT2], md, std::max(1, stride), seed, st);
+  }
+  void mlp_counts(long long* c) override {
+    ensure_mlp();
+    unsigned long long h[2];
+    LES_CUDA(cudaMemcpyAsync(h, md.counts, sizeof(h), cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+    c[0] = std::min<long long>(h[0], md.cap);
+    c[1] = std::min<long long>(h[1], md.cap);
+  }
+  void mlp_fit_stats() override {
+    ensure_mlp();
+    les::mlp_fit_stats(md, st);
+  }
+  void mlp_train(int epochs, int tiles_per_step, double lr, double* loss_epochs, double* val_loss) override {
+    ensure_mlp();
+    Tag tag_(this, "mlp_train");
+    long long c[2];
+    mlp_counts(c);
+    const long ntr = c[0], nva = c[1];
+    if (ntr < 128) throw CudaError(1, "learned closure: not enough training data");
+    float* dloss = nullptr;
+    LES_CUDA(cudaMalloc(&dloss, 2 * sizeof(float)));
+    const long chunk = long(std::max(1, tiles_per_step)) * 128;
+    const long nsteps = (ntr + chunk - 1) / chunk;
+    long mult = 1000003 % nsteps;
+    auto gcdl = [](long a, long b) { while (b) { long t = a % b; a = b; b = t; } return a; };
+    if (mult == 0 || gcdl(mult, nsteps) != 1) mult = 1;
+    for (int ep = 0; ep < epochs; ++ep) {
+      double sum = 0.0;
+      for (long s = 0; s < nsteps; ++s) {
+        const long cidx = (s * mult + long(ep) * 7919) % nsteps;
+        const long off = cidx * chunk;
+        const long n = std::min(chunk, ntr - off);
+        LES_CUDA(cudaMemsetAsync(dloss, 0, sizeof(float), st));
+        mlp_grad(md, md.dx + off * MLP_IN, md.dt + off, n, nullptr, dloss, dstatus, st);
+        mlp_adam(md, ++mlp_adam_step, float(lr), st);
+        if (s == nsteps - 1 || (s % 64) == 0) {
+          float h = 0;
+          LES_CUDA(cudaMemcpyAsync(&h, dloss, sizeof(float), cudaMemcpyDeviceToHost, st));
+          LES_CUDA(cudaStreamSynchronize(st));
+          sum = h;  // loss of the latest batch
+        }
+      }
+      if (loss_epochs) loss_epochs[ep] = sum;
+    }
+    if (val_loss) {
+      *val_loss = -1.0;
+      if (nva > 0) {
+        LES_CUDA(cudaMemsetAsync(dloss, 0, sizeof(float), st));
+        mlp_grad(md, md.vx, md.vt, nva, nullptr, dloss, dstatus, st);
+        float h = 0;
+        LES_CUDA(cudaMemcpyAsync(&h, dloss, sizeof(float), cudaMemcpyDeviceToHost, st));
+        LES_CUDA(cudaStreamSynchronize(st));
+        *val_loss = h;
+      }
+    }
+    cudaFree(dloss);
+    mlp_ready = true;
+  }
+  void mlp_forward_host(const float* x, long n, float* y) override {
+    ensure_mlp();
+    float *dxx = nullptr, *dtt = nullptr, *dyy = nullptr;
+    LES_CUDA(cudaMalloc(&dxx, sizeof(float) * n * MLP_IN));
+    LES_CUDA(cudaMalloc(&dtt, sizeof(float) * n));
+    LES_CUDA(cudaMalloc(&dyy, sizeof(float) * n));
+    LES_CUDA(cudaMemcpyAsync(dxx, x, sizeof(float) * n * MLP_IN, cudaMemcpyHostToDevice, st));
+    LES_CUDA(cudaMemsetAsync(dtt, 0, sizeof(float) * n, st));
+    mlp_grad(md, dxx, dtt, n, dyy, nullptr, dstatus, st);
+    LES_CUDA(cudaMemcpyAsync(y, dyy, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+    cudaFree(dxx);
+    cudaFree(dtt);
+    cudaFree(dyy);
+  }
+  void mlp_grad_host(const float* x, const float* t, long n, float* gr, float* loss) override {
+    ensure_mlp();
+    float *dxx = nullptr, *dtt = nullptr, *dl = nullptr;
+    LES_CUDA(cudaMalloc(&dxx, sizeof(float) * n * MLP_IN));
+    LES_CUDA(cudaMalloc(&dtt, sizeof(float) * n));
+    LES_CUDA(cudaMalloc(&dl, sizeof(float)));
+    LES_CUDA(cudaMemcpyAsync(dxx, x, sizeof(float) * n * MLP_IN, cudaMemcpyHostToDevice, st));
+    LES_CUDA(cudaMemcpyAsync(dtt, t, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    LES_CUDA(cudaMemsetAsync(dl, 0, sizeof(float), st));
+    mlp_grad(md, dxx, dtt, n, nullptr, dl, dstatus, st);
+    LES_CUDA(cudaMemcpyAsync(gr, md.grad, sizeof(float) * MLP_NP, cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaMemcpyAsync(loss, dl, sizeof(float), cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+    cudaFree(dxx);
+    cudaFree(dtt);
+    cudaFree(dl);
+  }
+  void mlp_set_check_every(int every) override { mlp_check_every = every; }
+  void mlp_info(double* out) override {
+    out[0] = mlp_last_err;
+    out[1] = mlp_last_flags;
+    out[2] = double(mlp_updates);
+    out[3] = mlp_ready ? 1.0 : 0.0;
+  }
+
+  // Cs^2 from the learned closure at the dynamic-update cadence; columns whose
+  // invariants left the training range take the dynamic procedure's value,
+  // which also checks the closure every mlp_check_every updates.
+  void mlp_sgs(SgsArgs<T>& a, int jtt) {
+    Tag tag_(this, "mlp");
+    if (jtt < P.dyn_init) {
+      fill(F[LES_CS_OPT2], 1, g.nz + 1, T(0.03));
+      return;
+    }
+    if (jtt % P.cs_count != 0) return;
+    if (!mlp_ready) throw CudaError(1, "learned closure has no weights (train it or load parameters)");
+    les::mlp_infer<T>(feat_in(), F[LES_CS_OPT2], md, dstatus, st);
+    ++mlp_updates;
+    mlp_last_flags = mlp_count_flags(md, dcount, st);
+    const bool check = mlp_check_every > 0 && (mlp_updates % mlp_check_every) == 0;
+    if (mlp_last_flags > 0 || check) {
+      // dynamic procedure without Lagrangian history (F initialisation
+      // semantics), into scratch: cs -> sc[11]
+      dynamic_mum(a, true);
+      const long n1 = (long)(g.nz + 1) * g.plane();
+      KL("k_lasd_update", 14.0 * n1 * sizeof(T),
+         k_lasd_update<T><<<grid_for(n1), 256, 0, st>>>(sc[0], sc[12], sc[13], sc[14], sc[7], sc[8], sc[9], sc[10],
+                                                       sc[11], sc[1], 1, g.plane(), g.nz, 1.5 * delta,
+                                                       P.dt * double(P.cs_count), beta_pow));
+      const double e = mlp_blend<T>(F[LES_CS_OPT2], sc[11], md, g.nz, check, derr, st);
+      if (check) mlp_last_err = e;
+    }
   }
 
   double* staging = nullptr;  // FP64 device staging field (mixed precision transfers)
@@ -868,6 +1108,8 @@ class Solver final : public SolverBase {
       lasd(a, jtt);
     } else if (P.sgs_model == LES_SGS_DYN_SMAG) {
       dynsmag(a, jt, jtt);
+    } else if (P.sgs_model == LES_SGS_MLP) {
+      mlp_sgs(a, jtt);
     } else {
       throw CudaError(1, "Invalid SGS model");
     }

@@ -110,6 +110,20 @@ struct SolverBase : LaunchHook {
   virtual void read_timers() = 0;
   // pinned-host FP64 transfers on the state's stream (converted on device in
   // mixed precision); the caller synchronises
+  // learned closure (mlp.cu)
+  virtual void set_sgs_model(int model) = 0;
+  virtual void mlp_init(unsigned seed) = 0;
+  virtual void mlp_set_params(const float* p, int n) = 0;
+  virtual void mlp_get_params(float* p, int n) = 0;
+  virtual void mlp_reset_data(long cap) = 0;
+  virtual void mlp_collect(int stride, unsigned seed) = 0;
+  virtual void mlp_counts(long long* c) = 0;
+  virtual void mlp_fit_stats() = 0;
+  virtual void mlp_train(int epochs, int tiles_per_step, double lr, double* loss_epochs, double* val_loss) = 0;
+  virtual void mlp_forward_host(const float* x, long n, float* y) = 0;
+  virtual void mlp_grad_host(const float* x, const float* t, long n, float* g, float* loss) = 0;
+  virtual void mlp_info(double* out) = 0;
+  virtual void mlp_set_check_every(int every) = 0;
   virtual void upload_async(int field, const double* pinned, int k0, int k1) = 0;
   virtual void download_async(int field, double* pinned, int k0, int k1) = 0;
   virtual void diagnostics_async(double* pinned4) = 0;

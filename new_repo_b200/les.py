@@ -37,6 +37,7 @@ nonzero library status raises ``LesError`` carrying the same code
 """
 from __future__ import annotations
 
+import copy
 import ctypes as C
 import math
 import re
@@ -198,12 +199,16 @@ def _dptr(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
 class LES:
     """One device-resident LES state on one GPU."""
 
     def __init__(self, params: RunParams, precision: str = "fp64", device: int = 0):
         self.lib = capi.load()
-        self.params = params
+        self.params = copy.copy(params)  # set_sgs_model changes this instance's copy only
         self.precision = precision
         self._cp = params.to_c(precision, device)
         h = C.c_void_p()
@@ -391,6 +396,72 @@ class LES:
 
     def diagnostics_async(self, pinned_ptr: int):
         check(self.lib.les_diagnostics_async(self._h, C.c_void_p(pinned_ptr)))
+
+    # ------------------------------------------------------ learned closure
+    def set_sgs_model(self, name: str):
+        """Switch the SGS closure ('cst_Smag', 'dyn_Smag', 'dyn_LagScaleDep', 'mlp')."""
+        if name not in capi.SGS_MODELS:
+            raise LesError(1, f"Invalid SGS model {name!r}")
+        check(self.lib.les_set_sgs_model(self._h, capi.SGS_MODELS[name]))
+        self.params.sgs_model = name
+
+    def mlp_init(self, seed: int = 0):
+        check(self.lib.les_mlp_init(self._h, int(seed) & 0xFFFFFFFF))
+
+    def mlp_params(self) -> np.ndarray:
+        """Flat float32 vector: the 4801 weights then the 34 feature/target statistics."""
+        out = np.zeros(capi.MLP_NPARAM + capi.MLP_NSTATS, np.float32)
+        check(self.lib.les_mlp_get_params(self._h, _fptr(out), out.size))
+        return out
+
+    def mlp_set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        check(self.lib.les_mlp_set_params(self._h, _fptr(p), p.size))
+
+    def mlp_reset_data(self, cap: int):
+        check(self.lib.les_mlp_reset_data(self._h, int(cap)))
+
+    def mlp_collect(self, stride: int = 1, seed: int = 0):
+        check(self.lib.les_mlp_collect(self._h, int(stride), int(seed) & 0xFFFFFFFF))
+
+    def mlp_counts(self) -> tuple:
+        out = (C.c_longlong * 2)()
+        check(self.lib.les_mlp_counts(self._h, out))
+        return int(out[0]), int(out[1])
+
+    def mlp_fit_stats(self):
+        check(self.lib.les_mlp_fit_stats(self._h))
+
+    def mlp_train(self, epochs: int, tiles_per_step: int = 8, lr: float = 2e-3) -> tuple:
+        """Adam epochs on the collected pairs; returns (last-batch loss per epoch, validation loss)."""
+        losses = np.zeros(max(1, epochs))
+        val = C.c_double()
+        check(self.lib.les_mlp_train(self._h, int(epochs), int(tiles_per_step), float(lr), _dptr(losses),
+                                     C.byref(val)))
+        return losses[:epochs], float(val.value)
+
+    def mlp_forward(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros(x.shape[0], np.float32)
+        check(self.lib.les_mlp_forward(self._h, _fptr(x), x.shape[0], _fptr(y)))
+        return y
+
+    def mlp_grad(self, x, t) -> tuple:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.zeros(capi.MLP_NPARAM, np.float32)
+        loss = np.zeros(1, np.float32)
+        check(self.lib.les_mlp_grad(self._h, _fptr(x), _fptr(t), x.shape[0], _fptr(g), _fptr(loss)))
+        return g, float(loss[0])
+
+    def mlp_info(self) -> dict:
+        out = np.zeros(4)
+        check(self.lib.les_mlp_info(self._h, _dptr(out)))
+        return {"check_rms_log_error": float(out[0]), "flagged_columns": int(out[1]), "updates": int(out[2]),
+                "ready": bool(out[3])}
+
+    def mlp_set_check_every(self, every: int):
+        check(self.lib.les_mlp_set_check_every(self._h, int(every)))
 
     def state_dict(self, names=None) -> dict:
         names = capi.FIELDS if names is None else names
