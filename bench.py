@@ -290,26 +290,30 @@ def run_ours(args, dist, rank, local, ws):
         print(json.dumps(line), flush=True)
 
 
+EPOCHS = 4
+
+
 def train_closure(les, p, T: int) -> dict:
-    """Untimed: T LASD steps; the (invariants, log Cs^2) pairs of every update
-    step from step 10 on (one point in 8) train the closure on the GPU; the
-    state then continues with the learned closure."""
+    """Untimed: T LASD steps; the (features, log Cs^2) pairs of consecutive
+    update steps (one point in 8, every point of the 8 lowest levels; the
+    first update only records the coefficient) train the closure on the
+    GPU; the state then continues with the learned closure."""
     les.mlp_init(0)
-    les.mlp_reset_data(1 << 22)
+    les.mlp_reset_data(1 << 23)
     t0 = time.perf_counter()
     for _ in range(T):
         les.step(1)
-        if les.jt_total >= 10 and les.jt_total % p.cs_count == 0:
-            les.mlp_collect(stride=8, seed=les.jt_total)
+        if les.jt_total >= p.dyn_init and les.jt_total % p.cs_count == 0:  # consecutive updates
+            les.mlp_collect(stride=8, seed=les.jt_total, dense_levels=8)
     les.sync()
     t1 = time.perf_counter()
     ntr, nva = les.mlp_counts()
     les.mlp_fit_stats()
-    losses, val = les.mlp_train(epochs=2, tiles_per_step=16, lr=2e-3)
+    losses, val = les.mlp_train(epochs=EPOCHS, tiles_per_step=16, lr=2e-3)
     les.sync()
     t2 = time.perf_counter()
     les.set_sgs_model("mlp")
-    return {"lasd_steps": T, "train_pairs": ntr, "validation_pairs": nva, "epochs": 2,
+    return {"lasd_steps": T, "train_pairs": ntr, "validation_pairs": nva, "epochs": EPOCHS,
             "batch": 16 * 128, "train_loss": [round(float(x), 4) for x in losses],
             "validation_loss": round(val, 4), "collect_s": round(t1 - t0, 3), "train_s": round(t2 - t1, 3)}
 

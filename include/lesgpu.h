@@ -184,15 +184,18 @@ int les_download_async(les_state* s, int field, double* pinned, int k0, int k1);
 int les_diagnostics_async(les_state* s, double* pinned_out4);
 
 /* ---- learned SGS closure (no reference counterpart) ---------------------
- * Cs^2 = exp(net(invariants)) from an 8 -> 64 -> 64 -> 1 GELU network with
+ * Cs^2 = exp(net(features)) from an 8 -> 64 -> 64 -> 1 GELU network with
  * BF16 weights and FP32 accumulation (tcgen05 tensor cores), evaluated at
  * the dynamic-update cadence of compute_sgs.f90:171 (every cs_count steps
  * after dyn_init).  Training data are (invariants, log Cs^2) pairs of the
  * Lagrangian scale-dependent procedure (LASD, compute_sgs.f90:286) collected
- * from a running state.  Columns whose invariants leave the training range
- * fall back to the dynamic procedure; every `check_every` updates the
- * dynamic procedure also runs on the whole domain and the RMS of
- * log Cs^2 - log Cs^2_dyn is recorded.
+ * from a running state.  Features: log1p |S|, log1p S:S, log1p W:W, signed
+ * log1p tr(S^3), log1p(z / Delta), log Cs^2 before the update (the memory
+ * the Lagrangian averages carry), log1p |u_h|, log(Delta / z0).  Columns
+ * whose features leave the training range take one Lagrangian relaxation
+ * step of the dynamic procedure from the previous coefficient; every
+ * `check_every` updates that step also runs on the whole domain and the RMS
+ * of log Cs^2 - log Cs^2_dyn is recorded.
  * Parameters: float[LES_MLP_NPARAM + LES_MLP_NSTATS] = W1[8][64], b1[64],
  * W2[64][64], b2[64], w3[64], b3, then feature mean[8], std[8],
  * min[8], max[8] (normalised units), target mean, target std. */
@@ -204,9 +207,13 @@ int les_mlp_set_params(les_state* s, const float* params, int n);
 int les_mlp_get_params(les_state* s, float* params, int n);
 /* (re)allocate room for `cap` training and `cap` validation samples, empty */
 int les_mlp_reset_data(les_state* s, long cap);
-/* append the current state's (invariants, log cs_opt2) pairs, one point in
- * `stride` (seeded hash), 10 % of them to the validation set */
-int les_mlp_collect(les_state* s, int stride, unsigned seed);
+/* append the current state's (features, log cs_opt2) pairs, one point in
+ * `stride` (seeded hash) and every point of levels 1..dense_levels, 10 % of
+ * them to the validation set; pairs beyond the capacity are dropped.  Call
+ * it right after consecutive dynamic-update steps: the previous coefficient
+ * of a pair is the one the previous call saw (the first call only records
+ * it). */
+int les_mlp_collect(les_state* s, int stride, int dense_levels, unsigned seed);
 int les_mlp_counts(les_state* s, long long out2[2]);
 /* feature/target statistics of the collected data; normalises it in place */
 int les_mlp_fit_stats(les_state* s);

@@ -286,7 +286,7 @@ __device__ __forceinline__ double f32max_tiny(double x) {
 template <typename T>
 __global__ void k_lasd_update(T* FLM, T* FMM, T* FQN, T* FNN, const T* LM, const T* MM, const T* QN, const T* NN,
                               T* cs, T* beta, int init, long plane, int nz, double opftdelta, double lagran_dt,
-                              double beta_pow) {
+                              double beta_pow, const T* cs_init = nullptr) {
   const long n = (long)(nz + 1) * plane;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const long o = plane + q;
@@ -294,10 +294,13 @@ __global__ void k_lasd_update(T* FLM, T* FMM, T* FQN, T* FNN, const T* LM, const
     double flm, fmm, fqn, fnn;
     const double lm = LM[o], mm = MM[o], qn = QN[o], nn = NN[o];
     if (init) {
+      // compute_lagscaledep.f90 initialisation: averages that imply Cs^2 = 0.03
+      // (or, for the learned closure's fallback, the current coefficient)
+      const double c0 = cs_init ? double(cs_init[o]) : 0.03;
       fmm = mm;
-      flm = 0.03 * mm;
+      flm = c0 * mm;
       fnn = nn;
-      fqn = 0.03 * nn;
+      fqn = c0 * nn;
     } else {
       flm = FLM[o];
       fmm = FMM[o];

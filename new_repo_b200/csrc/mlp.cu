@@ -47,7 +47,7 @@ __device__ __forceinline__ uint16_t bf16_bits(float x) {
   return *reinterpret_cast<uint16_t*>(&h);
 }
 
-// raw (transformed, not normalised) invariants at level k, offset o
+// raw (transformed, not normalised) features at level k, offset o
 template <typename T>
 __device__ __forceinline__ void raw_features(const MlpFeatIn<T>& a, long o, int k, float* t) {
   const long pl = a.plane;
@@ -93,9 +93,25 @@ __device__ __forceinline__ void raw_features(const MlpFeatIn<T>& a, long o, int 
   t[2] = log1pf(oo);
   t[3] = copysignf(log1pf(fabsf(r3)), r3);
   t[4] = log1pf(z / a.delta);
-  t[5] = 0.0f;  // gradient Richardson number: zero without buoyancy
+  // the coefficient before this update: the Lagrangian averages of the
+  // dynamic procedure relax from it (takes the slot of a gradient Richardson
+  // number, which is zero without buoyancy)
+  t[5] = logf(fmaxf(float(a.csprev[o]), 1e-6f));
   t[6] = log1pf(sqrtf(uh * uh + vh * vh));
   t[7] = a.log_delta_z0;
+}
+
+// order-preserving float -> int map (for atomic min / max of floats)
+__host__ __device__ inline int ordered_int(float f) {
+  int i;
+  memcpy(&i, &f, sizeof(int));
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__host__ __device__ inline float ordered_float(int i) {
+  i = i >= 0 ? i : i ^ 0x7fffffff;
+  float f;
+  memcpy(&f, &i, sizeof(float));
+  return f;
 }
 
 __device__ __forceinline__ unsigned hash32(unsigned x) {
@@ -109,23 +125,49 @@ __device__ __forceinline__ unsigned hash32(unsigned x) {
 
 // --------------------------------------------------------- collection ----
 template <typename T>
-__global__ void k_mlp_collect(const MlpFeatIn<T> a, const T* cs, MlpDevice m, int stride, unsigned seed) {
+__global__ void k_mlp_collect(const MlpFeatIn<T> a, const T* cs, MlpDevice m, int stride, int dense_levels,
+                              unsigned seed) {
   const long n = (long)(a.nz + 1) * a.plane;
+  float lmin[8], lmax[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    lmin[i] = 3.0e38f;
+    lmax[i] = -3.0e38f;
+  }
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
-    const unsigned h = hash32(unsigned(q) * 2654435761u ^ seed);
-    if (h % unsigned(stride) != 0) continue;
     const long o = a.plane + q;
     const int k = int(o / a.plane);
     float t[8];
-    raw_features(a, o, k, t);
+    raw_features(a, o, k, t);  // every point: the range covers the whole state
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      lmin[i] = fminf(lmin[i], t[i]);
+      lmax[i] = fmaxf(lmax[i], t[i]);
+    }
+    const unsigned h = hash32(unsigned(q) * 2654435761u ^ seed);
+    const unsigned st = k <= dense_levels ? 1u : unsigned(stride);  // every point of the lowest levels
+    if (h % st != 0) continue;
     const float y = fmaxf(logf(fmaxf(float(cs[o]), 1e-30f)), MLP_LOG_CS_FLOOR);
-    const int val = ((h / unsigned(stride)) % 10u) == 0u;  // 10 % held out
+    const int val = ((h / st) % 10u) == 0u;  // 10 % held out
     const unsigned long long idx = atomicAdd(&m.counts[val], 1ull);
     if ((long)idx >= m.cap) continue;
     float* x = (val ? m.vx : m.dx) + idx * MLP_IN;
 #pragma unroll
     for (int i = 0; i < MLP_IN; ++i) x[i] = t[i];
     (val ? m.vt : m.dt)[idx] = y;
+  }
+  // feature range of the state: warp reduction, one atomic per warp and bound
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    float a0 = lmin[i], b0 = lmax[i];
+    for (int off = 16; off > 0; off >>= 1) {
+      a0 = fminf(a0, __shfl_down_sync(0xffffffffu, a0, off));
+      b0 = fmaxf(b0, __shfl_down_sync(0xffffffffu, b0, off));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&m.range[i], ordered_int(a0));
+      atomicMax(&m.range[8 + i], ordered_int(b0));
+    }
   }
 }
 
@@ -397,7 +439,8 @@ struct TrainSmem {
 };
 
 __global__ void __launch_bounds__(TILE) k_mlp_train(MlpDevice m, const float* X, const float* Tg, long n,
-                                                    float inv_n, float* y_out, float* loss, unsigned* status) {
+                                                    float inv_n, float* y_out, float* loss, unsigned* status,
+                                                    MlpPerm pm) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   TrainSmem& TS = *reinterpret_cast<TrainSmem*>(smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023));
   MlpSmem& S = TS.s;
@@ -416,9 +459,10 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(MlpDevice m, const float* X,
   for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const long q = tile * TILE + tid;
     const bool valid = q < n;
+    const long src = pm.n ? long((pm.a * (unsigned long long)(pm.off + q) + pm.b) % (unsigned long long)pm.n) : q;
     float x[8];
-    for (int i = 0; i < 8; ++i) x[i] = valid ? X[q * 8 + i] : 0.0f;
-    const float tg = valid ? Tg[q] : 0.0f;
+    for (int i = 0; i < 8; ++i) x[i] = valid ? X[src * 8 + i] : 0.0f;
+    const float tg = valid ? Tg[src] : 0.0f;
     put_features(S, tid, x);
     for (int i = 0; i < 8; ++i) TS.xf[tid][i] = tile_val(S.A1, tid, i, 256);  // bf16-rounded inputs
     tc::fence_async_smem();
@@ -563,10 +607,11 @@ size_t train_smem() { return sizeof(TrainSmem) + 1024; }
 
 // ------------------------------------------------------------- host side ----
 template <typename T>
-void mlp_collect(const MlpFeatIn<T>& in, const T* cs, MlpDevice& m, int stride, unsigned seed, cudaStream_t st) {
+void mlp_collect(const MlpFeatIn<T>& in, const T* cs, MlpDevice& m, int stride, int dense_levels, unsigned seed,
+                 cudaStream_t st) {
   const long n = (long)(in.nz + 1) * in.plane;
   hook_before("k_mlp_collect", double(n) * 12 * sizeof(T));
-  k_mlp_collect<T><<<148 * 8, 256, 0, st>>>(in, cs, m, stride, seed);
+  k_mlp_collect<T><<<148 * 8, 256, 0, st>>>(in, cs, m, stride, dense_levels, seed);
   LES_CHECK_LAUNCH();
   hook_after();
 }
@@ -589,6 +634,16 @@ void init_mlp_attributes() {
   LES_CUDA(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem()));
 }
 
+void mlp_reset_range(MlpDevice& m, cudaStream_t st) {
+  int rg[16];
+  for (int i = 0; i < 8; ++i) {
+    rg[i] = ordered_int(3.0e38f);
+    rg[8 + i] = ordered_int(-3.0e38f);
+  }
+  LES_CUDA(cudaMemcpyAsync(m.range, rg, sizeof(rg), cudaMemcpyHostToDevice, st));
+  LES_CUDA(cudaStreamSynchronize(st));
+}
+
 void mlp_pack(MlpDevice& m, cudaStream_t st) {
   hook_before("k_mlp_pack", double(MLP_NP) * 4 + IMG_BYTES);
   k_mlp_pack<<<1, 256, 0, st>>>(m.params, m.img);
@@ -597,13 +652,13 @@ void mlp_pack(MlpDevice& m, cudaStream_t st) {
 }
 
 void mlp_grad(MlpDevice& m, const float* x, const float* t, long n, float* y_out, float* loss_dev, unsigned* status,
-              cudaStream_t st) {
+              cudaStream_t st, MlpPerm perm) {
   LES_CUDA(cudaMemsetAsync(m.grad, 0, sizeof(float) * MLP_NP, st));
   if (loss_dev) LES_CUDA(cudaMemsetAsync(loss_dev, 0, sizeof(float), st));
   const long ntiles = (n + TILE - 1) / TILE;
   const int grid = int(std::max<long>(1, std::min<long>(ntiles, 148L)));
   hook_before("k_mlp_train", double(n) * 36.0);
-  k_mlp_train<<<grid, TILE, train_smem(), st>>>(m, x, t, n, 1.0f / float(n), y_out, loss_dev, status);
+  k_mlp_train<<<grid, TILE, train_smem(), st>>>(m, x, t, n, 1.0f / float(n), y_out, loss_dev, status, perm);
   LES_CHECK_LAUNCH();
   hook_after();
 }
@@ -638,20 +693,25 @@ void mlp_fit_stats(MlpDevice& m, cudaStream_t st) {
   LES_CUDA(cudaMemcpyAsync(h.data(), acc, 36 * sizeof(double), cudaMemcpyDeviceToHost, st));
   LES_CUDA(cudaStreamSynchronize(st));
   cudaFree(acc);
+  // feature range: the sampled pairs and every point of the collected states
+  int rg[16];
+  LES_CUDA(cudaMemcpyAsync(rg, m.range, sizeof(rg), cudaMemcpyDeviceToHost, st));
+  LES_CUDA(cudaStreamSynchronize(st));
   float s[MLP_NS];
   auto unorder = [](double slot) {
     int iv;
     std::memcpy(&iv, &slot, sizeof(int));
-    iv = iv >= 0 ? iv : iv ^ 0x7fffffff;
-    float f;
-    std::memcpy(&f, &iv, sizeof(float));
-    return f;
+    return ordered_float(iv);
   };
   for (int i = 0; i < 9; ++i) {
     const double mean = h[2 * i] / double(nt);
     double var = h[2 * i + 1] / double(nt) - mean * mean;
     double sd = var > 1e-12 ? std::sqrt(var) : 1.0;
-    const float mn = unorder(h[18 + i]), mx = unorder(h[27 + i]);
+    float mn = unorder(h[18 + i]), mx = unorder(h[27 + i]);
+    if (i < 8) {
+      mn = std::min(mn, ordered_float(rg[i]));
+      mx = std::max(mx, ordered_float(rg[8 + i]));
+    }
     if (i < 8) {
       s[MLP_S_MU + i] = float(mean);
       s[MLP_S_SD + i] = float(sd);
@@ -703,8 +763,9 @@ double mlp_blend(T* cs, const T* cs_dyn, MlpDevice& m, int nz, bool check, doubl
 template double mlp_blend<float>(float*, const float*, MlpDevice&, int, bool, double*, cudaStream_t);
 template double mlp_blend<double>(double*, const double*, MlpDevice&, int, bool, double*, cudaStream_t);
 
-template void mlp_collect<float>(const MlpFeatIn<float>&, const float*, MlpDevice&, int, unsigned, cudaStream_t);
-template void mlp_collect<double>(const MlpFeatIn<double>&, const double*, MlpDevice&, int, unsigned, cudaStream_t);
+template void mlp_collect<float>(const MlpFeatIn<float>&, const float*, MlpDevice&, int, int, unsigned, cudaStream_t);
+template void mlp_collect<double>(const MlpFeatIn<double>&, const double*, MlpDevice&, int, int, unsigned,
+                                  cudaStream_t);
 template void mlp_infer<float>(const MlpFeatIn<float>&, float*, MlpDevice&, unsigned*, cudaStream_t);
 template void mlp_infer<double>(const MlpFeatIn<double>&, double*, MlpDevice&, unsigned*, cudaStream_t);
 

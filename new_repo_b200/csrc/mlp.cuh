@@ -29,6 +29,7 @@ struct MlpFeatIn {
   const T* d[9];  // dudx dudy dudz dvdx dvdy dvdz dwdx dwdy dwdz
   const T* u;
   const T* v;
+  const T* csprev;  // Cs^2 before this update (the closure's Lagrangian memory)
   long plane;
   int nz;
   int wall;
@@ -50,25 +51,39 @@ struct MlpDevice {
   long cap = 0;
   float* scratch = nullptr;    // forward outputs of the host-features path
   int* colflag = nullptr;      // per (i,j) column: 1 = features left the training range
+  int* range = nullptr;        // raw feature min[8], max[8] of the collected states (order-preserving ints)
   long plane = 0;
 };
 
 // feature transforms shared by inference and data collection
+// append (features, log cs) pairs: one point in `stride` (seeded hash), every
+// point of levels 1..dense_levels; the features' previous coefficient is
+// in.csprev
 template <typename T>
-void mlp_collect(const MlpFeatIn<T>& in, const T* cs, MlpDevice& m, int stride, unsigned seed, cudaStream_t st);
+void mlp_collect(const MlpFeatIn<T>& in, const T* cs, MlpDevice& m, int stride, int dense_levels, unsigned seed,
+                 cudaStream_t st);
 template <typename T>
 void mlp_infer(const MlpFeatIn<T>& in, T* cs, MlpDevice& m, unsigned* status, cudaStream_t st);
+// empty the collected feature range
+void mlp_reset_range(MlpDevice& m, cudaStream_t st);
 // statistics of the collected raw data, then normalisation in place
 void mlp_fit_stats(MlpDevice& m, cudaStream_t st);
 // opt the tensor-core kernels in to their shared-memory sizes (current device)
 void init_mlp_attributes();
 // pack the BF16 operand images from the FP32 master weights
 void mlp_pack(MlpDevice& m, cudaStream_t st);
-// one optimisation pass: gradients of the mean squared error over the
-// samples [first, first + n) of a buffer (x [n][8], t [n]) into m.grad;
-// with y_out != nullptr also writes the network outputs (normalised).
+// sample order of a training batch: row r of the batch reads sample
+// (a * (off + r) + b) mod n of the buffer (a coprime to n: a permutation of
+// the buffer per epoch); n = 0 reads rows in order
+struct MlpPerm {
+  unsigned long long a = 1, b = 0;
+  long n = 0, off = 0;
+};
+// one optimisation pass: gradients of the mean squared error over n samples
+// of a buffer (x [.][8], t [.]) into m.grad; with y_out != nullptr also
+// writes the network outputs (normalised), in batch-row order.
 void mlp_grad(MlpDevice& m, const float* x, const float* t, long n, float* y_out, float* loss_dev, unsigned* status,
-              cudaStream_t st);
+              cudaStream_t st, MlpPerm perm = MlpPerm());
 void mlp_adam(MlpDevice& m, int step, float lr, cudaStream_t st);
 // number of (i,j) columns flagged out of the training range by the last inference
 int mlp_count_flags(MlpDevice& m, int* dcount, cudaStream_t st);

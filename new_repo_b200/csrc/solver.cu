@@ -255,6 +255,9 @@ class Solver final : public SolverBase {
     const long n = (long)(k1 - k0 + 1) * g.plane();
     KL("k_fill", double(n) * sizeof(T), k_fill<T><<<grid_for(n), 256, 0, st>>>(lev(f, k0), n, v));
   }
+  void copy(T* dst, const T* src, long n) {
+    KL("k_copy", 2.0 * n * sizeof(T), k_copy<T><<<grid_for(n), 256, 0, st>>>(dst, src, n));
+  }
   void fill_plane(T* f, T v) {
     KL("k_fill", double(g.plane()) * sizeof(T), k_fill<T><<<grid_for(g.plane()), 256, 0, st>>>(f, g.plane(), v));
   }
@@ -357,6 +360,8 @@ class Solver final : public SolverBase {
   int* dcount = nullptr;
   double* derr = nullptr;
   int mlp_adam_step = 0;
+  T* cs_prev = nullptr;      // Cs^2 before the current update
+  bool have_prev = false;    // cs_prev holds the previous collection's coefficient
 
   void ensure_mlp() {
     if (mlp_alloc) return;
@@ -367,10 +372,12 @@ class Solver final : public SolverBase {
     md.adam_m = track(dalloc<float>(MLP_NP));
     md.adam_v = track(dalloc<float>(MLP_NP));
     md.colflag = track(dalloc<int>(g.plane()));
+    md.range = track(dalloc<int>(16));
     md.counts = track(dalloc<unsigned long long>(2));
     md.plane = g.plane();
     dcount = track(dalloc<int>(1));
     derr = track(dalloc<double>(1));
+    cs_prev = track(dalloc<T>(g.field()));
     init_mlp_attributes();
     mlp_alloc = true;
   }
@@ -380,6 +387,7 @@ class Solver final : public SolverBase {
     for (int q = 0; q < 9; ++q) a.d[q] = F[d[q]];
     a.u = F[LES_U];
     a.v = F[LES_V];
+    a.csprev = cs_prev;
     a.plane = g.plane();
     a.nz = g.nz;
     a.wall = P.wall_law;
@@ -450,12 +458,18 @@ class Solver final : public SolverBase {
       md.vt = track(dalloc<float>(cap));
     }
     LES_CUDA(cudaMemsetAsync(md.counts, 0, 2 * sizeof(unsigned long long), st));
-    LES_CUDA(cudaStreamSynchronize(st));
+    mlp_reset_range(md, st);
   }
-  void mlp_collect(int stride, unsigned seed) override {
+  void mlp_collect(int stride, int dense_levels, unsigned seed) override {
     if (!mlp_alloc || md.cap == 0) throw CudaError(1, "learned closure: call les_mlp_reset_data first");
     Tag tag_(this, "mlp");
-    les::mlp_collect<T>(feat_in(), F[LES_CS_OPT2], md, std::max(1, stride), seed, st);
+    ensure_mlp();
+    // pairs (features with the previous collection's coefficient, current
+    // coefficient): collect at consecutive dynamic updates; the first call
+    // only records the coefficient
+    if (have_prev) les::mlp_collect<T>(feat_in(), F[LES_CS_OPT2], md, std::max(1, stride), dense_levels, seed, st);
+    copy(cs_prev, F[LES_CS_OPT2], g.field());
+    have_prev = true;
   }
   void mlp_counts(long long* c) override {
     ensure_mlp();
@@ -476,35 +490,48 @@ class Solver final : public SolverBase {
     mlp_counts(c);
     const long ntr = c[0], nva = c[1];
     if (ntr < 128) throw CudaError(1, "learned closure: not enough training data");
-    float* dloss = nullptr;
-    LES_CUDA(cudaMalloc(&dloss, 2 * sizeof(float)));
     const long chunk = long(std::max(1, tiles_per_step)) * 128;
     const long nsteps = (ntr + chunk - 1) / chunk;
-    long mult = 1000003 % nsteps;
-    auto gcdl = [](long a, long b) { while (b) { long t = a % b; a = b; b = t; } return a; };
-    if (mult == 0 || gcdl(mult, nsteps) != 1) mult = 1;
-    for (int ep = 0; ep < epochs; ++ep) {
-      double sum = 0.0;
-      for (long s = 0; s < nsteps; ++s) {
-        const long cidx = (s * mult + long(ep) * 7919) % nsteps;
-        const long off = cidx * chunk;
-        const long n = std::min(chunk, ntr - off);
-        LES_CUDA(cudaMemsetAsync(dloss, 0, sizeof(float), st));
-        mlp_grad(md, md.dx + off * MLP_IN, md.dt + off, n, nullptr, dloss, dstatus, st);
-        mlp_adam(md, ++mlp_adam_step, float(lr), st);
-        if (s == nsteps - 1 || (s % 64) == 0) {
-          float h = 0;
-          LES_CUDA(cudaMemcpyAsync(&h, dloss, sizeof(float), cudaMemcpyDeviceToHost, st));
-          LES_CUDA(cudaStreamSynchronize(st));
-          sum = h;  // loss of the latest batch
-        }
+    float* dloss = nullptr;
+    LES_CUDA(cudaMalloc(&dloss, (nsteps + 1) * sizeof(float)));
+    std::vector<float> hl(nsteps);
+    std::mt19937_64 rng(0x5eed0000ull + (unsigned long long)mlp_adam_step);
+    auto gcdl = [](unsigned long long a, unsigned long long b) {
+      while (b) {
+        const unsigned long long t = a % b;
+        a = b;
+        b = t;
       }
-      if (loss_epochs) loss_epochs[ep] = sum;
+      return a;
+    };
+    for (int ep = 0; ep < epochs; ++ep) {
+      // a fresh permutation of the training pairs each epoch: batches mix
+      // levels and collection steps
+      MlpPerm pm;
+      pm.n = ntr;
+      do {
+        pm.a = 1 + rng() % (unsigned long long)(ntr - 1);
+      } while (gcdl(pm.a, (unsigned long long)ntr) != 1);
+      pm.b = rng() % (unsigned long long)ntr;
+      for (long s = 0; s < nsteps; ++s) {
+        pm.off = s * chunk;
+        const long n = std::min(chunk, ntr - pm.off);
+        mlp_grad(md, md.dx, md.dt, n, nullptr, dloss + s, dstatus, st, pm);
+        mlp_adam(md, ++mlp_adam_step, float(lr), st);
+      }
+      LES_CUDA(cudaMemcpyAsync(hl.data(), dloss, nsteps * sizeof(float), cudaMemcpyDeviceToHost, st));
+      LES_CUDA(cudaStreamSynchronize(st));
+      double sum = 0.0, wsum = 0.0;
+      for (long s = 0; s < nsteps; ++s) {
+        const double w = double(std::min(chunk, ntr - s * chunk));
+        sum += w * hl[s];
+        wsum += w;
+      }
+      if (loss_epochs) loss_epochs[ep] = sum / wsum;  // mean batch loss of the epoch
     }
     if (val_loss) {
       *val_loss = -1.0;
       if (nva > 0) {
-        LES_CUDA(cudaMemsetAsync(dloss, 0, sizeof(float), st));
         mlp_grad(md, md.vx, md.vt, nva, nullptr, dloss, dstatus, st);
         float h = 0;
         LES_CUDA(cudaMemcpyAsync(&h, dloss, sizeof(float), cudaMemcpyDeviceToHost, st));
@@ -566,19 +593,22 @@ class Solver final : public SolverBase {
     }
     if (jtt % P.cs_count != 0) return;
     if (!mlp_ready) throw CudaError(1, "learned closure has no weights (train it or load parameters)");
+    copy(cs_prev, F[LES_CS_OPT2], g.field());
+    have_prev = true;
     les::mlp_infer<T>(feat_in(), F[LES_CS_OPT2], md, dstatus, st);
     ++mlp_updates;
     mlp_last_flags = mlp_count_flags(md, dcount, st);
     const bool check = mlp_check_every > 0 && (mlp_updates % mlp_check_every) == 0;
     if (mlp_last_flags > 0 || check) {
-      // dynamic procedure without Lagrangian history (F initialisation
-      // semantics), into scratch: cs -> sc[11]
+      // one Lagrangian relaxation step of the dynamic procedure starting from
+      // the coefficient before this update (the reference's F initialisation
+      // with Cs^2 = cs_prev instead of 0.03), into scratch: cs -> sc[11]
       dynamic_mum(a, true);
       const long n1 = (long)(g.nz + 1) * g.plane();
       KL("k_lasd_update", 14.0 * n1 * sizeof(T),
          k_lasd_update<T><<<grid_for(n1), 256, 0, st>>>(sc[0], sc[12], sc[13], sc[14], sc[7], sc[8], sc[9], sc[10],
                                                        sc[11], sc[1], 1, g.plane(), g.nz, 1.5 * delta,
-                                                       P.dt * double(P.cs_count), beta_pow));
+                                                       P.dt * double(P.cs_count), beta_pow, cs_prev));
       const double e = mlp_blend<T>(F[LES_CS_OPT2], sc[11], md, g.nz, check, derr, st);
       if (check) mlp_last_err = e;
     }

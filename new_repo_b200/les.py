@@ -421,8 +421,10 @@ class LES:
     def mlp_reset_data(self, cap: int):
         check(self.lib.les_mlp_reset_data(self._h, int(cap)))
 
-    def mlp_collect(self, stride: int = 1, seed: int = 0):
-        check(self.lib.les_mlp_collect(self._h, int(stride), int(seed) & 0xFFFFFFFF))
+    def mlp_collect(self, stride: int = 1, seed: int = 0, dense_levels: int = 0):
+        """Append (invariants, log Cs^2) pairs of the current state: one point in
+        ``stride``, every point of levels 1..dense_levels."""
+        check(self.lib.les_mlp_collect(self._h, int(stride), int(dense_levels), int(seed) & 0xFFFFFFFF))
 
     def mlp_counts(self) -> tuple:
         out = (C.c_longlong * 2)()

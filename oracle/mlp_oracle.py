@@ -6,8 +6,10 @@ cadence.  This module restates the CUDA closure (``new_repo_b200/csrc/mlp.cu``)
 on the CPU so that tests can check the GPU's features, forward pass and
 training gradients.  Only ``tests/`` may import it.
 
-Network: 8 invariants -> 64 (GELU) -> 64 (GELU) -> 1, output y in normalised
-log Cs^2 units, ``Cs^2 = clamp(exp(ymu + ysd * y), 1e-24, 1)``.
+Network: 8 features (7 resolved invariants and the coefficient before the
+update, which carries the Lagrangian memory of the dynamic procedure) ->
+64 (GELU) -> 64 (GELU) -> 1, output y in normalised log Cs^2 units,
+``Cs^2 = clamp(exp(ymu + ysd * y), 1e-24, 1)``.
 
 Precision model of the GPU kernels (reproduced by ``forward``/``grad`` with
 ``bf16=True``):
@@ -106,12 +108,15 @@ def grad(p, x, t, bf16_ops=True):
     return g, loss
 
 
-def raw_features(d, u, v, k, dz, delta, log_delta_z0, wall):
-    """The 8 transformed invariants at level k (mlp.cu raw_features).
+def raw_features(d, u, v, cs_prev, k, dz, delta, log_delta_z0, wall):
+    """The 8 transformed features at level k (mlp.cu raw_features).
 
-    ``d`` maps 'dudx' .. 'dwdz' to (nz+2, ny, nx) arrays; returns [ny*nx, 8]
-    in float32 arithmetic.  Level 1 is the uvp node (w-node quantities
-    averaged up), levels >= 2 are w nodes (uvp quantities averaged down).
+    ``d`` maps 'dudx' .. 'dwdz' to (nz+2, ny, nx) arrays, ``cs_prev`` is the
+    coefficient before the update; returns [ny*nx, 8] in float32 arithmetic.
+    Level 1 is the uvp node (w-node quantities averaged up), levels >= 2 are
+    w nodes (uvp quantities averaged down).  Features: log1p |S|,
+    log1p S:S, log1p Omega:Omega, signed log1p tr(S^3), log1p(z / Delta),
+    log max(Cs^2_prev, 1e-6), log1p |u_h|, log(Delta / z0).
     """
     f = {key: np.asarray(a, np.float32) for key, a in d.items()}
     u = np.asarray(u, np.float32)
@@ -151,7 +156,7 @@ def raw_features(d, u, v, k, dz, delta, log_delta_z0, wall):
     out[..., 2] = np.log1p(oo)
     out[..., 3] = np.copysign(np.log1p(np.abs(r3)), r3)
     out[..., 4] = np.log1p(z / np.float32(delta))
-    out[..., 5] = 0.0
+    out[..., 5] = np.log(np.maximum(np.asarray(cs_prev, np.float32)[k], np.float32(1e-6)))
     out[..., 6] = np.log1p(np.sqrt(uh * uh + vh * vh))
     out[..., 7] = np.float32(log_delta_z0)
     return out.reshape(-1, 8)

@@ -128,14 +128,14 @@ def _fields(les):
     return {n: les.download(n) for n in names}, les.download("u"), les.download("v")
 
 
-def _oracle_cs(les, p, stats):
+def _oracle_cs(les, p, stats, cs_prev):
     """Cs^2 and the in-range mask of every level 1..nz+1 from the oracle's features."""
     rp = les.params
     d, u, v = _fields(les)
     delta = (rp.dx * rp.dy * rp.dz) ** (1.0 / 3.0)
     cs, ok = [], []
     for k in range(1, rp.nz + 2):
-        t = M.raw_features(d, u, v, k, rp.dz, delta, np.log(delta / rp.z0), 1)
+        t = M.raw_features(d, u, v, cs_prev, k, rp.dz, delta, np.log(delta / rp.z0), 1)
         xn = (t - stats[M.S_MU:M.S_MU + 8]) / stats[M.S_SD:M.S_SD + 8]
         cs.append(M.cs_from_output(M.forward(p, xn.astype(np.float32)), stats))
         ok.append(M.in_range(xn, stats))
@@ -156,9 +156,13 @@ def test_mlp_inference_in_step_matches_oracle(gpu, precision):
     les.mlp_set_params(np.concatenate([p, st]))
     les.step(4)
     les.compute_vel_grad()
+    # a non-uniform previous coefficient
+    cs_prev = 0.03 * np.exp(0.3 * np.random.default_rng(1).standard_normal(les.download("cs_opt2").shape))
+    les.upload("cs_opt2", cs_prev)
+    cs_prev = les.download("cs_opt2")
     les.sgs_stress(10, 10)
     cs = les.download("cs_opt2")[1:les.params.nz + 2]
-    cso, _ = _oracle_cs(les, p, st)
+    cso, _ = _oracle_cs(les, p, st, cs_prev)
     cso = cso.reshape(cs.shape)
     e = np.abs(np.log(cs) - np.log(cso))
     assert e.max() <= 2e-2 and np.median(e) <= 1e-4, (e.max(), np.median(e))
@@ -183,6 +187,9 @@ def test_mlp_fallback_equals_dynamic_procedure(gpu):
     les.mlp_set_params(np.concatenate([_params(8), st]))
     saved = {n: les.download(n) for n in ("F_LM", "F_MM", "F_QN", "F_NN", "beta")}
     les.compute_vel_grad()
+    # the fallback relaxes from the previous coefficient; from 0.03 it is the
+    # reference's first (initialising) LASD update
+    les.upload("cs_opt2", np.full_like(les.download("cs_opt2"), 0.03))
     les.sgs_stress(10, 10)
     info = les.mlp_info()
     assert info["flagged_columns"] == les.params.nx * les.params.ny
@@ -216,9 +223,10 @@ def test_mlp_partial_fallback_only_flagged_columns(gpu):
     # between neighbouring column maxima near the median, so float rounding
     # cannot move a column across it)
     d, u, v = _fields(les)
+    cs_prev = les.download("cs_opt2")
     rp = les.params
     delta = (rp.dx * rp.dy * rp.dz) ** (1.0 / 3.0)
-    f6 = np.stack([M.raw_features(d, u, v, k, rp.dz, delta, np.log(delta / rp.z0), 1)[:, 6]
+    f6 = np.stack([M.raw_features(d, u, v, cs_prev, k, rp.dz, delta, np.log(delta / rp.z0), 1)[:, 6]
                    for k in range(1, rp.nz + 2)])
     cm = np.sort(f6.max(axis=0))
     mid = cm[cm.size // 2 - 64:cm.size // 2 + 64]
@@ -229,7 +237,7 @@ def test_mlp_partial_fallback_only_flagged_columns(gpu):
     les.sgs_stress(10, 10)
     info = les.mlp_info()
     cs = les.download("cs_opt2")[1:rp.nz + 2].reshape(rp.nz + 1, -1)
-    cso, ok = _oracle_cs(les, p, st)
+    cso, ok = _oracle_cs(les, p, st, cs_prev)
     col_ok = ok.all(axis=0)
     assert 0 < info["flagged_columns"] < rp.nx * rp.ny
     e = np.abs(np.log(cs[:, col_ok]) - np.log(cso[:, col_ok]))
@@ -250,7 +258,7 @@ def test_mlp_training_gain_over_constant_coefficient(gpu):
     les.mlp_reset_data(1 << 20)
     while les.jt_total < 60:
         les.step(1)
-        if les.jt_total >= 10 and les.jt_total % 5 == 0:
+        if les.jt_total >= 5 and les.jt_total % 5 == 0:  # consecutive updates; the first only records
             les.mlp_collect(stride=2, seed=les.jt_total)
     ntr, nva = les.mlp_counts()
     assert ntr > 100000 and nva > 10000
