@@ -232,6 +232,26 @@ int les_mlp_info(les_state* s, double out4[4]);
 /* dynamic-procedure check every `every` closure updates (0 = never) */
 int les_mlp_set_check_every(les_state* s, int every);
 
+/* ---- allocation-free variant (no reference counterpart) ----------------
+ * The horizontal derivatives of les_grad_velocity_filt (the ddx/ddy of
+ * compute_derivatives.f90 on one field) for a field already on the device:
+ * f [nlev][ny][nx] (FP64) is replaced by its Nyquist-filtered version and
+ * dfdx, dfdy receive the derivatives (domain lengths lx, ly).  It allocates
+ * nothing: the tables and spectra live in one static device buffer of
+ * LES_NOALLOC_SCRATCH_BYTES, for callers that must not change the device
+ * memory footprint (an in-situ hook in a coupled run whose memory is fully
+ * committed, a process whose free memory a caching allocator holds).
+ * Sizes needing more scratch than the buffer are rejected (LES_ERR_INVALID,
+ * message in les_noalloc_last_error).  The first call on a device looks up
+ * the buffer's address and sets kernel attributes; make it before any stream
+ * capture.  All calls share the buffer of their device: calls in flight at
+ * the same time on one device race.  Asynchronous on `stream` (a
+ * cudaStream_t; NULL is the default stream). */
+#define LES_NOALLOC_SCRATCH_BYTES (32u << 20)
+int les_grad_xy_noalloc(double* f, double* dfdx, double* dfdy, int nx, int ny, int nlev, double lx, double ly,
+                        void* stream);
+const char* les_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -104,6 +104,7 @@ PROTOTYPES = {
     "les_mlp_grad": [_P, _F, _F, C.c_long, _F, _F],
     "les_mlp_info": [_P, _D],
     "les_mlp_set_check_every": [_P, _I],
+    "les_grad_xy_noalloc": [_P, _P, _P, _I, _I, _I, C.c_double, C.c_double, _P],
 }
 
 _lib = None
@@ -122,6 +123,8 @@ def load() -> C.CDLL:
             fn.restype = C.c_int
         lib.les_last_error.argtypes = []
         lib.les_last_error.restype = C.c_char_p
+        lib.les_noalloc_last_error.argtypes = []
+        lib.les_noalloc_last_error.restype = C.c_char_p
         _lib = lib
     return _lib
 

@@ -40,7 +40,7 @@ def test_library_exports_every_declared_symbol(lib):
 def test_prototypes_cover_header(lib):
     from new_repo_b200 import capi
 
-    declared = set(_declared_symbols()) - {"les_last_error"}
+    declared = set(_declared_symbols()) - {"les_last_error", "les_noalloc_last_error"}  # return strings
     assert declared <= set(capi.PROTOTYPES), declared - set(capi.PROTOTYPES)
 
 
