@@ -184,7 +184,7 @@ int les_download_async(les_state* s, int field, double* pinned, int k0, int k1);
 int les_diagnostics_async(les_state* s, double* pinned_out4);
 
 /* ---- learned SGS closure (no reference counterpart) ---------------------
- * Cs^2 = exp(net(features)) from an 8 -> 64 -> 64 -> 1 GELU network with
+ * Cs^2 = Cs^2_prev * exp(net(features)) from an 8 -> 64 -> 64 -> 1 GELU network with
  * BF16 weights and FP32 accumulation (tcgen05 tensor cores), evaluated at
  * the dynamic-update cadence of compute_sgs.f90:171 (every cs_count steps
  * after dyn_init).  Training data are (invariants, log Cs^2) pairs of the
@@ -198,9 +198,10 @@ int les_diagnostics_async(les_state* s, double* pinned_out4);
  * of log Cs^2 - log Cs^2_dyn is recorded.
  * Parameters: float[LES_MLP_NPARAM + LES_MLP_NSTATS] = W1[8][64], b1[64],
  * W2[64][64], b2[64], w3[64], b3, then feature mean[8], std[8],
- * min[8], max[8] (normalised units), target mean, target std. */
+ * min[8], max[8] (normalised units), target mean, target std, target
+ * min, max (normalised units; the output is clamped to them). */
 #define LES_MLP_NPARAM 4801
-#define LES_MLP_NSTATS 34
+#define LES_MLP_NSTATS 36
 int les_set_sgs_model(les_state* s, int model);
 int les_mlp_init(les_state* s, unsigned seed);
 int les_mlp_set_params(les_state* s, const float* params, int n);
@@ -226,9 +227,10 @@ int les_mlp_train(les_state* s, int epochs, int tiles_per_step, double lr, doubl
 int les_mlp_forward(les_state* s, const float* x, long n, float* y);
 /* gradient of mean((y - t)^2) over n host rows into grad[LES_MLP_NPARAM] */
 int les_mlp_grad(les_state* s, const float* x, const float* t, long n, float* grad, float* loss);
-/* out4: last check's RMS log error (-1 if none), flagged columns of the last
- * update, number of updates, weights loaded (1/0) */
-int les_mlp_info(les_state* s, double out4[4]);
+/* out12: last check's RMS log error (-1 if none), flagged columns of the
+ * last update, number of updates, weights loaded (1/0), then for each of the
+ * 8 features the columns where it left the training range at the last update */
+int les_mlp_info(les_state* s, double out12[12]);
 /* dynamic-procedure check every `every` closure updates (0 = never) */
 int les_mlp_set_check_every(les_state* s, int every);
 

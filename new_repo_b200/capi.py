@@ -14,7 +14,7 @@ LIB_PATH = Path(__file__).resolve().parent / "liblesgpu.so"
 LES_OK, LES_ERR_INVALID, LES_ERR_NOMEM, LES_ERR_NUMERICAL, LES_ERR_IO = 0, 1, 3, 9, 22
 SGS_MODELS = {"cst_Smag": 0, "dyn_Smag": 1, "dyn_LagScaleDep": 2, "mlp": 3}
 MLP_NPARAM = 4801
-MLP_NSTATS = 34
+MLP_NSTATS = 36
 WALL_MODELS = {"wall_filter": 0, "wall_inst": 1, "wall_homog": 2}
 DEALIAS = {"padd": 0, "trunc": 1}
 LAG_HALO = {"reference1x1": 0, "periodic": 1}

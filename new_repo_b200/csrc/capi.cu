@@ -305,10 +305,10 @@ int les_mlp_grad(les_state* s, const float* x, const float* t, long n, float* gr
   }
   return guard([&] { s->s->mlp_grad_host(x, t, n, grad, loss); });
 }
-int les_mlp_info(les_state* s, double out4[4]) {
+int les_mlp_info(les_state* s, double out12[12]) {
   STATE_OR_FAIL(s);
-  if (!out4) return bad_state();
-  return guard([&] { s->s->mlp_info(out4); });
+  if (!out12) return bad_state();
+  return guard([&] { s->s->mlp_info(out12); });
 }
 int les_mlp_set_check_every(les_state* s, int every) {
   STATE_OR_FAIL(s);

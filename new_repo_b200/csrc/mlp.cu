@@ -147,7 +147,9 @@ __global__ void k_mlp_collect(const MlpFeatIn<T> a, const T* cs, MlpDevice m, in
     const unsigned h = hash32(unsigned(q) * 2654435761u ^ seed);
     const unsigned st = k <= dense_levels ? 1u : unsigned(stride);  // every point of the lowest levels
     if (h % st != 0) continue;
-    const float y = fmaxf(logf(fmaxf(float(cs[o]), 1e-30f)), MLP_LOG_CS_FLOOR);
+    // target: the change of log Cs^2 over the update (residual form: the
+    // network's identity part is exact, it learns the relaxation)
+    const float y = fmaxf(logf(fmaxf(float(cs[o]), 1e-30f)), MLP_LOG_CS_FLOOR) - t[5];
     const int val = ((h / st) % 10u) == 0u;  // 10 % held out
     const unsigned long long idx = atomicAdd(&m.counts[val], 1ull);
     if ((long)idx >= m.cap) continue;
@@ -384,19 +386,21 @@ __global__ void __launch_bounds__(TILE) k_mlp_infer(const MlpFeatIn<T> a, T* cs,
     const long q = tile * TILE + threadIdx.x;
     const bool valid = q < npts;
     float x[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    float lprev = 0.0f;  // log Cs^2 before the update (floored)
     long o = 0;
     if (valid) {
       o = a.plane + q;
       const int k = int(o / a.plane);
       float t[8];
       raw_features(a, o, k, t);
-      bool out = false;
+      int out = 0;  // bit i: feature i outside the training range
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         x[i] = (t[i] - S.stats[MLP_S_MU + i]) / S.stats[MLP_S_SD + i];
-        out |= (x[i] < S.stats[MLP_S_MIN + i] - 0.25f) || (x[i] > S.stats[MLP_S_MAX + i] + 0.25f);
+        if ((x[i] < S.stats[MLP_S_MIN + i] - 0.25f) || (x[i] > S.stats[MLP_S_MAX + i] + 0.25f)) out |= 1 << i;
       }
-      if (out) m.colflag[q % a.plane] = 1;
+      if (out) atomicOr(&m.colflag[q % a.plane], out);
+      lprev = t[5];
     }
     put_features(S, threadIdx.x, x);
     tc::fence_async_smem();
@@ -417,7 +421,8 @@ __global__ void __launch_bounds__(TILE) k_mlp_infer(const MlpFeatIn<T> a, T* cs,
 #pragma unroll
     for (int i = 0; i < 64; ++i) y += S.w3[i] * gelu(h[i] + S.b2[i]);
     if (valid) {
-      const float lc = S.stats[MLP_S_YMU] + S.stats[MLP_S_YSD] * y;
+      y = fminf(fmaxf(y, S.stats[MLP_S_YMIN]), S.stats[MLP_S_YMAX]);  // no extrapolated coefficients
+      const float lc = lprev + S.stats[MLP_S_YMU] + S.stats[MLP_S_YSD] * y;
       cs[o] = T(fminf(fmaxf(expf(lc), 1e-24f), 1.0f));
     }
     tc::fence_before_sync();
@@ -575,11 +580,21 @@ __global__ void k_mlp_adam(float* p, const float* g, float* mm, float* vv, int s
   }
 }
 
+// out[0]: flagged columns; out[1 + i]: columns where feature i left the range
 __global__ void k_mlp_count_flags(const int* flag, long plane, int* out) {
-  int c = 0;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < plane; q += (long)gridDim.x * blockDim.x) c += flag[q];
-  for (int off = 16; off > 0; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
-  if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+  int c[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < plane; q += (long)gridDim.x * blockDim.x) {
+    const int f = flag[q];
+    c[0] += f != 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) c[1 + i] += (f >> i) & 1;
+  }
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    int v = c[i];
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(&out[i], v);
+  }
 }
 
 template <typename T>
@@ -720,6 +735,8 @@ void mlp_fit_stats(MlpDevice& m, cudaStream_t st) {
     } else {
       s[MLP_S_YMU] = float(mean);
       s[MLP_S_YSD] = float(sd);
+      s[MLP_S_YMIN] = float((mn - mean) / sd);
+      s[MLP_S_YMAX] = float((mx - mean) / sd);
     }
   }
   LES_CUDA(cudaMemcpyAsync(m.stats, s, sizeof(s), cudaMemcpyHostToDevice, st));
@@ -732,16 +749,18 @@ void mlp_fit_stats(MlpDevice& m, cudaStream_t st) {
   LES_CUDA(cudaStreamSynchronize(st));
 }
 
-int mlp_count_flags(MlpDevice& m, int* dcount, cudaStream_t st) {
-  LES_CUDA(cudaMemsetAsync(dcount, 0, sizeof(int), st));
+int mlp_count_flags(MlpDevice& m, int* dcount, int* per_feature, cudaStream_t st) {
+  LES_CUDA(cudaMemsetAsync(dcount, 0, 9 * sizeof(int), st));
   hook_before("k_mlp_count_flags", double(m.plane) * 4);
   k_mlp_count_flags<<<148, 256, 0, st>>>(m.colflag, m.plane, dcount);
   LES_CHECK_LAUNCH();
   hook_after();
-  int h = 0;
-  LES_CUDA(cudaMemcpyAsync(&h, dcount, sizeof(int), cudaMemcpyDeviceToHost, st));
+  int h[9];
+  LES_CUDA(cudaMemcpyAsync(h, dcount, sizeof(h), cudaMemcpyDeviceToHost, st));
   LES_CUDA(cudaStreamSynchronize(st));
-  return h;
+  if (per_feature)
+    for (int i = 0; i < 8; ++i) per_feature[i] = h[1 + i];
+  return h[0];
 }
 
 template <typename T>

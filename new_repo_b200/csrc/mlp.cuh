@@ -18,10 +18,13 @@ constexpr int MLP_O_W3 = MLP_O_B2 + MLP_H;
 constexpr int MLP_O_B3 = MLP_O_W3 + MLP_H;
 constexpr int MLP_NP = MLP_O_B3 + 1;  // 4801 trainable parameters
 // statistics: feature mean[8], std[8], min[8], max[8] (normalised units),
-// target mean, target std
+// target mean, target std, target min, max (normalised units: the output is
+// clamped to the range it was trained on).  The target is the change of
+// log Cs^2 over one dynamic update: Cs^2 = Cs^2_prev * exp(ymu + ysd * y).
 constexpr int MLP_S_MU = 0, MLP_S_SD = 8, MLP_S_MIN = 16, MLP_S_MAX = 24, MLP_S_YMU = 32, MLP_S_YSD = 33;
-constexpr int MLP_NS = 34;
-constexpr float MLP_LOG_CS_FLOOR = -13.815510557964274f;  // log(1e-6): targets below are clamped
+constexpr int MLP_S_YMIN = 34, MLP_S_YMAX = 35;
+constexpr int MLP_NS = 36;
+constexpr float MLP_LOG_CS_FLOOR = -13.815510557964274f;  // log(1e-6): coefficients below are clamped
 
 // inputs of the feature function (the state's gradients and velocity)
 template <typename T>
@@ -50,7 +53,7 @@ struct MlpDevice {
   unsigned long long* counts = nullptr;  // [0] train, [1] validation
   long cap = 0;
   float* scratch = nullptr;    // forward outputs of the host-features path
-  int* colflag = nullptr;      // per (i,j) column: 1 = features left the training range
+  int* colflag = nullptr;      // per (i,j) column: bit i = feature i left the training range
   int* range = nullptr;        // raw feature min[8], max[8] of the collected states (order-preserving ints)
   long plane = 0;
 };
@@ -85,8 +88,9 @@ struct MlpPerm {
 void mlp_grad(MlpDevice& m, const float* x, const float* t, long n, float* y_out, float* loss_dev, unsigned* status,
               cudaStream_t st, MlpPerm perm = MlpPerm());
 void mlp_adam(MlpDevice& m, int step, float lr, cudaStream_t st);
-// number of (i,j) columns flagged out of the training range by the last inference
-int mlp_count_flags(MlpDevice& m, int* dcount, cudaStream_t st);
+// number of (i,j) columns flagged out of the training range by the last
+// inference; per_feature[8] (may be null) gets the columns per feature
+int mlp_count_flags(MlpDevice& m, int* dcount, int* per_feature, cudaStream_t st);
 // replace flagged columns of cs by cs_dyn; with check, returns the RMS of
 // log(cs) - log(cs_dyn) over all points (both floored at 1e-6)
 template <typename T>

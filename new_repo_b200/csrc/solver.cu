@@ -357,6 +357,7 @@ class Solver final : public SolverBase {
   int mlp_check_every = 10;  // dynamic-procedure check every 10 updates (50 steps at cs_count 5)
   double mlp_last_err = -1.0;
   int mlp_last_flags = 0;
+  int mlp_feature_flags[8] = {};
   int* dcount = nullptr;
   double* derr = nullptr;
   int mlp_adam_step = 0;
@@ -375,7 +376,7 @@ class Solver final : public SolverBase {
     md.range = track(dalloc<int>(16));
     md.counts = track(dalloc<unsigned long long>(2));
     md.plane = g.plane();
-    dcount = track(dalloc<int>(1));
+    dcount = track(dalloc<int>(9));
     derr = track(dalloc<double>(1));
     cs_prev = track(dalloc<T>(g.field()));
     init_mlp_attributes();
@@ -418,8 +419,10 @@ class Solver final : public SolverBase {
       s[MLP_S_MIN + i] = -1e30f;
       s[MLP_S_MAX + i] = 1e30f;
     }
-    s[MLP_S_YMU] = std::log(0.03f);
+    s[MLP_S_YMU] = 0.0f;  // no change of the coefficient
     s[MLP_S_YSD] = 1.0f;
+    s[MLP_S_YMIN] = -1e30f;
+    s[MLP_S_YMAX] = 1e30f;
     std::vector<float> all(p);
     all.insert(all.end(), s.begin(), s.end());
     mlp_set_params(all.data(), MLP_NP + MLP_NS);
@@ -580,6 +583,7 @@ class Solver final : public SolverBase {
     out[1] = mlp_last_flags;
     out[2] = double(mlp_updates);
     out[3] = mlp_ready ? 1.0 : 0.0;
+    for (int i = 0; i < 8; ++i) out[4 + i] = mlp_feature_flags[i];
   }
 
   // Cs^2 from the learned closure at the dynamic-update cadence; columns whose
@@ -597,7 +601,7 @@ class Solver final : public SolverBase {
     have_prev = true;
     les::mlp_infer<T>(feat_in(), F[LES_CS_OPT2], md, dstatus, st);
     ++mlp_updates;
-    mlp_last_flags = mlp_count_flags(md, dcount, st);
+    mlp_last_flags = mlp_count_flags(md, dcount, mlp_feature_flags, st);
     const bool check = mlp_check_every > 0 && (mlp_updates % mlp_check_every) == 0;
     if (mlp_last_flags > 0 || check) {
       // one Lagrangian relaxation step of the dynamic procedure starting from

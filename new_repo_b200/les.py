@@ -457,10 +457,10 @@ class LES:
         return g, float(loss[0])
 
     def mlp_info(self) -> dict:
-        out = np.zeros(4)
+        out = np.zeros(12)
         check(self.lib.les_mlp_info(self._h, _dptr(out)))
         return {"check_rms_log_error": float(out[0]), "flagged_columns": int(out[1]), "updates": int(out[2]),
-                "ready": bool(out[3])}
+                "ready": bool(out[3]), "flagged_by_feature": [int(x) for x in out[4:12]]}
 
     def mlp_set_check_every(self, every: int):
         check(self.lib.les_mlp_set_check_every(self._h, int(every)))

@@ -8,8 +8,9 @@ training gradients.  Only ``tests/`` may import it.
 
 Network: 8 features (7 resolved invariants and the coefficient before the
 update, which carries the Lagrangian memory of the dynamic procedure) ->
-64 (GELU) -> 64 (GELU) -> 1, output y in normalised log Cs^2 units,
-``Cs^2 = clamp(exp(ymu + ysd * y), 1e-24, 1)``.
+64 (GELU) -> 64 (GELU) -> 1, output y the normalised change of log Cs^2 over
+the update, ``Cs^2 = clamp(Cs^2_prev * exp(ymu + ysd * y), 1e-24, 1)`` with
+Cs^2_prev floored at 1e-6.
 
 Precision model of the GPU kernels (reproduced by ``forward``/``grad`` with
 ``bf16=True``):
@@ -35,8 +36,8 @@ O_B2 = O_W2 + NH * NH
 O_W3 = O_B2 + NH
 O_B3 = O_W3 + NH
 NP = O_B3 + 1  # 4801
-S_MU, S_SD, S_MIN, S_MAX, S_YMU, S_YSD = 0, 8, 16, 24, 32, 33
-NS = 34
+S_MU, S_SD, S_MIN, S_MAX, S_YMU, S_YSD, S_YMIN, S_YMAX = 0, 8, 16, 24, 32, 33, 34, 35
+NS = 36
 LOG_CS_FLOOR = float(np.log(1e-6))
 
 
@@ -162,9 +163,12 @@ def raw_features(d, u, v, cs_prev, k, dz, delta, log_delta_z0, wall):
     return out.reshape(-1, 8)
 
 
-def cs_from_output(y, stats):
-    """Cs^2 from the normalised output (k_mlp_infer's epilogue)."""
-    lc = stats[S_YMU] + stats[S_YSD] * np.asarray(y, np.float64)
+def cs_from_output(y, stats, log_cs_prev):
+    """Cs^2 from the normalised output (k_mlp_infer's epilogue): the output,
+    clamped to the trained target range, is the change of log Cs^2 from the
+    floored previous coefficient (feature 5, unnormalised)."""
+    y = np.clip(np.asarray(y, np.float64), stats[S_YMIN], stats[S_YMAX])
+    lc = np.asarray(log_cs_prev, np.float64) + stats[S_YMU] + stats[S_YSD] * y
     return np.clip(np.exp(lc), 1e-24, 1.0)
 
 
