@@ -49,7 +49,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--closure", default="mlp", choices=["mlp", "lasd"], help="SGS closure of the headline arm")
-    ap.add_argument("--train-steps", type=int, default=20, help="LASD steps that produce the training pairs")
+    ap.add_argument("--train-steps", type=int, default=30, help="LASD steps that produce the training pairs")
+    ap.add_argument("--train-epochs", type=int, default=4)
+    ap.add_argument("--train-batch-tiles", type=int, default=16, help="training batch = 128 x this")
     return ap.parse_args()
 
 
@@ -188,7 +190,7 @@ def run_ours(args, dist, rank, local, ws):
     les = LES(p, precision="mixed", device=local)
     les.set_initial_conditions(u0, v0, w0)
     T = args.train_steps if args.closure == "mlp" else 0
-    train = train_closure(les, p, T) if T else None
+    train = train_closure(les, p, T, args.train_epochs, args.train_batch_tiles) if T else None
     les.step(W)
     les.sync()
     barrier(dist, local)
@@ -290,31 +292,29 @@ def run_ours(args, dist, rank, local, ws):
         print(json.dumps(line), flush=True)
 
 
-EPOCHS = 4
-
-
-def train_closure(les, p, T: int) -> dict:
+def train_closure(les, p, T: int, epochs: int = 4, tiles: int = 16) -> dict:
     """Untimed: T LASD steps; the (features, log Cs^2) pairs of consecutive
-    update steps (one point in 8, every point of the 8 lowest levels; the
-    first update only records the coefficient) train the closure on the
-    GPU; the state then continues with the learned closure."""
+    update steps (one point in 8, every point of the 8 lowest levels, the
+    two wall levels 4 times; the first update only records the coefficient)
+    train the closure on the GPU; the state then continues with the learned
+    closure."""
     les.mlp_init(0)
-    les.mlp_reset_data(1 << 23)
+    les.mlp_reset_data(1 << 24)
     t0 = time.perf_counter()
     for _ in range(T):
         les.step(1)
         if les.jt_total >= p.dyn_init and les.jt_total % p.cs_count == 0:  # consecutive updates
-            les.mlp_collect(stride=8, seed=les.jt_total, dense_levels=8)
+            les.mlp_collect(stride=8, seed=les.jt_total, dense_levels=8, wall_repeat=4)
     les.sync()
     t1 = time.perf_counter()
     ntr, nva = les.mlp_counts()
     les.mlp_fit_stats()
-    losses, val = les.mlp_train(epochs=EPOCHS, tiles_per_step=16, lr=2e-3)
+    losses, val = les.mlp_train(epochs=epochs, tiles_per_step=tiles, lr=2e-3)
     les.sync()
     t2 = time.perf_counter()
     les.set_sgs_model("mlp")
-    return {"lasd_steps": T, "train_pairs": ntr, "validation_pairs": nva, "epochs": EPOCHS,
-            "batch": 16 * 128, "train_loss": [round(float(x), 4) for x in losses],
+    return {"lasd_steps": T, "train_pairs": ntr, "validation_pairs": nva, "epochs": epochs,
+            "batch": tiles * 128, "train_loss": [round(float(x), 4) for x in losses],
             "validation_loss": round(val, 4), "collect_s": round(t1 - t0, 3), "train_s": round(t2 - t1, 3)}
 
 

@@ -210,11 +210,12 @@ int les_mlp_get_params(les_state* s, float* params, int n);
 int les_mlp_reset_data(les_state* s, long cap);
 /* append the current state's (features, log cs_opt2) pairs, one point in
  * `stride` (seeded hash) and every point of levels 1..dense_levels, 10 % of
- * them to the validation set; pairs beyond the capacity are dropped.  Call
+ * them to the validation set, the training pairs of levels 1 and 2
+ * wall_repeat (1..16) times; pairs beyond the capacity are dropped.  Call
  * it right after consecutive dynamic-update steps: the previous coefficient
  * of a pair is the one the previous call saw (the first call only records
  * it). */
-int les_mlp_collect(les_state* s, int stride, int dense_levels, unsigned seed);
+int les_mlp_collect(les_state* s, int stride, int dense_levels, int wall_repeat, unsigned seed);
 int les_mlp_counts(les_state* s, long long out2[2]);
 /* feature/target statistics of the collected data; normalises it in place */
 int les_mlp_fit_stats(les_state* s);

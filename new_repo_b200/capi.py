@@ -96,7 +96,7 @@ PROTOTYPES = {
     "les_mlp_set_params": [_P, _F, _I],
     "les_mlp_get_params": [_P, _F, _I],
     "les_mlp_reset_data": [_P, C.c_long],
-    "les_mlp_collect": [_P, _I, _I, C.c_uint],
+    "les_mlp_collect": [_P, _I, _I, _I, C.c_uint],
     "les_mlp_counts": [_P, C.POINTER(C.c_longlong)],
     "les_mlp_fit_stats": [_P],
     "les_mlp_train": [_P, _I, _I, C.c_double, _D, _D],

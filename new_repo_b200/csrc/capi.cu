@@ -268,9 +268,9 @@ int les_mlp_reset_data(les_state* s, long cap) {
   }
   return guard([&] { s->s->mlp_reset_data(cap); });
 }
-int les_mlp_collect(les_state* s, int stride, int dense_levels, unsigned seed) {
+int les_mlp_collect(les_state* s, int stride, int dense_levels, int wall_repeat, unsigned seed) {
   STATE_OR_FAIL(s);
-  return guard([&] { s->s->mlp_collect(stride, dense_levels, seed); });
+  return guard([&] { s->s->mlp_collect(stride, dense_levels, wall_repeat, seed); });
 }
 int les_mlp_counts(les_state* s, long long out2[2]) {
   STATE_OR_FAIL(s);

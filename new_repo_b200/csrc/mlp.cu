@@ -35,11 +35,23 @@ __host__ __device__ constexpr int kmaj_off(int row, int k, int sbo) {
   return (row >> 3) * sbo + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
 }
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752440f)); }
+// GELU in its tanh form (Hendrycks & Gimpel, 2016):
+//   gelu(x) = x / 2 * (1 + tanh(sqrt(2/pi) * (x + 0.044715 x^3)))
+// with the hardware tanh approximation (one MUFU operation)
+__device__ __forceinline__ float tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+constexpr float GELU_C0 = 0.7978845608028654f;  // sqrt(2 / pi)
+constexpr float GELU_C1 = 0.044715f;
+__device__ __forceinline__ float gelu(float x) {
+  const float t = tanh_fast(GELU_C0 * fmaf(GELU_C1 * x, x * x, x));
+  return 0.5f * x * (1.0f + t);
+}
 __device__ __forceinline__ float gelu_grad(float x) {
-  const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752440f));
-  const float pdf = 0.39894228040143267794f * expf(-0.5f * x * x);
-  return cdf + x * pdf;
+  const float t = tanh_fast(GELU_C0 * fmaf(GELU_C1 * x, x * x, x));
+  return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * GELU_C0 * fmaf(3.0f * GELU_C1, x * x, 1.0f);
 }
 
 __device__ __forceinline__ uint16_t bf16_bits(float x) {
@@ -126,7 +138,7 @@ __device__ __forceinline__ unsigned hash32(unsigned x) {
 // --------------------------------------------------------- collection ----
 template <typename T>
 __global__ void k_mlp_collect(const MlpFeatIn<T> a, const T* cs, MlpDevice m, int stride, int dense_levels,
-                              unsigned seed) {
+                              int wall_repeat, unsigned seed) {
   const long n = (long)(a.nz + 1) * a.plane;
   float lmin[8], lmax[8];
 #pragma unroll
@@ -144,6 +156,10 @@ __global__ void k_mlp_collect(const MlpFeatIn<T> a, const T* cs, MlpDevice m, in
       lmin[i] = fminf(lmin[i], t[i]);
       lmax[i] = fmaxf(lmax[i], t[i]);
     }
+    // the current coefficient is the next update's previous coefficient
+    const float lcur = logf(fmaxf(float(cs[o]), 1e-6f));
+    lmin[5] = fminf(lmin[5], lcur);
+    lmax[5] = fmaxf(lmax[5], lcur);
     const unsigned h = hash32(unsigned(q) * 2654435761u ^ seed);
     const unsigned st = k <= dense_levels ? 1u : unsigned(stride);  // every point of the lowest levels
     if (h % st != 0) continue;
@@ -151,12 +167,17 @@ __global__ void k_mlp_collect(const MlpFeatIn<T> a, const T* cs, MlpDevice m, in
     // network's identity part is exact, it learns the relaxation)
     const float y = fmaxf(logf(fmaxf(float(cs[o]), 1e-30f)), MLP_LOG_CS_FLOOR) - t[5];
     const int val = ((h / st) % 10u) == 0u;  // 10 % held out
-    const unsigned long long idx = atomicAdd(&m.counts[val], 1ull);
-    if ((long)idx >= m.cap) continue;
-    float* x = (val ? m.vx : m.dx) + idx * MLP_IN;
+    // the two levels next to the wall, where the SGS stress carries the
+    // momentum flux, enter the training set wall_repeat times
+    const int rep = (k <= 2 && !val) ? wall_repeat : 1;
+    const unsigned long long idx = atomicAdd(&m.counts[val], (unsigned long long)rep);
+    for (int r = 0; r < rep; ++r) {
+      if ((long)(idx + r) >= m.cap) break;
+      float* x = (val ? m.vx : m.dx) + (idx + r) * MLP_IN;
 #pragma unroll
-    for (int i = 0; i < MLP_IN; ++i) x[i] = t[i];
-    (val ? m.vt : m.dt)[idx] = y;
+      for (int i = 0; i < MLP_IN; ++i) x[i] = t[i];
+      (val ? m.vt : m.dt)[idx + r] = y;
+    }
   }
   // feature range of the state: warp reduction, one atomic per warp and bound
 #pragma unroll
@@ -243,13 +264,15 @@ __global__ void k_mlp_pack(const float* p, uint16_t* img) {
 }
 
 // -------------------------------------------------- shared tile layout ----
-struct __align__(1024) MlpSmem {
-  unsigned char A1[TILE * 16 * 2];   // 4 KB  features (K-major, sbo 256)
-  unsigned char A2[TILE * 64 * 2];   // 16 KB h1 (K-major, sbo 1024)
-  unsigned char G2[TILE * 64 * 2];   // 16 KB g2 (training: A of g2 . W2^T)
+// TRAIN adds the operands of the backward GEMM (g2 . W2^T)
+template <bool TRAIN>
+struct __align__(1024) MlpSmemT {
+  unsigned char A1[TILE * 16 * 2];                 // 4 KB  features (K-major, sbo 256)
+  unsigned char A2[TILE * 64 * 2];                 // 16 KB h1 (K-major, sbo 1024)
   unsigned char B1[2048];
   unsigned char B2[8192];
-  unsigned char B2T[8192];
+  unsigned char G2[TRAIN ? TILE * 64 * 2 : 16];    // 16 KB g2 (K-major, sbo 1024)
+  unsigned char B2T[TRAIN ? 8192 : 16];
   float b1[64], b2[64], w3[64];
   float stats[MLP_NS];
   float b3;
@@ -257,15 +280,19 @@ struct __align__(1024) MlpSmem {
   uint32_t tmem;
   int ok;
 };
+using InferSmem = MlpSmemT<false>;
+using MlpSmem = MlpSmemT<true>;
 
-__device__ __forceinline__ void load_images(MlpSmem& S, const uint16_t* img, const float* p, const float* stats,
-                                            bool with_b2t) {
+template <bool TRAIN>
+__device__ __forceinline__ void load_images(MlpSmemT<TRAIN>& S, const uint16_t* img, const float* p,
+                                            const float* stats) {
+  constexpr bool with_b2t = TRAIN;
   const uint4* src = reinterpret_cast<const uint4*>(img);
   uint4* d1 = reinterpret_cast<uint4*>(S.B1);
   for (int i = threadIdx.x; i < 2048 / 16; i += blockDim.x) d1[i] = src[i];
   uint4* d2 = reinterpret_cast<uint4*>(S.B2);
   for (int i = threadIdx.x; i < 8192 / 16; i += blockDim.x) d2[i] = src[2048 / 16 + i];
-  if (with_b2t) {
+  if constexpr (with_b2t) {
     uint4* d3 = reinterpret_cast<uint4*>(S.B2T);
     for (int i = threadIdx.x; i < 8192 / 16; i += blockDim.x) d3[i] = src[(2048 + 8192) / 16 + i];
   }
@@ -278,16 +305,20 @@ __device__ __forceinline__ void load_images(MlpSmem& S, const uint16_t* img, con
   if (threadIdx.x == 0) S.b3 = p[MLP_O_B3];
 }
 
+// two floats as a BF16 pair (round to nearest even), lo in the low half
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
 // write this thread's 8 normalised features as row `row` of A1
-__device__ __forceinline__ void put_features(MlpSmem& S, int row, const float* x) {
+template <class S_t>
+__device__ __forceinline__ void put_features(S_t& S, int row, const float* x) {
   uint4 c0, c1;
-  uint16_t h[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) h[i] = bf16_bits(x[i]);
-  c0.x = h[0] | (uint32_t(h[1]) << 16);
-  c0.y = h[2] | (uint32_t(h[3]) << 16);
-  c0.z = h[4] | (uint32_t(h[5]) << 16);
-  c0.w = h[6] | (uint32_t(h[7]) << 16);
+  c0.x = pack_bf16x2(x[0], x[1]);
+  c0.y = pack_bf16x2(x[2], x[3]);
+  c0.z = pack_bf16x2(x[4], x[5]);
+  c0.w = pack_bf16x2(x[6], x[7]);
   c1 = make_uint4(0, 0, 0, 0);
   *reinterpret_cast<uint4*>(S.A1 + kmaj_off(row, 0, 256)) = c0;
   *reinterpret_cast<uint4*>(S.A1 + kmaj_off(row, 8, 256)) = c1;
@@ -298,10 +329,10 @@ __device__ __forceinline__ void put_row64(unsigned char* tile, int row, const fl
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
     uint4 q;
-    q.x = bf16_bits(v[8 * c + 0]) | (uint32_t(bf16_bits(v[8 * c + 1])) << 16);
-    q.y = bf16_bits(v[8 * c + 2]) | (uint32_t(bf16_bits(v[8 * c + 3])) << 16);
-    q.z = bf16_bits(v[8 * c + 4]) | (uint32_t(bf16_bits(v[8 * c + 5])) << 16);
-    q.w = bf16_bits(v[8 * c + 6]) | (uint32_t(bf16_bits(v[8 * c + 7])) << 16);
+    q.x = pack_bf16x2(v[8 * c + 0], v[8 * c + 1]);
+    q.y = pack_bf16x2(v[8 * c + 2], v[8 * c + 3]);
+    q.z = pack_bf16x2(v[8 * c + 4], v[8 * c + 5]);
+    q.w = pack_bf16x2(v[8 * c + 6], v[8 * c + 7]);
     *reinterpret_cast<uint4*>(tile + kmaj_off(row, 8 * c, 1024)) = q;
   }
 }
@@ -320,22 +351,26 @@ __device__ __forceinline__ void tmem_row64(uint32_t tbase, int col, float* v) {
 
 // issue one tensor-core stage (thread 0) and wait for it (bounded);
 // returns false (and flags the status) when the wait ran out
-__device__ __forceinline__ bool tc_stage(MlpSmem& S, uint32_t& phase, unsigned* status, int which) {
+// stage 0: D = X . W1, 1: D = H1 . W2, 2: D = G2 . W2^T, D at TMEM column dcol
+template <bool TRAIN>
+__device__ __forceinline__ bool tc_stage(MlpSmemT<TRAIN>& S, uint32_t& phase, unsigned* status, int which,
+                                         uint32_t dcol) {
   if (threadIdx.x == 0) {
     tc::fence_after_sync();
-    const uint32_t a1 = tc::smem_u32(S.A1), a2 = tc::smem_u32(S.A2), g2 = tc::smem_u32(S.G2);
-    const uint32_t b1 = tc::smem_u32(S.B1), b2 = tc::smem_u32(S.B2), b2t = tc::smem_u32(S.B2T);
-    if (which == 0) {  // D1 = X . W1
-      tc::mma_bf16(S.tmem + 0, tc::smem_desc(a1, 128, 256), tc::smem_desc(b1, 128, 256), IDESC, 0);
-    } else if (which == 1) {  // D2 = H1 . W2
+    const uint32_t a1 = tc::smem_u32(S.A1), a2 = tc::smem_u32(S.A2);
+    const uint32_t b1 = tc::smem_u32(S.B1), b2 = tc::smem_u32(S.B2);
+    if (which == 0) {
+      tc::mma_bf16(S.tmem + dcol, tc::smem_desc(a1, 128, 256), tc::smem_desc(b1, 128, 256), IDESC, 0);
+    } else if (which == 1) {
 #pragma unroll
       for (int s = 0; s < 4; ++s)
-        tc::mma_bf16(S.tmem + 64, tc::smem_desc(a2 + 256 * s, 128, 1024), tc::smem_desc(b2 + 256 * s, 128, 1024),
+        tc::mma_bf16(S.tmem + dcol, tc::smem_desc(a2 + 256 * s, 128, 1024), tc::smem_desc(b2 + 256 * s, 128, 1024),
                      IDESC, s > 0);
-    } else {  // D3 = G2 . W2^T
+    } else if constexpr (TRAIN) {
+      const uint32_t g2 = tc::smem_u32(S.G2), b2t = tc::smem_u32(S.B2T);
 #pragma unroll
       for (int s = 0; s < 4; ++s)
-        tc::mma_bf16(S.tmem + 128, tc::smem_desc(g2 + 256 * s, 128, 1024), tc::smem_desc(b2t + 256 * s, 128, 1024),
+        tc::mma_bf16(S.tmem + dcol, tc::smem_desc(g2 + 256 * s, 128, 1024), tc::smem_desc(b2t + 256 * s, 128, 1024),
                      IDESC, s > 0);
     }
     tc::mma_commit(&S.mbar);
@@ -348,7 +383,8 @@ __device__ __forceinline__ bool tc_stage(MlpSmem& S, uint32_t& phase, unsigned* 
   return S.ok != 0;
 }
 
-__device__ __forceinline__ void tc_setup(MlpSmem& S, uint32_t ncols) {
+template <class S_t>
+__device__ __forceinline__ void tc_setup(S_t& S, uint32_t ncols) {
   if (threadIdx.x < 32) {
     tc::tmem_alloc(&S.tmem, ncols);
     tc::tmem_relinquish();
@@ -362,7 +398,8 @@ __device__ __forceinline__ void tc_setup(MlpSmem& S, uint32_t ncols) {
   __syncthreads();
   tc::fence_after_sync();
 }
-__device__ __forceinline__ void tc_teardown(MlpSmem& S, uint32_t ncols, uint32_t phase) {
+template <class S_t>
+__device__ __forceinline__ void tc_teardown(S_t& S, uint32_t ncols, uint32_t phase) {
   // after a timed-out stage, wait (bounded) for the MMA still in flight
   if (threadIdx.x == 0 && !S.ok) tc::mbar_wait(&S.mbar, phase ^ 1u);
   tc::fence_before_sync();
@@ -375,10 +412,10 @@ __device__ __forceinline__ void tc_teardown(MlpSmem& S, uint32_t ncols, uint32_t
 template <typename T>
 __global__ void __launch_bounds__(TILE) k_mlp_infer(const MlpFeatIn<T> a, T* cs, MlpDevice m, unsigned* status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  MlpSmem& S = *reinterpret_cast<MlpSmem*>(smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023));
-  load_images(S, m.img, m.params, m.stats, false);
+  InferSmem& S = *reinterpret_cast<InferSmem*>(smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023));
+  load_images(S, m.img, m.params, m.stats);
   if (threadIdx.x == 0) S.ok = 1;
-  tc_setup(S, 128);
+  tc_setup(S, 64);  // both layers accumulate in TMEM columns 0..63
   uint32_t phase = 0;
   const long npts = (long)(a.nz + 1) * a.plane;
   const long ntiles = (npts + TILE - 1) / TILE;
@@ -406,7 +443,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_infer(const MlpFeatIn<T> a, T* cs,
     tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
-    if (!tc_stage(S, phase, status, 0)) break;
+    if (!tc_stage(S, phase, status, 0, 0)) break;
     float h[64];
     tmem_row64(S.tmem, 0, h);
 #pragma unroll
@@ -415,20 +452,24 @@ __global__ void __launch_bounds__(TILE) k_mlp_infer(const MlpFeatIn<T> a, T* cs,
     tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
-    if (!tc_stage(S, phase, status, 1)) break;
-    tmem_row64(S.tmem, 64, h);
+    if (!tc_stage(S, phase, status, 1, 0)) break;
+    tmem_row64(S.tmem, 0, h);
     float y = S.b3;
 #pragma unroll
     for (int i = 0; i < 64; ++i) y += S.w3[i] * gelu(h[i] + S.b2[i]);
     if (valid) {
-      y = fminf(fmaxf(y, S.stats[MLP_S_YMIN]), S.stats[MLP_S_YMAX]);  // no extrapolated coefficients
-      const float lc = lprev + S.stats[MLP_S_YMU] + S.stats[MLP_S_YSD] * y;
+      // no extrapolation: the change is clamped to the trained range, the
+      // coefficient to the range of the previous coefficients seen in training
+      y = fminf(fmaxf(y, S.stats[MLP_S_YMIN]), S.stats[MLP_S_YMAX]);
+      float lc = lprev + S.stats[MLP_S_YMU] + S.stats[MLP_S_YSD] * y;
+      lc = fminf(fmaxf(lc, S.stats[MLP_S_MU + 5] + S.stats[MLP_S_SD + 5] * S.stats[MLP_S_MIN + 5]),
+                 S.stats[MLP_S_MU + 5] + S.stats[MLP_S_SD + 5] * S.stats[MLP_S_MAX + 5]);
       cs[o] = T(fminf(fmaxf(expf(lc), 1e-24f), 1.0f));
     }
     tc::fence_before_sync();
     __syncthreads();
   }
-  tc_teardown(S, 128, phase);
+  tc_teardown(S, 64, phase);
 }
 
 // ------------------------------------------------------------- training ----
@@ -449,7 +490,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(MlpDevice m, const float* X,
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   TrainSmem& TS = *reinterpret_cast<TrainSmem*>(smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023));
   MlpSmem& S = TS.s;
-  load_images(S, m.img, m.params, m.stats, true);
+  load_images(S, m.img, m.params, m.stats);
   if (threadIdx.x == 0) S.ok = 1;
   tc_setup(S, 256);
   const int tid = threadIdx.x;
@@ -473,7 +514,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(MlpDevice m, const float* X,
     tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
-    if (!tc_stage(S, phase, status, 0)) break;
+    if (!tc_stage(S, phase, status, 0, 0)) break;
     float z1[64], h[64];
     tmem_row64(S.tmem, 0, z1);
 #pragma unroll
@@ -485,7 +526,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(MlpDevice m, const float* X,
     tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
-    if (!tc_stage(S, phase, status, 1)) break;
+    if (!tc_stage(S, phase, status, 1, 64)) break;
     tmem_row64(S.tmem, 64, h);  // z2 (without bias)
     float y = S.b3;
     for (int i = 0; i < 64; ++i) {
@@ -529,7 +570,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(MlpDevice m, const float* X,
         for (int i = 0; i < 32; ++i) aw2[i] += hv * TS.g2f[r][n0 + i];
       }
     }
-    if (!tc_stage(S, phase, status, 2)) break;
+    if (!tc_stage(S, phase, status, 2, 128)) break;
     // delta1 = (g2 . W2^T) * gelu'(z1)
     float d1[64];
     tmem_row64(S.tmem, 128, d1);
@@ -615,18 +656,18 @@ __global__ void k_mlp_blend(T* cs, const T* cs_dyn, const int* flag, long plane,
   }
 }
 
-size_t infer_smem() { return sizeof(MlpSmem) + 1024; }
+size_t infer_smem() { return sizeof(InferSmem) + 1024; }
 size_t train_smem() { return sizeof(TrainSmem) + 1024; }
 
 }  // namespace
 
 // ------------------------------------------------------------- host side ----
 template <typename T>
-void mlp_collect(const MlpFeatIn<T>& in, const T* cs, MlpDevice& m, int stride, int dense_levels, unsigned seed,
-                 cudaStream_t st) {
+void mlp_collect(const MlpFeatIn<T>& in, const T* cs, MlpDevice& m, int stride, int dense_levels, int wall_repeat,
+                 unsigned seed, cudaStream_t st) {
   const long n = (long)(in.nz + 1) * in.plane;
   hook_before("k_mlp_collect", double(n) * 12 * sizeof(T));
-  k_mlp_collect<T><<<148 * 8, 256, 0, st>>>(in, cs, m, stride, dense_levels, seed);
+  k_mlp_collect<T><<<148 * 8, 256, 0, st>>>(in, cs, m, stride, dense_levels, wall_repeat, seed);
   LES_CHECK_LAUNCH();
   hook_after();
 }
@@ -636,7 +677,7 @@ void mlp_infer(const MlpFeatIn<T>& in, T* cs, MlpDevice& m, unsigned* status, cu
   LES_CUDA(cudaMemsetAsync(m.colflag, 0, sizeof(int) * m.plane, st));
   const long n = (long)(in.nz + 1) * in.plane;
   const long ntiles = (n + TILE - 1) / TILE;
-  const int grid = int(std::min<long>(ntiles, 148L * 4));
+  const int grid = int(std::min<long>(ntiles, 148L * 5));  // 5 CTAs per SM fit (registers)
   hook_before("k_mlp_infer", double(n) * 12 * sizeof(T));
   k_mlp_infer<T><<<grid, TILE, infer_smem(), st>>>(in, cs, m, status);
   LES_CHECK_LAUNCH();
@@ -782,8 +823,9 @@ double mlp_blend(T* cs, const T* cs_dyn, MlpDevice& m, int nz, bool check, doubl
 template double mlp_blend<float>(float*, const float*, MlpDevice&, int, bool, double*, cudaStream_t);
 template double mlp_blend<double>(double*, const double*, MlpDevice&, int, bool, double*, cudaStream_t);
 
-template void mlp_collect<float>(const MlpFeatIn<float>&, const float*, MlpDevice&, int, int, unsigned, cudaStream_t);
-template void mlp_collect<double>(const MlpFeatIn<double>&, const double*, MlpDevice&, int, int, unsigned,
+template void mlp_collect<float>(const MlpFeatIn<float>&, const float*, MlpDevice&, int, int, int, unsigned,
+                                 cudaStream_t);
+template void mlp_collect<double>(const MlpFeatIn<double>&, const double*, MlpDevice&, int, int, int, unsigned,
                                   cudaStream_t);
 template void mlp_infer<float>(const MlpFeatIn<float>&, float*, MlpDevice&, unsigned*, cudaStream_t);
 template void mlp_infer<double>(const MlpFeatIn<double>&, double*, MlpDevice&, unsigned*, cudaStream_t);

@@ -60,11 +60,11 @@ struct MlpDevice {
 
 // feature transforms shared by inference and data collection
 // append (features, log cs) pairs: one point in `stride` (seeded hash), every
-// point of levels 1..dense_levels; the features' previous coefficient is
-// in.csprev
+// point of levels 1..dense_levels, the training pairs of levels 1 and 2
+// wall_repeat times; the features' previous coefficient is in.csprev
 template <typename T>
-void mlp_collect(const MlpFeatIn<T>& in, const T* cs, MlpDevice& m, int stride, int dense_levels, unsigned seed,
-                 cudaStream_t st);
+void mlp_collect(const MlpFeatIn<T>& in, const T* cs, MlpDevice& m, int stride, int dense_levels, int wall_repeat,
+                 unsigned seed, cudaStream_t st);
 template <typename T>
 void mlp_infer(const MlpFeatIn<T>& in, T* cs, MlpDevice& m, unsigned* status, cudaStream_t st);
 // empty the collected feature range

@@ -463,14 +463,16 @@ class Solver final : public SolverBase {
     LES_CUDA(cudaMemsetAsync(md.counts, 0, 2 * sizeof(unsigned long long), st));
     mlp_reset_range(md, st);
   }
-  void mlp_collect(int stride, int dense_levels, unsigned seed) override {
+  void mlp_collect(int stride, int dense_levels, int wall_repeat, unsigned seed) override {
     if (!mlp_alloc || md.cap == 0) throw CudaError(1, "learned closure: call les_mlp_reset_data first");
     Tag tag_(this, "mlp");
     ensure_mlp();
     // pairs (features with the previous collection's coefficient, current
     // coefficient): collect at consecutive dynamic updates; the first call
     // only records the coefficient
-    if (have_prev) les::mlp_collect<T>(feat_in(), F[LES_CS_OPT2], md, std::max(1, stride), dense_levels, seed, st);
+    if (have_prev)
+      les::mlp_collect<T>(feat_in(), F[LES_CS_OPT2], md, std::max(1, stride), dense_levels,
+                          std::min(16, std::max(1, wall_repeat)), seed, st);
     copy(cs_prev, F[LES_CS_OPT2], g.field());
     have_prev = true;
   }

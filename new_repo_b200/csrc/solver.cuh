@@ -116,7 +116,7 @@ struct SolverBase : LaunchHook {
   virtual void mlp_set_params(const float* p, int n) = 0;
   virtual void mlp_get_params(float* p, int n) = 0;
   virtual void mlp_reset_data(long cap) = 0;
-  virtual void mlp_collect(int stride, int dense_levels, unsigned seed) = 0;
+  virtual void mlp_collect(int stride, int dense_levels, int wall_repeat, unsigned seed) = 0;
   virtual void mlp_counts(long long* c) = 0;
   virtual void mlp_fit_stats() = 0;
   virtual void mlp_train(int epochs, int tiles_per_step, double lr, double* loss_epochs, double* val_loss) = 0;

@@ -421,10 +421,13 @@ class LES:
     def mlp_reset_data(self, cap: int):
         check(self.lib.les_mlp_reset_data(self._h, int(cap)))
 
-    def mlp_collect(self, stride: int = 1, seed: int = 0, dense_levels: int = 0):
-        """Append (invariants, log Cs^2) pairs of the current state: one point in
-        ``stride``, every point of levels 1..dense_levels."""
-        check(self.lib.les_mlp_collect(self._h, int(stride), int(dense_levels), int(seed) & 0xFFFFFFFF))
+    def mlp_collect(self, stride: int = 1, seed: int = 0, dense_levels: int = 0, wall_repeat: int = 1):
+        """Append (features, log Cs^2) pairs of the current state: one point in
+        ``stride``, every point of levels 1..dense_levels, the training pairs of
+        levels 1 and 2 ``wall_repeat`` times.  Call right after consecutive
+        dynamic-update steps (the first call only records the coefficient)."""
+        check(self.lib.les_mlp_collect(self._h, int(stride), int(dense_levels), int(wall_repeat),
+                                       int(seed) & 0xFFFFFFFF))
 
     def mlp_counts(self) -> tuple:
         out = (C.c_longlong * 2)()

@@ -26,7 +26,6 @@ FP64 network (checked against finite differences in ``tests/test_mlp.py``).
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 NIN, NH = 8, 64
 O_W1 = 0
@@ -55,12 +54,18 @@ def unpack(p):
             p[O_W3:O_B3], p[O_B3])
 
 
+GELU_C0 = np.sqrt(2.0 / np.pi)
+GELU_C1 = 0.044715
+
+
 def gelu(x):
-    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+    """GELU in its tanh form (Hendrycks & Gimpel, 2016), as the kernels use it."""
+    return 0.5 * x * (1.0 + np.tanh(GELU_C0 * (x + GELU_C1 * x ** 3)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(GELU_C0 * (x + GELU_C1 * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * GELU_C0 * (1.0 + 3.0 * GELU_C1 * x * x)
 
 
 def forward(p, x, bf16_ops=True):
@@ -166,9 +171,13 @@ def raw_features(d, u, v, cs_prev, k, dz, delta, log_delta_z0, wall):
 def cs_from_output(y, stats, log_cs_prev):
     """Cs^2 from the normalised output (k_mlp_infer's epilogue): the output,
     clamped to the trained target range, is the change of log Cs^2 from the
-    floored previous coefficient (feature 5, unnormalised)."""
+    floored previous coefficient (feature 5, unnormalised); log Cs^2 is then
+    clamped to the range of feature 5 seen in training."""
     y = np.clip(np.asarray(y, np.float64), stats[S_YMIN], stats[S_YMAX])
     lc = np.asarray(log_cs_prev, np.float64) + stats[S_YMU] + stats[S_YSD] * y
+    lo = stats[S_MU + 5] + stats[S_SD + 5] * stats[S_MIN + 5]
+    hi = stats[S_MU + 5] + stats[S_SD + 5] * stats[S_MAX + 5]
+    lc = np.clip(lc, lo, hi)
     return np.clip(np.exp(lc), 1e-24, 1.0)
 
 

@@ -2,11 +2,13 @@
 (tcgen05 forward, training gradients, features, fallback to the dynamic
 procedure) against it.
 
-Tolerances: the GPU network uses BF16 operands with FP32 accumulation; the
-oracle reproduces that rounding, so outputs agree to accumulation-order
-noise except where a BF16 rounding of a hidden activation flips (rare; one
-BF16 ulp is 2^-8 relative).  Outputs: max |dy| <= 2e-3 * (1 + |y|).
-Gradients: per parameter block, max |dg| <= 2e-3 * max |g| of the block.
+Tolerances: the GPU network uses BF16 operands with FP32 accumulation and
+the hardware tanh approximation (relative error below 2^-10.9) inside GELU;
+the oracle reproduces the BF16 rounding with an exact tanh, so outputs
+differ by the tanh error and by the BF16 roundings of hidden activations it
+flips (one BF16 ulp is 2^-8 relative).  Outputs: max |dy| <= 2e-3 * (1 + |y|),
+median |dy| <= 2e-4.  Gradients: per parameter block, max |dg| <= 2e-3 *
+max |g| of the block.
 """
 import numpy as np
 import pytest
@@ -103,7 +105,7 @@ def test_mlp_forward_matches_oracle(gpu, n):
     yo = M.forward(p, x)
     err = np.abs(y - yo)
     assert err.max() <= 2e-3 * (1 + np.abs(yo).max()), err.max()
-    assert np.median(err) <= 1e-5
+    assert np.median(err) <= 2e-4
     les.close()
 
 
@@ -167,7 +169,7 @@ def test_mlp_inference_in_step_matches_oracle(gpu, precision):
     cso, _ = _oracle_cs(les, p, st, cs_prev)
     cso = cso.reshape(cs.shape)
     e = np.abs(np.log(cs) - np.log(cso))
-    assert e.max() <= 2e-2 and np.median(e) <= 1e-4, (e.max(), np.median(e))
+    assert e.max() <= 2e-2 and np.median(e) <= 3e-4, (e.max(), np.median(e))
     assert les.mlp_info()["flagged_columns"] == 0
     les.close()
 
