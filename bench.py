@@ -3,10 +3,11 @@
 
 Headline arm: the mixed-precision step (FP32 fields, FFTs, convection and
 SGS; FP64 tridiagonal pressure solve, mean mode and compensated diagnostics)
-with the learned SGS closure (8 invariants -> 64 -> 64 -> Cs^2 on the tcgen05
+with the learned SGS closure (8 features -> 64 -> 64 -> Cs^2 on the tcgen05
 tensor cores, trained on the GPU from Lagrangian scale-dependent dynamic
-(LASD) pairs of the first steps, untimed; LASD fallback for columns outside
-the training range and an LASD check of the closure every 10 updates).
+(LASD) pairs of the first 30 steps, untimed; the 8 levels next to the wall
+keep the LASD procedure, LASD fallback for columns outside the training
+range and an LASD check of the closure every 10 updates).
 Beside it, the same step with the LASD closure and the plain FP64 GPU step
 (LASD) of the same seed: their throughputs and the velocity error between
 the headline and FP64 runs are part of the JSON line.
@@ -51,6 +52,8 @@ def parse():
     ap.add_argument("--closure", default="mlp", choices=["mlp", "lasd"], help="SGS closure of the headline arm")
     ap.add_argument("--train-steps", type=int, default=30, help="LASD steps that produce the training pairs")
     ap.add_argument("--train-epochs", type=int, default=4)
+    ap.add_argument("--wall-levels", type=int, default=8,
+                    help="levels next to the wall that keep the LASD procedure under the learned closure")
     ap.add_argument("--train-batch-tiles", type=int, default=16, help="training batch = 128 x this")
     return ap.parse_args()
 
@@ -191,6 +194,9 @@ def run_ours(args, dist, rank, local, ws):
     les.set_initial_conditions(u0, v0, w0)
     T = args.train_steps if args.closure == "mlp" else 0
     train = train_closure(les, p, T, args.train_epochs, args.train_batch_tiles) if T else None
+    if T:
+        les.mlp_set_wall_levels(args.wall_levels)
+        train["wall_levels"] = args.wall_levels
     les.step(W)
     les.sync()
     barrier(dist, local)
@@ -208,6 +214,10 @@ def run_ours(args, dist, rank, local, ws):
     status = les.status()
     if train is not None:
         train.update(les.mlp_info())
+        prof_chk = les.mlp_check_profile()
+        kmax = int(np.argmax(prof_chk))
+        train["check_profile_max"] = {"level": kmax + 1, "rms_log_error": round(float(prof_chk[kmax]), 4)}
+        train["check_profile_levels_1_12"] = [round(float(x), 4) for x in prof_chk[:12]]
     # ---- roofline of the dominant kernel (live events of the timed region) ----
     top = max(prof.items(), key=lambda kv: kv[1]["ms"])
     label, rec = top
@@ -278,7 +288,8 @@ def run_ours(args, dist, rank, local, ws):
             "dtype": "f32 (fields, FFTs, convection, SGS) + f64 (pressure solve, mean mode, diagnostics)",
             "data": "synthetic: log-law profile + seeded uniform +-0.1 noise (counter-based hash)",
             "config": {"workload": f"LES time step {p.nx}x{p.ny}x{p.nz}, 3/2 dealiasing, "
-                                   + ("learned SGS closure (LASD fallback/check)" if T else "LASD SGS")
+                                   + (f"learned SGS closure above level {args.wall_levels} (LASD on the "
+                                      f"{args.wall_levels} wall levels, LASD fallback/check)" if T else "LASD SGS")
                                    + " (cs_count 5, closure update every 5th step), log-law wall, "
                                      "FP32+FP64-pressure",
                        "grid": [p.nx, p.ny, p.nz], "dt": p.dt_nd, "sgs_model": "mlp" if T else p.sgs_model,

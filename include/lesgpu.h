@@ -191,7 +191,8 @@ int les_diagnostics_async(les_state* s, double* pinned_out4);
  * Lagrangian scale-dependent procedure (LASD, compute_sgs.f90:286) collected
  * from a running state.  Features: log1p |S|, log1p S:S, log1p W:W, signed
  * log1p tr(S^3), log1p(z / Delta), log Cs^2 before the update (the memory
- * the Lagrangian averages carry), log1p |u_h|, log(Delta / z0).  Columns
+ * the Lagrangian averages carry), signed log1p of the vortex stretching
+ * w_i S_ij w_j, log(Delta / z0).  Columns
  * whose features leave the training range take one Lagrangian relaxation
  * step of the dynamic procedure from the previous coefficient; every
  * `check_every` updates that step also runs on the whole domain and the RMS
@@ -234,12 +235,19 @@ int les_mlp_grad(les_state* s, const float* x, const float* t, long n, float* gr
 int les_mlp_info(les_state* s, double out12[12]);
 /* dynamic-procedure check every `every` closure updates (0 = never) */
 int les_mlp_set_check_every(les_state* s, int every);
+/* levels 1..nlev next to the wall keep the plain LASD procedure (with its
+ * Lagrangian averages) under the learned closure; 0 (default) = none */
+int les_mlp_set_wall_levels(les_state* s, int nlev);
+/* per level 1..nz+1 (out[0..nz]), the RMS of log Cs^2 - log Cs^2_dyn at the
+ * last check (-1 before the first); n >= nz + 1 */
+int les_mlp_check_profile(les_state* s, double* out, int n);
 
 /* ---- allocation-free variant (no reference counterpart) ----------------
  * The horizontal derivatives of les_grad_velocity_filt (the ddx/ddy of
  * compute_derivatives.f90 on one field) for a field already on the device:
  * f [nlev][ny][nx] (FP64) is replaced by its Nyquist-filtered version and
- * dfdx, dfdy receive the derivatives (domain lengths lx, ly).  It allocates
+ * dfdx, dfdy receive the derivatives (domain lengths lx, ly); the three
+ * pointers must be 16-byte aligned (rejected otherwise).  It allocates
  * nothing: the tables and spectra live in one static device buffer of
  * LES_NOALLOC_SCRATCH_BYTES, for callers that must not change the device
  * memory footprint (an in-situ hook in a coupled run whose memory is fully

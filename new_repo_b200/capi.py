@@ -104,6 +104,8 @@ PROTOTYPES = {
     "les_mlp_grad": [_P, _F, _F, C.c_long, _F, _F],
     "les_mlp_info": [_P, _D],
     "les_mlp_set_check_every": [_P, _I],
+    "les_mlp_set_wall_levels": [_P, _I],
+    "les_mlp_check_profile": [_P, _D, _I],
     "les_grad_xy_noalloc": [_P, _P, _P, _I, _I, _I, C.c_double, C.c_double, _P],
 }
 

@@ -319,6 +319,21 @@ int les_mlp_set_check_every(les_state* s, int every) {
   return guard([&] { s->s->mlp_set_check_every(every); });
 }
 
+int les_mlp_set_wall_levels(les_state* s, int nlev) {
+  STATE_OR_FAIL(s);
+  if (nlev < 0) {
+    g_last_error = "learned closure: wall levels must be >= 0";
+    return LES_ERR_INVALID;
+  }
+  return guard([&] { s->s->mlp_set_wall_levels(nlev); });
+}
+
+int les_mlp_check_profile(les_state* s, double* out, int n) {
+  STATE_OR_FAIL(s);
+  if (!out) return bad_state();
+  return guard([&] { s->s->mlp_check_profile(out, n); });
+}
+
 int les_timers(les_state* s, double out[5]) {
   STATE_OR_FAIL(s);
   return guard([&] {

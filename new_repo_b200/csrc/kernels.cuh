@@ -198,6 +198,7 @@ struct LagGeom {
   long plane;
   int mode;  // 0 reference 1x1 halo, 1 periodic
   double dt, dx, dy, dz, cs;
+  int nlev;  // levels 1..nlev are interpolated (nz + 1: all)
 };
 
 // FF(i, j, k) of compute_interpolag_coeff (1-based i, j; level k in 0..nz+2)
@@ -228,7 +229,7 @@ template <typename T>
 __global__ void k_lag_interp(const T* ul, const T* vl, const T* wl, const T* F0, const T* F1, const T* F2,
                              const T* F3, T* N0, T* N1, T* N2, T* N3, LagGeom g) {
   const long pl = g.plane;
-  const long n = (long)(g.nz + 1) * pl;
+  const long n = (long)g.nlev * pl;
   const T cs = T(g.cs);
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const long o = pl + q;
@@ -286,8 +287,8 @@ __device__ __forceinline__ double f32max_tiny(double x) {
 template <typename T>
 __global__ void k_lasd_update(T* FLM, T* FMM, T* FQN, T* FNN, const T* LM, const T* MM, const T* QN, const T* NN,
                               T* cs, T* beta, int init, long plane, int nz, double opftdelta, double lagran_dt,
-                              double beta_pow, const T* cs_init = nullptr) {
-  const long n = (long)(nz + 1) * plane;
+                              double beta_pow, const T* cs_init = nullptr, int nlev = -1) {
+  const long n = (long)(nlev < 0 ? nz + 1 : nlev) * plane;  // levels 1..nlev
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const long o = plane + q;
     const int k = int(o / plane);

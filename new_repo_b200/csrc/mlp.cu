@@ -63,7 +63,7 @@ __device__ __forceinline__ uint16_t bf16_bits(float x) {
 template <typename T>
 __device__ __forceinline__ void raw_features(const MlpFeatIn<T>& a, long o, int k, float* t) {
   const long pl = a.plane;
-  float ux, uy, uz, vx, vy, vz, wx, wy, wz, uh, vh;
+  float ux, uy, uz, vx, vy, vz, wx, wy, wz;
   if (k == 1) {
     ux = float(a.d[0][o]);
     uy = float(a.d[1][o]);
@@ -74,8 +74,6 @@ __device__ __forceinline__ void raw_features(const MlpFeatIn<T>& a, long o, int 
     wx = 0.5f * float(a.d[6][o] + a.d[6][o + pl]);
     wy = 0.5f * float(a.d[7][o] + a.d[7][o + pl]);
     wz = float(a.d[8][o]);
-    uh = float(a.u[o]);
-    vh = float(a.v[o]);
   } else {
     ux = 0.5f * float(a.d[0][o] + a.d[0][o - pl]);
     uy = 0.5f * float(a.d[1][o] + a.d[1][o - pl]);
@@ -86,8 +84,6 @@ __device__ __forceinline__ void raw_features(const MlpFeatIn<T>& a, long o, int 
     wx = float(a.d[6][o]);
     wy = float(a.d[7][o]);
     wz = 0.5f * float(a.d[8][o] + a.d[8][o - pl]);
-    uh = 0.5f * float(a.u[o] + a.u[o - pl]);
-    vh = 0.5f * float(a.v[o] + a.v[o - pl]);
   }
   const float s11 = ux, s22 = vy, s33 = wz;
   const float s12 = 0.5f * (uy + vx), s13 = 0.5f * (uz + wx), s23 = 0.5f * (vz + wy);
@@ -109,7 +105,11 @@ __device__ __forceinline__ void raw_features(const MlpFeatIn<T>& a, long o, int 
   // dynamic procedure relax from it (takes the slot of a gradient Richardson
   // number, which is zero without buoyancy)
   t[5] = logf(fmaxf(float(a.csprev[o]), 1e-6f));
-  t[6] = log1pf(sqrtf(uh * uh + vh * vh));
+  // vortex stretching w_i S_ij w_j (w = vorticity), Galilean invariant
+  const float w1 = -2.0f * o23, w2 = 2.0f * o13, w3 = -2.0f * o12;
+  const float vs = s11 * w1 * w1 + s22 * w2 * w2 + s33 * w3 * w3 +
+                   2.0f * (s12 * w1 * w2 + s13 * w1 * w3 + s23 * w2 * w3);
+  t[6] = copysignf(log1pf(fabsf(vs)), vs);
   t[7] = a.log_delta_z0;
 }
 
@@ -430,13 +430,15 @@ __global__ void __launch_bounds__(TILE) k_mlp_infer(const MlpFeatIn<T> a, T* cs,
       const int k = int(o / a.plane);
       float t[8];
       raw_features(a, o, k, t);
-      int out = 0;  // bit i: feature i outside the training range
+      int out = 0;  // bit i: feature i outside the training range (margin: 0.25 sd + 5 % of the range)
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         x[i] = (t[i] - S.stats[MLP_S_MU + i]) / S.stats[MLP_S_SD + i];
-        if ((x[i] < S.stats[MLP_S_MIN + i] - 0.25f) || (x[i] > S.stats[MLP_S_MAX + i] + 0.25f)) out |= 1 << i;
+        const float mn = S.stats[MLP_S_MIN + i], mx = S.stats[MLP_S_MAX + i];
+        const float margin = 0.25f + 0.05f * (mx - mn);
+        if ((x[i] < mn - margin) || (x[i] > mx + margin)) out |= 1 << i;
       }
-      if (out) atomicOr(&m.colflag[q % a.plane], out);
+      if (out && k > a.wall_levels) atomicOr(&m.colflag[q % a.plane], out);
       lprev = t[5];
     }
     put_features(S, threadIdx.x, x);
@@ -638,21 +640,22 @@ __global__ void k_mlp_count_flags(const int* flag, long plane, int* out) {
   }
 }
 
+// blockIdx.y = level - 1; err2[k] accumulates the squared log differences of level k
 template <typename T>
-__global__ void k_mlp_blend(T* cs, const T* cs_dyn, const int* flag, long plane, int nz, double* err2, int check) {
-  const long n = (long)(nz + 1) * plane;
+__global__ void k_mlp_blend(T* cs, const T* cs_dyn, const int* flag, long plane, double* err2, int check) {
+  const int k = 1 + blockIdx.y;
   double e = 0.0;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
-    const long o = plane + q;
+  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < plane; p += (long)gridDim.x * blockDim.x) {
+    const long o = (long)k * plane + p;
     if (check) {
       const double d = log(fmax(double(cs[o]), 1e-6)) - log(fmax(double(cs_dyn[o]), 1e-6));
       e += d * d;
     }
-    if (flag[q % plane]) cs[o] = cs_dyn[o];
+    if (flag[p]) cs[o] = cs_dyn[o];
   }
   if (check) {
     for (int off = 16; off > 0; off >>= 1) e += __shfl_down_sync(0xffffffffu, e, off);
-    if ((threadIdx.x & 31) == 0) atomicAdd(err2, e);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&err2[k], e);
   }
 }
 
@@ -666,7 +669,7 @@ template <typename T>
 void mlp_collect(const MlpFeatIn<T>& in, const T* cs, MlpDevice& m, int stride, int dense_levels, int wall_repeat,
                  unsigned seed, cudaStream_t st) {
   const long n = (long)(in.nz + 1) * in.plane;
-  hook_before("k_mlp_collect", double(n) * 12 * sizeof(T));
+  hook_before("k_mlp_collect", double(n) * 11 * sizeof(T));
   k_mlp_collect<T><<<148 * 8, 256, 0, st>>>(in, cs, m, stride, dense_levels, wall_repeat, seed);
   LES_CHECK_LAUNCH();
   hook_after();
@@ -678,7 +681,7 @@ void mlp_infer(const MlpFeatIn<T>& in, T* cs, MlpDevice& m, unsigned* status, cu
   const long n = (long)(in.nz + 1) * in.plane;
   const long ntiles = (n + TILE - 1) / TILE;
   const int grid = int(std::min<long>(ntiles, 148L * 5));  // 5 CTAs per SM fit (registers)
-  hook_before("k_mlp_infer", double(n) * 12 * sizeof(T));
+  hook_before("k_mlp_infer", double(n) * 11 * sizeof(T));
   k_mlp_infer<T><<<grid, TILE, infer_smem(), st>>>(in, cs, m, status);
   LES_CHECK_LAUNCH();
   hook_after();
@@ -805,23 +808,22 @@ int mlp_count_flags(MlpDevice& m, int* dcount, int* per_feature, cudaStream_t st
 }
 
 template <typename T>
-double mlp_blend(T* cs, const T* cs_dyn, MlpDevice& m, int nz, bool check, double* derr, cudaStream_t st) {
-  LES_CUDA(cudaMemsetAsync(derr, 0, sizeof(double), st));
+void mlp_blend(T* cs, const T* cs_dyn, MlpDevice& m, int nz, bool check, double* derr, double* profile,
+               cudaStream_t st) {
+  LES_CUDA(cudaMemsetAsync(derr, 0, sizeof(double) * (nz + 2), st));
   const long n = (long)(nz + 1) * m.plane;
   hook_before("k_mlp_blend", double(n) * 3 * sizeof(T));
-  k_mlp_blend<T><<<148 * 4, 256, 0, st>>>(cs, cs_dyn, m.colflag, m.plane, nz, derr, check ? 1 : 0);
+  k_mlp_blend<T><<<dim3(4, nz + 1), 256, 0, st>>>(cs, cs_dyn, m.colflag, m.plane, derr, check ? 1 : 0);
   LES_CHECK_LAUNCH();
   hook_after();
-  double h = 0;
   if (check) {
-    LES_CUDA(cudaMemcpyAsync(&h, derr, sizeof(double), cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaMemcpyAsync(profile, derr, sizeof(double) * (nz + 2), cudaMemcpyDeviceToHost, st));
     LES_CUDA(cudaStreamSynchronize(st));
-    h = std::sqrt(h / double(n));
+    for (int k = 0; k <= nz + 1; ++k) profile[k] = std::sqrt(profile[k] / double(m.plane));
   }
-  return h;
 }
-template double mlp_blend<float>(float*, const float*, MlpDevice&, int, bool, double*, cudaStream_t);
-template double mlp_blend<double>(double*, const double*, MlpDevice&, int, bool, double*, cudaStream_t);
+template void mlp_blend<float>(float*, const float*, MlpDevice&, int, bool, double*, double*, cudaStream_t);
+template void mlp_blend<double>(double*, const double*, MlpDevice&, int, bool, double*, double*, cudaStream_t);
 
 template void mlp_collect<float>(const MlpFeatIn<float>&, const float*, MlpDevice&, int, int, int, unsigned,
                                  cudaStream_t);

@@ -30,9 +30,8 @@ constexpr float MLP_LOG_CS_FLOOR = -13.815510557964274f;  // log(1e-6): coeffici
 template <typename T>
 struct MlpFeatIn {
   const T* d[9];  // dudx dudy dudz dvdx dvdy dvdz dwdx dwdy dwdz
-  const T* u;
-  const T* v;
   const T* csprev;  // Cs^2 before this update (the closure's Lagrangian memory)
+  int wall_levels;  // levels 1..wall_levels keep the LASD procedure: no range flags there
   long plane;
   int nz;
   int wall;
@@ -91,9 +90,11 @@ void mlp_adam(MlpDevice& m, int step, float lr, cudaStream_t st);
 // number of (i,j) columns flagged out of the training range by the last
 // inference; per_feature[8] (may be null) gets the columns per feature
 int mlp_count_flags(MlpDevice& m, int* dcount, int* per_feature, cudaStream_t st);
-// replace flagged columns of cs by cs_dyn; with check, returns the RMS of
-// log(cs) - log(cs_dyn) over all points (both floored at 1e-6)
+// replace flagged columns of cs by cs_dyn; with check, profile[k] (host,
+// nz + 2 values) gets the RMS over level k of log(cs) - log(cs_dyn), both
+// floored at 1e-6 (derr: nz + 2 device doubles)
 template <typename T>
-double mlp_blend(T* cs, const T* cs_dyn, MlpDevice& m, int nz, bool check, double* derr, cudaStream_t st);
+void mlp_blend(T* cs, const T* cs_dyn, MlpDevice& m, int nz, bool check, double* derr, double* profile,
+               cudaStream_t st);
 
 }  // namespace les

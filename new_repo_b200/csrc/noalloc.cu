@@ -131,6 +131,8 @@ extern "C" int les_grad_xy_noalloc(double* f, double* dfdx, double* dfdy, int nx
     return code;
   };
   if (!f || !dfdx || !dfdy) return fail(LES_ERR_INVALID, "les_grad_xy_noalloc: null field pointer");
+  if ((reinterpret_cast<uintptr_t>(f) | reinterpret_cast<uintptr_t>(dfdx) | reinterpret_cast<uintptr_t>(dfdy)) & 15u)
+    return fail(LES_ERR_INVALID, "les_grad_xy_noalloc: field pointers must be 16-byte aligned");
   if (nx <= 0 || ny <= 0 || nlev <= 0 || !(lx > 0) || !(ly > 0))
     return fail(LES_ERR_INVALID, "les_grad_xy_noalloc: invalid grid or domain size");
   if (!supported_length(nx) || !supported_length(ny))

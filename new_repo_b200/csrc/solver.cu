@@ -355,7 +355,9 @@ class Solver final : public SolverBase {
   bool mlp_alloc = false, mlp_ready = false;
   long mlp_updates = 0;
   int mlp_check_every = 10;  // dynamic-procedure check every 10 updates (50 steps at cs_count 5)
+  int mlp_wall_levels = 0;   // levels 1..n next to the wall keep the LASD procedure
   double mlp_last_err = -1.0;
+  std::vector<double> mlp_profile;  // RMS log error per level at the last check
   int mlp_last_flags = 0;
   int mlp_feature_flags[8] = {};
   int* dcount = nullptr;
@@ -377,7 +379,8 @@ class Solver final : public SolverBase {
     md.counts = track(dalloc<unsigned long long>(2));
     md.plane = g.plane();
     dcount = track(dalloc<int>(9));
-    derr = track(dalloc<double>(1));
+    derr = track(dalloc<double>(g.L));
+    mlp_profile.assign(g.L, -1.0);
     cs_prev = track(dalloc<T>(g.field()));
     init_mlp_attributes();
     mlp_alloc = true;
@@ -386,9 +389,8 @@ class Solver final : public SolverBase {
     MlpFeatIn<T> a;
     const int d[9] = {LES_DUDX, LES_DUDY, LES_DUDZ, LES_DVDX, LES_DVDY, LES_DVDZ, LES_DWDX, LES_DWDY, LES_DWDZ};
     for (int q = 0; q < 9; ++q) a.d[q] = F[d[q]];
-    a.u = F[LES_U];
-    a.v = F[LES_V];
     a.csprev = cs_prev;
+    a.wall_levels = std::min(mlp_wall_levels, g.nz + 1);
     a.plane = g.plane();
     a.nz = g.nz;
     a.wall = P.wall_law;
@@ -580,6 +582,11 @@ class Solver final : public SolverBase {
     cudaFree(dl);
   }
   void mlp_set_check_every(int every) override { mlp_check_every = every; }
+  void mlp_set_wall_levels(int n) override { mlp_wall_levels = std::max(0, n); }
+  void mlp_check_profile(double* out, int n) override {
+    if (n < g.nz + 1) throw CudaError(1, "learned closure: profile needs nz + 1 values");
+    for (int k = 1; k <= g.nz + 1; ++k) out[k - 1] = mlp_profile.empty() ? -1.0 : mlp_profile[k];
+  }
   void mlp_info(double* out) override {
     out[0] = mlp_last_err;
     out[1] = mlp_last_flags;
@@ -593,11 +600,15 @@ class Solver final : public SolverBase {
   // which also checks the closure every mlp_check_every updates.
   void mlp_sgs(SgsArgs<T>& a, int jtt) {
     Tag tag_(this, "mlp");
+    const int nb = std::min(mlp_wall_levels, g.nz + 1);
     if (jtt < P.dyn_init) {
       fill(F[LES_CS_OPT2], 1, g.nz + 1, T(0.03));
       return;
     }
-    if (jtt % P.cs_count != 0) return;
+    if (jtt % P.cs_count != 0) {
+      if (nb > 0) lasd(a, jtt, nb);  // Lagrangian accumulation of the wall band
+      return;
+    }
     if (!mlp_ready) throw CudaError(1, "learned closure has no weights (train it or load parameters)");
     copy(cs_prev, F[LES_CS_OPT2], g.field());
     have_prev = true;
@@ -615,9 +626,18 @@ class Solver final : public SolverBase {
          k_lasd_update<T><<<grid_for(n1), 256, 0, st>>>(sc[0], sc[12], sc[13], sc[14], sc[7], sc[8], sc[9], sc[10],
                                                        sc[11], sc[1], 1, g.plane(), g.nz, 1.5 * delta,
                                                        P.dt * double(P.cs_count), beta_pow, cs_prev));
-      const double e = mlp_blend<T>(F[LES_CS_OPT2], sc[11], md, g.nz, check, derr, st);
-      if (check) mlp_last_err = e;
+      std::vector<double> prof(g.L, 0.0);
+      mlp_blend<T>(F[LES_CS_OPT2], sc[11], md, g.nz, check, derr, prof.data(), st);
+      if (check) {
+        // the closure's error where it is used: levels above the wall band
+        double s2 = 0.0;
+        int nl = 0;
+        for (int k = nb + 1; k <= g.nz + 1; ++k, ++nl) s2 += prof[k] * prof[k];
+        mlp_last_err = nl ? std::sqrt(s2 / nl) : 0.0;
+        mlp_profile = prof;
+      }
     }
+    if (nb > 0) lasd(a, jtt, nb);  // the wall band: the plain procedure, Lagrangian history kept
   }
 
   double* staging = nullptr;  // FP64 device staging field (mixed precision transfers)
@@ -871,8 +891,7 @@ class Solver final : public SolverBase {
       }
       launch_ypass<T>(g.ny, g.ny, e, nz, 3, st);
     }
-    const bool is_rhs = (cx == LES_RHSX && cy == LES_RHSY && cz == LES_RHSZ);
-    auto h = xi(is_rhs ? XI_CONV : XI_STORE, 3, 1, nz, g.nx, g.ny, nkout);
+    auto h = xi(XI_STORE, 3, 1, nz, g.nx, g.ny, nkout);
     const int outs[3] = {cx, cy, cz};
     for (int q = 0; q < 3; ++q) {
       h.in[q] = spec[3 + q];
@@ -880,11 +899,6 @@ class Solver final : public SolverBase {
       h.lo[q] = 1;
       h.hi[q] = nz;
       if (mixed()) h.refin[q] = refbuf[6 + q];
-    }
-    if (is_rhs) {
-      h.out[3] = F[LES_RHSX_F];
-      h.out[4] = F[LES_RHSY_F];
-      h.out[5] = F[LES_RHSZ_F];
     }
     launch_xinv<T>(g.nx, h, st);
     // ghost levels of the outputs (compute_convective_padd.f90:251-259)
@@ -1153,10 +1167,14 @@ class Solver final : public SolverBase {
   }
 
   // dynamic-procedure contractions at both test scales (compute_dynamic_mum x2)
-  void dynamic_mum(SgsArgs<T>& a, bool both) {
-    const long n1 = (long)(g.nz + 1) * g.plane();
-    KL("k_sij", 16.0 * (g.nz + 1) * g.plane() * sizeof(T), k_sij<T><<<grid_for(n1), 256, 0, st>>>(a));
-    auto x = xf(XF_LASD, 21, 1, g.nz + 1, g.nx, g.ny, nk2);
+  // nlev: levels 1..nlev (all: nz + 1)
+  void dynamic_mum(SgsArgs<T>& a, bool both, int nlev = -1) {
+    if (nlev < 0) nlev = g.nz + 1;
+    const long n1 = (long)nlev * g.plane();
+    SgsArgs<T> ab = a;
+    ab.nz = nlev - 1;  // k_sij covers levels 1..nz+1 of its arguments
+    KL("k_sij", 16.0 * n1 * sizeof(T), k_sij<T><<<grid_for(n1), 256, 0, st>>>(ab));
+    auto x = xf(XF_LASD, 21, 1, nlev, g.nx, g.ny, nk2);
     x.in[0] = F[LES_U];
     x.in[1] = F[LES_V];
     x.in[2] = F[LES_W];
@@ -1176,11 +1194,11 @@ class Solver final : public SolverBase {
       y.out[(both ? 2 : 1) * q] = spec[q];
       if (both) y.out[2 * q + 1] = spec4[q];
     }
-    launch_ypass<T>(g.ny, g.ny, y, g.nz + 1, 21, st);
+    launch_ypass<T>(g.ny, g.ny, y, nlev, 21, st);
     const double cst = 2.0 * delta * delta;
     for (int sc_i = 0; sc_i < (both ? 2 : 1); ++sc_i) {
       const int nk = sc_i == 0 ? nk2 : nk4;
-      auto z = xi(XI_LASD, 21, 1, g.nz + 1, g.nx, g.ny, nk);
+      auto z = xi(XI_LASD, 21, 1, nlev, g.nx, g.ny, nk);
       z.c0 = cst;
       z.c1 = sc_i == 0 ? 4.0 : 16.0;
       for (int q = 0; q < 21; ++q) z.in[q] = sc_i == 0 ? spec[q] : spec4[q];
@@ -1190,38 +1208,47 @@ class Solver final : public SolverBase {
     }
   }
 
-  void lasd(SgsArgs<T>& a, int jtt) {
+  // compute_LagScaleDep_coeff on levels 1..nlev (all: nz + 1); the learned
+  // closure runs it on a band of levels next to the wall
+  void lasd(SgsArgs<T>& a, int jtt, int nlev = -1) {
     Tag tag_(this, "lasd");
     const int nz = g.nz;
+    if (nlev < 0) nlev = nz + 1;
+    const long nacc = std::min<long>(g.field(), (long)(nlev + 1) * g.plane());  // levels 0..nlev
     if (jtt >= P.dyn_init) {
-      KL("k_lag_accum", 9.0 * g.field() * sizeof(T), k_lag_accum<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_U_LAG], F[LES_V_LAG], F[LES_W_LAG], F[LES_U],
-                                                         F[LES_V], F[LES_W], g.field()));
+      KL("k_lag_accum", 9.0 * nacc * sizeof(T), k_lag_accum<T><<<grid_for(nacc), 256, 0, st>>>(F[LES_U_LAG], F[LES_V_LAG], F[LES_W_LAG], F[LES_U],
+                                                         F[LES_V], F[LES_W], nacc));
     }
     if (jtt < P.dyn_init) {
       fill(F[LES_CS_OPT2], 1, nz + 1, T(0.03));
       return;
     }
     if (jtt % P.cs_count != 0) return;
-    dynamic_mum(a, true);
-    const long n1 = (long)(nz + 1) * g.plane();
+    dynamic_mum(a, true, nlev);
+    const long n1 = (long)nlev * g.plane();
     if (f_coeff_init) {
       LagGeom geo{g.nx, g.ny, nz, g.plane(), P.lag_halo, P.dt, P.lx / double(g.nx), P.ly / double(g.ny), dz(),
-                  double(P.cs_count)};
-      KL("k_lag_interp", 11.0 * (g.nz + 1) * g.plane() * sizeof(T), k_lag_interp<T><<<grid_for(n1), 256, 0, st>>>(F[LES_U_LAG], F[LES_V_LAG], F[LES_W_LAG], F[LES_F_LM],
+                  double(P.cs_count), nlev};
+      KL("k_lag_interp", 11.0 * n1 * sizeof(T), k_lag_interp<T><<<grid_for(n1), 256, 0, st>>>(F[LES_U_LAG], F[LES_V_LAG], F[LES_W_LAG], F[LES_F_LM],
                                                    F[LES_F_MM], F[LES_F_QN], F[LES_F_NN], sc[11], sc[12], sc[13],
                                                    sc[14], geo));
-      std::swap(F[LES_F_LM], sc[11]);
-      std::swap(F[LES_F_MM], sc[12]);
-      std::swap(F[LES_F_QN], sc[13]);
-      std::swap(F[LES_F_NN], sc[14]);
+      if (nlev == nz + 1) {
+        std::swap(F[LES_F_LM], sc[11]);
+        std::swap(F[LES_F_MM], sc[12]);
+        std::swap(F[LES_F_QN], sc[13]);
+        std::swap(F[LES_F_NN], sc[14]);
+      } else {  // a band: the levels above keep their averages
+        const int fl[4] = {LES_F_LM, LES_F_MM, LES_F_QN, LES_F_NN};
+        for (int t = 0; t < 4; ++t) copy(lev(F[fl[t]], 1), lev(sc[11 + t], 1), n1);
+      }
     }
-    KL("k_lasd_update", 14.0 * (g.nz + 1) * g.plane() * sizeof(T), k_lasd_update<T><<<grid_for(n1), 256, 0, st>>>(F[LES_F_LM], F[LES_F_MM], F[LES_F_QN], F[LES_F_NN], sc[7],
+    KL("k_lasd_update", 14.0 * n1 * sizeof(T), k_lasd_update<T><<<grid_for(n1), 256, 0, st>>>(F[LES_F_LM], F[LES_F_MM], F[LES_F_QN], F[LES_F_NN], sc[7],
                                                   sc[8], sc[9], sc[10], F[LES_CS_OPT2], F[LES_BETA],
                                                   f_coeff_init ? 0 : 1, g.plane(), nz, 1.5 * delta,
-                                                  P.dt * double(P.cs_count), beta_pow));
+                                                  P.dt * double(P.cs_count), beta_pow, nullptr, nlev));
     f_coeff_init = true;
     lagran_init = true;
-    for (int q : {LES_U_LAG, LES_V_LAG, LES_W_LAG}) fill(F[q], 0, nz + 1, T(0));
+    for (int q : {LES_U_LAG, LES_V_LAG, LES_W_LAG}) fill(F[q], 0, std::min(nlev, nz + 1), T(0));
   }
 
   void dynsmag(SgsArgs<T>& a, int jt, int jtt);
@@ -1251,7 +1278,20 @@ class Solver final : public SolverBase {
 
   // -------------------------------------------------------- LES_engine ----
   void compute_rhs_adv() override {
-    // rhs_f = rhs ; rhs = convective term (fused in the convective store)
+    // LES_engine.f90:516-527: rhs_f(1:nz) = rhs(1:nz); rhs = convective term.
+    // The copy is a buffer exchange: the old rhs buffer becomes rhs_f after
+    // taking rhs_f's ghost levels (the reference leaves those untouched), and
+    // the old rhs_f buffer receives the convective term on levels 1..nz and
+    // the convective routine's ghost values.
+    {
+      Tag tag_(this, "convec");
+      const int r[3] = {LES_RHSX, LES_RHSY, LES_RHSZ}, rf[3] = {LES_RHSX_F, LES_RHSY_F, LES_RHSZ_F};
+      for (int q = 0; q < 3; ++q) {
+        copy(lev(F[r[q]], 0), lev(F[rf[q]], 0), g.plane());
+        copy(lev(F[r[q]], g.nz + 1), lev(F[rf[q]], g.nz + 1), g.plane());
+        std::swap(F[r[q]], F[rf[q]]);
+      }
+    }
     dealias_convec(LES_RHSX, LES_RHSY, LES_RHSZ);
     DivEq e[3] = {{LES_RHSX, LES_TXX, LES_TXY, LES_TXZ, 1, P.pfx},
                   {LES_RHSY, LES_TXY, LES_TYY, LES_TYZ, 1, P.pfy},

@@ -124,6 +124,8 @@ struct SolverBase : LaunchHook {
   virtual void mlp_grad_host(const float* x, const float* t, long n, float* g, float* loss) = 0;
   virtual void mlp_info(double* out) = 0;
   virtual void mlp_set_check_every(int every) = 0;
+  virtual void mlp_set_wall_levels(int n) = 0;
+  virtual void mlp_check_profile(double* out, int n) = 0;
   virtual void upload_async(int field, const double* pinned, int k0, int k1) = 0;
   virtual void download_async(int field, double* pinned, int k0, int k1) = 0;
   virtual void diagnostics_async(double* pinned4) = 0;

@@ -20,6 +20,8 @@
 // read and write whole contiguous rows and the y pass reads C consecutive kx
 // columns per row (128-byte segments).
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 #include "fft2.cuh"
 
@@ -61,27 +63,115 @@ struct XFArgs {
   const cplx<T>* tw; // exp(-2 pi i m / NX), m < NX
 };
 
-// Values of every field at level l, row j, column i (input grid), written to
-// v[f * vs] (shared memory).
+// Four consecutive x points of one row, moved with 16-byte loads and stores.
 template <typename T>
-__device__ __forceinline__ void xf_load_point(const XFArgs<T>& a, int l, int j, int i, T* v, int vs) {
+struct V4 {
+  T e[4];
+};
+template <typename T>
+__device__ __forceinline__ V4<T> operator+(const V4<T>& a, const V4<T>& b) {
+  return {{a.e[0] + b.e[0], a.e[1] + b.e[1], a.e[2] + b.e[2], a.e[3] + b.e[3]}};
+}
+template <typename T>
+__device__ __forceinline__ V4<T> operator-(const V4<T>& a, const V4<T>& b) {
+  return {{a.e[0] - b.e[0], a.e[1] - b.e[1], a.e[2] - b.e[2], a.e[3] - b.e[3]}};
+}
+template <typename T>
+__device__ __forceinline__ V4<T> operator*(const V4<T>& a, const V4<T>& b) {
+  return {{a.e[0] * b.e[0], a.e[1] * b.e[1], a.e[2] * b.e[2], a.e[3] * b.e[3]}};
+}
+template <typename T>
+__device__ __forceinline__ V4<T> operator*(T c, const V4<T>& b) {
+  return {{c * b.e[0], c * b.e[1], c * b.e[2], c * b.e[3]}};
+}
+template <typename T>
+__device__ __forceinline__ V4<T> operator/(const V4<T>& a, T c) {
+  return {{a.e[0] / c, a.e[1] / c, a.e[2] / c, a.e[3] / c}};
+}
+template <typename T>
+__device__ __forceinline__ V4<T> operator-(const V4<T>& a) {
+  return {{-a.e[0], -a.e[1], -a.e[2], -a.e[3]}};
+}
+
+// value type V (T: one point, V4<T>: four points) loaded from S* at off
+template <typename V, typename S>
+struct VLd;
+template <typename S>
+struct VLd<float, S> {
+  static __device__ __forceinline__ float ld(const S* p, long o) { return float(p[o]); }
+};
+template <typename S>
+struct VLd<double, S> {
+  static __device__ __forceinline__ double ld(const S* p, long o) { return double(p[o]); }
+};
+template <>
+struct VLd<V4<float>, float> {
+  static __device__ __forceinline__ V4<float> ld(const float* p, long o) {
+    const float4 q = *reinterpret_cast<const float4*>(p + o);
+    return {{q.x, q.y, q.z, q.w}};
+  }
+};
+template <>
+struct VLd<V4<double>, double> {
+  static __device__ __forceinline__ V4<double> ld(const double* p, long o) {
+    const double2 q0 = *reinterpret_cast<const double2*>(p + o);
+    const double2 q1 = *reinterpret_cast<const double2*>(p + o + 2);
+    return {{q0.x, q0.y, q1.x, q1.y}};
+  }
+};
+template <>
+struct VLd<V4<double>, float> {
+  static __device__ __forceinline__ V4<double> ld(const float* p, long o) {
+    const float4 q = *reinterpret_cast<const float4*>(p + o);
+    return {{double(q.x), double(q.y), double(q.z), double(q.w)}};
+  }
+};
+template <typename V, typename S>
+__device__ __forceinline__ V vld(const S* p, long o) {
+  return VLd<V, S>::ld(p, o);
+}
+template <typename T>
+__device__ __forceinline__ void vst(T* p, T x) {
+  *p = x;
+}
+__device__ __forceinline__ void vst(float* p, const V4<float>& x) {
+  *reinterpret_cast<float4*>(p) = make_float4(x.e[0], x.e[1], x.e[2], x.e[3]);
+}
+__device__ __forceinline__ void vst(double* p, const V4<double>& x) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(x.e[0], x.e[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(x.e[2], x.e[3]);
+}
+template <typename V, typename T>
+__device__ __forceinline__ V vsplat(T x) {
+  if constexpr (std::is_same<V, T>::value) return x;
+  else return V{{x, x, x, x}};
+}
+
+// Values of every field at level l, row j, columns i (one point for V = T,
+// four for V = V4<T>; i a multiple of 4 then), stored at v + f * vs.
+template <typename T, typename V>
+__device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i, T* v, int vs) {
   const long off = (long)l * a.in_pstride + (long)j * a.in_rstride + i;
   switch (a.op) {
     case XF_SCALE: {
-      for (int f = 0; f < a.nf; ++f) v[f * vs] = T(a.c0) * (a.in_f32 ? T(a.inf[f][off]) : a.in[f][off]);
+      for (int f = 0; f < a.nf; ++f)
+        vst(v + f * vs, T(a.c0) * (a.in_f32 ? vld<V>(a.inf[f], off) : vld<V>(a.in[f], off)));
       break;
     }
     case XF_PRESS: {
-      for (int f = 0; f < a.nf; ++f)
-        v[f * vs] = T(a.c0) * ((a.in_f32 ? T(a.inf[f][off]) : a.in[f][off]) / T(a.c1));
+      // compute_pressure.f90:138-140
+      for (int f = 0; f < a.nf; ++f) {
+        const V x = a.in_f32 ? vld<V>(a.inf[f], off) : vld<V>(a.in[f], off);
+        vst(v + f * vs, T(a.c0) * (x / T(a.c1)));
+      }
       break;
     }
     case XF_CONV_IN: {
       // compute_convective_padd.f90:133-165
       const T c = T(a.c0);
-      v[0 * vs] = -c * a.in[0][off];
-      v[1 * vs] = -c * a.in[1][off];
-      v[2 * vs] = -c * a.in[2][off];
+      vst(v + 0 * vs, -c * vld<V>(a.in[0], off));
+      vst(v + 1 * vs, -c * vld<V>(a.in[1], off));
+      vst(v + 2 * vs, -c * vld<V>(a.in[2], off));
       const T* dwdy = a.in[3];
       const T* dvdz = a.in[4];
       const T* dudz = a.in[5];
@@ -89,17 +179,17 @@ __device__ __forceinline__ void xf_load_point(const XFArgs<T>& a, int l, int j, 
       const T* dvdx = a.in[7];
       const T* dudy = a.in[8];
       if (a.wall && l == 0) {
-        v[3 * vs] = T(0);
-        v[4 * vs] = T(0);
+        vst(v + 3 * vs, vsplat<V>(T(0)));
+        vst(v + 4 * vs, vsplat<V>(T(0)));
       } else if (a.wall && l == 1) {
         const long up = off + a.in_pstride;
-        v[3 * vs] = c * (T(0.5) * (dwdy[off] + dwdy[up]) - dvdz[off]);
-        v[4 * vs] = c * (dudz[off] - T(0.5) * (dwdx[off] + dwdx[up]));
+        vst(v + 3 * vs, c * (T(0.5) * (vld<V>(dwdy, off) + vld<V>(dwdy, up)) - vld<V>(dvdz, off)));
+        vst(v + 4 * vs, c * (vld<V>(dudz, off) - T(0.5) * (vld<V>(dwdx, off) + vld<V>(dwdx, up))));
       } else {
-        v[3 * vs] = c * (dwdy[off] - dvdz[off]);
-        v[4 * vs] = c * (dudz[off] - dwdx[off]);
+        vst(v + 3 * vs, c * (vld<V>(dwdy, off) - vld<V>(dvdz, off)));
+        vst(v + 4 * vs, c * (vld<V>(dudz, off) - vld<V>(dwdx, off)));
       }
-      v[5 * vs] = c * (dvdx[off] - dudy[off]);
+      vst(v + 5 * vs, c * (vld<V>(dvdx, off) - vld<V>(dudy, off)));
       break;
     }
     case XF_PROD: {
@@ -114,14 +204,17 @@ __device__ __forceinline__ void xf_load_point(const XFArgs<T>& a, int l, int j, 
       const T* o3 = a.in[5];
       const long up = off + a.in_pstride;
       const long dn = off - a.in_pstride;
+      const V vb0 = vld<V>(vb, off), o30 = vld<V>(o3, off), ub0 = vld<V>(ub, off);
+      const V wbu = vld<V>(wb, up), o2u = vld<V>(o2, up), o1u = vld<V>(o1, up);
       if (l == 1) {
-        v[0 * vs] = c * (-vb[off] * o3[off] + T(0.5) * wb[up] * o2[up]);
-        v[1 * vs] = c * (ub[off] * o3[off] + T(0.5) * wb[up] * (-o1[up]));
-        v[2 * vs] = T(0);
+        vst(v + 0 * vs, c * (-vb0 * o30 + T(0.5) * wbu * o2u));
+        vst(v + 1 * vs, c * (ub0 * o30 + T(0.5) * wbu * (-o1u)));
+        vst(v + 2 * vs, vsplat<V>(T(0)));
       } else {
-        v[0 * vs] = c * (-vb[off] * o3[off] + T(0.5) * (wb[up] * o2[up] + wb[off] * o2[off]));
-        v[1 * vs] = c * (ub[off] * o3[off] + T(0.5) * (wb[off] * (-o1[off]) + wb[up] * (-o1[up])));
-        v[2 * vs] = c * T(0.5) * ((ub[off] + ub[dn]) * (-o2[off]) + (vb[off] + vb[dn]) * (o1[off]));
+        const V wb0 = vld<V>(wb, off), o20 = vld<V>(o2, off), o10 = vld<V>(o1, off);
+        vst(v + 0 * vs, c * (-vb0 * o30 + T(0.5) * (wbu * o2u + wb0 * o20)));
+        vst(v + 1 * vs, c * (ub0 * o30 + T(0.5) * (wb0 * (-o10) + wbu * (-o1u))));
+        vst(v + 2 * vs, c * T(0.5) * ((ub0 + vld<V>(ub, dn)) * (-o20) + (vb0 + vld<V>(vb, dn)) * o10));
       }
       break;
     }
@@ -130,46 +223,50 @@ __device__ __forceinline__ void xf_load_point(const XFArgs<T>& a, int l, int j, 
       const T* u = a.in[0];
       const T* vv = a.in[1];
       const T* w = a.in[2];
-      T uf, vf, wf;
+      V uf, vf, wf;
       if (l == 1) {
-        uf = u[off];
-        vf = vv[off];
-        wf = T(0.25) * w[off + a.in_pstride];
+        uf = vld<V>(u, off);
+        vf = vld<V>(vv, off);
+        wf = T(0.25) * vld<V>(w, off + a.in_pstride);
       } else {
         const long dn = off - a.in_pstride;
-        uf = T(0.5) * (u[off] + u[dn]);
-        vf = T(0.5) * (vv[off] + vv[dn]);
-        wf = w[off];
+        uf = T(0.5) * (vld<V>(u, off) + vld<V>(u, dn));
+        vf = T(0.5) * (vld<V>(vv, off) + vld<V>(vv, dn));
+        wf = vld<V>(w, off);
       }
       if (a.fluct) {
         // L_ij = filt(u_i u_j) - filt(u_i) filt(u_j) is unchanged when a
         // per-level constant is removed from u_i; FP32 keeps the fluctuation.
         const long o0 = (long)l * a.in_pstride;
+        T u0, v0, w0;
         if (l == 1) {
-          uf -= u[o0];
-          vf -= vv[o0];
-          wf -= T(0.25) * w[o0 + a.in_pstride];
+          u0 = u[o0];
+          v0 = vv[o0];
+          w0 = T(0.25) * w[o0 + a.in_pstride];
         } else {
-          uf -= T(0.5) * (u[o0] + u[o0 - a.in_pstride]);
-          vf -= T(0.5) * (vv[o0] + vv[o0 - a.in_pstride]);
-          wf -= w[o0];
+          u0 = T(0.5) * (u[o0] + u[o0 - a.in_pstride]);
+          v0 = T(0.5) * (vv[o0] + vv[o0 - a.in_pstride]);
+          w0 = w[o0];
         }
+        uf = uf - vsplat<V>(u0);
+        vf = vf - vsplat<V>(v0);
+        wf = wf - vsplat<V>(w0);
       }
-      v[0 * vs] = uf;
-      v[1 * vs] = vf;
-      v[2 * vs] = wf;
-      v[3 * vs] = uf * uf;  // A11
-      v[4 * vs] = uf * vf;  // A12
-      v[5 * vs] = uf * wf;  // A13
-      v[6 * vs] = vf * vf;  // A22
-      v[7 * vs] = vf * wf;  // A23
-      v[8 * vs] = wf * wf;  // A33
-      const T S = a.in[9][off];
+      vst(v + 0 * vs, uf);
+      vst(v + 1 * vs, vf);
+      vst(v + 2 * vs, wf);
+      vst(v + 3 * vs, uf * uf);  // A11
+      vst(v + 4 * vs, uf * vf);  // A12
+      vst(v + 5 * vs, uf * wf);  // A13
+      vst(v + 6 * vs, vf * vf);  // A22
+      vst(v + 7 * vs, vf * wf);  // A23
+      vst(v + 8 * vs, wf * wf);  // A33
+      const V S = vld<V>(a.in[9], off);
 #pragma unroll
       for (int q = 0; q < 6; ++q) {  // s11 s12 s13 s22 s23 s33
-        const T s = a.in[3 + q][off];
-        v[(9 + q) * vs] = s;
-        v[(15 + q) * vs] = S * s;
+        const V sq = vld<V>(a.in[3 + q], off);
+        vst(v + (9 + q) * vs, sq);
+        vst(v + (15 + q) * vs, S * sq);
       }
       break;
     }
@@ -212,7 +309,7 @@ __global__ void __launch_bounds__(256, 2) k_xfwd(const XFArgs<T> a) {
       if (g >= a.nrows) continue;
       const int l = a.plane0 + int(g / a.rows_pp);
       const int j = int(g % a.rows_pp);
-      xf_load_point(a, l, 0, 0, refs + r * a.nf, 1);
+      xf_load<T, T>(a, l, 0, 0, refs + r * a.nf, 1);
       for (int f = 0; f < a.nf; ++f) {
         if (!a.refout[f]) refs[r * a.nf + f] = T(0);
         else if (j == 0) a.refout[f][l] = T(double(refs[r * a.nf + f]) * a.ref_mul);
@@ -220,21 +317,26 @@ __global__ void __launch_bounds__(256, 2) k_xfwd(const XFArgs<T> a) {
     }
     __syncthreads();
   }
-  // load: one thread per point; sequence s = r*nf + f holds the packed row
-  // z_m = x_{2m} + i x_{2m+1}, i.e. the real row itself viewed as complex.
+  // load: four consecutive points per thread (16-byte accesses); sequence
+  // s = r*nf + f holds the packed row z_m = x_{2m} + i x_{2m+1}, i.e. the
+  // real row itself viewed as complex.
   T* xr = reinterpret_cast<T*>(buf);
-  for (int idx = threadIdx.x; idx < a.R * NX; idx += blockDim.x) {
-    const int r = idx / NX;
-    const int i = idx - r * NX;
+  for (int idx = threadIdx.x; idx < a.R * (NX / 4); idx += blockDim.x) {
+    const int r = idx / (NX / 4);
+    const int i = 4 * (idx - r * (NX / 4));
     T* dst = xr + (long)(r * a.nf) * NX + i;
     const int l = rowl[r];
     if (l >= 0) {
       const int j = rowj[r];
-      xf_load_point(a, l, j, i, dst, NX);
+      xf_load<T, V4<T>>(a, l, j, i, dst, NX);
       if (a.use_ref)
-        for (int f = 0; f < a.nf; ++f) dst[f * NX] -= refs[r * a.nf + f];
+        for (int f = 0; f < a.nf; ++f) {
+          const T rf = refs[r * a.nf + f];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) dst[f * NX + q] -= rf;
+        }
     } else {
-      for (int f = 0; f < a.nf; ++f) dst[f * NX] = T(0);
+      for (int f = 0; f < a.nf; ++f) vst(dst + f * NX, vsplat<V4<T>>(T(0)));
     }
   }
   for (int idx = nseq * M + threadIdx.x; idx < npad * M; idx += blockDim.x) buf[idx] = cplx<T>{T(0), T(0)};
@@ -293,6 +395,7 @@ enum YPOp : int {
 template <typename T>
 struct YPArgs {
   int op, nin, nout, C, lc;  // C = 1 << lc columns per CTA
+  int SI, SO;                // column strides of the shared input / output staging
   int ncols;           // columns processed
   int ncols1;          // columns stored for the second FILTER2 output
   int nk_in, nk_out, nk_out1;
@@ -360,8 +463,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPA
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* twi = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* two = twi + NY;
-  constexpr int SI = NY + 1;
-  constexpr int SO = NYO + 1;
+  const int SI = a.SI;  // >= NY
+  const int SO = a.SO;  // >= NYO
   const int C = a.C;
   cplx<T>* bin = two + NYO;           // [nin][C][SI]
   cplx<T>* bout = bin + a.nin * C * SI;  // [C][SO]
@@ -508,7 +611,6 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPA
 // ---------------------------------------------------------------- xinv ----
 enum XIOp : int {
   XI_STORE = 0,  // out[f](l) = x_f for lo[f] <= l <= hi[f]
-  XI_CONV = 1,   // rhs_f = rhs ; rhs = x   (levels 1..nz)
   XI_DIV = 2,    // rhs += x + dz(tz) + pf ; pressure-BC layers of the w equation
   XI_LASD = 3,   // 21 filtered fields -> L:M and M:M
   XI_WALL = 4,   // filtered u1, v1 -> u*, Neumann ghost value, wall stress
@@ -628,17 +730,48 @@ __global__ void __launch_bounds__(256, 2) k_xinv(const XIArgs<T> a) {
   if (direct) return;
   __syncthreads();
   const T* xs = reinterpret_cast<const T*>(buf);  // x_i of sequence s at xs[s*NX + i]
-  for (int idx = threadIdx.x; idx < a.R * NX; idx += blockDim.x) {
-    const int r = idx / NX;
-    const int i = idx - r * NX;
+  // four consecutive points per thread
+  for (int idx = threadIdx.x; idx < a.R * (NX / 4); idx += blockDim.x) {
+    const int r = idx / (NX / 4);
+    const int i0 = 4 * (idx - r * (NX / 4));
     const int l = rowl[r];
     if (l < 0) continue;
     const int j = rowj[r];
+    T* xw0 = const_cast<T*>(xs) + (long)(r * a.nin) * NX + i0;
+    for (int f = 0; f < a.nin; ++f)  // this thread alone touches (r, i0..i0+3)
+      if (a.refin[f]) {
+        const T rf = a.refin[f][l];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) xw0[f * NX + q] += rf;
+      }
+    if (a.op == XI_DIV) {
+      // compute_derivatives.f90:544-574 + LES_engine.f90:546-551, one
+      // equation per input: out[q] = rhs, aux[q] = tz, lo[q] = stag,
+      // pf[q] = forcing; out[8]/out[9] = bottom/top pressure-BC layers of
+      // the non-staggered (w) equation.  c0 = 1/dz.
+      using V = V4<T>;
+      const T rdz = T(a.c0);
+      const long pl = a.out_pstride;
+      const long off = (long)l * pl + (long)j * NX + i0;
+      const long p2 = (long)j * NX + i0;
+      for (int q = 0; q < a.nin; ++q) {
+        const T* tz = a.aux[q];
+        const V xq = vld<V>(static_cast<const T*>(xw0), (long)q * NX);
+        if (l >= 1 && l <= a.nz) {
+          const V dzq = a.lo[q] ? rdz * (vld<V>(tz, off + pl) - vld<V>(tz, off))   // ddz_w
+                                : rdz * (vld<V>(tz, off) - vld<V>(tz, off - pl));  // ddz_uv
+          vst(a.out[q] + off, ((vld<V>(a.out[q], off) + xq) + dzq) + vsplat<V>(T(a.pf[q])));
+          if (!a.lo[q] && l == 1 && a.out[8]) vst(a.out[8] + p2, xq + dzq);
+        }
+        if (!a.lo[q] && l == a.nz + 1 && a.out[9]) vst(a.out[9] + p2, xq);
+      }
+      continue;
+    }
+#pragma unroll 1
+    for (int q4 = 0; q4 < 4; ++q4) {
+    const int i = i0 + q4;
     const long off = (long)l * a.out_pstride + (long)j * NX + i;
-    T* xw = const_cast<T*>(xs) + (long)(r * a.nin) * NX + i;
-    for (int f = 0; f < a.nin; ++f)  // this thread alone touches (r, i)
-      if (a.refin[f]) xw[f * NX] += a.refin[f][l];
-    const T* x = xw;  // field f at x[f*NX]
+    const T* x = xw0 + q4;  // field f at x[f*NX]
     switch (a.op) {
       case XI_STORE: {
         for (int f = 0; f < a.nin; ++f)
@@ -646,37 +779,6 @@ __global__ void __launch_bounds__(256, 2) k_xinv(const XIArgs<T> a) {
             if (a.out_f32) a.outf[f][off] = float(x[f * NX]);
             else a.out[f][off] = x[f * NX];
           }
-        break;
-      }
-      case XI_CONV: {
-        // LES_engine.f90:516-533: rhs_f = rhs ; rhs = convective term
-        if (l >= 1 && l <= a.nz) {
-          for (int f = 0; f < 3; ++f) {
-            a.out[3 + f][off] = a.out[f][off];
-            a.out[f][off] = x[f * NX];
-          }
-        }
-        break;
-      }
-      case XI_DIV: {
-        // compute_derivatives.f90:544-574 + LES_engine.f90:546-551, one
-        // equation per input: out[q] = rhs, aux[q] = tz, lo[q] = stag,
-        // pf[q] = forcing; out[8]/out[9] = bottom/top pressure-BC layers of
-        // the non-staggered (w) equation.  c0 = 1/dz.
-        const T rdz = T(a.c0);
-        const long pl = a.out_pstride;
-        const long p2 = (long)j * NX + i;
-        for (int q = 0; q < a.nin; ++q) {
-          const T* tz = a.aux[q];
-          const T xq = x[q * NX];
-          if (l >= 1 && l <= a.nz) {
-            const T dzq = a.lo[q] ? rdz * (tz[off + pl] - tz[off])   // ddz_w
-                                  : rdz * (tz[off] - tz[off - pl]);  // ddz_uv
-            a.out[q][off] = (a.out[q][off] + xq) + dzq + T(a.pf[q]);
-            if (!a.lo[q] && l == 1 && a.out[8]) a.out[8][p2] = xq + dzq;
-          }
-          if (!a.lo[q] && l == a.nz + 1 && a.out[9]) a.out[9][p2] = xq;
-        }
         break;
       }
       case XI_LASD: {
@@ -729,6 +831,7 @@ __global__ void __launch_bounds__(256, 2) k_xinv(const XIArgs<T> a) {
         a.out[6][o1] = T(bv);
         break;
       }
+    }
     }
   }
 }

@@ -95,8 +95,7 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
   {
     const size_t osz = (a.out_f32 ? sizeof(float) : sizeof(T));
     int nout = a.nin, rmw = 0;
-    if (a.op == XI_CONV) { nout = 6; rmw = 3; }
-    else if (a.op == XI_DIV) { nout = a.nin; rmw = 2 * a.nin; }
+    if (a.op == XI_DIV) { nout = a.nin; rmw = 2 * a.nin; }
     else if (a.op == XI_LASD) nout = 2;
     else if (a.op == XI_WALL) nout = 7;
     hook_before("xinv", double(a.nrows) * a.nin * a.nk * sizeof(cplx<T>) + double(a.nrows) * NX * (nout + rmw) * osz);
@@ -117,13 +116,26 @@ template <typename T>
 void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaStream_t st) {
   const int TL = lanes(NY);
   if (lanes(NYO) != TL) throw CudaError(1, "ypass: length pair with different lane counts");
-  const size_t per_col = (size_t)(a.nin * (NY + 1) + (NYO + 1)) * sizeof(cplx<T>);
+  // column stride of the shared staging buffers: the load and store loops
+  // run c (column) fastest and 32/C rows per warp, so a stride congruent to
+  // 32/C modulo the complex values per 128-byte wavefront spreads a warp
+  // evenly over the banks
+  const int W = 128 / int(sizeof(cplx<T>));
+  auto stride = [&](int n, int C) {
+    const int target = (32 / C) % W;
+    return n + ((target - n % W) % W + W) % W;
+  };
+  auto per_col = [&](int C) {
+    return (size_t)(a.nin * stride(NY, C) + stride(NYO, C)) * sizeof(cplx<T>);
+  };
   int lc = 0;  // C = 1 << lc columns per CTA, C * TL <= 256 threads
-  while ((2 << lc) * TL <= 256 && (size_t(2) << lc) * per_col <= 96 * 1024 && (1 << lc) < a.ncols) ++lc;
+  while ((2 << lc) * TL <= 256 && (size_t(2) << lc) * per_col(2 << lc) <= 96 * 1024 && (1 << lc) < a.ncols) ++lc;
   while ((1 << lc) * TL < 32) ++lc;  // at least one full warp
   a.lc = lc;
   a.C = 1 << lc;
-  const size_t smem = sizeof(cplx<T>) * (NY + NYO) + (size_t)a.C * per_col;
+  a.SI = stride(NY, a.C);
+  a.SO = stride(NYO, a.C);
+  const size_t smem = sizeof(cplx<T>) * (NY + NYO) + (size_t)a.C * per_col(a.C);
   if (smem > SMEM_CAP) throw CudaError(1, "ypass: shared memory request too large");
   const int threads = a.C * TL;
   dim3 grid(ceil_div(a.ncols, a.C), nplanes, ngroups);

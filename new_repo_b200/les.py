@@ -468,6 +468,16 @@ class LES:
     def mlp_set_check_every(self, every: int):
         check(self.lib.les_mlp_set_check_every(self._h, int(every)))
 
+    def mlp_check_profile(self) -> np.ndarray:
+        """RMS log error of the closure against the dynamic procedure per level 1..nz+1 at the last check."""
+        out = np.zeros(self.params.nz + 1)
+        check(self.lib.les_mlp_check_profile(self._h, _dptr(out), out.size))
+        return out
+
+    def mlp_set_wall_levels(self, nlev: int):
+        """Levels 1..nlev next to the wall keep the plain LASD procedure."""
+        check(self.lib.les_mlp_set_wall_levels(self._h, int(nlev)))
+
     def state_dict(self, names=None) -> dict:
         names = capi.FIELDS if names is None else names
         d = {n: self.download(n) for n in names}

@@ -114,7 +114,7 @@ def grad(p, x, t, bf16_ops=True):
     return g, loss
 
 
-def raw_features(d, u, v, cs_prev, k, dz, delta, log_delta_z0, wall):
+def raw_features(d, cs_prev, k, dz, delta, log_delta_z0, wall):
     """The 8 transformed features at level k (mlp.cu raw_features).
 
     ``d`` maps 'dudx' .. 'dwdz' to (nz+2, ny, nx) arrays, ``cs_prev`` is the
@@ -122,11 +122,10 @@ def raw_features(d, u, v, cs_prev, k, dz, delta, log_delta_z0, wall):
     Level 1 is the uvp node (w-node quantities averaged up), levels >= 2 are
     w nodes (uvp quantities averaged down).  Features: log1p |S|,
     log1p S:S, log1p Omega:Omega, signed log1p tr(S^3), log1p(z / Delta),
-    log max(Cs^2_prev, 1e-6), log1p |u_h|, log(Delta / z0).
+    log max(Cs^2_prev, 1e-6), signed log1p of the vortex stretching
+    w_i S_ij w_j, log(Delta / z0).
     """
     f = {key: np.asarray(a, np.float32) for key, a in d.items()}
-    u = np.asarray(u, np.float32)
-    v = np.asarray(v, np.float32)
     h = np.float32(0.5)
     if k == 1:
         ux, uy, vx, vy = f["dudx"][1], f["dudy"][1], f["dvdx"][1], f["dvdy"][1]
@@ -135,7 +134,6 @@ def raw_features(d, u, v, cs_prev, k, dz, delta, log_delta_z0, wall):
         wx = h * (f["dwdx"][1] + f["dwdx"][2])
         wy = h * (f["dwdy"][1] + f["dwdy"][2])
         wz = f["dwdz"][1]
-        uh, vh = u[1], v[1]
     else:
         ux = h * (f["dudx"][k] + f["dudx"][k - 1])
         uy = h * (f["dudy"][k] + f["dudy"][k - 1])
@@ -145,8 +143,6 @@ def raw_features(d, u, v, cs_prev, k, dz, delta, log_delta_z0, wall):
         vz = f["dvdz"][k]
         wx, wy = f["dwdx"][k], f["dwdy"][k]
         wz = h * (f["dwdz"][k] + f["dwdz"][k - 1])
-        uh = h * (u[k] + u[k - 1])
-        vh = h * (v[k] + v[k - 1])
     s11, s22, s33 = ux, vy, wz
     s12, s13, s23 = h * (uy + vx), h * (uz + wx), h * (vz + wy)
     o12, o13, o23 = h * (uy - vx), h * (uz - wx), h * (vz - wy)
@@ -163,7 +159,9 @@ def raw_features(d, u, v, cs_prev, k, dz, delta, log_delta_z0, wall):
     out[..., 3] = np.copysign(np.log1p(np.abs(r3)), r3)
     out[..., 4] = np.log1p(z / np.float32(delta))
     out[..., 5] = np.log(np.maximum(np.asarray(cs_prev, np.float32)[k], np.float32(1e-6)))
-    out[..., 6] = np.log1p(np.sqrt(uh * uh + vh * vh))
+    w1, w2, w3 = -2 * o23, 2 * o13, -2 * o12
+    vs = s11 * w1 * w1 + s22 * w2 * w2 + s33 * w3 * w3 + 2 * (s12 * w1 * w2 + s13 * w1 * w3 + s23 * w2 * w3)
+    out[..., 6] = np.copysign(np.log1p(np.abs(vs)), vs)
     out[..., 7] = np.float32(log_delta_z0)
     return out.reshape(-1, 8)
 
@@ -181,8 +179,11 @@ def cs_from_output(y, stats, log_cs_prev):
     return np.clip(np.exp(lc), 1e-24, 1.0)
 
 
-def in_range(xn, stats, margin=0.25):
-    """True where every normalised feature lies within the training range +- margin."""
-    lo = stats[S_MIN:S_MIN + 8] - margin
-    hi = stats[S_MAX:S_MAX + 8] + margin
+def in_range(xn, stats):
+    """True where every normalised feature lies within the training range
+    +- (0.25 sd + 5 % of the range), as k_mlp_infer tests it."""
+    mn, mx = stats[S_MIN:S_MIN + 8], stats[S_MAX:S_MAX + 8]
+    margin = 0.25 + 0.05 * (mx - mn)
+    lo = mn - margin
+    hi = mx + margin
     return np.all((xn >= lo) & (xn <= hi), axis=-1)

@@ -129,17 +129,17 @@ def test_mlp_gradient_matches_oracle(gpu, n):
 
 def _fields(les):
     names = ("dudx", "dudy", "dudz", "dvdx", "dvdy", "dvdz", "dwdx", "dwdy", "dwdz")
-    return {n: les.download(n) for n in names}, les.download("u"), les.download("v")
+    return {n: les.download(n) for n in names}
 
 
 def _oracle_cs(les, p, stats, cs_prev):
     """Cs^2 and the in-range mask of every level 1..nz+1 from the oracle's features."""
     rp = les.params
-    d, u, v = _fields(les)
+    d = _fields(les)
     delta = (rp.dx * rp.dy * rp.dz) ** (1.0 / 3.0)
     cs, ok = [], []
     for k in range(1, rp.nz + 2):
-        t = M.raw_features(d, u, v, cs_prev, k, rp.dz, delta, np.log(delta / rp.z0), 1)
+        t = M.raw_features(d, cs_prev, k, rp.dz, delta, np.log(delta / rp.z0), 1)
         xn = (t - stats[M.S_MU:M.S_MU + 8]) / stats[M.S_SD:M.S_SD + 8]
         cs.append(M.cs_from_output(M.forward(p, xn.astype(np.float32)), stats, t[:, 5]))
         ok.append(M.in_range(xn, stats))
@@ -222,21 +222,25 @@ def test_mlp_partial_fallback_only_flagged_columns(gpu):
     les.compute_vel_grad()
     p = _params(9, scale=0.5)
     st = _stats()
-    # feature 6 (log1p |u_h|): exclude the columns whose largest value lies
+    # feature 6 (vortex stretching): exclude the columns whose largest value lies
     # above about the median of the column maxima (threshold in the widest gap
     # between neighbouring column maxima near the median, so float rounding
     # cannot move a column across it)
-    d, u, v = _fields(les)
+    d = _fields(les)
     cs_prev = les.download("cs_opt2")
     rp = les.params
     delta = (rp.dx * rp.dy * rp.dz) ** (1.0 / 3.0)
-    f6 = np.stack([M.raw_features(d, u, v, cs_prev, k, rp.dz, delta, np.log(delta / rp.z0), 1)[:, 6]
+    f6 = np.stack([M.raw_features(d, cs_prev, k, rp.dz, delta, np.log(delta / rp.z0), 1)[:, 6]
                    for k in range(1, rp.nz + 2)])
     cm = np.sort(f6.max(axis=0))
     mid = cm[cm.size // 2 - 64:cm.size // 2 + 64]
     i = int(np.argmax(np.diff(mid)))
     assert mid[i + 1] - mid[i] > 1e-5
-    st[M.S_MAX + 6] = 0.5 * (mid[i] + mid[i + 1]) - 0.25
+    # the test flags x > MAX + 0.25 + 0.05 (MAX - MIN): put that bound at the gap
+    lo6 = float(f6.min()) - 1.0
+    bound = 0.5 * (mid[i] + mid[i + 1])
+    st[M.S_MIN + 6] = lo6
+    st[M.S_MAX + 6] = (bound - 0.25 + 0.05 * lo6) / 1.05
     les.mlp_set_params(np.concatenate([p, st]))
     les.sgs_stress(10, 10)
     info = les.mlp_info()
@@ -283,3 +287,33 @@ def test_mlp_training_gain_over_constant_coefficient(gpu):
           f"val loss {val:.3f}")
     assert e_mlp < 0.8 * e_mean and e_mlp < e_smag
     les.close()
+
+
+@pytest.mark.gpu
+def test_wall_band_keeps_the_lasd_procedure(gpu):
+    """With the wall band covering every level the learned-closure run is the
+    LASD run; a 3-level band reproduces LASD's first update on those levels."""
+    from new_repo_b200 import log_law_noise
+
+    ref = _les(sgs="dyn_LagScaleDep")
+    ic = log_law_noise(ref.params, seed=13)
+    ref.set_initial_conditions(*ic)
+    full = _les()
+    full.set_initial_conditions(*ic)
+    full.mlp_set_params(np.concatenate([_params(10, scale=0.5), _stats()]))
+    full.mlp_set_wall_levels(full.params.nz + 1)
+    band = _les()
+    band.set_initial_conditions(*ic)
+    band.mlp_set_params(np.concatenate([_params(10, scale=0.5), _stats()]))
+    band.mlp_set_wall_levels(3)
+    ref.step(5)  # step 5 is the first dynamic update
+    full.step(5)
+    band.step(5)
+    cs_ref = ref.download("cs_opt2")
+    np.testing.assert_allclose(band.download("cs_opt2")[1:4], cs_ref[1:4], rtol=1e-13, atol=0)
+    ref.step(7)
+    full.step(7)
+    for n in ("u", "v", "w", "cs_opt2", "F_LM", "F_MM"):
+        np.testing.assert_allclose(full.download(n)[1:-1], ref.download(n)[1:-1], rtol=1e-12, atol=1e-14)
+    for x in (ref, full, band):
+        x.close()
