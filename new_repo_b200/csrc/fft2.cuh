@@ -215,6 +215,17 @@ struct Geo {
   static constexpr int T = N / E;
 };
 
+// Exchange slots are padded by one element every 16: the pass outputs are
+// written at stride R, which would otherwise put a warp's lanes on a few
+// banks.  A sequence of N elements needs N + N/16 elements of slot;
+// slot_len<N>() rounds that up to even so that consecutive slots of FP32
+// complex values stay 16-byte aligned (the x passes move 4 reals at once).
+template <int N>
+__host__ __device__ constexpr int slot_len() {
+  return (N + N / 16 + 1) & ~1;
+}
+__device__ __forceinline__ int xpad(int i) { return i + (i >> 4); }
+
 // one pass of radix R with Ns = product of the previous radices; then the
 // exchange into the next pass's input layout (if any)
 template <typename T, int N, int E, bool INV, int TWS, int Ns, int R, int... Rest>
@@ -241,7 +252,7 @@ __device__ __forceinline__ void reg_passes(cplx<T>* v, cplx<T>* seq, int t, cons
       const int j = t + TL * g;
       const int k = j % Ns;
 #pragma unroll
-      for (int r = 0; r < R; ++r) seq[(j / Ns) * Ns * R + k + r * Ns] = v[g * R + r];
+      for (int r = 0; r < R; ++r) seq[xpad((j / Ns) * Ns * R + k + r * Ns)] = v[g * R + r];
     }
     __syncwarp();
     constexpr int R2 = FirstOf<Rest...>::value;
@@ -249,7 +260,7 @@ __device__ __forceinline__ void reg_passes(cplx<T>* v, cplx<T>* seq, int t, cons
 #pragma unroll
     for (int g = 0; g < G2; ++g)
 #pragma unroll
-      for (int r = 0; r < R2; ++r) v[g * R2 + r] = seq[t + TL * g + r * (N / R2)];
+      for (int r = 0; r < R2; ++r) v[g * R2 + r] = seq[xpad(t + TL * g + r * (N / R2))];
     reg_passes<T, N, E, INV, TWS, Ns * R, Rest...>(v, seq, t, tw);
   }
 }
@@ -280,7 +291,7 @@ struct PassOrder {
 };
 
 // The transform: v as in the layout contract above; seq is this sequence's
-// shared slot of N elements (private to its T lanes); tw holds
+// shared slot of slot_len<N>() elements (private to its T lanes); tw holds
 // exp(-2 pi i m / (N*TWS)) read at stride TWS.  Forward transforms run the
 // plan's radices in order, inverse transforms in reverse order.
 template <typename T, int N, bool INV, int TWS = 1>

@@ -287,12 +287,14 @@ __global__ void __launch_bounds__(256, 2) k_xfwd(const XFArgs<T> a) {
   constexpr int E = Geo<M>::E;
   constexpr int RI = Layout<M, false>::in;
   constexpr int RO = Layout<M, false>::out;
+  constexpr int SL = slot_len<M>();  // complex values per sequence slot
+  constexpr int XS = 2 * SL;         // the same slot viewed as reals
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* buf = tw + NX;
   const int nseq = a.R * a.nf;
   const int npad = seq_pad<M>(nseq);
-  T* refs = reinterpret_cast<T*>(buf + (long)npad * M);  // R * nf per-row references
+  T* refs = reinterpret_cast<T*>(buf + (long)npad * SL);  // R * nf per-row references
   int* rowl = reinterpret_cast<int*>(refs + a.R * a.nf);  // level of row r (-1: beyond the grid)
   int* rowj = rowl + a.R;
   for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
@@ -324,29 +326,29 @@ __global__ void __launch_bounds__(256, 2) k_xfwd(const XFArgs<T> a) {
   for (int idx = threadIdx.x; idx < a.R * (NX / 4); idx += blockDim.x) {
     const int r = idx / (NX / 4);
     const int i = 4 * (idx - r * (NX / 4));
-    T* dst = xr + (long)(r * a.nf) * NX + i;
+    T* dst = xr + (long)(r * a.nf) * XS + i;
     const int l = rowl[r];
     if (l >= 0) {
       const int j = rowj[r];
-      xf_load<T, V4<T>>(a, l, j, i, dst, NX);
+      xf_load<T, V4<T>>(a, l, j, i, dst, XS);
       if (a.use_ref)
         for (int f = 0; f < a.nf; ++f) {
           const T rf = refs[r * a.nf + f];
 #pragma unroll
-          for (int q = 0; q < 4; ++q) dst[f * NX + q] -= rf;
+          for (int q = 0; q < 4; ++q) dst[f * XS + q] -= rf;
         }
     } else {
-      for (int f = 0; f < a.nf; ++f) vst(dst + f * NX, vsplat<V4<T>>(T(0)));
+      for (int f = 0; f < a.nf; ++f) vst(dst + f * XS, vsplat<V4<T>>(T(0)));
     }
   }
-  for (int idx = nseq * M + threadIdx.x; idx < npad * M; idx += blockDim.x) buf[idx] = cplx<T>{T(0), T(0)};
+  for (int idx = nseq * SL + threadIdx.x; idx < npad * SL; idx += blockDim.x) buf[idx] = cplx<T>{T(0), T(0)};
   __syncthreads();
   // complex FFT of length M per sequence in registers, then the r2c split
   const int lane_t = threadIdx.x % TL;
   for (int base = 0; base < npad; base += blockDim.x / TL) {
     const int s = base + threadIdx.x / TL;
     if (base + (threadIdx.x / 32) * (32 / TL) >= npad) break;  // whole warp beyond the slots
-    cplx<T>* seq = buf + (long)s * M;
+    cplx<T>* seq = buf + (long)s * SL;
     cplx<T> v[E];
 #pragma unroll
     for (int g = 0; g < E / RI; ++g)
@@ -645,12 +647,14 @@ __global__ void __launch_bounds__(256, 2) k_xinv(const XIArgs<T> a) {
   constexpr int E = Geo<M>::E;
   constexpr int RI = Layout<M, true>::in;
   constexpr int RO = Layout<M, true>::out;
+  constexpr int SL = slot_len<M>();  // complex values per sequence slot
+  constexpr int XS = 2 * SL;         // the same slot viewed as reals
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* buf = tw + NX;
   const int nseq = a.R * a.nin;
   const int npad = seq_pad<M>(nseq);
-  int* rowl = reinterpret_cast<int*>(buf + (long)npad * M);  // level of row r (-1: beyond the grid)
+  int* rowl = reinterpret_cast<int*>(buf + (long)npad * SL);  // level of row r (-1: beyond the grid)
   int* rowj = rowl + a.R;
   for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
   const long g0 = (long)blockIdx.x * a.R;
@@ -675,7 +679,7 @@ __global__ void __launch_bounds__(256, 2) k_xinv(const XIArgs<T> a) {
       l = rowl[r];
       j = rowj[r];
     }
-    cplx<T>* seq = buf + (long)s * M;
+    cplx<T>* seq = buf + (long)s * SL;
     // c2r split: Z_m = (X_m + conj X_{M-m}) + i W^{-m} (X_m - conj X_{M-m}),
     // imaginary parts of the DC and Nyquist bins ignored
     cplx<T> v[E];
@@ -729,7 +733,7 @@ __global__ void __launch_bounds__(256, 2) k_xinv(const XIArgs<T> a) {
   }
   if (direct) return;
   __syncthreads();
-  const T* xs = reinterpret_cast<const T*>(buf);  // x_i of sequence s at xs[s*NX + i]
+  const T* xs = reinterpret_cast<const T*>(buf);  // x_i of sequence s at xs[s*XS + i]
   // four consecutive points per thread
   for (int idx = threadIdx.x; idx < a.R * (NX / 4); idx += blockDim.x) {
     const int r = idx / (NX / 4);
@@ -737,12 +741,12 @@ __global__ void __launch_bounds__(256, 2) k_xinv(const XIArgs<T> a) {
     const int l = rowl[r];
     if (l < 0) continue;
     const int j = rowj[r];
-    T* xw0 = const_cast<T*>(xs) + (long)(r * a.nin) * NX + i0;
+    T* xw0 = const_cast<T*>(xs) + (long)(r * a.nin) * XS + i0;
     for (int f = 0; f < a.nin; ++f)  // this thread alone touches (r, i0..i0+3)
       if (a.refin[f]) {
         const T rf = a.refin[f][l];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) xw0[f * NX + q] += rf;
+        for (int q = 0; q < 4; ++q) xw0[f * XS + q] += rf;
       }
     if (a.op == XI_DIV) {
       // compute_derivatives.f90:544-574 + LES_engine.f90:546-551, one
@@ -756,7 +760,7 @@ __global__ void __launch_bounds__(256, 2) k_xinv(const XIArgs<T> a) {
       const long p2 = (long)j * NX + i0;
       for (int q = 0; q < a.nin; ++q) {
         const T* tz = a.aux[q];
-        const V xq = vld<V>(static_cast<const T*>(xw0), (long)q * NX);
+        const V xq = vld<V>(static_cast<const T*>(xw0), (long)q * XS);
         if (l >= 1 && l <= a.nz) {
           const V dzq = a.lo[q] ? rdz * (vld<V>(tz, off + pl) - vld<V>(tz, off))   // ddz_w
                                 : rdz * (vld<V>(tz, off) - vld<V>(tz, off - pl));  // ddz_uv
@@ -771,36 +775,36 @@ __global__ void __launch_bounds__(256, 2) k_xinv(const XIArgs<T> a) {
     for (int q4 = 0; q4 < 4; ++q4) {
     const int i = i0 + q4;
     const long off = (long)l * a.out_pstride + (long)j * NX + i;
-    const T* x = xw0 + q4;  // field f at x[f*NX]
+    const T* x = xw0 + q4;  // field f at x[f*XS]
     switch (a.op) {
       case XI_STORE: {
         for (int f = 0; f < a.nin; ++f)
           if (l >= a.lo[f] && l <= a.hi[f]) {
-            if (a.out_f32) a.outf[f][off] = float(x[f * NX]);
-            else a.out[f][off] = x[f * NX];
+            if (a.out_f32) a.outf[f][off] = float(x[f * XS]);
+            else a.out[f][off] = x[f * XS];
           }
         break;
       }
       case XI_LASD: {
         // compute_LagScaleDep.f90:541-594; c0 = 2 delta^2, c1 = alpha^2
-        const T uf = x[0], vf = x[NX], wf = x[2 * NX];
-        const T a11 = x[3 * NX] - uf * uf;
-        const T a12 = x[4 * NX] - uf * vf;
-        const T a13 = x[5 * NX] - uf * wf;
-        const T a22 = x[6 * NX] - vf * vf;
-        const T a23 = x[7 * NX] - vf * wf;
-        const T a33 = x[8 * NX] - wf * wf;
-        const T s11 = x[9 * NX], s12 = x[10 * NX], s13 = x[11 * NX];
-        const T s22 = x[12 * NX], s23 = x[13 * NX], s33 = x[14 * NX];
+        const T uf = x[0], vf = x[XS], wf = x[2 * XS];
+        const T a11 = x[3 * XS] - uf * uf;
+        const T a12 = x[4 * XS] - uf * vf;
+        const T a13 = x[5 * XS] - uf * wf;
+        const T a22 = x[6 * XS] - vf * vf;
+        const T a23 = x[7 * XS] - vf * wf;
+        const T a33 = x[8 * XS] - wf * wf;
+        const T s11 = x[9 * XS], s12 = x[10 * XS], s13 = x[11 * XS];
+        const T s22 = x[12 * XS], s23 = x[13 * XS], s33 = x[14 * XS];
         const T sft = sqrt(T(2) * (s11 * s11 + s22 * s22 + s33 * s33 +
                                    T(2) * (s12 * s12 + s13 * s13 + s23 * s23)));
         const T cst = T(a.c0), tf2 = T(a.c1);
-        const T b11 = cst * (x[15 * NX] - tf2 * sft * s11);
-        const T b12 = cst * (x[16 * NX] - tf2 * sft * s12);
-        const T b13 = cst * (x[17 * NX] - tf2 * sft * s13);
-        const T b22 = cst * (x[18 * NX] - tf2 * sft * s22);
-        const T b23 = cst * (x[19 * NX] - tf2 * sft * s23);
-        const T b33 = cst * (x[20 * NX] - tf2 * sft * s33);
+        const T b11 = cst * (x[15 * XS] - tf2 * sft * s11);
+        const T b12 = cst * (x[16 * XS] - tf2 * sft * s12);
+        const T b13 = cst * (x[17 * XS] - tf2 * sft * s13);
+        const T b22 = cst * (x[18 * XS] - tf2 * sft * s22);
+        const T b23 = cst * (x[19 * XS] - tf2 * sft * s23);
+        const T b33 = cst * (x[20 * XS] - tf2 * sft * s33);
         a.out[0][off] = a11 * b11 + a22 * b22 + a33 * b33 + T(2) * (a12 * b12 + a13 * b13 + a23 * b23);
         a.out[1][off] = b11 * b11 + b22 * b22 + b33 * b33 + T(2) * (b12 * b12 + b13 * b13 + b23 * b23);
         break;
@@ -810,7 +814,7 @@ __global__ void __launch_bounds__(256, 2) k_xinv(const XIArgs<T> a) {
         // c0 = dz, c1 = 1/log-free constant unused; aux[0] = z0 plane.
         // out: u_star_avg, lbc_u, lbc_v, txz(1), tyz(1), dudz(1), dvdz(1)
         const long p2 = (long)j * NX + i;
-        const double u1 = double(x[0]), v1 = double(x[NX]);
+        const double u1 = double(x[0]), v1 = double(x[XS]);
         const double uavg = sqrt(u1 * u1 + v1 * v1);
         const double dz = a.c0;
         const double ustar = KVONK * uavg / log((0.5 * dz) / double(a.aux[0][p2]));

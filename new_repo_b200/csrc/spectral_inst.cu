@@ -63,7 +63,8 @@ void launch_xfwd(int NX, XFArgs<T> a, cudaStream_t st) {
   const int M = NX / 2;
   a.R = rows_per_cta<T>(a.nf, M);
   a.in_rstride = NX;
-  const size_t smem = sizeof(cplx<T>) * (NX + (size_t)pad_seqs(a.R * a.nf, M) * M) + sizeof(T) * a.R * a.nf +
+  const int SL = (M + M / 16 + 1) & ~1;  // slot_len<M>()
+  const size_t smem = sizeof(cplx<T>) * (NX + (size_t)pad_seqs(a.R * a.nf, M) * SL) + sizeof(T) * a.R * a.nf +
                       2 * sizeof(int) * a.R + 16;
   if (smem > SMEM_CAP) throw CudaError(1, "xfwd: shared memory request too large");
   const int grid = ceil_div(a.nrows, a.R);
@@ -88,7 +89,8 @@ template <typename T>
 void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
   const int M = NX / 2;
   a.R = rows_per_cta<T>(a.nin, M);
-  const size_t smem = sizeof(cplx<T>) * (NX + (size_t)pad_seqs(a.R * a.nin, M) * M) + 2 * sizeof(int) * a.R;
+  const int SL = (M + M / 16 + 1) & ~1;  // slot_len<M>()
+  const size_t smem = sizeof(cplx<T>) * (NX + (size_t)pad_seqs(a.R * a.nin, M) * SL) + 2 * sizeof(int) * a.R;
   if (smem > SMEM_CAP) throw CudaError(1, "xinv: shared memory request too large");
   const int grid = ceil_div(a.nrows, a.R);
   if (grid == 0) return;
@@ -123,7 +125,8 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
   const int W = 128 / int(sizeof(cplx<T>));
   auto stride = [&](int n, int C) {
     const int target = (32 / C) % W;
-    return n + ((target - n % W) % W + W) % W;
+    const int base = n + n / 16;  // room for the FFT's padded exchange (slot_len)
+    return base + ((target - base % W) % W + W) % W;
   };
   auto per_col = [&](int C) {
     return (size_t)(a.nin * stride(NY, C) + stride(NYO, C)) * sizeof(cplx<T>);
