@@ -281,7 +281,7 @@ __host__ __device__ constexpr int seq_pad(int nseq) {
 }
 
 template <typename T, int NX>
-__global__ void __launch_bounds__(256, 2) k_xfwd(const XFArgs<T> a) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd(const XFArgs<T> a) {
   constexpr int M = NX / 2;
   constexpr int TL = Geo<M>::T;
   constexpr int E = Geo<M>::E;
@@ -641,7 +641,7 @@ struct XIArgs {
 };
 
 template <typename T, int NX>
-__global__ void __launch_bounds__(256, 2) k_xinv(const XIArgs<T> a) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIArgs<T> a) {
   constexpr int M = NX / 2;
   constexpr int TL = Geo<M>::T;
   constexpr int E = Geo<M>::E;
