@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=256, help="grid nx = ny (= nz unless --nz)")
+    ap.add_argument("--n", "--grid-n", dest="n", type=int, default=256, help="grid nx = ny (= nz unless --nz)")
     ap.add_argument("--nz", type=int, default=None, help="vertical levels (default: --n)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
