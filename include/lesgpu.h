@@ -183,6 +183,18 @@ int les_upload_async(les_state* s, int field, const double* pinned, int k0, int 
 int les_download_async(les_state* s, int field, double* pinned, int k0, int k1);
 int les_diagnostics_async(les_state* s, double* pinned_out4);
 
+/* Checkpoint file of write_checkpoint_file / read_checkpoint_file
+ * (IO_checkpoint.f90:119-256) on one rank, byte for byte: native FP64
+ * records of nx*ny*(nz+1) values (levels 1..nz+1, x fastest) for u, v, w,
+ * rhsx, rhsy, rhsz, cs_opt2 and, when the Lagrangian averages exist
+ * (Lagran_init), F_LM, F_MM, F_QN, F_NN.  Reading with lagran_init = 1 also
+ * sets the Lagrangian-init flag (compute_LagScaleDep.f90:66); the Lagrangian
+ * accumulators restart at zero, w(0) takes its allocation value and the
+ * wall law sets the lower u, v conditions to Neumann (LES_engine.f90:160-171).  Errors: 1 cannot open / short file (the
+ * reference aborts with 1), 22 read or write failure. */
+int les_checkpoint_write(les_state* s, const char* path);
+int les_checkpoint_read(les_state* s, const char* path, int lagran_init);
+
 /* ---- learned SGS closure (no reference counterpart) ---------------------
  * Cs^2 = Cs^2_prev * exp(net(features)) from an 8 -> 64 -> 64 -> 1 GELU network with
  * BF16 weights and FP32 accumulation (tcgen05 tensor cores), evaluated at

@@ -91,6 +91,8 @@ PROTOTYPES = {
     "les_upload_async": [_P, _I, C.c_void_p, _I, _I],
     "les_download_async": [_P, _I, C.c_void_p, _I, _I],
     "les_diagnostics_async": [_P, C.c_void_p],
+    "les_checkpoint_write": [_P, C.c_char_p],
+    "les_checkpoint_read": [_P, C.c_char_p, _I],
     "les_set_sgs_model": [_P, _I],
     "les_mlp_init": [_P, C.c_uint],
     "les_mlp_set_params": [_P, _F, _I],

@@ -334,6 +334,17 @@ int les_mlp_check_profile(les_state* s, double* out, int n) {
   return guard([&] { s->s->mlp_check_profile(out, n); });
 }
 
+int les_checkpoint_write(les_state* s, const char* path) {
+  STATE_OR_FAIL(s);
+  if (!path) return bad_state();
+  return guard([&] { s->s->checkpoint_write(path); });
+}
+int les_checkpoint_read(les_state* s, const char* path, int lagran_init) {
+  STATE_OR_FAIL(s);
+  if (!path) return bad_state();
+  return guard([&] { s->s->checkpoint_read(path, lagran_init); });
+}
+
 int les_timers(les_state* s, double out[5]) {
   STATE_OR_FAIL(s);
   return guard([&] {

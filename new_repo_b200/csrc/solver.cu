@@ -1,6 +1,7 @@
 // Device-resident LES state and the operator sequence of one time step
 // (LES_engine.f90:189-360), for FP64 and mixed (FP32 fields) precision.
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -638,6 +639,68 @@ class Solver final : public SolverBase {
       }
     }
     if (nb > 0) lasd(a, jtt, nb);  // the wall band: the plain procedure, Lagrangian history kept
+  }
+
+  // ------------------------------------------------------------ restart ----
+  // IO_checkpoint.f90:119-256 on one rank: native FP64 records of
+  // nx*ny*(nz+1) values (levels 1..nz+1, x fastest): u, v, w, rhsx, rhsy,
+  // rhsz, cs_opt2, then F_LM, F_MM, F_QN, F_NN when the Lagrangian averages
+  // exist (Lagran_init).
+  std::vector<int> checkpoint_fields(bool with_f) const {
+    std::vector<int> ids = {LES_U, LES_V, LES_W, LES_RHSX, LES_RHSY, LES_RHSZ, LES_CS_OPT2};
+    if (with_f)
+      for (int q : {LES_F_LM, LES_F_MM, LES_F_QN, LES_F_NN}) ids.push_back(q);
+    return ids;
+  }
+  void checkpoint_write(const char* path) override {
+    FILE* f = std::fopen(path, "wb");
+    if (!f) throw CudaError(1, std::string("[checkpoint error] cannot open checkpoint file ") + path);
+    const long n = (long)(g.nz + 1) * g.plane();
+    std::vector<double> buf(n);
+    bool ok = true;
+    for (int id : checkpoint_fields(lagran_init)) {
+      download(id, buf.data(), 1, g.nz + 1);
+      ok = ok && std::fwrite(buf.data(), sizeof(double), n, f) == size_t(n);
+    }
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) throw CudaError(22, std::string("[checkpoint error] cannot write checkpoint file ") + path);
+  }
+  void checkpoint_read(const char* path, int with_f) override {
+    FILE* f = std::fopen(path, "rb");
+    if (!f) throw CudaError(1, std::string("[Restart error] cannot open checkpoint file ") + path);
+    const long n = (long)(g.nz + 1) * g.plane();
+    const auto ids = checkpoint_fields(with_f != 0);
+    std::fseek(f, 0, SEEK_END);
+    const long bytes = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    if (bytes < long(ids.size()) * n * long(sizeof(double))) {
+      std::fclose(f);
+      throw CudaError(1, std::string("[Restart error] checkpoint file too short for this grid: ") + path);
+    }
+    std::vector<double> buf(n);
+    for (int id : ids) {
+      if (std::fread(buf.data(), sizeof(double), n, f) != size_t(n)) {
+        std::fclose(f);
+        throw CudaError(22, std::string("[Restart error] cannot read checkpoint file ") + path);
+      }
+      upload(id, buf.data(), 1, g.nz + 1);
+    }
+    std::fclose(f);
+    // the Lagrangian accumulators restart empty (they are not in the file);
+    // w(0) keeps its allocation value (system.f90:196-198), and the wall law
+    // switches the lower u, v conditions to Neumann as after the initial
+    // conditions (LES_engine.f90:160-171)
+    for (int q : {LES_U_LAG, LES_V_LAG, LES_W_LAG}) fill(F[q], 0, g.nz + 1, T(0));
+    fill(F[LES_W], 0, 0, T(BOGUS));
+    if (P.wall_law) {
+      lbc_t[0] = 2;
+      lbc_t[1] = 2;
+    }
+    if (with_f) {  // compute_LagScaleDep.f90:66
+      f_coeff_init = true;
+      lagran_init = true;
+    }
+    LES_CUDA(cudaStreamSynchronize(st));
   }
 
   double* staging = nullptr;  // FP64 device staging field (mixed precision transfers)

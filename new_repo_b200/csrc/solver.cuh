@@ -125,6 +125,8 @@ struct SolverBase : LaunchHook {
   virtual void mlp_info(double* out) = 0;
   virtual void mlp_set_check_every(int every) = 0;
   virtual void mlp_set_wall_levels(int n) = 0;
+  virtual void checkpoint_write(const char* path) = 0;
+  virtual void checkpoint_read(const char* path, int with_f) = 0;
   virtual void mlp_check_profile(double* out, int n) = 0;
   virtual void upload_async(int field, const double* pinned, int k0, int k1) = 0;
   virtual void download_async(int field, double* pinned, int k0, int k1) = 0;

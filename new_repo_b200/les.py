@@ -129,16 +129,9 @@ _NML_KEYS = {"p_on_y", "p_on_z", "nx", "ny", "nz", "nt", "dt", "dim_dt_flag", "r
              "dyn_init", "lbc_special", "wall_model"}
 
 
-def read_namelist(path: str | Path) -> tuple[RunParams, dict]:
-    """Parse a ``parameters.nlst`` (parameters_IO.f90:151-234) into RunParams.
-
-    Returns (params, raw) where raw holds every key=value found.  Raises
-    LesError(22) when the file cannot be read, like the reference's
-    MPI_Abort(22) (parameters_IO.f90:173-234)."""
-    try:
-        text = Path(path).read_text()
-    except OSError as e:
-        raise LesError(capi.LES_ERR_IO, f"Could not open {path} for reading ({e})") from e
+def _namelist_values(text: str) -> dict:
+    """key = value pairs of a Fortran namelist (keys lower-cased; logicals,
+    integers, reals with d/e exponents and quoted strings)."""
     raw = {}
     for m in re.finditer(r"(\w+)\s*=\s*('[^']*'|\"[^\"]*\"|[^\s,/]+)", text):
         key, val = m.group(1).lower(), m.group(2).strip()
@@ -154,6 +147,20 @@ def read_namelist(path: str | Path) -> tuple[RunParams, dict]:
             except ValueError:
                 v = float(val.lower().replace("d", "e"))
         raw[key] = v
+    return raw
+
+
+def read_namelist(path: str | Path) -> tuple[RunParams, dict]:
+    """Parse a ``parameters.nlst`` (parameters_IO.f90:151-234) into RunParams.
+
+    Returns (params, raw) where raw holds every key=value found.  Raises
+    LesError(22) when the file cannot be read, like the reference's
+    MPI_Abort(22) (parameters_IO.f90:173-234)."""
+    try:
+        text = Path(path).read_text()
+    except OSError as e:
+        raise LesError(capi.LES_ERR_IO, f"Could not open {path} for reading ({e})") from e
+    raw = _namelist_values(text)
     kw = dict(nx=raw.get("nx", 32), ny=raw.get("ny", 32), nz=raw.get("nz", 32), dt=float(raw.get("dt", 2e-4)),
               dim_dt_flag=bool(raw.get("dim_dt_flag", False)), xy_pi=bool(raw.get("xy_pi", True)),
               lx_in=float(raw.get("lx", 2.0)), ly_in=float(raw.get("ly", 2.0)), lz_in=float(raw.get("lz", 1.0)),
@@ -164,6 +171,36 @@ def read_namelist(path: str | Path) -> tuple[RunParams, dict]:
               dyn_init=int(raw.get("dyn_init", 1500)), lbc_special=str(raw.get("lbc_special", "std")),
               wall_model=str(raw.get("wall_model", "wall_filter")))
     return RunParams(**kw), raw
+
+
+def write_parameters_restart(path: str | Path, p: RunParams, jt_total: int, lagran_init: bool) -> None:
+    """``parameters_restart.nlst`` as write_parameters_restart writes it
+    (parameters_IO.f90:333-369): the restart_param namelist of one rank."""
+    t = "T" if lagran_init else "F"
+    text = (f"&RESTART_PARAM\n P_ON_Y_F=1,\n P_ON_Z_F=1,\n NX_F={p.nx},\n NY_F={p.ny},\n NZ_F={p.nz},\n"
+            f" JT_TOTAL={int(jt_total)},\n DYN_INIT={int(p.dyn_init)},\n LAGRAN_INIT={t},\n"
+            f" SGS_MODEL='{p.sgs_model}',\n /\n")
+    try:
+        Path(path).write_text(text)
+    except OSError as e:
+        raise LesError(capi.LES_ERR_IO, f"Could not open {path} for writing ({e})") from e
+
+
+def read_parameters_restart(path: str | Path, p: RunParams) -> dict:
+    """read_parameters_restart (parameters_IO.f90:380-435): jt_total,
+    dyn_init, Lagran_init and sgs_model of a restart; LesError(22) when the
+    file cannot be read, LesError(1) when the grid differs from ``p``."""
+    try:
+        raw = _namelist_values(Path(path).read_text())
+    except OSError as e:
+        raise LesError(capi.LES_ERR_IO, f"Could not open {path} for reading ({e})") from e
+    need = ("nx_f", "ny_f", "nz_f", "jt_total", "lagran_init")
+    if any(k not in raw for k in need):
+        raise LesError(capi.LES_ERR_IO, f"Error in namelist restart_param of {path}")
+    if (raw["nx_f"], raw["ny_f"], raw["nz_f"]) != (p.nx, p.ny, p.nz):
+        raise LesError(capi.LES_ERR_INVALID, "[Restart error] invalid restart parameters")
+    return {"jt_total": int(raw["jt_total"]), "dyn_init": int(raw.get("dyn_init", p.dyn_init)),
+            "lagran_init": bool(raw["lagran_init"]), "sgs_model": str(raw.get("sgs_model", p.sgs_model))}
 
 
 def log_law_noise(p: RunParams, seed: int = 0, amp: float = 0.1):
@@ -477,6 +514,34 @@ class LES:
     def mlp_set_wall_levels(self, nlev: int):
         """Levels 1..nlev next to the wall keep the plain LASD procedure."""
         check(self.lib.les_mlp_set_wall_levels(self._h, int(nlev)))
+
+    # ----------------------------------------------------------------- restart
+    @property
+    def lagran_init(self) -> bool:
+        return self.f_coeff_init
+
+    def checkpoint_out(self, directory: str | Path = ".", jt_total: int | None = None) -> Path:
+        """checkpoint_out + write_parameters_restart (IO_checkpoint.f90:84-98,
+        parameters_IO.f90:333-369): ``checkpoint_<jt_total:09d>`` (byte for
+        byte the reference's file on one rank) and ``parameters_restart.nlst``."""
+        jt_total = self.jt_total if jt_total is None else int(jt_total)
+        d = Path(directory)
+        path = d / f"checkpoint_{jt_total:09d}"
+        check(self.lib.les_checkpoint_write(self._h, str(path).encode()))
+        write_parameters_restart(d / "parameters_restart.nlst", self.params, jt_total, self.lagran_init)
+        return path
+
+    def checkpoint_in(self, directory: str | Path = ".") -> dict:
+        """read_parameters_restart + checkpoint_in (LES_engine.f90:117-164):
+        restores u, v, w, rhs, cs_opt2 (and the Lagrangian averages) and the
+        step counter; the run continues with jt = 0, jt_total as saved."""
+        d = Path(directory)
+        rp = read_parameters_restart(d / "parameters_restart.nlst", self.params)
+        path = d / f"checkpoint_{rp['jt_total']:09d}"
+        check(self.lib.les_checkpoint_read(self._h, str(path).encode(), 1 if rp["lagran_init"] else 0))
+        self.jt_total = rp["jt_total"]
+        self.jt = 0
+        return rp
 
     def state_dict(self, names=None) -> dict:
         names = capi.FIELDS if names is None else names

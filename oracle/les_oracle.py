@@ -1091,3 +1091,39 @@ def make_state(p: Params, seed: int = 0, amp: float = 0.1):
     u, v, w = log_law_fields(p, seed, amp)
     set_initial_conditions(p, st, u, v, w)
     return st
+
+
+# ---------------------------------------------------------------------------
+# checkpoint files (IO_checkpoint.f90:119-256 on a 1x1 process grid)
+# ---------------------------------------------------------------------------
+CHECKPOINT_FIELDS = ("u", "v", "w", "rhsx", "rhsy", "rhsz", "cs_opt2")
+CHECKPOINT_F = ("F_LM", "F_MM", "F_QN", "F_NN")
+
+
+def write_checkpoint(st: State, path) -> None:
+    """write_checkpoint_file: each variable as nx*ny*(nz+1) native float64
+    values, levels 1..nz+1 in Fortran order (write_var_tbg / write_var_tg
+    start at var(1,1,1)); the F averages only when Lagran_init is set."""
+    names = CHECKPOINT_FIELDS + (CHECKPOINT_F if st.lagran_init else ())
+    with open(path, "wb") as f:
+        for n in names:
+            f.write(np.ascontiguousarray(getattr(st, n)[1:], dtype="<f8").tobytes())
+
+
+def read_checkpoint(st: State, path, lagran_init: bool) -> None:
+    """read_checkpoint_file + checkpoint_in: levels 1..nz+1 of each variable;
+    the ghost updates of checkpoint_in do nothing on one rank.  With
+    Lagran_init the Lagrangian-init flag is set (compute_LagScaleDep.f90:66)."""
+    shp = st.u[1:].shape  # (nz+1, ny, nx); st.p is the pressure field
+    n = int(np.prod(shp))
+    names = CHECKPOINT_FIELDS + (CHECKPOINT_F if lagran_init else ())
+    data = np.fromfile(path, dtype="<f8")
+    if data.size < n * len(names):
+        raise ValueError("[Restart error] checkpoint file too short for this grid")
+    for q, name in enumerate(names):
+        getattr(st, name)[1:] = data[q * n:(q + 1) * n].reshape(shp)
+    for name in ("u_lag", "v_lag", "w_lag"):
+        getattr(st, name)[:] = 0.0
+    if lagran_init:
+        st.f_coeff_init = True
+        st.lagran_init = True
