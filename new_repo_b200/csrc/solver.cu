@@ -103,9 +103,9 @@ class Solver final : public SolverBase {
     for (int i = 0; i < LES_NFIELDS; ++i) F[i] = track(dalloc<T>(nf));
     for (int i = 0; i < LES_NPLANES; ++i) PL[i] = track(dalloc<T>(g.plane()));
     build_tables();
-    const long se = (long)g.L * std::max((long)g.ny * g.lhx, (long)g.ny2 * (g.nx / 2));
+    const long se = (long)g.L * std::max((long)g.ny * pitch(g.lhx), (long)g.ny2 * pitch(g.nx / 2));
     for (int i = 0; i < NSPEC; ++i) spec[i] = track(dalloc<cplx<T>>(se));
-    for (int i = 0; i < NSPEC; ++i) spec4[i] = track(dalloc<cplx<T>>((long)g.L * g.ny * nk4));
+    for (int i = 0; i < NSPEC; ++i) spec4[i] = track(dalloc<cplx<T>>((long)g.L * g.ny * pitch(nk4)));
     const long fe = (long)g.L * g.ny2 * g.nx2;
     for (auto& f : fine) f = track(dalloc<T>(fe));
     for (auto& f : sc) f = track(dalloc<T>(nf));
@@ -263,6 +263,10 @@ class Solver final : public SolverBase {
     KL("k_fill", double(g.plane()) * sizeof(T), k_fill<T><<<grid_for(g.plane()), 256, 0, st>>>(f, g.plane(), v));
   }
 
+  // row pitch of the spectral buffers: whole 8-value groups (64 B in FP32),
+  // so that column blocks of the y pass start on sector boundaries
+  static int pitch(int nk) { return (nk + 7) & ~7; }
+
   XFArgs<T> xf(int op, int nf, int plane0, int nplanes, int NX, int rows_pp, int nk) {
     XFArgs<T> a;
     std::memset(&a, 0, sizeof(a));
@@ -272,10 +276,11 @@ class Solver final : public SolverBase {
     a.rows_pp = rows_pp;
     a.nrows = (long)nplanes * rows_pp;
     a.nk = nk;
+    a.opitch = pitch(nk);
     a.nz = g.nz;
     a.wall = P.wall_law;
     a.in_pstride = (long)rows_pp * NX;
-    a.out_pstride = (long)rows_pp * nk;
+    a.out_pstride = (long)rows_pp * a.opitch;
     a.tw = twiddles(NX);
     return a;
   }
@@ -288,8 +293,10 @@ class Solver final : public SolverBase {
     a.ncols = ncols;
     a.nk_in = nk_in;
     a.nk_out = nk_out;
-    a.in_pstride = (long)NY * nk_in;
-    a.out_pstride = (long)NYO * nk_out;
+    a.ipitch = pitch(nk_in);
+    a.opitch = pitch(nk_out);
+    a.in_pstride = (long)NY * a.ipitch;
+    a.out_pstride = (long)NYO * a.opitch;
     a.plane0 = plane0;
     a.nxh = g.nx / 2;
     a.lhx = g.lhx;
@@ -308,8 +315,9 @@ class Solver final : public SolverBase {
     a.rows_pp = rows_pp;
     a.nrows = (long)nplanes * rows_pp;
     a.nk = nk;
+    a.ipitch = pitch(nk);
     a.nz = g.nz;
-    a.in_pstride = (long)rows_pp * nk;
+    a.in_pstride = (long)rows_pp * a.ipitch;
     a.out_pstride = (long)rows_pp * NX;
     a.tw = twiddles(NX);
     return a;
@@ -1251,7 +1259,8 @@ class Solver final : public SolverBase {
     y.G1 = gtt;
     y.ncols1 = nk4;
     y.nk_out1 = nk4;
-    y.out_pstride1 = (long)g.ny * nk4;
+    y.opitch1 = pitch(nk4);
+    y.out_pstride1 = (long)g.ny * y.opitch1;
     for (int q = 0; q < 21; ++q) {
       y.in[q] = spec[q];
       y.out[(both ? 2 : 1) * q] = spec[q];

@@ -46,6 +46,7 @@ struct XFArgs {
   int rows_pp;     // rows per plane of the input grid
   int plane0;      // first level
   int nk;          // modes stored per output row
+  int opitch;      // complex values between output rows (>= nk; 0: nk)
   int nz;
   int wall;        // wall-law special rows at k=1
   int use_ref;     // subtract each field's value at (i,j)=(0,0) of the level
@@ -367,7 +368,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd(const XFAr
       const int l = rowl[r];
       if (l >= 0) {
         const int j = rowj[r];
-        cplx<T>* orow = a.out[f] + (long)l * a.out_pstride + (long)j * a.nk;
+        cplx<T>* orow = a.out[f] + (long)l * a.out_pstride + (long)j * a.opitch;
         for (int k = lane_t; k < a.nk; k += TL) {
           // X_k = E_k + W^k O_k, E = (Z_k + conj Z_{M-k})/2, O = (Z_k - conj Z_{M-k})/(2i)
           const cplx<T> zk = seq[k == M ? 0 : k];
@@ -401,6 +402,8 @@ struct YPArgs {
   int ncols;           // columns processed
   int ncols1;          // columns stored for the second FILTER2 output
   int nk_in, nk_out, nk_out1;
+  int ipitch, opitch, opitch1;  // complex values between rows of in / out / second out (0: the nk)
+  int nplanes, ngroups;         // work items: column blocks x planes x groups
   int plane0;
   long in_pstride, out_pstride, out_pstride1;
   int nxh, lhx;        // base-grid Nyquist column and row length of kkx/kky/G
@@ -450,6 +453,44 @@ __device__ __forceinline__ cplx<T> yp_op(const YPArgs<T>& a, int q, int kx, int 
   }
 }
 
+// ---- asynchronous global -> shared copies (cp.async) ----
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  const int n = valid ? BYTES : 0;  // 0: zero fill, nothing read
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gmem), "r"(n) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(d), "l"(gmem), "n"(BYTES), "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// y pass: start the copies of work item `item` (C columns x NY rows of every
+// input field) into the shared stage `bin` ([nin][C][SI])
+template <typename T, int NY>
+__device__ __forceinline__ void yp_issue(const YPArgs<T>& a, long item, int ncb, cplx<T>* bin) {
+  const int C = a.C, SI = a.SI;
+  const int col0 = int(item % ncb) * C;
+  const int l = a.plane0 + int((item / ncb) % a.nplanes);
+  const int grp = int(item / ((long)ncb * a.nplanes));
+  for (int idx = threadIdx.x; idx < a.nin * NY * C; idx += blockDim.x) {
+    const int c = idx & (C - 1);
+    const int t = idx >> a.lc;
+    const int ky = t % NY;
+    const int q = t / NY;
+    const int kx = col0 + c;
+    const cplx<T>* base = a.in[grp * a.nin + q];
+    const bool valid = kx < a.ncols;
+    const cplx<T>* src = valid ? base + (long)l * a.in_pstride + (long)ky * a.ipitch + kx : base;
+    cp_async<int(sizeof(cplx<T>))>(bin + (q * C + c) * SI + ky, src, valid);
+  }
+}
+
 template <typename T, int NY, int NYO>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPArgs<T> a) {
   constexpr int TL = Geo<NY>::T;
@@ -468,25 +509,35 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPA
   const int SI = a.SI;  // >= NY
   const int SO = a.SO;  // >= NYO
   const int C = a.C;
-  cplx<T>* bin = two + NYO;           // [nin][C][SI]
-  cplx<T>* bout = bin + a.nin * C * SI;  // [C][SO]
+  cplx<T>* bin0 = two + NYO;               // input stage 0: [nin][C][SI]
+  cplx<T>* bin1 = bin0 + a.nin * C * SI;   // input stage 1
+  cplx<T>* bout = bin1 + a.nin * C * SI;   // [C][SO]
   for (int i = threadIdx.x; i < NY; i += blockDim.x) twi[i] = a.tw_in[i];
   for (int i = threadIdx.x; i < NYO; i += blockDim.x) two[i] = a.tw_out[i];
-  const int col0 = blockIdx.x * C;
-  const int l = a.plane0 + blockIdx.y;
-  const int grp = blockIdx.z;
-  // coalesced load of C columns of every input field
-  for (int idx = threadIdx.x; idx < a.nin * NY * C; idx += blockDim.x) {
-    const int c = idx & (C - 1);
-    const int t = idx >> a.lc;
-    const int ky = t % NY;
-    const int q = t / NY;
-    const int kx = col0 + c;
-    cplx<T> v = {T(0), T(0)};
-    if (kx < a.ncols) v = a.in[grp * a.nin + q][(long)l * a.in_pstride + (long)ky * a.nk_in + kx];
-    bin[(q * C + c) * SI + ky] = v;
+  // persistent CTAs: work item = (column block, plane, group); the columns
+  // of the next item are copied into the other input stage asynchronously
+  // while this one is transformed
+  const int ncb = (a.ncols + C - 1) / C;
+  const long nitems = (long)ncb * a.nplanes * a.ngroups;
+  if ((long)blockIdx.x < nitems) {
+    yp_issue<T, NY>(a, blockIdx.x, ncb, bin0);
+    cp_async_commit();
+  }
+  int stage = 0;
+  for (long item = blockIdx.x; item < nitems; item += gridDim.x) {
+  const long next = item + gridDim.x;
+  cplx<T>* bin = stage ? bin1 : bin0;
+  if (next < nitems) {
+    yp_issue<T, NY>(a, next, ncb, stage ? bin0 : bin1);
+    cp_async_commit();
+    cp_async_wait<1>();
+  } else {
+    cp_async_wait<0>();
   }
   __syncthreads();
+  const int col0 = int(item % ncb) * C;
+  const int l = a.plane0 + int((item / ncb) % a.nplanes);
+  const int grp = int(item / ((long)ncb * a.nplanes));
   const int c = threadIdx.x / TL;
   const int lt = threadIdx.x % TL;
   const int kx = col0 + c;
@@ -602,11 +653,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPA
       const int kxx = col0 + cc;
       if (kxx < lim) {
         const cplx<T> val = bout[cc * SO + ky];
-        if (second) a.out[grp * a.nout + q][(long)l * a.out_pstride1 + (long)ky * a.nk_out1 + kxx] = val;
-        else a.out[grp * a.nout + q][(long)l * a.out_pstride + (long)ky * a.nk_out + kxx] = val;
+        if (second) a.out[grp * a.nout + q][(long)l * a.out_pstride1 + (long)ky * a.opitch1 + kxx] = val;
+        else a.out[grp * a.nout + q][(long)l * a.out_pstride + (long)ky * a.opitch + kxx] = val;
       }
     }
     __syncthreads();
+  }
+  stage ^= 1;
   }
 }
 
@@ -625,6 +678,7 @@ struct XIArgs {
   int rows_pp;
   int plane0;
   int nk;          // modes present in the input rows (rest zero)
+  int ipitch;      // complex values between input rows (>= nk; 0: nk)
   int nz;
   long in_pstride;
   long out_pstride;  // elements per plane of the output grid
@@ -683,7 +737,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
     // c2r split: Z_m = (X_m + conj X_{M-m}) + i W^{-m} (X_m - conj X_{M-m}),
     // imaginary parts of the DC and Nyquist bins ignored
     cplx<T> v[E];
-    const cplx<T>* row = valid ? a.in[f] + (long)l * a.in_pstride + (long)j * a.nk : nullptr;
+    const cplx<T>* row = valid ? a.in[f] + (long)l * a.in_pstride + (long)j * a.ipitch : nullptr;
 #pragma unroll
     for (int gg = 0; gg < E / RI; ++gg)
 #pragma unroll

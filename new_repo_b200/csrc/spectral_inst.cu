@@ -1,6 +1,9 @@
 // Instantiation and launch of the spectral pass kernels for every supported
 // transform length (2^a 3^b: the grid sizes 16..512 and their 3/2 padding).
 #include "spectral.cuh"
+#include <algorithm>
+#include <mutex>
+
 #include "launch.cuh"
 
 namespace les {
@@ -61,6 +64,7 @@ bool supported_length(int n) {
 template <typename T>
 void launch_xfwd(int NX, XFArgs<T> a, cudaStream_t st) {
   const int M = NX / 2;
+  if (a.opitch == 0) a.opitch = a.nk;
   a.R = rows_per_cta<T>(a.nf, M);
   a.in_rstride = NX;
   const int SL = (M + M / 16 + 1) & ~1;  // slot_len<M>()
@@ -88,6 +92,7 @@ void launch_xfwd(int NX, XFArgs<T> a, cudaStream_t st) {
 template <typename T>
 void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
   const int M = NX / 2;
+  if (a.ipitch == 0) a.ipitch = a.nk;
   a.R = rows_per_cta<T>(a.nin, M);
   const int SL = (M + M / 16 + 1) & ~1;  // slot_len<M>()
   const size_t smem = sizeof(cplx<T>) * (NX + (size_t)pad_seqs(a.R * a.nin, M) * SL) + 2 * sizeof(int) * a.R;
@@ -114,8 +119,40 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
   hook_after();
 }
 
+// CTAs of `kern` resident on the current device at once; cached in a fixed
+// table (no heap allocation: the allocation-free entry point launches these
+// kernels too)
+struct ResidentEntry {
+  int dev;
+  const void* kern;
+  int threads;
+  size_t smem;
+  int n;
+};
+static int resident_ctas(const void* kern, int threads, size_t smem) {
+  static std::mutex mu;
+  static ResidentEntry table[256];
+  static int used = 0;
+  int dev = 0;
+  LES_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  for (int i = 0; i < used; ++i) {
+    const ResidentEntry& e = table[i];
+    if (e.dev == dev && e.kern == kern && e.threads == threads && e.smem == smem) return e.n;
+  }
+  int per_sm = 0, sms = 0;
+  LES_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+  LES_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int n = std::max(1, per_sm) * std::max(1, sms);
+  if (used < 256) table[used++] = ResidentEntry{dev, kern, threads, smem, n};
+  return n;
+}
+
 template <typename T>
 void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaStream_t st) {
+  if (a.ipitch == 0) a.ipitch = a.nk_in;
+  if (a.opitch == 0) a.opitch = a.nk_out;
+  if (a.opitch1 == 0) a.opitch1 = a.nk_out1;
   const int TL = lanes(NY);
   if (lanes(NYO) != TL) throw CudaError(1, "ypass: length pair with different lane counts");
   // column stride of the shared staging buffers: the load and store loops
@@ -128,11 +165,11 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
     const int base = n + n / 16;  // room for the FFT's padded exchange (slot_len)
     return base + ((target - base % W) % W + W) % W;
   };
-  auto per_col = [&](int C) {
-    return (size_t)(a.nin * stride(NY, C) + stride(NYO, C)) * sizeof(cplx<T>);
+  auto per_col = [&](int C) {  // two input stages + the output slot
+    return (size_t)(2 * a.nin * stride(NY, C) + stride(NYO, C)) * sizeof(cplx<T>);
   };
-  int lc = 0;  // C = 1 << lc columns per CTA, C * TL <= 256 threads
-  while ((2 << lc) * TL <= 256 && (size_t(2) << lc) * per_col(2 << lc) <= 96 * 1024 && (1 << lc) < a.ncols) ++lc;
+  int lc = 0;  // C = 1 << lc columns per CTA, C * TL <= 256 threads, two CTAs per SM
+  while ((2 << lc) * TL <= 256 && (size_t(2) << lc) * per_col(2 << lc) <= 112 * 1024 && (1 << lc) < a.ncols) ++lc;
   while ((1 << lc) * TL < 32) ++lc;  // at least one full warp
   a.lc = lc;
   a.C = 1 << lc;
@@ -141,14 +178,15 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
   const size_t smem = sizeof(cplx<T>) * (NY + NYO) + (size_t)a.C * per_col(a.C);
   if (smem > SMEM_CAP) throw CudaError(1, "ypass: shared memory request too large");
   const int threads = a.C * TL;
-  dim3 grid(ceil_div(a.ncols, a.C), nplanes, ngroups);
-  if (grid.x == 0 || nplanes == 0 || ngroups == 0) return;
+  a.nplanes = nplanes;
+  a.ngroups = ngroups;
+  const long nitems = (long)ceil_div(a.ncols, a.C) * nplanes * ngroups;
+  if (nitems == 0) return;
   const int key = NY * 10000 + NYO;
-  hook_before("ypass", double(nplanes) * ngroups * a.ncols * sizeof(cplx<T>) *
-                           (double(a.op == YP_PGRAD ? 1 : a.nin) * NY + double(a.nout) * NYO));
+  void (*kern)(YPArgs<T>) = nullptr;
   switch (key) {
 #define YP_CASE(A, B) \
-  case A * 10000 + B: k_ypass<T, A, B><<<grid, threads, smem, st>>>(a); break;
+  case A * 10000 + B: kern = k_ypass<T, A, B>; break;
     YP_CASE(16, 16) YP_CASE(32, 32) YP_CASE(64, 64) YP_CASE(128, 128) YP_CASE(256, 256) YP_CASE(512, 512)
     YP_CASE(16, 24) YP_CASE(32, 48) YP_CASE(64, 96) YP_CASE(128, 192) YP_CASE(256, 384) YP_CASE(512, 768)
     YP_CASE(24, 16) YP_CASE(48, 32) YP_CASE(96, 64) YP_CASE(192, 128) YP_CASE(384, 256) YP_CASE(768, 512)
@@ -156,6 +194,11 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
     default:
       throw CudaError(1, "ypass: unsupported length pair " + std::to_string(NY) + "->" + std::to_string(NYO));
   }
+  // persistent grid: the CTAs that fit on the device at once
+  const int grid = int(std::min<long>(nitems, (long)resident_ctas((const void*)kern, threads, smem)));
+  hook_before("ypass", double(nplanes) * ngroups * a.ncols * sizeof(cplx<T>) *
+                           (double(a.op == YP_PGRAD ? 1 : a.nin) * NY + double(a.nout) * NYO));
+  kern<<<grid, threads, smem, st>>>(a);
   LES_CHECK_LAUNCH();
   hook_after();
 }
