@@ -694,6 +694,27 @@ struct XIArgs {
   const cplx<T>* tw;  // exp(-2 pi i m / NX), m < NX
 };
 
+// x inverse pass: start the copies of the spectral rows of batch `item`
+// (R rows x nin fields, nk values each) into the shared stage
+template <typename T>
+__device__ __forceinline__ void xi_issue(const XIArgs<T>& a, long item, cplx<T>* stage) {
+  // one warp per row: the row address is formed once, the lanes copy its
+  // nk values
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const int nseq = a.R * a.nin;
+  for (int s = warp; s < nseq; s += nwarps) {
+    const int r = s / a.nin;
+    const int f = s - r * a.nin;
+    const long g = item * a.R + r;
+    const bool valid = g < a.nrows;
+    const cplx<T>* base = a.in[f];
+    const cplx<T>* row =
+        valid ? base + (long)(a.plane0 + int(g / a.rows_pp)) * a.in_pstride + (g % a.rows_pp) * a.ipitch : base;
+    cplx<T>* dst = stage + (long)s * a.nk;
+    for (int m = lane; m < a.nk; m += 32) cp_async<int(sizeof(cplx<T>))>(dst + m, valid ? row + m : base, valid);
+  }
+}
+
 template <typename T, int NX>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIArgs<T> a) {
   constexpr int M = NX / 2;
@@ -705,13 +726,33 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
   constexpr int XS = 2 * SL;         // the same slot viewed as reals
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
-  cplx<T>* buf = tw + NX;
   const int nseq = a.R * a.nin;
   const int npad = seq_pad<M>(nseq);
+  cplx<T>* stage0 = tw + NX;                         // input rows of a work item: [R][nin][nk]
+  cplx<T>* stage1 = stage0 + (long)nseq * a.nk;
+  cplx<T>* buf = stage1 + (long)nseq * a.nk;         // sequence slots
   int* rowl = reinterpret_cast<int*>(buf + (long)npad * SL);  // level of row r (-1: beyond the grid)
   int* rowj = rowl + a.R;
   for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
-  const long g0 = (long)blockIdx.x * a.R;
+  // persistent CTAs over batches of R rows; the spectral rows of the next
+  // batch are copied into the other stage while this one is transformed
+  const long nitems = (a.nrows + a.R - 1) / a.R;
+  if ((long)blockIdx.x < nitems) {
+    xi_issue<T>(a, blockIdx.x, stage0);
+    cp_async_commit();
+  }
+  int stg = 0;
+  for (long item = blockIdx.x; item < nitems; item += gridDim.x) {
+  const long next = item + gridDim.x;
+  const cplx<T>* stage = stg ? stage1 : stage0;
+  if (next < nitems) {
+    xi_issue<T>(a, next, stg ? stage0 : stage1);
+    cp_async_commit();
+    cp_async_wait<1>();
+  } else {
+    cp_async_wait<0>();
+  }
+  const long g0 = item * a.R;
   for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
     const long g = g0 + r;
     rowl[r] = (g < a.nrows) ? a.plane0 + int(g / a.rows_pp) : -1;
@@ -737,7 +778,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
     // c2r split: Z_m = (X_m + conj X_{M-m}) + i W^{-m} (X_m - conj X_{M-m}),
     // imaginary parts of the DC and Nyquist bins ignored
     cplx<T> v[E];
-    const cplx<T>* row = valid ? a.in[f] + (long)l * a.in_pstride + (long)j * a.ipitch : nullptr;
+    const cplx<T>* row = valid ? stage + (long)s * a.nk : nullptr;  // the staged spectral row
 #pragma unroll
     for (int gg = 0; gg < E / RI; ++gg)
 #pragma unroll
@@ -785,7 +826,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
         for (int rr = 0; rr < RO; ++rr) seq[lane_t + TL * gg + rr * (M / RO)] = v[gg * RO + rr];
     }
   }
-  if (direct) return;
+  if (!direct) {
   __syncthreads();
   const T* xs = reinterpret_cast<const T*>(buf);  // x_i of sequence s at xs[s*XS + i]
   // four consecutive points per thread
@@ -891,6 +932,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
       }
     }
     }
+  }
+  }  // the combining ops
+  __syncthreads();
+  stg ^= 1;
   }
 }
 

@@ -10,13 +10,43 @@ namespace les {
 
 thread_local LaunchHook* g_hook = nullptr;
 
+// CTAs of `kern` resident on the current device at once; cached in a fixed
+// table (no heap allocation: the allocation-free entry point launches these
+// kernels too)
+struct ResidentEntry {
+  int dev;
+  const void* kern;
+  int threads;
+  size_t smem;
+  int n;
+};
+static int resident_ctas(const void* kern, int threads, size_t smem) {
+  static std::mutex mu;
+  static ResidentEntry table[256];
+  static int used = 0;
+  int dev = 0;
+  LES_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  for (int i = 0; i < used; ++i) {
+    const ResidentEntry& e = table[i];
+    if (e.dev == dev && e.kern == kern && e.threads == threads && e.smem == smem) return e.n;
+  }
+  int per_sm = 0, sms = 0;
+  LES_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+  LES_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int n = std::max(1, per_sm) * std::max(1, sms);
+  if (used < 256) table[used++] = ResidentEntry{dev, kern, threads, smem, n};
+  return n;
+}
+
+
 namespace {
 constexpr int SMEM_CAP = 200 * 1024;
 
 template <typename T>
-int rows_per_cta(int nseq_per_row, int M) {
-  // keep the in-place sequence buffer near 32 KB so several CTAs fit on an SM
-  const int target = int((32 * 1024) / sizeof(cplx<T>));
+int rows_per_cta(int nseq_per_row, int M, int target_bytes = 32 * 1024) {
+  // keep the in-place sequence buffer near target_bytes so several CTAs fit on an SM
+  const int target = int(target_bytes / sizeof(cplx<T>));
   int R = target / (nseq_per_row * M);
   if (R < 1) R = 1;
   if (R > 32) R = 32;
@@ -93,12 +123,29 @@ template <typename T>
 void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
   const int M = NX / 2;
   if (a.ipitch == 0) a.ipitch = a.nk;
-  a.R = rows_per_cta<T>(a.nin, M);
+  // enough rows that every thread holds a sequence (256 / lanes sequences),
+  // within ~100 KB of slots and input stages (two CTAs per SM)
   const int SL = (M + M / 16 + 1) & ~1;  // slot_len<M>()
-  const size_t smem = sizeof(cplx<T>) * (NX + (size_t)pad_seqs(a.R * a.nin, M) * SL) + 2 * sizeof(int) * a.R;
+  auto smem_for = [&](int R) {
+    return sizeof(cplx<T>) * (NX + 2 * (size_t)R * a.nin * a.nk + (size_t)pad_seqs(R * a.nin, M) * SL) +
+           2 * sizeof(int) * R;
+  };
+  a.R = std::min(32, std::max(rows_per_cta<T>(a.nin, M), ceil_div(256 / lanes(M), a.nin)));
+  while (a.R > 1 && smem_for(a.R) > 100 * 1024) --a.R;
+  const size_t smem = smem_for(a.R);
   if (smem > SMEM_CAP) throw CudaError(1, "xinv: shared memory request too large");
-  const int grid = ceil_div(a.nrows, a.R);
-  if (grid == 0) return;
+  const long nitems = ceil_div(a.nrows, a.R);
+  if (nitems == 0) return;
+  void (*kern)(XIArgs<T>) = nullptr;
+  switch (NX) {
+#define XI_CASE(N) \
+  case N: kern = k_xinv<T, N>; break;
+    LES_LENGTHS(XI_CASE)
+#undef XI_CASE
+    default:
+      throw CudaError(1, "xinv: unsupported transform length " + std::to_string(NX));
+  }
+  const int grid = int(std::min<long>(nitems, (long)resident_ctas((const void*)kern, 256, smem)));
   {
     const size_t osz = (a.out_f32 ? sizeof(float) : sizeof(T));
     int nout = a.nin, rmw = 0;
@@ -107,45 +154,9 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
     else if (a.op == XI_WALL) nout = 7;
     hook_before("xinv", double(a.nrows) * a.nin * a.nk * sizeof(cplx<T>) + double(a.nrows) * NX * (nout + rmw) * osz);
   }
-  switch (NX) {
-#define XI_CASE(N) \
-  case N: k_xinv<T, N><<<grid, 256, smem, st>>>(a); break;
-    LES_LENGTHS(XI_CASE)
-#undef XI_CASE
-    default:
-      throw CudaError(1, "xinv: unsupported transform length " + std::to_string(NX));
-  }
+  kern<<<grid, 256, smem, st>>>(a);
   LES_CHECK_LAUNCH();
   hook_after();
-}
-
-// CTAs of `kern` resident on the current device at once; cached in a fixed
-// table (no heap allocation: the allocation-free entry point launches these
-// kernels too)
-struct ResidentEntry {
-  int dev;
-  const void* kern;
-  int threads;
-  size_t smem;
-  int n;
-};
-static int resident_ctas(const void* kern, int threads, size_t smem) {
-  static std::mutex mu;
-  static ResidentEntry table[256];
-  static int used = 0;
-  int dev = 0;
-  LES_CUDA(cudaGetDevice(&dev));
-  std::lock_guard<std::mutex> lock(mu);
-  for (int i = 0; i < used; ++i) {
-    const ResidentEntry& e = table[i];
-    if (e.dev == dev && e.kern == kern && e.threads == threads && e.smem == smem) return e.n;
-  }
-  int per_sm = 0, sms = 0;
-  LES_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
-  LES_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const int n = std::max(1, per_sm) * std::max(1, sms);
-  if (used < 256) table[used++] = ResidentEntry{dev, kern, threads, smem, n};
-  return n;
 }
 
 template <typename T>
