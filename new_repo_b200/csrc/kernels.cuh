@@ -148,12 +148,13 @@ __global__ void k_sij(const SgsArgs<T> a) {
 
 // nu_t = |S| Cs^2 l^2 and tau_ij (compute_sgs.f90:177-242).
 template <typename T>
+// grid: (plane / blockDim.x, nz + 1); blockIdx.y + 1 is the level
 __global__ void k_sgs_tau(const SgsArgs<T> a) {
   const long pl = a.plane;
-  const long n = (long)(a.nz + 1) * pl;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
-    const long o = pl + q;
-    const int k = int(o / pl);
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (p < pl) {
+    const int k = 1 + blockIdx.y;
+    const long o = (long)k * pl + p;
     T s[6];
     sij_at(a, o, k, s);
     const T nuk = strain_norm(s) * a.cs[o] * T(a.l2[k]);
@@ -425,9 +426,13 @@ __global__ void k_tridiag(const cplx<T>* Hx, const cplx<T>* Hy, const cplx<T>* H
   cplx<double> x = {r.x / bet, r.y / bet};
   xs[col] = x;
   bool bad = false;
+  // Hz(k+1) of one level is Hz(k) of the next; unrolled so that the loads of
+  // several levels are in flight ahead of the recurrence
+  cplx<T> hz = Hz[sp + col];
+#pragma unroll 4
   for (int k = 1; k <= nz; ++k) {
     const long o = k * sp + col;
-    const cplx<T> hx = Hx[o], hy = Hy[o], hz = Hz[o];
+    const cplx<T> hx = Hx[o], hy = Hy[o];
     const cplx<T> hzp = (k < nz) ? Hz[o + sp] : cplx<T>{T(0), T(0)};
     const double sx = kxv * double(hx.x) + kyv * double(hy.x);
     const double sy = kxv * double(hx.y) + kyv * double(hy.y);
@@ -439,6 +444,7 @@ __global__ void k_tridiag(const cplx<T>* Hx, const cplx<T>* Hy, const cplx<T>* H
     gam[o] = g;
     xs[o] = x;
     cprev = a_in;
+    hz = hzp;
   }
   {  // top row: -p(nz) + p(nz+1) = dz * top layer
     const long o = (long)(nz + 1) * sp + col;
@@ -451,6 +457,7 @@ __global__ void k_tridiag(const cplx<T>* Hx, const cplx<T>* Hy, const cplx<T>* H
   }
   if (bad) atomicOr(status, ST_PIVOT);
   phat[(long)(nz + 1) * sp + col] = cplx<T>{T(0), T(0)};
+#pragma unroll 4
   for (int k = nz; k >= 0; --k) {
     const long o = k * sp + col;
     const cplx<double> xk = xs[o];

@@ -1234,7 +1234,7 @@ class Solver final : public SolverBase {
     } else {
       throw CudaError(1, "Invalid SGS model");
     }
-    KL("k_sgs_tau", 17.0 * (g.nz + 1) * g.plane() * sizeof(T), k_sgs_tau<T><<<grid_for(n1), 256, 0, st>>>(a));
+    KL("k_sgs_tau", 17.0 * (g.nz + 1) * g.plane() * sizeof(T), k_sgs_tau<T><<<dim3(unsigned((g.plane() + 255) / 256), unsigned(g.nz + 1)), 256, 0, st>>>(a));
   }
 
   // dynamic-procedure contractions at both test scales (compute_dynamic_mum x2)
