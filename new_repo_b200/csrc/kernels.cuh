@@ -400,9 +400,11 @@ __global__ void k_p_finish(T* p, const double* pmean, long plane, int nz) {
 // pressure: one Thomas solve per (kx, ky) (compute_pressure.f90:256-305,
 // 448-493, matrix of build_matrix :544-619), always in FP64.
 template <typename T>
-__global__ void k_tridiag(const cplx<T>* Hx, const cplx<T>* Hy, const cplx<T>* Hz, const cplx<T>* bot,
-                          const cplx<T>* top, const double* kkx, const double* kky, cplx<T>* phat,
-                          cplx<double>* xs, double* gam, double* pmean, unsigned* status, int lhx, int ny, int nz,
+__global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restrict__ Hy,
+                          const cplx<T>* __restrict__ Hz, const cplx<T>* __restrict__ bot,
+                          const cplx<T>* __restrict__ top, const double* __restrict__ kkx,
+                          const double* __restrict__ kky, cplx<T>* __restrict__ phat, cplx<double>* __restrict__ xs,
+                          double* __restrict__ gam, double* pmean, unsigned* status, int lhx, int ny, int nz,
                           double dz, int drop_mean) {
   const int kx = blockIdx.x * blockDim.x + threadIdx.x;
   const int ky = blockIdx.y;

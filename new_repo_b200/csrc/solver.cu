@@ -789,19 +789,24 @@ class Solver final : public SolverBase {
     }
     use_refs(a, nfld);
     launch_xfwd<T>(g.nx, a, st);
-    auto b = yp(YP_GRAD, 1, 3, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 0);
+    // y pass: F and i ky F; the x inverse forms i kx F from the staged F row
+    auto b = yp(YP_GRADY, 1, 2, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 0);
     for (int q = 0; q < nfld; ++q) {
       b.in[q] = spec[q];
-      b.out[3 * q + 0] = spec[q];
-      b.out[3 * q + 1] = spec[3 + 2 * q];
-      b.out[3 * q + 2] = spec[4 + 2 * q];
+      b.out[2 * q + 0] = spec[q];
+      b.out[2 * q + 1] = spec[3 + q];
     }
     launch_ypass<T>(g.ny, g.ny, b, L, nfld, st);
     auto c = xi(XI_STORE, 3 * nfld, 0, L, g.nx, g.ny, g.lhx);
+    c.nstage = 2 * nfld;
+    c.kxr = kkx;  // row ky = 0 of the wavenumber table (Nyquist column zero)
     for (int q = 0; q < nfld; ++q) {
-      c.in[3 * q + 0] = spec[q];
-      c.in[3 * q + 1] = spec[3 + 2 * q];
-      c.in[3 * q + 2] = spec[4 + 2 * q];
+      c.in[2 * q + 0] = spec[q];
+      c.in[2 * q + 1] = spec[3 + q];
+      c.src[3 * q + 0] = 2 * q;
+      c.src[3 * q + 1] = 2 * q;
+      c.dx[3 * q + 1] = 1;
+      c.src[3 * q + 2] = 2 * q + 1;
       c.out[3 * q + 0] = F[f[q]];
       c.out[3 * q + 1] = F[dx[q]];
       c.out[3 * q + 2] = F[dy[q]];

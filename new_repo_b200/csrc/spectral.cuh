@@ -393,6 +393,7 @@ enum YPOp : int {
   YP_TRUNC = 6,    // 3ny/2 -> ny truncation (ky Nyquist zeroed)
   YP_MASK = 7,     // keep |ky| <= tt (2/3-rule truncation)
   YP_FILTER1 = 8,  // f -> G0 f
+  YP_GRADY = 9,    // f -> f, i ky f                    (Nyquist killed; i kx f in the x inverse)
 };
 
 template <typename T>
@@ -428,6 +429,11 @@ __device__ __forceinline__ cplx<T> yp_op(const YPArgs<T>& a, int q, int kx, int 
       if (ky == NY / 2 || kx == a.nxh) return zero;
       if (q == 0) return F0;
       if (q == 1) return ik_mul(a.kkx[ky * a.lhx + kx], F0);
+      return ik_mul(a.kky[ky * a.lhx + kx], F0);
+    }
+    case YP_GRADY: {
+      if (ky == NY / 2 || kx == a.nxh) return zero;
+      if (q == 0) return F0;
       return ik_mul(a.kky[ky * a.lhx + kx], F0);
     }
     case YP_DIV2: {
@@ -692,6 +698,13 @@ struct XIArgs {
   int out_f32;
   const T* aux[8];
   const cplx<T>* tw;  // exp(-2 pi i m / NX), m < NX
+  // several transforms of one staged row: nstage rows per grid row are
+  // staged (0: nin); transform f reads staged row src[f] and, with dx[f],
+  // multiplies it by i kx (kxr[m], the x wavenumbers, Nyquist zero) first
+  int nstage;
+  int src[MAXIN];
+  int dx[MAXIN];
+  const T* kxr;
 };
 
 // x inverse pass: start the copies of the spectral rows of batch `item`
@@ -701,10 +714,11 @@ __device__ __forceinline__ void xi_issue(const XIArgs<T>& a, long item, cplx<T>*
   // one warp per row: the row address is formed once, the lanes copy its
   // nk values
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  const int nseq = a.R * a.nin;
-  for (int s = warp; s < nseq; s += nwarps) {
-    const int r = s / a.nin;
-    const int f = s - r * a.nin;
+  const int ns = a.nstage ? a.nstage : a.nin;
+  const int nrow = a.R * ns;
+  for (int s = warp; s < nrow; s += nwarps) {
+    const int r = s / ns;
+    const int f = s - r * ns;
     const long g = item * a.R + r;
     const bool valid = g < a.nrows;
     const cplx<T>* base = a.in[f];
@@ -728,12 +742,16 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
   cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
   const int nseq = a.R * a.nin;
   const int npad = seq_pad<M>(nseq);
-  cplx<T>* stage0 = tw + NX;                         // input rows of a work item: [R][nin][nk]
-  cplx<T>* stage1 = stage0 + (long)nseq * a.nk;
-  cplx<T>* buf = stage1 + (long)nseq * a.nk;         // sequence slots
+  const int ns = a.nstage ? a.nstage : a.nin;        // staged rows per grid row
+  cplx<T>* stage0 = tw + NX;                         // input rows of a work item: [R][ns][nk]
+  cplx<T>* stage1 = stage0 + (long)a.R * ns * a.nk;
+  cplx<T>* buf = stage1 + (long)a.R * ns * a.nk;     // sequence slots
   int* rowl = reinterpret_cast<int*>(buf + (long)npad * SL);  // level of row r (-1: beyond the grid)
   int* rowj = rowl + a.R;
+  T* kxs = reinterpret_cast<T*>(rowj + a.R);          // x wavenumbers (nstage > 0)
   for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
+  if (a.nstage)
+    for (int i = threadIdx.x; i < a.nk; i += blockDim.x) kxs[i] = a.kxr[i];
   // persistent CTAs over batches of R rows; the spectral rows of the next
   // batch are copied into the other stage while this one is transformed
   const long nitems = (a.nrows + a.R - 1) / a.R;
@@ -778,7 +796,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
     // c2r split: Z_m = (X_m + conj X_{M-m}) + i W^{-m} (X_m - conj X_{M-m}),
     // imaginary parts of the DC and Nyquist bins ignored
     cplx<T> v[E];
-    const cplx<T>* row = valid ? stage + (long)s * a.nk : nullptr;  // the staged spectral row
+    const int fs = a.nstage ? a.src[f] : f;
+    const bool dxf = a.nstage && a.dx[f];
+    const cplx<T>* row = valid ? stage + (long)(r * ns + fs) * a.nk : nullptr;  // the staged spectral row
 #pragma unroll
     for (int gg = 0; gg < E / RI; ++gg)
 #pragma unroll
@@ -788,6 +808,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
         if (valid) {
           cplx<T> xk = (m < a.nk) ? row[m] : cplx<T>{T(0), T(0)};
           cplx<T> xm = (M - m < a.nk) ? row[M - m] : cplx<T>{T(0), T(0)};
+          if (dxf) {  // d/dx: i kx X (compute_derivatives.f90:94-137)
+            xk = (m < a.nk) ? ik_mul(kxs[m], xk) : xk;
+            xm = (M - m < a.nk) ? ik_mul(kxs[M - m], xm) : xm;
+          }
           if (m == 0) {
             xk.y = T(0);
             xm.y = T(0);

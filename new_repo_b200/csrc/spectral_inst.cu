@@ -126,9 +126,10 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
   // enough rows that every thread holds a sequence (256 / lanes sequences),
   // within ~100 KB of slots and input stages (two CTAs per SM)
   const int SL = (M + M / 16 + 1) & ~1;  // slot_len<M>()
+  const int ns = a.nstage ? a.nstage : a.nin;  // staged rows per grid row
   auto smem_for = [&](int R) {
-    return sizeof(cplx<T>) * (NX + 2 * (size_t)R * a.nin * a.nk + (size_t)pad_seqs(R * a.nin, M) * SL) +
-           2 * sizeof(int) * R;
+    return sizeof(cplx<T>) * (NX + 2 * (size_t)R * ns * a.nk + (size_t)pad_seqs(R * a.nin, M) * SL) +
+           2 * sizeof(int) * R + (a.nstage ? sizeof(T) * (a.nk + 2) : 0);
   };
   a.R = std::min(32, std::max(rows_per_cta<T>(a.nin, M), ceil_div(256 / lanes(M), a.nin)));
   while (a.R > 1 && smem_for(a.R) > 100 * 1024) --a.R;
@@ -152,7 +153,7 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
     if (a.op == XI_DIV) { nout = a.nin; rmw = 2 * a.nin; }
     else if (a.op == XI_LASD) nout = 2;
     else if (a.op == XI_WALL) nout = 7;
-    hook_before("xinv", double(a.nrows) * a.nin * a.nk * sizeof(cplx<T>) + double(a.nrows) * NX * (nout + rmw) * osz);
+    hook_before("xinv", double(a.nrows) * ns * a.nk * sizeof(cplx<T>) + double(a.nrows) * NX * (nout + rmw) * osz);
   }
   kern<<<grid, 256, smem, st>>>(a);
   LES_CHECK_LAUNCH();
