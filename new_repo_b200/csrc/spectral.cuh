@@ -30,6 +30,23 @@ namespace les {
 constexpr int MAXIN = 24;
 constexpr int MAXOUT = 48;
 
+// ---- asynchronous global -> shared copies (cp.async) ----
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  const int n = valid ? BYTES : 0;  // 0: zero fill, nothing read
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gmem), "r"(n) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(d), "l"(gmem), "n"(BYTES), "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // ---------------------------------------------------------------- xfwd ----
 enum XFOp : int {
   XF_SCALE = 0,   // field f = c0 * in[f]
@@ -61,6 +78,10 @@ struct XFArgs {
   int in_f32;
   cplx<T>* out[MAXIN];
   long out_pstride;  // rows_pp * nk
+  // staged kernel (k_xfwd_st): input rows copied per grid row, source q is
+  // field sf[q] at level offset sdl[q]; scond[q]: only on the wall row (l = 1)
+  int nsrc;
+  int sf[16], sdl[16], scond[16];
   const cplx<T>* tw; // exp(-2 pi i m / NX), m < NX
 };
 
@@ -382,6 +403,189 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd(const XFAr
   }
 }
 
+// Values of the staged ops at level l, columns i..i+3 of row r, from the
+// staged input rows (rows[q] = source q of this grid row).
+template <typename T, typename S>
+__device__ __forceinline__ void xf_load_st(const XFArgs<T>& a, int l, const S* const* rows, int i, T* v, int vs) {
+  using V = V4<T>;
+  auto ld = [&](int q) { return vld<V>(rows[q], (long)i); };
+  switch (a.op) {
+    case XF_SCALE:
+      for (int f = 0; f < a.nf; ++f) vst(v + f * vs, T(a.c0) * ld(f));
+      break;
+    case XF_PRESS:  // compute_pressure.f90:138-140
+      for (int f = 0; f < a.nf; ++f) vst(v + f * vs, T(a.c0) * (ld(f) / T(a.c1)));
+      break;
+    case XF_CONV_IN: {
+      // compute_convective_padd.f90:133-165; sources 0..8 = the inputs at
+      // level l, 9 / 10 = dwdy / dwdx at l + 1 (wall row only)
+      const T c = T(a.c0);
+      vst(v + 0 * vs, -c * ld(0));
+      vst(v + 1 * vs, -c * ld(1));
+      vst(v + 2 * vs, -c * ld(2));
+      if (a.wall && l == 0) {
+        vst(v + 3 * vs, vsplat<V>(T(0)));
+        vst(v + 4 * vs, vsplat<V>(T(0)));
+      } else if (a.wall && l == 1) {
+        vst(v + 3 * vs, c * (T(0.5) * (ld(3) + ld(9)) - ld(4)));
+        vst(v + 4 * vs, c * (ld(5) - T(0.5) * (ld(6) + ld(10))));
+      } else {
+        vst(v + 3 * vs, c * (ld(3) - ld(4)));
+        vst(v + 4 * vs, c * (ld(5) - ld(6)));
+      }
+      vst(v + 5 * vs, c * (ld(7) - ld(8)));
+      break;
+    }
+    default:
+      break;
+  }
+}
+
+// start the copies of the staged input rows of batch `item` (one warp per
+// row, 16-byte pieces)
+template <typename T, typename S, int NX>
+__device__ __forceinline__ void xf_issue(const XFArgs<T>& a, long item, S* stage) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  constexpr int PIECES = NX * int(sizeof(S)) / 16;
+  const int nrow = a.R * a.nsrc;
+  for (int s = warp; s < nrow; s += nwarps) {
+    const int r = s / a.nsrc;
+    const int q = s - r * a.nsrc;
+    const long g = item * a.R + r;
+    const int l = a.plane0 + int(g / a.rows_pp);
+    const bool valid = g < a.nrows && (!a.scond[q] || (a.wall && l == 1));
+    const S* base = reinterpret_cast<const S*>(std::is_same<S, T>::value ? (const void*)a.in[a.sf[q]]
+                                                                          : (const void*)a.inf[a.sf[q]]);
+    const S* row = valid ? base + (long)(l + a.sdl[q]) * a.in_pstride + (g % a.rows_pp) * a.in_rstride : base;
+    S* dst = stage + (long)s * NX;
+    for (int k = lane; k < PIECES; k += 32)
+      cp_async<16>(reinterpret_cast<unsigned char*>(dst) + 16 * k,
+                   valid ? reinterpret_cast<const unsigned char*>(row) + 16 * k
+                         : reinterpret_cast<const unsigned char*>(base),
+                   valid);
+  }
+}
+
+// The x forward pass for the ops whose inputs are whole rows (scale,
+// pressure input, convective inputs): persistent CTAs over batches of R rows,
+// the input rows of the next batch copied into the other shared stage with
+// cp.async while the current batch is transformed.  S: input element type.
+template <typename T, int NX, typename S>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd_st(const XFArgs<T> a) {
+  constexpr int M = NX / 2;
+  constexpr int TL = Geo<M>::T;
+  constexpr int E = Geo<M>::E;
+  constexpr int RI = Layout<M, false>::in;
+  constexpr int RO = Layout<M, false>::out;
+  constexpr int SL = slot_len<M>();
+  constexpr int XS = 2 * SL;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  const int nseq = a.R * a.nf;
+  const int npad = seq_pad<M>(nseq);
+  S* stage0 = reinterpret_cast<S*>(tw + NX);
+  S* stage1 = stage0 + (long)a.R * a.nsrc * NX;
+  cplx<T>* buf = reinterpret_cast<cplx<T>*>(stage1 + (long)a.R * a.nsrc * NX);
+  T* refs = reinterpret_cast<T*>(buf + (long)npad * SL);
+  int* rowl = reinterpret_cast<int*>(refs + a.R * a.nf);
+  int* rowj = rowl + a.R;
+  for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
+  const long nitems = (a.nrows + a.R - 1) / a.R;
+  if ((long)blockIdx.x < nitems) {
+    xf_issue<T, S, NX>(a, blockIdx.x, stage0);
+    cp_async_commit();
+  }
+  int stg = 0;
+  for (long item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const long next = item + gridDim.x;
+    const S* stage = stg ? stage1 : stage0;
+    if (next < nitems) {
+      xf_issue<T, S, NX>(a, next, stg ? stage0 : stage1);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    const long g0 = item * a.R;
+    for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
+      const long g = g0 + r;
+      rowl[r] = (g < a.nrows) ? a.plane0 + int(g / a.rows_pp) : -1;
+      rowj[r] = (g < a.nrows) ? int(g % a.rows_pp) : 0;
+    }
+    __syncthreads();
+    if (a.use_ref) {  // per-level references: the (0,0) value of each field (from global)
+      for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
+        const int l = rowl[r];
+        if (l < 0) continue;
+        xf_load<T, T>(a, l, 0, 0, refs + r * a.nf, 1);
+        for (int f = 0; f < a.nf; ++f) {
+          if (!a.refout[f]) refs[r * a.nf + f] = T(0);
+          else if (rowj[r] == 0) a.refout[f][l] = T(double(refs[r * a.nf + f]) * a.ref_mul);
+        }
+      }
+      __syncthreads();
+    }
+    T* xr = reinterpret_cast<T*>(buf);
+    for (int idx = threadIdx.x; idx < a.R * (NX / 4); idx += blockDim.x) {
+      const int r = idx / (NX / 4);
+      const int i = 4 * (idx - r * (NX / 4));
+      T* dst = xr + (long)(r * a.nf) * XS + i;
+      const int l = rowl[r];
+      if (l >= 0) {
+        const S* rows[16];
+        for (int q = 0; q < a.nsrc; ++q) rows[q] = stage + (long)(r * a.nsrc + q) * NX;
+        xf_load_st<T, S>(a, l, rows, i, dst, XS);
+        if (a.use_ref)
+          for (int f = 0; f < a.nf; ++f) {
+            const T rf = refs[r * a.nf + f];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) dst[f * XS + q] -= rf;
+          }
+      } else {
+        for (int f = 0; f < a.nf; ++f) vst(dst + f * XS, vsplat<V4<T>>(T(0)));
+      }
+    }
+    for (int idx = nseq * SL + threadIdx.x; idx < npad * SL; idx += blockDim.x) buf[idx] = cplx<T>{T(0), T(0)};
+    __syncthreads();
+    const int lane_t = threadIdx.x % TL;
+    for (int base = 0; base < npad; base += blockDim.x / TL) {
+      const int s = base + threadIdx.x / TL;
+      if (base + (threadIdx.x / 32) * (32 / TL) >= npad) break;
+      cplx<T>* seq = buf + (long)s * SL;
+      cplx<T> v[E];
+#pragma unroll
+      for (int g = 0; g < E / RI; ++g)
+#pragma unroll
+        for (int r = 0; r < RI; ++r) v[g * RI + r] = seq[lane_t + TL * g + r * (M / RI)];
+      reg_fft<T, M, false, 2>(v, seq, lane_t, tw);
+      __syncwarp();
+#pragma unroll
+      for (int g = 0; g < E / RO; ++g)
+#pragma unroll
+        for (int r = 0; r < RO; ++r) seq[lane_t + TL * g + r * (M / RO)] = v[g * RO + r];
+      __syncwarp();
+      if (s < nseq) {
+        const int r = s / a.nf;
+        const int f = s - r * a.nf;
+        const int l = rowl[r];
+        if (l >= 0) {
+          const int j = rowj[r];
+          cplx<T>* orow = a.out[f] + (long)l * a.out_pstride + (long)j * a.opitch;
+          for (int k = lane_t; k < a.nk; k += TL) {
+            const cplx<T> zk = seq[k == M ? 0 : k];
+            const cplx<T> zm = seq[(M - k) % M];
+            const cplx<T> e = {T(0.5) * (zk.x + zm.x), T(0.5) * (zk.y - zm.y)};
+            const cplx<T> o = {T(0.5) * (zk.y + zm.y), T(-0.5) * (zk.x - zm.x)};
+            orow[k] = c_add(e, c_mul(o, tw[k]));
+          }
+        }
+      }
+    }
+    __syncthreads();
+    stg ^= 1;
+  }
+}
+
 // --------------------------------------------------------------- ypass ----
 enum YPOp : int {
   YP_GRAD = 0,     // f -> f, i kx f, i ky f           (Nyquist killed)
@@ -457,23 +661,6 @@ __device__ __forceinline__ cplx<T> yp_op(const YPArgs<T>& a, int q, int kx, int 
     default:
       return F0;  // YP_PAD / YP_TRUNC: position remap only
   }
-}
-
-// ---- asynchronous global -> shared copies (cp.async) ----
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void* smem, const void* gmem, bool valid) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  const int n = valid ? BYTES : 0;  // 0: zero fill, nothing read
-  if constexpr (BYTES == 16)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gmem), "r"(n) : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(d), "l"(gmem), "n"(BYTES), "r"(n)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // y pass: start the copies of work item `item` (C columns x NY rows of every

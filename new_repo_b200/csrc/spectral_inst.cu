@@ -91,10 +91,76 @@ bool supported_length(int n) {
 
 #define LES_LENGTHS(X) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768)
 
+// the staged x forward pass (ops whose inputs are whole rows)
+template <typename T, typename S>
+static void launch_xfwd_st(int NX, XFArgs<T>& a, cudaStream_t st) {
+  const int M = NX / 2;
+  a.nsrc = 0;
+  if (a.op == XF_CONV_IN) {
+    for (int f = 0; f < 9; ++f) {
+      a.sf[a.nsrc] = f;
+      a.sdl[a.nsrc] = 0;
+      a.scond[a.nsrc++] = 0;
+    }
+    for (int f : {3, 6}) {  // dwdy, dwdx one level up, read on the wall row only
+      a.sf[a.nsrc] = f;
+      a.sdl[a.nsrc] = 1;
+      a.scond[a.nsrc++] = 1;
+    }
+  } else {
+    for (int f = 0; f < a.nf; ++f) {
+      a.sf[a.nsrc] = f;
+      a.sdl[a.nsrc] = 0;
+      a.scond[a.nsrc++] = 0;
+    }
+  }
+  const int SL = (M + M / 16 + 1) & ~1;  // slot_len<M>()
+  auto smem_for = [&](int R) {
+    return sizeof(cplx<T>) * (NX + (size_t)pad_seqs(R * a.nf, M) * SL) + 2 * sizeof(S) * (size_t)R * a.nsrc * NX +
+           sizeof(T) * R * a.nf + 2 * sizeof(int) * R + 16;
+  };
+  a.R = std::min(32, std::max(rows_per_cta<T>(a.nf, M), ceil_div(256 / lanes(M), a.nf)));
+  while (a.R > 1 && smem_for(a.R) > 100 * 1024) --a.R;
+  const size_t smem = smem_for(a.R);
+  if (smem > SMEM_CAP) throw CudaError(1, "xfwd: shared memory request too large");
+  const long nitems = ceil_div(a.nrows, a.R);
+  if (nitems == 0) return;
+  void (*kern)(XFArgs<T>) = nullptr;
+  switch (NX) {
+#define XS_CASE(N) \
+  case N: kern = k_xfwd_st<T, N, S>; break;
+    LES_LENGTHS(XS_CASE)
+#undef XS_CASE
+    default:
+      throw CudaError(1, "xfwd: unsupported transform length " + std::to_string(NX));
+  }
+  const int grid = int(std::min<long>(nitems, (long)resident_ctas((const void*)kern, 256, smem)));
+  kern<<<grid, 256, smem, st>>>(a);
+  LES_CHECK_LAUNCH();
+}
+
 template <typename T>
 void launch_xfwd(int NX, XFArgs<T> a, cudaStream_t st) {
   const int M = NX / 2;
   if (a.opitch == 0) a.opitch = a.nk;
+  // the staged kernel pays for its two input stages with occupancy: it wins
+  // for the pressure inputs and for scalings of few fields (measured at 256^3)
+  const bool staged = a.op == XF_PRESS || (a.op == XF_SCALE && a.nf <= 3);
+  if (staged) {
+    a.in_rstride = NX;
+    static const int nin_of_op[] = {0, 9, 6, 10, 0};
+    const int nin = (a.op == XF_SCALE || a.op == XF_PRESS) ? a.nf : nin_of_op[a.op];
+    const size_t isz = (a.in_f32 ? sizeof(float) : sizeof(T));
+    hook_before("xfwd", double(a.nrows) * NX * nin * isz + double(a.nrows) * a.nf * a.nk * sizeof(cplx<T>));
+    if (a.in_f32) {
+      if constexpr (std::is_same<T, double>::value) launch_xfwd_st<T, float>(NX, a, st);
+      else throw CudaError(1, "xfwd: FP32 inputs are for FP64 transforms");
+    } else {
+      launch_xfwd_st<T, T>(NX, a, st);
+    }
+    hook_after();
+    return;
+  }
   a.R = rows_per_cta<T>(a.nf, M);
   a.in_rstride = NX;
   const int SL = (M + M / 16 + 1) & ~1;  // slot_len<M>()
@@ -219,6 +285,9 @@ template <typename T>
 static void set_attrs() {
 #define XA(N)                                                                                       \
   LES_CUDA(cudaFuncSetAttribute(k_xfwd<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_CAP)); \
+  LES_CUDA(cudaFuncSetAttribute(k_xfwd_st<T, N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_CAP)); \
+  if constexpr (std::is_same<T, double>::value)                                                       \
+    LES_CUDA(cudaFuncSetAttribute(k_xfwd_st<T, N, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_CAP)); \
   LES_CUDA(cudaFuncSetAttribute(k_xinv<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_CAP));
   LES_LENGTHS(XA)
 #undef XA
