@@ -399,20 +399,24 @@ __global__ void k_p_finish(T* p, const double* pmean, long plane, int nz) {
 // ---------------------------------------------------------------------------
 // pressure: one Thomas solve per (kx, ky) (compute_pressure.f90:256-305,
 // 448-493, matrix of build_matrix :544-619), always in FP64.
-template <typename T>
+// O: type of the pressure spectrum written (FP32 in mixed precision, whose
+// inverse transforms run in FP32); its rows are opitch values apart
+template <typename T, typename O = T>
 __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restrict__ Hy,
                           const cplx<T>* __restrict__ Hz, const cplx<T>* __restrict__ bot,
                           const cplx<T>* __restrict__ top, const double* __restrict__ kkx,
-                          const double* __restrict__ kky, cplx<T>* __restrict__ phat, cplx<double>* __restrict__ xs,
+                          const double* __restrict__ kky, cplx<O>* __restrict__ phat, cplx<double>* __restrict__ xs,
                           double* __restrict__ gam, double* pmean, unsigned* status, int lhx, int ny, int nz,
-                          double dz, int drop_mean) {
+                          double dz, int drop_mean, int opitch) {
   const int kx = blockIdx.x * blockDim.x + threadIdx.x;
   const int ky = blockIdx.y;
   if (kx >= lhx) return;
   const long col = (long)ky * lhx + kx;
   const long sp = (long)ny * lhx;
+  const long ocol = (long)ky * opitch + kx;
+  const long osp = (long)ny * opitch;
   if (kx == lhx - 1 || ky == ny / 2) {
-    for (int l = 0; l <= nz + 1; ++l) phat[l * sp + col] = cplx<T>{T(0), T(0)};
+    for (int l = 0; l <= nz + 1; ++l) phat[l * osp + ocol] = cplx<O>{O(0), O(0)};
     return;
   }
   const bool mean = (kx == 0 && ky == 0);
@@ -458,7 +462,7 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
     gam[o] = g;
   }
   if (bad) atomicOr(status, ST_PIVOT);
-  phat[(long)(nz + 1) * sp + col] = cplx<T>{T(0), T(0)};
+  phat[(long)(nz + 1) * osp + ocol] = cplx<O>{O(0), O(0)};
 #pragma unroll 4
   for (int k = nz; k >= 0; --k) {
     const long o = k * sp + col;
@@ -466,7 +470,7 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
     const double g = gam[o + sp];
     x = {xk.x - g * x.x, xk.y - g * x.y};
     if (mean && pmean) pmean[k] = x.x;
-    phat[o] = (mean && drop_mean) ? cplx<T>{T(0), T(0)} : cplx<T>{T(x.x), T(x.y)};
+    phat[k * osp + ocol] = (mean && drop_mean) ? cplx<O>{O(0), O(0)} : cplx<O>{O(x.x), O(x.y)};
   }
   if (mean && pmean) pmean[nz + 1] = 0.0;
 }

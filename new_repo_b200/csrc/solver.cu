@@ -1123,8 +1123,40 @@ class Solver final : public SolverBase {
     // tridiagonal solve per (kx, ky) -> p^ in sp[5], levels 0..nz+1; in
     // mixed precision the mean mode is kept apart in FP64 (pmean)
     dim3 tg(ceil_div(g.lhx, 64), g.ny);
+    if constexpr (std::is_same<T, float>::value) {
+      // mixed precision: p^ leaves the FP64 solve as FP32 (its mean mode is
+      // kept apart in FP64); the inverse transforms of p run in FP32 -- only
+      // the forward right-hand side needs FP64, where div u* cancels
+      KL("k_tridiag", 96.0 * double(g.L) * g.ny * g.lhx,
+         k_tridiag<S, T><<<tg, 64, 0, st>>>(sp[2], sp[3], sp[4], bot, top, kkxd, kkyd, spec[0], xs, gam, pmean, dstatus,
+                                            g.lhx, g.ny, nz, dz(), 1, pitch(g.lhx)));
+      auto e = yp(YP_PGRAD, 1, 3, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 0);
+      e.in[0] = spec[0];
+      e.out[0] = spec[1];
+      e.out[1] = spec[2];
+      e.out[2] = spec[0];
+      launch_ypass<T>(g.ny, g.ny, e, g.L, 1, st);
+      auto h = xi(XI_STORE, 3, 0, g.L, g.nx, g.ny, g.lhx);
+      h.in[0] = spec[1];
+      h.in[1] = spec[2];
+      h.in[2] = spec[0];
+      h.out[0] = F[LES_DPDX];
+      h.out[1] = F[LES_DPDY];
+      h.out[2] = F[LES_P];
+      h.lo[0] = 1;
+      h.hi[0] = nz;
+      h.lo[1] = 1;
+      h.hi[1] = nz;
+      h.lo[2] = 0;
+      h.hi[2] = nz + 1;
+      launch_xinv<T>(g.nx, h, st);
+      dpdz_only();
+      KL("k_p_finish", 2.0 * g.field() * sizeof(T),
+         k_p_finish<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_P], pmean, g.plane(), nz));
+      return;
+    }
     KL("k_tridiag", 112.0 * double(g.L) * g.ny * g.lhx, k_tridiag<S><<<tg, 64, 0, st>>>(sp[2], sp[3], sp[4], bot, top, kkxd, kkyd, sp[5], xs, gam,
-                                   mixed() ? pmean : nullptr, dstatus, g.lhx, g.ny, nz, dz(), mixed() ? 1 : 0));
+                                   mixed() ? pmean : nullptr, dstatus, g.lhx, g.ny, nz, dz(), mixed() ? 1 : 0, g.lhx));
     // compute_press_grad: i kx p^, i ky p^, p^ -> dpdx, dpdy (1..nz), p (0..nz+1)
     auto e = yp_s<S>(YP_PGRAD, 1, 3, 0);
     e.in[0] = sp[5];
