@@ -432,25 +432,53 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
   cplx<double> x = {r.x / bet, r.y / bet};
   xs[col] = x;
   bool bad = false;
-  // Hz(k+1) of one level is Hz(k) of the next; unrolled so that the loads of
-  // several levels are in flight ahead of the recurrence
+  // The levels are loaded in batches of TB: the loads of the next batch are
+  // issued before the recurrence runs through the current one, so that a
+  // thread keeps 2 TB levels of reads in flight (the grid holds only one
+  // thread per (kx, ky), too few warps to hide DRAM latency otherwise).
+  // Hz(k+1) of one level is Hz(k) of the next.
+  constexpr int TB = 4;
   cplx<T> hz = Hz[sp + col];
-#pragma unroll 4
-  for (int k = 1; k <= nz; ++k) {
-    const long o = k * sp + col;
-    const cplx<T> hx = Hx[o], hy = Hy[o];
-    const cplx<T> hzp = (k < nz) ? Hz[o + sp] : cplx<T>{T(0), T(0)};
-    const double sx = kxv * double(hx.x) + kyv * double(hy.x);
-    const double sy = kxv * double(hx.y) + kyv * double(hy.y);
-    r = {-sy + (double(hzp.x) - double(hz.x)) / dz, sx + (double(hzp.y) - double(hz.y)) / dz};
-    const double g = cprev / bet;
-    bet = b_in - a_in * g;
-    bad |= (bet == 0.0);
-    x = {(r.x - a_in * x.x) / bet, (r.y - a_in * x.y) / bet};
-    gam[o] = g;
-    xs[o] = x;
-    cprev = a_in;
-    hz = hzp;
+  cplx<T> cx[TB], cy[TB], cz[TB];
+  auto load_fwd = [&](int k0, cplx<T>* ax, cplx<T>* ay, cplx<T>* az) {
+#pragma unroll
+    for (int j = 0; j < TB; ++j) {
+      const int k = k0 + j;
+      const long o = (long)k * sp + col;
+      ax[j] = (k <= nz) ? Hx[o] : cplx<T>{T(0), T(0)};
+      ay[j] = (k <= nz) ? Hy[o] : cplx<T>{T(0), T(0)};
+      az[j] = (k < nz) ? Hz[o + sp] : cplx<T>{T(0), T(0)};
+    }
+  };
+  load_fwd(1, cx, cy, cz);
+  for (int k0 = 1; k0 <= nz; k0 += TB) {
+    cplx<T> nx_[TB], ny_[TB], nz_[TB];
+    load_fwd(k0 + TB, nx_, ny_, nz_);
+#pragma unroll
+    for (int j = 0; j < TB; ++j) {
+      const int k = k0 + j;
+      if (k <= nz) {
+        const long o = (long)k * sp + col;
+        const cplx<T> hx = cx[j], hy = cy[j], hzp = cz[j];
+        const double sx = kxv * double(hx.x) + kyv * double(hy.x);
+        const double sy = kxv * double(hx.y) + kyv * double(hy.y);
+        r = {-sy + (double(hzp.x) - double(hz.x)) / dz, sx + (double(hzp.y) - double(hz.y)) / dz};
+        const double g = cprev / bet;
+        bet = b_in - a_in * g;
+        bad |= (bet == 0.0);
+        x = {(r.x - a_in * x.x) / bet, (r.y - a_in * x.y) / bet};
+        gam[o] = g;
+        xs[o] = x;
+        cprev = a_in;
+        hz = hzp;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < TB; ++j) {
+      cx[j] = nx_[j];
+      cy[j] = ny_[j];
+      cz[j] = nz_[j];
+    }
   }
   {  // top row: -p(nz) + p(nz+1) = dz * top layer
     const long o = (long)(nz + 1) * sp + col;
@@ -463,14 +491,37 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
   }
   if (bad) atomicOr(status, ST_PIVOT);
   phat[(long)(nz + 1) * osp + ocol] = cplx<O>{O(0), O(0)};
-#pragma unroll 4
-  for (int k = nz; k >= 0; --k) {
-    const long o = k * sp + col;
-    const cplx<double> xk = xs[o];
-    const double g = gam[o + sp];
-    x = {xk.x - g * x.x, xk.y - g * x.y};
-    if (mean && pmean) pmean[k] = x.x;
-    phat[k * osp + ocol] = (mean && drop_mean) ? cplx<O>{O(0), O(0)} : cplx<O>{O(x.x), O(x.y)};
+  // backward sweep, levels nz..0, batched the same way
+  cplx<double> bxs[TB];
+  double bg[TB];
+  auto load_bwd = [&](int k0, cplx<double>* axs, double* ag) {
+#pragma unroll
+    for (int j = 0; j < TB; ++j) {
+      const int k = k0 - j;
+      const long o = (long)k * sp + col;
+      axs[j] = (k >= 0) ? xs[o] : cplx<double>{0.0, 0.0};
+      ag[j] = (k >= 0) ? gam[o + sp] : 0.0;
+    }
+  };
+  load_bwd(nz, bxs, bg);
+  for (int k0 = nz; k0 >= 0; k0 -= TB) {
+    cplx<double> nxs[TB];
+    double ng[TB];
+    load_bwd(k0 - TB, nxs, ng);
+#pragma unroll
+    for (int j = 0; j < TB; ++j) {
+      const int k = k0 - j;
+      if (k >= 0) {
+        x = {bxs[j].x - bg[j] * x.x, bxs[j].y - bg[j] * x.y};
+        if (mean && pmean) pmean[k] = x.x;
+        phat[k * osp + ocol] = (mean && drop_mean) ? cplx<O>{O(0), O(0)} : cplx<O>{O(x.x), O(x.y)};
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < TB; ++j) {
+      bxs[j] = nxs[j];
+      bg[j] = ng[j];
+    }
   }
   if (mean && pmean) pmean[nz + 1] = 0.0;
 }
