@@ -195,6 +195,51 @@ int les_diagnostics_async(les_state* s, double* pinned_out4);
 int les_checkpoint_write(les_state* s, const char* path);
 int les_checkpoint_read(les_state* s, const char* path, int lagran_init);
 
+/* ---- post-step statistics (one rank) ------------------------------------
+ * Running sums of IO_statistics.f90.  les_stat_init replaces io_stat_init
+ * (:40-250): it allocates (or zeroes) 26 FP64 volumes of nx*ny*nz and one
+ * u* plane.  les_stat_averages replaces io_stat_averages(jt, jt_total)
+ * (:265-291 with io_2D_stat_averages :300-354 and io_3D_stat_averages
+ * :363-518): it adds the current state to the sums and, when
+ * mod(jt_total, running_period) == 0 and jt_total > start_stats, writes
+ * <out_path>RAV_<jt_total:09>_info.txt ("%6d%6d%6d%10d": nx, ny, nz,
+ * iterations), _2D.dat (the u* sum, nx*ny FP64) and _3D.dat (the 26 sums in
+ * the order u v w p u2 v2 w2 u3 v3 w3 u4 v4 w4 uv uw vw txx tyy tzz txy txz
+ * tyz dudz dvdz nu_t cs, nx*ny*nz FP64 each, x fastest), then restarts the
+ * sums.  out_path is prefixed as is (the reference's trim(out_path)).  The
+ * caller applies the driver's condition stat_flag .and. jt_total >
+ * start_stats (LES_engine.f90:368-370).  les_stat_sums copies sum index
+ * 0..25 (nx*ny*nz values) or 26 (the u* plane) to the host.
+ * les_stat_spectra replaces io_stat_spectra (:566-620): inside the four
+ * fixed jt_total windows and every 10th jt it writes
+ * <out_path>SP_<jt_total:09>.dat with u, v, w on levels 1..nz.
+ * Errors: 1 not initialised / invalid period, 22 file open or write. */
+int les_stat_init(les_state* s);
+int les_stat_averages(les_state* s, int jt, int jt_total, int start_stats, int running_period, const char* out_path);
+int les_stat_sums(les_state* s, int index, double* out);
+int les_stat_iterations(les_state* s, int* out);
+int les_stat_spectra(les_state* s, int jt, int jt_total, const char* out_path);
+
+/* Plane-averaged TKE budget of tke_budget1D.f90.  les_tke_init replaces
+ * tke_budget_init (:61-160): it creates <out_path>ta1_profiles/ (an existing
+ * folder is fine) and zeroes 61 FP64 profiles of nz levels; the record
+ * counter starts at 1.  les_tke_budget replaces compute_tke_budget(jt)
+ * (:209-390): it adds the plane averages of the 61 quantities (names and
+ * order of its avg_var calls: u v w dudx dudy dudz dvdx dvdy dvdz dwdx dwdy
+ * dwdz uu vv ww uv uw vw txx tyy tzz txy txz tyz cs uuw vvw www uww wtzz
+ * utxz vtyz dxx dyy dzz dxy dxz dyz dudx2 dudy2 dudz2 dvdx2 dvdy2 dvdz2 dwdx2
+ * dwdy2 dwdz2 dudxdwdx dudydwdy dudzdwdz p dpdx dpdy dpdz pw pu pdudx pdvdy
+ * pdwdz pdwdx pdudz) and, when mod(jt, tke_period) == 0, writes record ii
+ * (nz FP64 values at byte offset (ii-1)*8*nz: direct access with recl = 2*nz
+ * in 4-byte units) of ta1_profiles/<name>.out holding profile / tke_period,
+ * then restarts the profiles and advances ii.  The caller applies
+ * tke_flag .and. jt_total > start_tke (LES_engine.f90:377-380).
+ * les_tke_sums copies the 61 x nz profiles (name-major) and the next record
+ * number.  Errors: 1 not initialised / invalid period, 22 file open or write. */
+int les_tke_init(les_state* s, const char* out_path);
+int les_tke_budget(les_state* s, int jt, int tke_period);
+int les_tke_sums(les_state* s, double* out, int* record);
+
 /* ---- learned SGS closure (no reference counterpart) ---------------------
  * Cs^2 = Cs^2_prev * exp(net(features)) from an 8 -> 64 -> 64 -> 1 GELU network with
  * BF16 weights and FP32 accumulation (tcgen05 tensor cores), evaluated at

@@ -93,6 +93,14 @@ PROTOTYPES = {
     "les_diagnostics_async": [_P, C.c_void_p],
     "les_checkpoint_write": [_P, C.c_char_p],
     "les_checkpoint_read": [_P, C.c_char_p, _I],
+    "les_stat_init": [_P],
+    "les_stat_averages": [_P, _I, _I, _I, _I, C.c_char_p],
+    "les_stat_sums": [_P, _I, _D],
+    "les_stat_iterations": [_P, C.POINTER(_I)],
+    "les_stat_spectra": [_P, _I, _I, C.c_char_p],
+    "les_tke_init": [_P, C.c_char_p],
+    "les_tke_budget": [_P, _I, _I],
+    "les_tke_sums": [_P, _D, C.POINTER(_I)],
     "les_set_sgs_model": [_P, _I],
     "les_mlp_init": [_P, C.c_uint],
     "les_mlp_set_params": [_P, _F, _I],
@@ -112,6 +120,18 @@ PROTOTYPES = {
 }
 
 _lib = None
+
+
+# running sums of IO_statistics.f90:447-488, in the order of the RAV_*_3D.dat file
+STAT_NAMES = ("u", "v", "w", "p", "u2", "v2", "w2", "u3", "v3", "w3", "u4", "v4", "w4", "uv", "uw", "vw",
+              "txx", "tyy", "tzz", "txy", "txz", "tyz", "dudz", "dvdz", "nut", "cs")
+# TKE budget profiles of tke_budget1D.f90:218-383, in the order of its avg_var calls
+TKE_NAMES = ("u", "v", "w", "dudx", "dudy", "dudz", "dvdx", "dvdy", "dvdz", "dwdx", "dwdy", "dwdz",
+             "uu", "vv", "ww", "uv", "uw", "vw", "txx", "tyy", "tzz", "txy", "txz", "tyz", "cs",
+             "uuw", "vvw", "www", "uww", "wtzz", "utxz", "vtyz", "dxx", "dyy", "dzz", "dxy", "dxz", "dyz",
+             "dudx2", "dudy2", "dudz2", "dvdx2", "dvdy2", "dvdz2", "dwdx2", "dwdy2", "dwdz2",
+             "dudxdwdx", "dudydwdy", "dudzdwdz",
+             "p", "dpdx", "dpdy", "dpdz", "pw", "pu", "pdudx", "pdvdy", "pdwdz", "pdwdx", "pdudz")
 
 
 def load() -> C.CDLL:

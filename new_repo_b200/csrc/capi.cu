@@ -30,6 +30,10 @@ int bad_state() {
   g_last_error = "null les_state";
   return LES_ERR_INVALID;
 }
+int bad_arg(const char* what) {
+  g_last_error = std::string("null argument: ") + what;
+  return LES_ERR_INVALID;
+}
 }  // namespace
 
 #define STATE_OR_FAIL(s)            \
@@ -343,6 +347,45 @@ int les_checkpoint_read(les_state* s, const char* path, int lagran_init) {
   STATE_OR_FAIL(s);
   if (!path) return bad_state();
   return guard([&] { s->s->checkpoint_read(path, lagran_init); });
+}
+
+int les_stat_init(les_state* s) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->stat_init(); });
+}
+int les_stat_averages(les_state* s, int jt, int jt_total, int start_stats, int running_period, const char* out_path) {
+  STATE_OR_FAIL(s);
+  if (!out_path) return bad_arg("out_path");
+  return guard([&] { s->s->stat_averages(jt, jt_total, start_stats, running_period, out_path); });
+}
+int les_stat_sums(les_state* s, int index, double* out) {
+  STATE_OR_FAIL(s);
+  if (!out) return bad_arg("out");
+  return guard([&] { s->s->stat_sums(index, out); });
+}
+int les_stat_iterations(les_state* s, int* out) {
+  STATE_OR_FAIL(s);
+  if (!out) return bad_arg("out");
+  return guard([&] { *out = s->s->stat_iteration_count(); });
+}
+int les_stat_spectra(les_state* s, int jt, int jt_total, const char* out_path) {
+  STATE_OR_FAIL(s);
+  if (!out_path) return bad_arg("out_path");
+  return guard([&] { s->s->stat_spectra(jt, jt_total, out_path); });
+}
+int les_tke_init(les_state* s, const char* out_path) {
+  STATE_OR_FAIL(s);
+  if (!out_path) return bad_arg("out_path");
+  return guard([&] { s->s->tke_init(out_path); });
+}
+int les_tke_budget(les_state* s, int jt, int tke_period) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->tke_budget(jt, tke_period); });
+}
+int les_tke_sums(les_state* s, double* out, int* record) {
+  STATE_OR_FAIL(s);
+  if (!out || !record) return bad_arg("out/record");
+  return guard([&] { s->s->tke_sums(out, record); });
 }
 
 int les_timers(les_state* s, double out[5]) {

@@ -3,12 +3,15 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <string>
+#include <sys/stat.h>
 #include <map>
 #include <memory>
 #include <vector>
 #include <type_traits>
 
 #include "kernels.cuh"
+#include "stats.cuh"
 #include "mlp.cuh"
 #include <algorithm>
 #include <random>
@@ -46,6 +49,16 @@ T* dalloc(size_t n) {
   return reinterpret_cast<T*>(p);
 }
 }  // namespace
+
+// file names of the TKE budget profiles, in the order of the avg_var calls
+// of compute_tke_budget (tke_budget1D.f90:218-383)
+const char* const TKE_NAMES[TKE_NQ] = {
+    "u",     "v",     "w",     "dudx",  "dudy",  "dudz",     "dvdx",     "dvdy",     "dvdz",  "dwdx",  "dwdy",
+    "dwdz",  "uu",    "vv",    "ww",    "uv",    "uw",       "vw",       "txx",      "tyy",   "tzz",   "txy",
+    "txz",   "tyz",   "cs",    "uuw",   "vvw",   "www",      "uww",      "wtzz",     "utxz",  "vtyz",  "dxx",
+    "dyy",   "dzz",   "dxy",   "dxz",   "dyz",   "dudx2",    "dudy2",    "dudz2",    "dvdx2", "dvdy2", "dvdz2",
+    "dwdx2", "dwdy2", "dwdz2", "dudxdwdx", "dudydwdy", "dudzdwdz", "p", "dpdx", "dpdy", "dpdz", "pw",
+    "pu",    "pdudx", "pdvdy", "pdwdz", "pdwdx", "pdudz"};
 
 template <typename T>
 class Solver final : public SolverBase {
@@ -711,6 +724,176 @@ class Solver final : public SolverBase {
     LES_CUDA(cudaStreamSynchronize(st));
   }
 
+  // --------------------------------------------------------- statistics ----
+  // Running sums of IO_statistics.f90 (io_stat_init :40-250, io_stat_averages
+  // :265-291, 2D :300-354, 3D :363-518) and the plane-averaged TKE budget of
+  // tke_budget1D.f90 (tke_budget_init :61-160, compute_tke_budget :209-390,
+  // avg_var :396-420), one rank.
+  double* stat_acc = nullptr;    // [26][nz][ny][nx] running sums
+  double* stat_ustar = nullptr;  // [ny][nx] running sum of u*
+  int stat_iterations = 0;
+  T* tke_f[3] = {};  // cleaned pressure (filtered), its x and y derivatives
+  double* tke_part = nullptr;
+  double* tke_avar = nullptr;  // [61][nz] running plane averages
+  int tke_nch = 1, tke_ii = 1;
+  std::string tke_dir;
+
+  static std::string nine(int v) {
+    char b[32];
+    std::snprintf(b, sizeof b, "%09d", v);
+    return b;
+  }
+  void write_host(const std::string& path, const std::vector<const double*>& parts, long n) {
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) throw CudaError(22, "cannot open statistics file " + path);
+    bool ok = true;
+    for (const double* p : parts) ok = ok && std::fwrite(p, sizeof(double), n, f) == size_t(n);
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) throw CudaError(22, "cannot write statistics file " + path);
+  }
+  std::vector<double> to_host(const double* d, long n) {
+    std::vector<double> h(n);
+    LES_CUDA(cudaMemcpyAsync(h.data(), d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+    return h;
+  }
+
+  void stat_init() override {
+    const long n = (long)STAT_NQ * g.nz * g.plane();
+    if (!stat_acc) {
+      stat_acc = track(dalloc<double>(n));
+      stat_ustar = track(dalloc<double>(g.plane()));
+    } else {
+      LES_CUDA(cudaMemsetAsync(stat_acc, 0, n * sizeof(double), st));
+      LES_CUDA(cudaMemsetAsync(stat_ustar, 0, g.plane() * sizeof(double), st));
+    }
+    stat_iterations = 0;
+  }
+  void stat_averages(int jt, int jtt, int start_stats, int running_period, const char* out_path) override {
+    (void)jt;
+    if (!stat_acc) throw CudaError(1, "running statistics are not initialised (les_stat_init)");
+    if (running_period <= 0) throw CudaError(1, "running_period must be positive");
+    Tag tag_(this, "stats");
+    const long plane = g.plane(), n = (long)g.nz * plane;
+    const bool write = (jtt % running_period == 0) && jtt > start_stats;
+    const std::string base = std::string(out_path) + "RAV_" + nine(jtt);
+    ++stat_iterations;
+    if (write) {
+      FILE* f = std::fopen((base + "_info.txt").c_str(), "w");
+      if (!f) throw CudaError(22, "cannot open statistics file " + base + "_info.txt");
+      std::fprintf(f, "%6d%6d%6d%10d\n", g.nx, g.ny, g.nz, stat_iterations);
+      if (std::fclose(f) != 0) throw CudaError(22, "cannot write statistics file " + base + "_info.txt");
+      stat_iterations = 0;
+    }
+    KL("k_plane_accum", 20.0 * plane,
+       k_plane_accum<T><<<grid_for(plane), 256, 0, st>>>(PL[LES_U_STAR_AVG], stat_ustar, plane));
+    if (write) {
+      const auto h = to_host(stat_ustar, plane);
+      write_host(base + "_2D.dat", {h.data()}, plane);
+      LES_CUDA(cudaMemsetAsync(stat_ustar, 0, plane * sizeof(double), st));
+    }
+    StatFields<T> sf{F[LES_U],   F[LES_V],   F[LES_W],   F[LES_P],    F[LES_TXX],  F[LES_TYY], F[LES_TZZ],
+                     F[LES_TXY], F[LES_TXZ], F[LES_TYZ], F[LES_DUDZ], F[LES_DVDZ], F[LES_NU_T], F[LES_CS_OPT2]};
+    KL("k_stat_accum", double(n) * (16.0 * STAT_NQ + 16.0 * sizeof(T)),
+       k_stat_accum<T><<<grid_for(n), 256, 0, st>>>(sf, stat_acc, plane, g.nz));
+    if (write) {
+      const auto h = to_host(stat_acc, STAT_NQ * n);
+      std::vector<const double*> parts;
+      for (int q = 0; q < STAT_NQ; ++q) parts.push_back(h.data() + q * n);
+      write_host(base + "_3D.dat", parts, n);
+      LES_CUDA(cudaMemsetAsync(stat_acc, 0, STAT_NQ * n * sizeof(double), st));
+    }
+    LES_CUDA(cudaStreamSynchronize(st));
+  }
+  void stat_sums(int index, double* out) override {
+    if (!stat_acc) throw CudaError(1, "running statistics are not initialised (les_stat_init)");
+    if (index < 0 || index > STAT_NQ) throw CudaError(1, "statistics index out of range");
+    const long n = (long)g.nz * g.plane();
+    const double* src = index == STAT_NQ ? stat_ustar : stat_acc + (long)index * n;
+    const long cnt = index == STAT_NQ ? g.plane() : n;
+    LES_CUDA(cudaMemcpyAsync(out, src, cnt * sizeof(double), cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+  }
+  int stat_iteration_count() override { return stat_iterations; }
+
+  // io_stat_spectra (IO_statistics.f90:566-581, out :583-620): u, v, w on
+  // levels 1..nz in the four fixed windows of jt_total, every 10th jt
+  void stat_spectra(int jt, int jtt, const char* out_path) override {
+    bool hit = false;
+    for (int lo : {1500000, 1550000, 1600000, 1650000}) hit = hit || (jtt >= lo && jtt <= lo + 2000 && jt % 10 == 0);
+    if (!hit) return;
+    const long n = (long)g.nz * g.plane();
+    std::vector<double> u(n), v(n), w(n);
+    download(LES_U, u.data(), 1, g.nz);
+    download(LES_V, v.data(), 1, g.nz);
+    download(LES_W, w.data(), 1, g.nz);
+    write_host(std::string(out_path) + "SP_" + nine(jtt) + ".dat", {u.data(), v.data(), w.data()}, n);
+  }
+
+  void tke_init(const char* out_path) override {
+    tke_dir = std::string(out_path) + "ta1_profiles/";
+    ::mkdir(tke_dir.c_str(), 0755);  // like the reference's system('mkdir'): an existing folder is fine
+    const int per_level = std::max(1, std::min(64, (4 * 148 + g.nz - 1) / g.nz));
+    tke_nch = int(std::min<long>(per_level, (g.plane() + 255) / 256));
+    if (!tke_avar) {
+      for (auto& f : tke_f) f = track(dalloc<T>(g.field()));
+      tke_part = track(dalloc<double>((long)g.nz * 64 * TKE_NQ));
+      tke_avar = track(dalloc<double>((long)TKE_NQ * g.nz));
+    } else {
+      LES_CUDA(cudaMemsetAsync(tke_avar, 0, (long)TKE_NQ * g.nz * sizeof(double), st));
+    }
+    tke_ii = 1;  // (actLaunch-1)*(nt/tke_period)+1 with actLaunch = 1
+  }
+  void tke_budget(int jt, int tke_period) override {
+    if (!tke_avar) throw CudaError(1, "TKE budget is not initialised (les_tke_init)");
+    if (tke_period <= 0) throw CudaError(1, "tke_period must be positive");
+    Tag tag_(this, "tke");
+    const long plane = g.plane();
+    KL("k_tke_cpress", 6.0 * g.field() * sizeof(T),
+       k_tke_cpress<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_P], F[LES_U], F[LES_V], F[LES_W], F[LES_CS_OPT2],
+                                                             tke_f[0], plane, g.nz));
+    grad_ptrs(&tke_f[0], &tke_f[1], &tke_f[2], 1);
+    TkeFields<T> tf{F[LES_U],    F[LES_V],    F[LES_W],    F[LES_DUDX], F[LES_DUDY], F[LES_DUDZ],
+                    F[LES_DVDX], F[LES_DVDY], F[LES_DVDZ], F[LES_DWDX], F[LES_DWDY], F[LES_DWDZ],
+                    F[LES_TXX],  F[LES_TYY],  F[LES_TZZ],  F[LES_TXY],  F[LES_TXZ],  F[LES_TYZ],
+                    F[LES_CS_OPT2], tke_f[0], tke_f[1], tke_f[2]};
+    const dim3 grid(tke_nch, g.nz);
+    const double idz = 1.0 / dz(), bytes = 26.0 * g.nz * plane * sizeof(T);
+    KL("k_tke_partial", bytes, k_tke_partial<T, 0, 16><<<grid, 256, 0, st>>>(tf, tke_part, plane, P.wall_law, idz));
+    KL("k_tke_partial", bytes, k_tke_partial<T, 16, 16><<<grid, 256, 0, st>>>(tf, tke_part, plane, P.wall_law, idz));
+    KL("k_tke_partial", bytes, k_tke_partial<T, 32, 16><<<grid, 256, 0, st>>>(tf, tke_part, plane, P.wall_law, idz));
+    KL("k_tke_partial", bytes, k_tke_partial<T, 48, 13><<<grid, 256, 0, st>>>(tf, tke_part, plane, P.wall_law, idz));
+    KL("k_tke_final", 8.0 * g.nz * tke_nch * TKE_NQ,
+       k_tke_final<<<grid_for((long)g.nz * TKE_NQ), 256, 0, st>>>(tke_part, tke_nch, g.nz,
+                                                                 double(g.nx) * double(g.ny), tke_avar));
+    if (jt % tke_period == 0) {
+      // avg_var :408-418: record ii (nz FP64 values, the 4-byte record units
+      // of recl = 2*nz) of <name>.out holds the sums over tke_period
+      const auto h = to_host(tke_avar, (long)TKE_NQ * g.nz);
+      std::vector<double> rec(g.nz);
+      for (int q = 0; q < TKE_NQ; ++q) {
+        for (int k = 0; k < g.nz; ++k) rec[k] = h[(long)q * g.nz + k] / double(tke_period);
+        const std::string path = tke_dir + TKE_NAMES[q] + ".out";
+        FILE* f = std::fopen(path.c_str(), "r+b");
+        if (!f) f = std::fopen(path.c_str(), "w+b");
+        if (!f) throw CudaError(22, "cannot open TKE budget file " + path);
+        bool ok = std::fseek(f, long(tke_ii - 1) * g.nz * long(sizeof(double)), SEEK_SET) == 0;
+        ok = ok && std::fwrite(rec.data(), sizeof(double), g.nz, f) == size_t(g.nz);
+        ok = (std::fclose(f) == 0) && ok;
+        if (!ok) throw CudaError(22, "cannot write TKE budget file " + path);
+      }
+      LES_CUDA(cudaMemsetAsync(tke_avar, 0, (long)TKE_NQ * g.nz * sizeof(double), st));
+      ++tke_ii;
+    }
+    LES_CUDA(cudaStreamSynchronize(st));
+  }
+  void tke_sums(double* out, int* record) override {
+    if (!tke_avar) throw CudaError(1, "TKE budget is not initialised (les_tke_init)");
+    LES_CUDA(cudaMemcpyAsync(out, tke_avar, (long)TKE_NQ * g.nz * sizeof(double), cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+    *record = tke_ii;
+  }
+
   double* staging = nullptr;  // FP64 device staging field (mixed precision transfers)
   void upload_async(int field, const double* h, int k0, int k1) override {
     check_field(field, k0, k1);
@@ -779,12 +962,21 @@ class Solver final : public SolverBase {
   // ------------------------------------------------ compute_derivatives ----
   // grad_velocity_filt for up to three fields at once
   void grad_fields(const int* f, const int* dx, const int* dy, int nfld) {
+    T *pf[3], *pdx[3], *pdy[3];
+    for (int q = 0; q < nfld; ++q) {
+      pf[q] = F[f[q]];
+      pdx[q] = F[dx[q]];
+      pdy[q] = F[dy[q]];
+    }
+    grad_ptrs(pf, pdx, pdy, nfld);
+  }
+  void grad_ptrs(T* const* f, T* const* dx, T* const* dy, int nfld) {
     Tag tag_(this, "grad");
     const int L = g.L;
     auto a = xf(XF_SCALE, nfld, 0, L, g.nx, g.ny, g.lhx);
     a.c0 = 1.0 / double(g.nx * g.ny);
     for (int q = 0; q < nfld; ++q) {
-      a.in[q] = F[f[q]];
+      a.in[q] = f[q];
       a.out[q] = spec[q];
     }
     use_refs(a, nfld);
@@ -807,9 +999,9 @@ class Solver final : public SolverBase {
       c.src[3 * q + 1] = 2 * q;
       c.dx[3 * q + 1] = 1;
       c.src[3 * q + 2] = 2 * q + 1;
-      c.out[3 * q + 0] = F[f[q]];
-      c.out[3 * q + 1] = F[dx[q]];
-      c.out[3 * q + 2] = F[dy[q]];
+      c.out[3 * q + 0] = f[q];
+      c.out[3 * q + 1] = dx[q];
+      c.out[3 * q + 2] = dy[q];
     }
     for (int q = 0; q < 3 * nfld; ++q) {
       c.lo[q] = 0;

@@ -131,6 +131,14 @@ struct SolverBase : LaunchHook {
   virtual void upload_async(int field, const double* pinned, int k0, int k1) = 0;
   virtual void download_async(int field, double* pinned, int k0, int k1) = 0;
   virtual void diagnostics_async(double* pinned4) = 0;
+  virtual void stat_init() = 0;
+  virtual void stat_averages(int jt, int jtt, int start_stats, int running_period, const char* out_path) = 0;
+  virtual void stat_sums(int index, double* out) = 0;
+  virtual int stat_iteration_count() = 0;
+  virtual void stat_spectra(int jt, int jtt, const char* out_path) = 0;
+  virtual void tke_init(const char* out_path) = 0;
+  virtual void tke_budget(int jt, int tke_period) = 0;
+  virtual void tke_sums(double* out, int* record) = 0;
   // timing events on the state's stream
   cudaEvent_t slots[16] = {};
   void record_event(int i) {

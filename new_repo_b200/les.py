@@ -29,6 +29,13 @@ compute_RHS_adv LES_engine.f90:509     ``LES.compute_RHS_adv``
 time loop body LES_engine.f90:189-360  ``LES.step``
 compute_running_diagnistics            ``LES.diagnostics``
 running_diagnostics.f90:80
+checkpoint_out / checkpoint_in         ``LES.checkpoint_out`` / ``checkpoint_in``
+IO_checkpoint.f90:53-256
+io_stat_init / io_stat_averages        ``LES.stat_init`` / ``LES.stat_averages``
+IO_statistics.f90:40 / :265
+io_stat_spectra  IO_statistics:566     ``LES.stat_spectra``
+tke_budget_init / compute_tke_budget   ``LES.tke_init`` / ``LES.tke_budget``
+tke_budget1D.f90:61 / :209
 =====================================  ==========================================
 
 Errors: the reference aborts through ``decomp_2d_abort(code, msg)``; here a
@@ -80,6 +87,15 @@ class RunParams:
     wall_model: str = "wall_filter"
     dealias: str = "padd"
     lag_halo: str = "reference1x1"
+    # output_param (parameters_IO.f90:103-111,153-157): post-step statistics
+    out_path: str = "./"
+    stat_flag: bool = False
+    start_stats: int = 0
+    running_period: int = 1000
+    tke_flag: bool = False
+    start_tke: int = 0
+    tke_period: int = 100
+    spectra_flag: bool = False
 
     lx: float = field(init=False, default=0.0)
     ly: float = field(init=False, default=0.0)
@@ -126,7 +142,9 @@ class RunParams:
 
 _NML_KEYS = {"p_on_y", "p_on_z", "nx", "ny", "nz", "nt", "dt", "dim_dt_flag", "restart_flag", "xy_pi", "lx",
              "ly", "lz", "u_scale", "zi", "lbc_dz0", "re", "pfx", "pfy", "cs0", "sgs_model", "cs_count",
-             "dyn_init", "lbc_special", "wall_model"}
+             "dyn_init", "lbc_special", "wall_model",
+             "out_path", "stat_flag", "start_stats", "running_period", "tke_flag", "start_tke", "tke_period",
+             "spectra_flag"}
 
 
 def _namelist_values(text: str) -> dict:
@@ -170,6 +188,10 @@ def read_namelist(path: str | Path) -> tuple[RunParams, dict]:
               sgs_model=str(raw.get("sgs_model", "cst_Smag")), cs_count=int(raw.get("cs_count", 5)),
               dyn_init=int(raw.get("dyn_init", 1500)), lbc_special=str(raw.get("lbc_special", "std")),
               wall_model=str(raw.get("wall_model", "wall_filter")))
+    for key, typ in (("out_path", str), ("stat_flag", bool), ("start_stats", int), ("running_period", int),
+                     ("tke_flag", bool), ("start_tke", int), ("tke_period", int), ("spectra_flag", bool)):
+        if key in raw:
+            kw[key] = typ(raw[key])
     return RunParams(**kw), raw
 
 
@@ -253,6 +275,11 @@ class LES:
         self._h = h
         self.jt_total = 0
         self.jt = 0
+        # io_stat_init / tke_budget_init when their flags are on (LES_engine.f90:149-150)
+        if self.params.stat_flag:
+            self.stat_init()
+        if self.params.tke_flag:
+            self.tke_init()
 
     # ------------------------------------------------------------- lifetime
     def close(self):
@@ -373,11 +400,77 @@ class LES:
         check(self.lib.les_projection(self._h, float(tadv1)))
 
     def step(self, n: int = 1):
-        """Advance n time steps (the LES_engine.f90:189-360 loop body)."""
+        """Advance n time steps (the LES_engine.f90:189-360 loop body), each
+        followed by the statistics its output flags ask for (:366-380)."""
+        p = self.params
         for _ in range(n):
             self.jt += 1
             self.jt_total += 1
             check(self.lib.les_step(self._h, self.jt, self.jt_total))
+            if p.stat_flag and self.jt_total > p.start_stats:
+                self.stat_averages()
+            if p.spectra_flag:
+                self.stat_spectra()
+            if p.tke_flag and self.jt_total > p.start_tke:
+                self.tke_budget()
+
+    # --------------------------------------------------------------- statistics
+    def stat_init(self):
+        """io_stat_init (IO_statistics.f90:40-250): running sums allocated and zeroed."""
+        check(self.lib.les_stat_init(self._h))
+
+    def stat_averages(self, jt: int | None = None, jt_total: int | None = None):
+        """io_stat_averages(jt, jt_total) (IO_statistics.f90:265-518): add the
+        state to the running sums; RAV_<jt_total>_{info.txt,2D.dat,3D.dat}
+        under out_path every running_period steps after start_stats."""
+        p = self.params
+        jt = self.jt if jt is None else int(jt)
+        jt_total = self.jt_total if jt_total is None else int(jt_total)
+        check(self.lib.les_stat_averages(self._h, jt, jt_total, int(p.start_stats), int(p.running_period),
+                                         p.out_path.encode()))
+
+    def stat_sums(self, name: str) -> np.ndarray:
+        """The running sum ``name`` (STAT_NAMES order, or "ustar") as
+        (nz, ny, nx) / (ny, nx) FP64."""
+        p = self.params
+        if name == "ustar":
+            out = np.empty((p.ny, p.nx))
+            idx = len(capi.STAT_NAMES)
+        else:
+            if name not in capi.STAT_NAMES:
+                raise LesError(capi.LES_ERR_INVALID, f"unknown statistic {name!r}")
+            out = np.empty((p.nz, p.ny, p.nx))
+            idx = capi.STAT_NAMES.index(name)
+        check(self.lib.les_stat_sums(self._h, idx, _dptr(out)))
+        return out
+
+    def stat_iterations(self) -> int:
+        v = C.c_int()
+        check(self.lib.les_stat_iterations(self._h, C.byref(v)))
+        return int(v.value)
+
+    def stat_spectra(self, jt: int | None = None, jt_total: int | None = None):
+        """io_stat_spectra (IO_statistics.f90:566-620)."""
+        jt = self.jt if jt is None else int(jt)
+        jt_total = self.jt_total if jt_total is None else int(jt_total)
+        check(self.lib.les_stat_spectra(self._h, jt, jt_total, self.params.out_path.encode()))
+
+    def tke_init(self):
+        """tke_budget_init (tke_budget1D.f90:61-160): out_path/ta1_profiles/,
+        61 zeroed profiles, record counter 1."""
+        check(self.lib.les_tke_init(self._h, self.params.out_path.encode()))
+
+    def tke_budget(self, jt: int | None = None):
+        """compute_tke_budget(jt) (tke_budget1D.f90:209-390)."""
+        jt = self.jt if jt is None else int(jt)
+        check(self.lib.les_tke_budget(self._h, jt, int(self.params.tke_period)))
+
+    def tke_profiles(self) -> tuple[np.ndarray, int]:
+        """(61, nz) running plane averages (TKE_NAMES order) and the next record number."""
+        out = np.empty((len(capi.TKE_NAMES), self.params.nz))
+        rec = C.c_int()
+        check(self.lib.les_tke_sums(self._h, _dptr(out), C.byref(rec)))
+        return out, int(rec.value)
 
     def diagnostics(self) -> tuple:
         """(cfl, mke, u_star, rms div u) of running_diagnostics.f90:148-305."""
