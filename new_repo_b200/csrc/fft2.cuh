@@ -215,21 +215,84 @@ struct Geo {
   static constexpr int T = N / E;
 };
 
-// Exchange slots are padded by one element every 16: the pass outputs are
-// written at stride R, which would otherwise put a warp's lanes on a few
-// banks.  A sequence of N elements needs N + N/16 elements of slot;
-// slot_len<N>() rounds that up to even so that consecutive slots of FP32
-// complex values stay 16-byte aligned (the x passes move 4 reals at once).
-template <int N>
-__host__ __device__ constexpr int slot_len() {
-  return (N + N / 16 + 1) & ~1;
-}
-__device__ __forceinline__ int xpad(int i) { return i + (i >> 4); }
 
-// one pass of radix R with Ns = product of the previous radices; then the
-// exchange into the next pass's input layout (if any)
-template <typename T, int N, int E, bool INV, int TWS, int Ns, int R, int... Rest>
-__device__ __forceinline__ void reg_passes(cplx<T>* v, cplx<T>* seq, int t, const cplx<T>* __restrict__ tw) {
+// Exchange layout of a sequence in its slot.  S = -1: element i at i + i/16
+// (one element of padding every 16; the pass outputs are written at stride
+// R, which would otherwise put a warp's lanes on a few banks).  S >= 1:
+// element i at i ^ ((i >> S) & 15), a permutation within each aligned block
+// of 16.  Each exchange (length N, element size ES bytes, stores of a
+// radix-R pass after radices of product NS, loads of the next radix R2)
+// takes the padding where that already puts a half warp (FP32 complex) or a
+// quarter warp (FP64 complex) on distinct banks for both its stores and its
+// loads -- its addresses differ by constants, which cost no instructions --
+// and otherwise the permutation whose shift S does, found by enumerating the
+// access patterns of every plan with the sequences that share a half (or
+// quarter) warp at their slot_stride apart.
+constexpr int exch_shift(int N, int ES, int R, int NS, int R2) {
+  if (N == 32 && ES == 8 && R == 4 && NS == 1 && R2 == 8) return 2;
+  if (N == 32 && ES == 8 && R == 8 && NS == 1 && R2 == 4) return 3;
+  if (N == 32 && ES == 16 && R == 4 && NS == 1 && R2 == 8) return 2;
+  if (N == 32 && ES == 16 && R == 8 && NS == 1 && R2 == 4) return 3;
+  if (N == 48 && ES == 8 && R == 4 && NS == 1 && R2 == 12) return 2;
+  if (N == 48 && ES == 8 && R == 12 && NS == 1 && R2 == 4) return 2;
+  if (N == 48 && ES == 16 && R == 4 && NS == 1 && R2 == 12) return 2;
+  if (N == 48 && ES == 16 && R == 12 && NS == 1 && R2 == 4) return 2;
+  if (N == 64 && ES == 8 && R == 4 && NS == 1 && R2 == 16) return 2;
+  if (N == 64 && ES == 8 && R == 16 && NS == 1 && R2 == 4) return -1;
+  if (N == 64 && ES == 16 && R == 4 && NS == 1 && R2 == 16) return 2;
+  if (N == 64 && ES == 16 && R == 16 && NS == 1 && R2 == 4) return -1;
+  if (N == 96 && ES == 8 && R == 4 && NS == 1 && R2 == 24) return 2;
+  if (N == 96 && ES == 8 && R == 24 && NS == 1 && R2 == 4) return 3;
+  if (N == 96 && ES == 16 && R == 4 && NS == 1 && R2 == 24) return 2;
+  if (N == 96 && ES == 16 && R == 24 && NS == 1 && R2 == 4) return 3;
+  if (N == 128 && ES == 8 && R == 8 && NS == 1 && R2 == 16) return 3;
+  if (N == 128 && ES == 8 && R == 16 && NS == 1 && R2 == 8) return -1;
+  if (N == 128 && ES == 16 && R == 8 && NS == 1 && R2 == 16) return 3;
+  if (N == 128 && ES == 16 && R == 16 && NS == 1 && R2 == 8) return -1;
+  if (N == 192 && ES == 8 && R == 8 && NS == 1 && R2 == 24) return 3;
+  if (N == 192 && ES == 8 && R == 24 && NS == 1 && R2 == 8) return 3;
+  if (N == 192 && ES == 16 && R == 8 && NS == 1 && R2 == 24) return 3;
+  if (N == 192 && ES == 16 && R == 24 && NS == 1 && R2 == 8) return 3;
+  if (N == 256 && ES == 8 && R == 16 && NS == 1 && R2 == 16) return -1;
+  if (N == 256 && ES == 16 && R == 16 && NS == 1 && R2 == 16) return -1;
+  if (N == 384 && ES == 8 && R == 4 && NS == 1 && R2 == 4) return -1;
+  if (N == 384 && ES == 8 && R == 4 && NS == 4 && R2 == 24) return 2;
+  if (N == 384 && ES == 8 && R == 4 && NS == 24 && R2 == 4) return 3;
+  if (N == 384 && ES == 8 && R == 24 && NS == 1 && R2 == 4) return 3;
+  if (N == 384 && ES == 16 && R == 4 && NS == 1 && R2 == 4) return 2;
+  if (N == 384 && ES == 16 && R == 4 && NS == 4 && R2 == 24) return 2;
+  if (N == 384 && ES == 16 && R == 4 && NS == 24 && R2 == 4) return -1;
+  if (N == 384 && ES == 16 && R == 24 && NS == 1 && R2 == 4) return 3;
+  if (N == 512 && ES == 8 && R == 2 && NS == 1 && R2 == 16) return -1;
+  if (N == 512 && ES == 8 && R == 16 && NS == 1 && R2 == 16) return -1;
+  if (N == 512 && ES == 8 && R == 16 && NS == 2 && R2 == 16) return -1;
+  if (N == 512 && ES == 8 && R == 16 && NS == 16 && R2 == 2) return -1;
+  if (N == 512 && ES == 16 && R == 2 && NS == 1 && R2 == 16) return 1;
+  if (N == 512 && ES == 16 && R == 16 && NS == 1 && R2 == 16) return -1;
+  if (N == 512 && ES == 16 && R == 16 && NS == 2 && R2 == 16) return -1;
+  if (N == 512 && ES == 16 && R == 16 && NS == 16 && R2 == 2) return -1;
+  if (N == 768 && ES == 8 && R == 4 && NS == 1 && R2 == 8) return -1;
+  if (N == 768 && ES == 8 && R == 8 && NS == 4 && R2 == 24) return 3;
+  if (N == 768 && ES == 8 && R == 8 && NS == 24 && R2 == 4) return 3;
+  if (N == 768 && ES == 8 && R == 24 && NS == 1 && R2 == 8) return 3;
+  if (N == 768 && ES == 16 && R == 4 && NS == 1 && R2 == 8) return 2;
+  if (N == 768 && ES == 16 && R == 8 && NS == 4 && R2 == 24) return 3;
+  if (N == 768 && ES == 16 && R == 8 && NS == 24 && R2 == 4) return -1;
+  if (N == 768 && ES == 16 && R == 24 && NS == 1 && R2 == 8) return 3;
+  return -1;
+}
+template <int S>
+__device__ __forceinline__ int exch_pos(int i) {
+  if constexpr (S < 0) return i + (i >> 4);
+  else if constexpr (S == 0) return i;
+  else return i ^ ((i >> S) & 15);
+}
+
+// one pass of radix R with Ns = product of the previous radices, its
+// twiddle factors at twm[OFF + (r-1) Ns + k]; then the exchange into the next
+// pass's input layout (if any)
+template <typename T, int N, int E, bool INV, int Ns, int OFF, int R, int... Rest>
+__device__ __forceinline__ void reg_passes(cplx<T>* v, cplx<T>* seq, int t, const cplx<T>* __restrict__ twm) {
   constexpr int TL = N / E;
   constexpr int G = E / R;
 #pragma unroll
@@ -239,36 +302,37 @@ __device__ __forceinline__ void reg_passes(cplx<T>* v, cplx<T>* seq, int t, cons
       const int k = j % Ns;
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        const cplx<T> w = tw[(r * k * (N / (Ns * R))) * TWS];
+        const cplx<T> w = twm[OFF + (r - 1) * Ns + k];
         v[g * R + r] = INV ? c_mulc(v[g * R + r], w) : c_mul(v[g * R + r], w);
       }
     }
     RegDFT<T, R, INV>::run(v + g * R);
   }
   if constexpr (sizeof...(Rest) > 0) {
+    constexpr int R2 = FirstOf<Rest...>::value;
+    constexpr int G2 = E / R2;
+    constexpr int SW = exch_shift(N, int(sizeof(cplx<T>)), R, Ns, R2);
     __syncwarp();
 #pragma unroll
     for (int g = 0; g < G; ++g) {
       const int j = t + TL * g;
       const int k = j % Ns;
 #pragma unroll
-      for (int r = 0; r < R; ++r) seq[xpad((j / Ns) * Ns * R + k + r * Ns)] = v[g * R + r];
+      for (int r = 0; r < R; ++r) seq[exch_pos<SW>((j / Ns) * Ns * R + k + r * Ns)] = v[g * R + r];
     }
     __syncwarp();
-    constexpr int R2 = FirstOf<Rest...>::value;
-    constexpr int G2 = E / R2;
 #pragma unroll
     for (int g = 0; g < G2; ++g)
 #pragma unroll
-      for (int r = 0; r < R2; ++r) v[g * R2 + r] = seq[xpad(t + TL * g + r * (N / R2))];
-    reg_passes<T, N, E, INV, TWS, Ns * R, Rest...>(v, seq, t, tw);
+      for (int r = 0; r < R2; ++r) v[g * R2 + r] = seq[exch_pos<SW>(t + TL * g + r * (N / R2))];
+    reg_passes<T, N, E, INV, Ns * R, OFF + (Ns > 1 ? (R - 1) * Ns : 0), Rest...>(v, seq, t, twm);
   }
 }
 
-template <typename T, int N, bool INV, int TWS, int... Rs>
-__device__ __forceinline__ void reg_fft_impl(cplx<T>* v, cplx<T>* seq, int t, const cplx<T>* tw,
+template <typename T, int N, bool INV, int... Rs>
+__device__ __forceinline__ void reg_fft_impl(cplx<T>* v, cplx<T>* seq, int t, const cplx<T>* twm,
                                              std::integer_sequence<int, Rs...>) {
-  reg_passes<T, N, Geo<N>::E, INV, TWS, 1, Rs...>(v, seq, t, tw);
+  reg_passes<T, N, Geo<N>::E, INV, 1, 0, Rs...>(v, seq, t, twm);
 }
 
 // reversed radix list (the inverse runs the plan backwards)
@@ -290,13 +354,115 @@ struct PassOrder {
       typename PlanRadices<N>::seq>::type;
 };
 
-// The transform: v as in the layout contract above; seq is this sequence's
-// shared slot of slot_len<N>() elements (private to its T lanes); tw holds
-// exp(-2 pi i m / (N*TWS)) read at stride TWS.  Forward transforms run the
-// plan's radices in order, inverse transforms in reverse order.
+// ------------------------------------------------ twiddle matrices ----
+// The twiddle factors of every pass after the first (radix R after radices
+// of product Ns) are W^(r k N/(Ns R)) for r = 1..R-1, k = 0..Ns-1 with
+// k = (lane + T g) mod Ns.  Read from a table of W^m they sit at stride
+// r k, which puts the lanes of a sequence on a few banks; the matrix of a
+// pass stores them as [r-1][k], so those lanes read consecutive entries.
+// Matrices of all passes of a plan follow each other (twm_len entries).
+template <int Ns, int R, int... Rest>
+struct TwmLen {
+  static constexpr int value = (Ns > 1 ? (R - 1) * Ns : 0) + TwmLen<Ns * R, Rest...>::value;
+};
+template <int Ns, int R>
+struct TwmLen<Ns, R> {
+  static constexpr int value = (Ns > 1 ? (R - 1) * Ns : 0);
+};
+template <int... Rs>
+constexpr int twm_len_impl(std::integer_sequence<int, Rs...>) {
+  return TwmLen<1, Rs...>::value;
+}
+template <int N, bool INV>
+struct Twm {
+  static constexpr int len = twm_len_impl(typename PassOrder<N, INV>::seq{});
+};
+
+// radix i of the forward plan of length N (0 past the last), for the host's
+// shared-memory sizing; matches PlanRadices
+__host__ __device__ constexpr int plan_radix(int N, int i) {
+  switch (N) {
+    case 8: return i == 0 ? 8 : 0;
+    case 12: return i == 0 ? 12 : 0;
+    case 16: return i == 0 ? 16 : 0;
+    case 24: return i == 0 ? 24 : 0;
+    case 32: return i == 0 ? 8 : (i == 1 ? 4 : 0);
+    case 48: return i == 0 ? 12 : (i == 1 ? 4 : 0);
+    case 64: return i == 0 ? 16 : (i == 1 ? 4 : 0);
+    case 96: return i == 0 ? 24 : (i == 1 ? 4 : 0);
+    case 128: return i == 0 ? 16 : (i == 1 ? 8 : 0);
+    case 192: return i == 0 ? 24 : (i == 1 ? 8 : 0);
+    case 256: return i == 0 ? 16 : (i == 1 ? 16 : 0);
+    case 384: return i == 0 ? 24 : (i == 1 ? 4 : (i == 2 ? 4 : 0));
+    case 512: return i == 0 ? 16 : (i == 1 ? 16 : (i == 2 ? 2 : 0));
+    case 768: return i == 0 ? 24 : (i == 1 ? 8 : (i == 2 ? 4 : 0));
+    default: return 0;
+  }
+}
+// Distance between the shared-memory slots of consecutive sequences, in
+// complex values of ES bytes: room for N + N/16 values (the padded exchange
+// layout), then raised to TL (mod W), W = 128 / ES values per wavefront, when
+// the TL lanes of a sequence fill less than a half (FP32) or quarter (FP64)
+// warp: the W/TL sequences of one wavefront then cover disjoint banks in the
+// loads, stores and splits that walk consecutive elements.  FP32 slots stay
+// even (16-byte aligned: the x passes move four reals at once).
+__host__ __device__ constexpr int slot_stride(int N, int ES) {
+  const int TL = N / plan_radix(N, 0);
+  const int W = 128 / ES;
+  const int base = (N + N / 16 + 1) & ~1;
+  if (TL >= W) return base;
+  int want = TL % W;
+  if (ES == 8 && (want & 1)) want = 2;
+  return base + ((want - base % W) % W + W) % W;
+}
+
+// entries of the twiddle matrices of the forward (inv = false) or inverse
+// transform of length N
+__host__ __device__ constexpr int twm_len(int N, bool inv) {
+  int n = 0;
+  while (n < 4 && plan_radix(N, n) != 0) ++n;
+  int len = 0, ns = 1;
+  for (int p = 0; p < n; ++p) {
+    const int r = plan_radix(N, inv ? n - 1 - p : p);
+    if (p > 0) len += (r - 1) * ns;
+    ns *= r;
+  }
+  return len;
+}
+
+template <typename T, int N, int TWS, int Ns, int OFF, int R, int... Rest>
+__device__ __forceinline__ void twm_fill(const cplx<T>* __restrict__ tw, cplx<T>* twm, int tid, int nth) {
+  if constexpr (Ns > 1) {
+    for (int i = tid; i < (R - 1) * Ns; i += nth) {
+      const int r = 1 + i / Ns, k = i % Ns;
+      twm[OFF + i] = tw[(r * k * (N / (Ns * R))) * TWS];
+    }
+  }
+  if constexpr (sizeof...(Rest) > 0)
+    twm_fill<T, N, TWS, Ns * R, OFF + (Ns > 1 ? (R - 1) * Ns : 0), Rest...>(tw, twm, tid, nth);
+}
+template <typename T, int N, int TWS, int... Rs>
+__device__ __forceinline__ void twm_build_impl(const cplx<T>* tw, cplx<T>* twm, int tid, int nth,
+                                               std::integer_sequence<int, Rs...>) {
+  twm_fill<T, N, TWS, 1, 0, Rs...>(tw, twm, tid, nth);
+}
+// Fill the matrices of the length-N transform (direction INV) from a table
+// tw of exp(-2 pi i m / (N*TWS)) read at stride TWS; threads tid of nth share
+// the work.  The caller synchronises before the first transform.
 template <typename T, int N, bool INV, int TWS = 1>
-__device__ __forceinline__ void reg_fft(cplx<T>* v, cplx<T>* seq, int t, const cplx<T>* tw) {
-  reg_fft_impl<T, N, INV, TWS>(v, seq, t, tw, typename PassOrder<N, INV>::seq{});
+__device__ __forceinline__ void twm_build(const cplx<T>* tw, cplx<T>* twm, int tid, int nth) {
+  static_assert(Twm<N, INV>::len == twm_len(N, INV), "plan table and host sizing disagree");
+  twm_build_impl<T, N, TWS>(tw, twm, tid, nth, typename PassOrder<N, INV>::seq{});
+}
+
+// The transform: v as in the layout contract above; seq is this sequence's
+// shared slot of slot_stride(N, sizeof(cplx<T>)) elements (private to its T
+// lanes); twm holds the twiddle matrices built by twm_build<T, N, INV>.
+// Forward transforms run the plan's radices in order, inverse transforms in
+// reverse order.
+template <typename T, int N, bool INV>
+__device__ __forceinline__ void reg_fft(cplx<T>* v, cplx<T>* seq, int t, const cplx<T>* twm) {
+  reg_fft_impl<T, N, INV>(v, seq, t, twm, typename PassOrder<N, INV>::seq{});
 }
 
 template <int N, int... Rs>

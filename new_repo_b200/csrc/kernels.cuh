@@ -536,123 +536,166 @@ struct Neu {
     else c += (x - t) + s;
     s = t;
   }
+  __device__ __forceinline__ void merge(const Neu& o) {
+    add(o.s);
+    c += o.c;
+  }
   __device__ __forceinline__ double val() const { return s + c; }
 };
 
 constexpr int DIAG_BLOCKS = 1184;
 constexpr int DIAG_NV = 9;  // umax vmax wmax | usum vsum wsum divsum | nan | u* sum
 
+// Per-thread partials of the diagnostics, combined in a fixed order: a
+// shuffle tree within each warp (lane 0 keeps the result), then the warps in
+// order.  The maxima and the NaN flag do not depend on the order; the
+// compensated sums give the same bits on every run.
+struct DiagAcc {
+  double mx[3] = {-1234567890.0, -1234567890.0, -1234567890.0};
+  Neu sum[5];  // u, v, w (uvp node), (div u)^2, u*
+  double nan = 0.0;
+  __device__ __forceinline__ void merge(const DiagAcc& o) {
+    for (int i = 0; i < 3; ++i) mx[i] = fmax(mx[i], o.mx[i]);
+    for (int i = 0; i < 5; ++i) sum[i].merge(o.sum[i]);
+    nan = fmax(nan, o.nan);
+  }
+  __device__ __forceinline__ void warp_reduce() {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      DiagAcc o;
+      for (int i = 0; i < 3; ++i) o.mx[i] = __shfl_down_sync(0xffffffffu, mx[i], off);
+      for (int i = 0; i < 5; ++i) {
+        o.sum[i].s = __shfl_down_sync(0xffffffffu, sum[i].s, off);
+        o.sum[i].c = __shfl_down_sync(0xffffffffu, sum[i].c, off);
+      }
+      o.nan = __shfl_down_sync(0xffffffffu, nan, off);
+      merge(o);
+    }
+  }
+};
+
+// block reduction of DiagAcc (blockDim.x == 256): the result is valid in thread 0
+__device__ __forceinline__ void diag_block_reduce(DiagAcc& a) {
+  constexpr int NW = 14;  // mx[3], sum[5] (s, c), nan
+  __shared__ double wsum[8][NW];
+  a.warp_reduce();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    double* r = wsum[wid];
+    for (int i = 0; i < 3; ++i) r[i] = a.mx[i];
+    for (int i = 0; i < 5; ++i) {
+      r[3 + 2 * i] = a.sum[i].s;
+      r[4 + 2 * i] = a.sum[i].c;
+    }
+    r[13] = a.nan;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int w = 1; w < 8; ++w) {
+      DiagAcc o;
+      const double* r = wsum[w];
+      for (int i = 0; i < 3; ++i) o.mx[i] = r[i];
+      for (int i = 0; i < 5; ++i) {
+        o.sum[i].s = r[3 + 2 * i];
+        o.sum[i].c = r[4 + 2 * i];
+      }
+      o.nan = r[13];
+      a.merge(o);
+    }
+}
+
+// four consecutive values (16-byte aligned for FP32, 32-byte for FP64)
+__device__ __forceinline__ void ld4(const float* p, float* o) {
+  const float4 x = *reinterpret_cast<const float4*>(p);
+  o[0] = x.x;
+  o[1] = x.y;
+  o[2] = x.z;
+  o[3] = x.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double* o) {
+  const double2 x = reinterpret_cast<const double2*>(p)[0], y = reinterpret_cast<const double2*>(p)[1];
+  o[0] = x.x;
+  o[1] = x.y;
+  o[2] = y.x;
+  o[3] = y.y;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_diag_partial(const T* u, const T* v, const T* w, const T* dudx,
                                                       const T* dvdy, const T* dwdz, const T* ustar, long plane,
                                                       int nz, double* part) {
-  double mx[3] = {-1234567890.0, -1234567890.0, -1234567890.0};
-  Neu su, sv, sw, sd, sus;
-  int nan = 0;
+  DiagAcc a;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < plane; q += (long)gridDim.x * blockDim.x)
-    sus.add(double(ustar[q]));
+    a.sum[4].add(double(ustar[q]));
   const long n = (long)nz * plane;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
-    const long o = plane + q;
-    const double uu = u[o], vv = v[o], ww = w[o];
+  int nan = 0;
+  auto point = [&](double uu, double vv, double ww, double wu, double dx, double dy, double dz) {
     nan |= (uu != uu) | (vv != vv) | (ww != ww);
-    mx[0] = fmax(mx[0], fabs(uu));
-    mx[1] = fmax(mx[1], fabs(vv));
-    mx[2] = fmax(mx[2], fabs(ww));
-    su.add(uu);
-    sv.add(vv);
-    sw.add(0.5 * (ww + double(w[o + plane])));
-    const double dv = double(dudx[o]) + double(dvdy[o]) + double(dwdz[o]);
-    sd.add(dv * dv);
-  }
-  __shared__ double sm[DIAG_NV + 6][256];
-  const int t = threadIdx.x;
-  sm[DIAG_NV + 4][t] = sus.s;
-  sm[DIAG_NV + 5][t] = sus.c;
-  sm[0][t] = mx[0];
-  sm[1][t] = mx[1];
-  sm[2][t] = mx[2];
-  sm[3][t] = su.s;
-  sm[4][t] = sv.s;
-  sm[5][t] = sw.s;
-  sm[6][t] = sd.s;
-  sm[7][t] = nan;
-  sm[8][t] = su.c;
-  sm[9][t] = sv.c;
-  sm[10][t] = sw.c;
-  sm[11][t] = sd.c;
-  __syncthreads();
-  if (t == 0) {
-    double m0 = sm[0][0], m1 = sm[1][0], m2 = sm[2][0], fl = 0;
-    Neu a[4], us;
-    for (int i = 0; i < 256; ++i) {
-      us.add(sm[DIAG_NV + 4][i]);
-      us.add(sm[DIAG_NV + 5][i]);
-      m0 = fmax(m0, sm[0][i]);
-      m1 = fmax(m1, sm[1][i]);
-      m2 = fmax(m2, sm[2][i]);
-      for (int q = 0; q < 4; ++q) {
-        a[q].add(sm[3 + q][i]);
-        a[q].add(sm[8 + q][i]);
-      }
-      fl = fmax(fl, sm[7][i]);
+    a.mx[0] = fmax(a.mx[0], fabs(uu));
+    a.mx[1] = fmax(a.mx[1], fabs(vv));
+    a.mx[2] = fmax(a.mx[2], fabs(ww));
+    a.sum[0].add(uu);
+    a.sum[1].add(vv);
+    a.sum[2].add(0.5 * (ww + wu));
+    const double dv = dx + dy + dz;
+    a.sum[3].add(dv * dv);
+  };
+  if (plane % 4 == 0) {
+    // four consecutive points per thread and iteration: all 28 loads are
+    // issued (as 16-byte vectors for FP32) before the compensated sums run
+    const long n4 = n / 4;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n4; q += (long)gridDim.x * blockDim.x) {
+      const long o = plane + 4 * q;
+      T U[4], V[4], W[4], WU[4], DX[4], DY[4], DZ[4];
+      ld4(u + o, U);
+      ld4(v + o, V);
+      ld4(w + o, W);
+      ld4(w + o + plane, WU);
+      ld4(dudx + o, DX);
+      ld4(dvdy + o, DY);
+      ld4(dwdz + o, DZ);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) point(U[i], V[i], W[i], WU[i], DX[i], DY[i], DZ[i]);
     }
+  } else {
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+      const long o = plane + q;
+      point(u[o], v[o], w[o], w[o + plane], dudx[o], dvdy[o], dwdz[o]);
+    }
+  }
+  a.nan = nan;
+  diag_block_reduce(a);
+  if (threadIdx.x == 0) {
     double* out = part + (long)blockIdx.x * DIAG_NV;
-    out[0] = m0;
-    out[1] = m1;
-    out[2] = m2;
-    for (int q = 0; q < 4; ++q) out[3 + q] = a[q].val();
-    out[7] = fl;
-    out[8] = us.val();
+    for (int i = 0; i < 3; ++i) out[i] = a.mx[i];
+    for (int q = 0; q < 4; ++q) out[3 + q] = a.sum[q].val();
+    out[7] = a.nan;
+    out[8] = a.sum[4].val();
   }
 }
 
-__global__ void k_diag_final(const double* part, int nblocks, long plane, double dt, double dx, double dy,
-                             double dz, double npts, double* out, unsigned* status) {
+__global__ void __launch_bounds__(256) k_diag_final(const double* part, int nblocks, long plane, double dt,
+                                                    double dx, double dy, double dz, double npts, double* out,
+                                                    unsigned* status) {
   // fixed-order combination of the block partials (deterministic)
-  __shared__ double sm[9][256];
-  __shared__ double cm[6][256];
-  const int t = threadIdx.x;
-  double m0 = -1e300, m1 = -1e300, m2 = -1e300, fl = 0;
-  Neu a[5];
-  for (int b = t; b < nblocks; b += blockDim.x) {
+  DiagAcc a;
+  a.mx[0] = a.mx[1] = a.mx[2] = -1e300;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
     const double* q = part + (long)b * DIAG_NV;
-    m0 = fmax(m0, q[0]);
-    m1 = fmax(m1, q[1]);
-    m2 = fmax(m2, q[2]);
-    for (int i = 0; i < 4; ++i) a[i].add(q[3 + i]);
-    a[4].add(q[8]);
-    fl = fmax(fl, q[7]);
+    for (int i = 0; i < 3; ++i) a.mx[i] = fmax(a.mx[i], q[i]);
+    for (int i = 0; i < 4; ++i) a.sum[i].add(q[3 + i]);
+    a.sum[4].add(q[8]);
+    a.nan = fmax(a.nan, q[7]);
   }
-  sm[0][t] = m0;
-  sm[1][t] = m1;
-  sm[2][t] = m2;
-  sm[3][t] = fl;
-  for (int i = 0; i < 5; ++i) {
-    sm[4 + i][t] = a[i].s;
-    if (i < 5) cm[i][t] = a[i].c;
-  }
-  __syncthreads();
-  if (t == 0) {
-    double x0 = sm[0][0], x1 = sm[1][0], x2 = sm[2][0], f = 0;
-    Neu s[5];
-    for (int i = 0; i < blockDim.x; ++i) {
-      x0 = fmax(x0, sm[0][i]);
-      x1 = fmax(x1, sm[1][i]);
-      x2 = fmax(x2, sm[2][i]);
-      f = fmax(f, sm[3][i]);
-      for (int q = 0; q < 5; ++q) {
-        s[q].add(sm[4 + q][i]);
-        s[q].add(cm[q][i]);
-      }
-    }
-    const double cfl = dt * (x0 / dx + x1 / dy + x2 / dz);
-    const double um = s[0].val() / npts, vm = s[1].val() / npts, wm = s[2].val() / npts;
+  diag_block_reduce(a);
+  if (threadIdx.x == 0) {
+    const double cfl = dt * (a.mx[0] / dx + a.mx[1] / dy + a.mx[2] / dz);
+    const double um = a.sum[0].val() / npts, vm = a.sum[1].val() / npts, wm = a.sum[2].val() / npts;
     out[0] = cfl;
     out[1] = 0.5 * (um * um + vm * vm + wm * wm);
-    out[2] = s[4].val() / double(plane);
-    out[3] = sqrt(s[3].val() / npts);
-    if (f != 0.0) atomicOr(status, ST_NAN);
+    out[2] = a.sum[4].val() / double(plane);
+    out[3] = sqrt(a.sum[3].val() / npts);
+    if (a.nan != 0.0) atomicOr(status, ST_NAN);
   }
 }
 

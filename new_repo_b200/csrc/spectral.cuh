@@ -309,17 +309,19 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd(const XFAr
   constexpr int E = Geo<M>::E;
   constexpr int RI = Layout<M, false>::in;
   constexpr int RO = Layout<M, false>::out;
-  constexpr int SL = slot_len<M>();  // complex values per sequence slot
+  constexpr int SL = slot_stride(M, int(sizeof(cplx<T>)));  // complex values per sequence slot
   constexpr int XS = 2 * SL;         // the same slot viewed as reals
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
-  cplx<T>* buf = tw + NX;
+  cplx<T>* twm = tw + NX;  // twiddle matrices of the M-point transform
+  cplx<T>* buf = twm + Twm<M, false>::len;
   const int nseq = a.R * a.nf;
   const int npad = seq_pad<M>(nseq);
   T* refs = reinterpret_cast<T*>(buf + (long)npad * SL);  // R * nf per-row references
   int* rowl = reinterpret_cast<int*>(refs + a.R * a.nf);  // level of row r (-1: beyond the grid)
   int* rowj = rowl + a.R;
   for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
+  twm_build<T, M, false, 2>(a.tw, twm, threadIdx.x, blockDim.x);
   const long g0 = (long)blockIdx.x * a.R;
   for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
     const long g = g0 + r;
@@ -376,7 +378,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd(const XFAr
     for (int g = 0; g < E / RI; ++g)
 #pragma unroll
       for (int r = 0; r < RI; ++r) v[g * RI + r] = seq[lane_t + TL * g + r * (M / RI)];
-    reg_fft<T, M, false, 2>(v, seq, lane_t, tw);
+    reg_fft<T, M, false>(v, seq, lane_t, twm);
     __syncwarp();
 #pragma unroll
     for (int g = 0; g < E / RO; ++g)
@@ -477,19 +479,21 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd_st(const X
   constexpr int E = Geo<M>::E;
   constexpr int RI = Layout<M, false>::in;
   constexpr int RO = Layout<M, false>::out;
-  constexpr int SL = slot_len<M>();
+  constexpr int SL = slot_stride(M, int(sizeof(cplx<T>)));
   constexpr int XS = 2 * SL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* twm = tw + NX;  // twiddle matrices of the M-point transform
   const int nseq = a.R * a.nf;
   const int npad = seq_pad<M>(nseq);
-  S* stage0 = reinterpret_cast<S*>(tw + NX);
+  S* stage0 = reinterpret_cast<S*>(twm + Twm<M, false>::len);
   S* stage1 = stage0 + (long)a.R * a.nsrc * NX;
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(stage1 + (long)a.R * a.nsrc * NX);
   T* refs = reinterpret_cast<T*>(buf + (long)npad * SL);
   int* rowl = reinterpret_cast<int*>(refs + a.R * a.nf);
   int* rowj = rowl + a.R;
   for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
+  twm_build<T, M, false, 2>(a.tw, twm, threadIdx.x, blockDim.x);
   const long nitems = (a.nrows + a.R - 1) / a.R;
   if ((long)blockIdx.x < nitems) {
     xf_issue<T, S, NX>(a, blockIdx.x, stage0);
@@ -557,7 +561,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd_st(const X
       for (int g = 0; g < E / RI; ++g)
 #pragma unroll
         for (int r = 0; r < RI; ++r) v[g * RI + r] = seq[lane_t + TL * g + r * (M / RI)];
-      reg_fft<T, M, false, 2>(v, seq, lane_t, tw);
+      reg_fft<T, M, false>(v, seq, lane_t, twm);
       __syncwarp();
 #pragma unroll
       for (int g = 0; g < E / RO; ++g)
@@ -671,16 +675,19 @@ __device__ __forceinline__ void yp_issue(const YPArgs<T>& a, long item, int ncb,
   const int col0 = int(item % ncb) * C;
   const int l = a.plane0 + int((item / ncb) % a.nplanes);
   const int grp = int(item / ((long)ncb * a.nplanes));
-  for (int idx = threadIdx.x; idx < a.nin * NY * C; idx += blockDim.x) {
-    const int c = idx & (C - 1);
-    const int t = idx >> a.lc;
-    const int ky = t % NY;
-    const int q = t / NY;
-    const int kx = col0 + c;
+  // thread -> fixed column c, rows ky0, ky0 + kstep, ...: the addresses
+  // advance by constant strides (blockDim.x is a multiple of C)
+  const int c = threadIdx.x & (C - 1);
+  const int ky0 = threadIdx.x >> a.lc;
+  const int kstep = blockDim.x >> a.lc;
+  const int kx = col0 + c;
+  const bool valid = kx < a.ncols;
+  for (int q = 0; q < a.nin; ++q) {
     const cplx<T>* base = a.in[grp * a.nin + q];
-    const bool valid = kx < a.ncols;
-    const cplx<T>* src = valid ? base + (long)l * a.in_pstride + (long)ky * a.ipitch + kx : base;
-    cp_async<int(sizeof(cplx<T>))>(bin + (q * C + c) * SI + ky, src, valid);
+    const cplx<T>* src = base + (long)l * a.in_pstride + kx;
+    cplx<T>* dst = bin + (q * C + c) * SI;
+    for (int ky = ky0; ky < NY; ky += kstep)
+      cp_async<int(sizeof(cplx<T>))>(dst + ky, valid ? src + (long)ky * a.ipitch : base, valid);
   }
 }
 
@@ -697,16 +704,16 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPA
   constexpr bool SAME = (NY == NYO);
   static_assert(!SAME || FO == II, "forward output layout must feed the inverse");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<T>* twi = reinterpret_cast<cplx<T>*>(smem_raw);
-  cplx<T>* two = twi + NY;
+  cplx<T>* twi = reinterpret_cast<cplx<T>*>(smem_raw);  // twiddle matrices, forward NY
+  cplx<T>* two = twi + Twm<NY, false>::len;                 // and inverse NYO
   const int SI = a.SI;  // >= NY
   const int SO = a.SO;  // >= NYO
   const int C = a.C;
-  cplx<T>* bin0 = two + NYO;               // input stage 0: [nin][C][SI]
+  cplx<T>* bin0 = two + Twm<NYO, true>::len;  // input stage 0: [nin][C][SI]
   cplx<T>* bin1 = bin0 + a.nin * C * SI;   // input stage 1
   cplx<T>* bout = bin1 + a.nin * C * SI;   // [C][SO]
-  for (int i = threadIdx.x; i < NY; i += blockDim.x) twi[i] = a.tw_in[i];
-  for (int i = threadIdx.x; i < NYO; i += blockDim.x) two[i] = a.tw_out[i];
+  twm_build<T, NY, false>(a.tw_in, twi, threadIdx.x, blockDim.x);
+  twm_build<T, NYO, true>(a.tw_out, two, threadIdx.x, blockDim.x);
   // persistent CTAs: work item = (column block, plane, group); the columns
   // of the next item are copied into the other input stage asynchronously
   // while this one is transformed
@@ -797,30 +804,31 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPA
           }
       }
     } else {
-      // 3/2 pad or truncate: remap the forward output through the slot
-      for (int i = lt; i < NYO; i += TL) sout[i] = cplx<T>{T(0), T(0)};
-      __syncwarp();
-#pragma unroll
-      for (int g = 0; g < EI / FO; ++g)
-#pragma unroll
-        for (int r = 0; r < FO; ++r) {
-          const int ky = lt + TL * g + r * (NY / FO);
-          int ko = -1;
-          if (a.op == YP_PAD) {
-            if (ky < NY / 2) ko = ky;
-            else if (ky > NY / 2) ko = ky + (NYO - NY);
-          } else {  // YP_TRUNC, NY = 3 NYO / 2
-            if (ky < NYO / 2) ko = ky;
-            else if (ky > NY - NYO / 2) ko = ky - (NY - NYO);
-          }
-          if (ko >= 0 && kx < a.ncols) sout[ko] = f0[g * FO + r];
+      // 3/2 pad or truncate.  Lane lt holds the forward output at ky = lt +
+      // TL m (m < EI) and the inverse wants ko = lt + TL m' (m' < EO); pad
+      // and truncation map ky to ko by a shift of whole multiples of TL, so
+      // the remap stays in the lane: a permutation of registers with zeros.
+      // PAD: ko = ky (ky < NY/2), ky + NY/2 (ky > NY/2), ky = NY/2 dropped;
+      // TRUNC: ko = ky (ky < NYO/2), ky - NYO/2 (ky > NYO), ky = NYO dropped.
+      constexpr int GI = EI / FO;  // forward output: f0[g FO + r] holds m = g + r GI
+      constexpr int GO = EO / II;  // inverse input: w[g II + r] wants m' = g + r GO
+      const bool live = kx < a.ncols;
+      static_for<EO>([&](auto mc) {
+        constexpr int mo = decltype(mc)::value;
+        constexpr int wi = (mo % GO) * II + mo / GO;
+        constexpr bool PAD = NYO > NY;
+        // source m of output m' (-1: zero), and whether lane 0 drops it
+        constexpr int ms = PAD ? (mo < EI / 2 ? mo : (mo < EI ? -1 : mo - EI / 2))
+                               : (mo < EO / 2 ? mo : mo + EO / 2);
+        constexpr bool drop0 = PAD ? (mo == EI) : (mo == EO / 2);
+        if constexpr (ms < 0) {
+          w[wi] = cplx<T>{T(0), T(0)};
+        } else {
+          constexpr int fi = (ms % GI) * FO + ms / GI;
+          const bool keep = live && !(drop0 && lt == 0);
+          w[wi] = keep ? f0[fi] : cplx<T>{T(0), T(0)};
         }
-      __syncwarp();
-#pragma unroll
-      for (int g = 0; g < EO / II; ++g)
-#pragma unroll
-        for (int r = 0; r < II; ++r) w[g * II + r] = sout[lt + TL * g + r * (NYO / II)];
-      __syncwarp();
+      });
     }
     if (a.op == YP_FWDKILL) {
       // no inverse: the op output is in the forward output layout (groups FO)
@@ -840,14 +848,16 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPA
     // coalesced store of output q
     const bool second = (a.op == YP_FILTER2 && q == 1);
     const int lim = second ? a.ncols1 : a.ncols;
-    for (int idx = threadIdx.x; idx < NYO * C; idx += blockDim.x) {
-      const int cc = idx & (C - 1);
-      const int ky = idx >> a.lc;
+    {
+      // thread -> fixed column cc, rows ky0 + kstep i (as in yp_issue)
+      const int cc = threadIdx.x & (C - 1);
       const int kxx = col0 + cc;
       if (kxx < lim) {
-        const cplx<T> val = bout[cc * SO + ky];
-        if (second) a.out[grp * a.nout + q][(long)l * a.out_pstride1 + (long)ky * a.opitch1 + kxx] = val;
-        else a.out[grp * a.nout + q][(long)l * a.out_pstride + (long)ky * a.opitch + kxx] = val;
+        const int ky0 = threadIdx.x >> a.lc, kstep = blockDim.x >> a.lc;
+        const long opitch = second ? a.opitch1 : a.opitch;
+        cplx<T>* dst = a.out[grp * a.nout + q] + (long)l * (second ? a.out_pstride1 : a.out_pstride) + kxx;
+        const cplx<T>* srow = bout + cc * SO;
+        for (int ky = ky0; ky < NYO; ky += kstep) dst[(long)ky * opitch] = srow[ky];
       }
     }
     __syncthreads();
@@ -872,6 +882,7 @@ struct XIArgs {
   int plane0;
   int nk;          // modes present in the input rows (rest zero)
   int ipitch;      // complex values between input rows (>= nk; 0: nk)
+  int nks;         // complex values between staged rows in shared memory (set by the launcher)
   int nz;
   long in_pstride;
   long out_pstride;  // elements per plane of the output grid
@@ -892,6 +903,9 @@ struct XIArgs {
   int src[MAXIN];
   int dx[MAXIN];
   const T* kxr;
+  // set by the launcher: every output (and the plane stride) admits stores of
+  // whole (x_2m, x_2m+1) pairs
+  int pair_store;
 };
 
 // x inverse pass: start the copies of the spectral rows of batch `item`
@@ -911,7 +925,7 @@ __device__ __forceinline__ void xi_issue(const XIArgs<T>& a, long item, cplx<T>*
     const cplx<T>* base = a.in[f];
     const cplx<T>* row =
         valid ? base + (long)(a.plane0 + int(g / a.rows_pp)) * a.in_pstride + (g % a.rows_pp) * a.ipitch : base;
-    cplx<T>* dst = stage + (long)s * a.nk;
+    cplx<T>* dst = stage + (long)s * a.nks;
     for (int m = lane; m < a.nk; m += 32) cp_async<int(sizeof(cplx<T>))>(dst + m, valid ? row + m : base, valid);
   }
 }
@@ -923,20 +937,22 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
   constexpr int E = Geo<M>::E;
   constexpr int RI = Layout<M, true>::in;
   constexpr int RO = Layout<M, true>::out;
-  constexpr int SL = slot_len<M>();  // complex values per sequence slot
+  constexpr int SL = slot_stride(M, int(sizeof(cplx<T>)));  // complex values per sequence slot
   constexpr int XS = 2 * SL;         // the same slot viewed as reals
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* twm = tw + NX;  // twiddle matrices of the M-point inverse transform
   const int nseq = a.R * a.nin;
   const int npad = seq_pad<M>(nseq);
   const int ns = a.nstage ? a.nstage : a.nin;        // staged rows per grid row
-  cplx<T>* stage0 = tw + NX;                         // input rows of a work item: [R][ns][nk]
-  cplx<T>* stage1 = stage0 + (long)a.R * ns * a.nk;
-  cplx<T>* buf = stage1 + (long)a.R * ns * a.nk;     // sequence slots
+  cplx<T>* stage0 = twm + Twm<M, true>::len;         // input rows of a work item: [R][ns][nk]
+  cplx<T>* stage1 = stage0 + (long)a.R * ns * a.nks;
+  cplx<T>* buf = stage1 + (long)a.R * ns * a.nks;    // sequence slots
   int* rowl = reinterpret_cast<int*>(buf + (long)npad * SL);  // level of row r (-1: beyond the grid)
   int* rowj = rowl + a.R;
   T* kxs = reinterpret_cast<T*>(rowj + a.R);          // x wavenumbers (nstage > 0)
   for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
+  twm_build<T, M, true, 2>(a.tw, twm, threadIdx.x, blockDim.x);
   if (a.nstage)
     for (int i = threadIdx.x; i < a.nk; i += blockDim.x) kxs[i] = a.kxr[i];
   // persistent CTAs over batches of R rows; the spectral rows of the next
@@ -985,7 +1001,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
     cplx<T> v[E];
     const int fs = a.nstage ? a.src[f] : f;
     const bool dxf = a.nstage && a.dx[f];
-    const cplx<T>* row = valid ? stage + (long)(r * ns + fs) * a.nk : nullptr;  // the staged spectral row
+    const cplx<T>* row = valid ? stage + (long)(r * ns + fs) * a.nks : nullptr;  // the staged spectral row
 #pragma unroll
     for (int gg = 0; gg < E / RI; ++gg)
 #pragma unroll
@@ -1010,7 +1026,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
         }
         v[gg * RI + rr] = z;
       }
-    reg_fft<T, M, true, 2>(v, seq, lane_t, tw);
+    reg_fft<T, M, true>(v, seq, lane_t, twm);
     if (direct) {
       if (valid && l >= a.lo[f] && l <= a.hi[f]) {
         const T ref = a.refin[f] ? a.refin[f][l] : T(0);
@@ -1023,6 +1039,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
             const cplx<T> z = v[gg * RO + rr];
             if (a.out_f32) {
               *reinterpret_cast<float2*>(a.outf[f] + off + 2 * m) = make_float2(float(z.x + ref), float(z.y + ref));
+            } else if (a.pair_store) {
+              // one 8-byte (FP32) / 16-byte (FP64) store per output pair
+              *reinterpret_cast<cplx<T>*>(a.out[f] + off + 2 * m) = cplx<T>{z.x + ref, z.y + ref};
             } else {
               a.out[f][off + 2 * m] = z.x + ref;
               a.out[f][off + 2 * m + 1] = z.y + ref;

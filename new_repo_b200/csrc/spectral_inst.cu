@@ -2,6 +2,7 @@
 // transform length (2^a 3^b: the grid sizes 16..512 and their 3/2 padding).
 #include "spectral.cuh"
 #include <algorithm>
+#include <cstdint>
 #include <mutex>
 
 #include "launch.cuh"
@@ -114,9 +115,10 @@ static void launch_xfwd_st(int NX, XFArgs<T>& a, cudaStream_t st) {
       a.scond[a.nsrc++] = 0;
     }
   }
-  const int SL = (M + M / 16 + 1) & ~1;  // slot_len<M>()
+  const int SL = slot_stride(M, int(sizeof(cplx<T>)));
   auto smem_for = [&](int R) {
-    return sizeof(cplx<T>) * (NX + (size_t)pad_seqs(R * a.nf, M) * SL) + 2 * sizeof(S) * (size_t)R * a.nsrc * NX +
+    return sizeof(cplx<T>) * (NX + twm_len(M, false) + (size_t)pad_seqs(R * a.nf, M) * SL) +
+           2 * sizeof(S) * (size_t)R * a.nsrc * NX +
            sizeof(T) * R * a.nf + 2 * sizeof(int) * R + 16;
   };
   a.R = std::min(32, std::max(rows_per_cta<T>(a.nf, M), ceil_div(256 / lanes(M), a.nf)));
@@ -163,8 +165,9 @@ void launch_xfwd(int NX, XFArgs<T> a, cudaStream_t st) {
   }
   a.R = rows_per_cta<T>(a.nf, M);
   a.in_rstride = NX;
-  const int SL = (M + M / 16 + 1) & ~1;  // slot_len<M>()
-  const size_t smem = sizeof(cplx<T>) * (NX + (size_t)pad_seqs(a.R * a.nf, M) * SL) + sizeof(T) * a.R * a.nf +
+  const int SL = slot_stride(M, int(sizeof(cplx<T>)));
+  const size_t smem = sizeof(cplx<T>) * (NX + twm_len(M, false) + (size_t)pad_seqs(a.R * a.nf, M) * SL) +
+                      sizeof(T) * a.R * a.nf +
                       2 * sizeof(int) * a.R + 16;
   if (smem > SMEM_CAP) throw CudaError(1, "xfwd: shared memory request too large");
   const int grid = ceil_div(a.nrows, a.R);
@@ -189,12 +192,24 @@ template <typename T>
 void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
   const int M = NX / 2;
   if (a.ipitch == 0) a.ipitch = a.nk;
+  a.pair_store = (a.out_pstride % 2 == 0);
+  for (int f = 0; f < a.nin && f < 16; ++f)
+    if (a.out[f] && reinterpret_cast<uintptr_t>(a.out[f]) % (2 * sizeof(T)) != 0) a.pair_store = 0;
   // enough rows that every thread holds a sequence (256 / lanes sequences),
   // within ~100 KB of slots and input stages (two CTAs per SM)
-  const int SL = (M + M / 16 + 1) & ~1;  // slot_len<M>()
+  const int SL = slot_stride(M, int(sizeof(cplx<T>)));
   const int ns = a.nstage ? a.nstage : a.nin;  // staged rows per grid row
+  {
+    // staged row stride: the split reads a row's modes at consecutive
+    // lanes, the TL lanes of 32 / TL sequences per warp in different rows;
+    // a stride of TL (mod the values per wavefront) puts those rows on
+    // disjoint banks, as slot_stride does for the sequence slots
+    const int W = 128 / int(sizeof(cplx<T>)), TL = lanes(M);
+    a.nks = a.nk;
+    if (TL < W) a.nks += ((TL % W - a.nk % W) % W + W) % W;
+  }
   auto smem_for = [&](int R) {
-    return sizeof(cplx<T>) * (NX + 2 * (size_t)R * ns * a.nk + (size_t)pad_seqs(R * a.nin, M) * SL) +
+    return sizeof(cplx<T>) * (NX + twm_len(M, true) + 2 * (size_t)R * ns * a.nks + (size_t)pad_seqs(R * a.nin, M) * SL) +
            2 * sizeof(int) * R + (a.nstage ? sizeof(T) * (a.nk + 2) : 0);
   };
   a.R = std::min(32, std::max(rows_per_cta<T>(a.nin, M), ceil_div(256 / lanes(M), a.nin)));
@@ -240,7 +255,7 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
   const int W = 128 / int(sizeof(cplx<T>));
   auto stride = [&](int n, int C) {
     const int target = (32 / C) % W;
-    const int base = n + n / 16;  // room for the FFT's padded exchange (slot_len)
+    const int base = n + n / 16;  // room for the FFT's padded exchange layout
     return base + ((target - base % W) % W + W) % W;
   };
   auto per_col = [&](int C) {  // two input stages + the output slot
@@ -253,7 +268,7 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
   a.C = 1 << lc;
   a.SI = stride(NY, a.C);
   a.SO = stride(NYO, a.C);
-  const size_t smem = sizeof(cplx<T>) * (NY + NYO) + (size_t)a.C * per_col(a.C);
+  const size_t smem = sizeof(cplx<T>) * (twm_len(NY, false) + twm_len(NYO, true)) + (size_t)a.C * per_col(a.C);
   if (smem > SMEM_CAP) throw CudaError(1, "ypass: shared memory request too large");
   const int threads = a.C * TL;
   a.nplanes = nplanes;
