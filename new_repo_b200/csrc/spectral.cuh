@@ -883,6 +883,8 @@ struct XIArgs {
   int nk;          // modes present in the input rows (rest zero)
   int ipitch;      // complex values between input rows (>= nk; 0: nk)
   int nks;         // complex values between staged rows in shared memory (set by the launcher)
+  int stage_rows;  // staged rows per stage (set by the launcher)
+  int merged;      // 1: each sequence is transformed in its own staged row (plain store, nstage 0)
   int nz;
   long in_pstride;
   long out_pstride;  // elements per plane of the output grid
@@ -946,9 +948,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
   const int npad = seq_pad<M>(nseq);
   const int ns = a.nstage ? a.nstage : a.nin;        // staged rows per grid row
   cplx<T>* stage0 = twm + Twm<M, true>::len;         // input rows of a work item: [R][ns][nk]
-  cplx<T>* stage1 = stage0 + (long)a.R * ns * a.nks;
-  cplx<T>* buf = stage1 + (long)a.R * ns * a.nks;    // sequence slots
-  int* rowl = reinterpret_cast<int*>(buf + (long)npad * SL);  // level of row r (-1: beyond the grid)
+  cplx<T>* stage1 = stage0 + (long)a.stage_rows * a.nks;
+  cplx<T>* buf = stage1 + (long)a.stage_rows * a.nks;  // sequence slots (none when merged)
+  int* rowl = reinterpret_cast<int*>(buf + (a.merged ? 0L : (long)npad * SL));  // level of row r (-1: beyond the grid)
   int* rowj = rowl + a.R;
   T* kxs = reinterpret_cast<T*>(rowj + a.R);          // x wavenumbers (nstage > 0)
   for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
@@ -995,7 +997,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
       l = rowl[r];
       j = rowj[r];
     }
-    cplx<T>* seq = buf + (long)s * SL;
+    // merged: the staged row of sequence s (staged rows are sequences) is its slot
+    cplx<T>* seq = a.merged ? const_cast<cplx<T>*>(stage) + (long)s * a.nks : buf + (long)s * SL;
     // c2r split: Z_m = (X_m + conj X_{M-m}) + i W^{-m} (X_m - conj X_{M-m}),
     // imaginary parts of the DC and Nyquist bins ignored
     cplx<T> v[E];

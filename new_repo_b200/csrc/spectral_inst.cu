@@ -41,17 +41,57 @@ static int resident_ctas(const void* kern, int threads, size_t smem) {
 }
 
 
+// registers per thread of `kern` on the current device (fixed table, as above)
+static int kernel_regs(const void* kern) {
+  static std::mutex mu;
+  static struct {
+    int dev;
+    const void* kern;
+    int regs;
+  } table[128];
+  static int used = 0;
+  int dev = 0;
+  LES_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  for (int i = 0; i < used; ++i)
+    if (table[i].dev == dev && table[i].kern == kern) return table[i].regs;
+  cudaFuncAttributes fa;
+  LES_CUDA(cudaFuncGetAttributes(&fa, kern));
+  if (used < 128) table[used++] = {dev, kern, fa.numRegs};
+  return fa.numRegs;
+}
+
 namespace {
 constexpr int SMEM_CAP = 200 * 1024;
+constexpr size_t SM_SMEM = 228 * 1024;  // shared memory per SM (1 KB of it reserved per CTA)
 
-template <typename T>
-int rows_per_cta(int nseq_per_row, int M, int target_bytes = 32 * 1024) {
-  // keep the in-place sequence buffer near target_bytes so several CTAs fit on an SM
-  const int target = int(target_bytes / sizeof(cplx<T>));
-  int R = target / (nseq_per_row * M);
-  if (R < 1) R = 1;
-  if (R > 32) R = 32;
-  return R;
+// Rows per work item of an x pass (256-thread CTAs, TL lanes per sequence,
+// seq_per_row sequences per grid row): the count that keeps the most sequence
+// slots of an SM busy -- resident CTAs (shared memory, registers) times the
+// fraction of the 256 / TL slots of each pass that hold a sequence; on a tie
+// the larger count (fewer items).
+template <typename SmemFn>
+int best_rows(const void* kern, int seq_per_row, int TL, SmemFn smem_for, int rmax = 32) {
+  const int regs = kernel_regs(kern);
+  const int warp_regs = ((regs * 32 + 255) / 256) * 256;
+  const int by_regs = std::max(1, 65536 / (warp_regs * 8));
+  const int S = 256 / TL;
+  double best = -1.0;
+  int best_r = 1;
+  for (int R = 1; R <= rmax; ++R) {
+    const size_t sm = smem_for(R);
+    if (sm > SMEM_CAP) break;
+    const int ctas = std::min({int(SM_SMEM / (sm + 1024)), by_regs, 8});
+    if (ctas < 1) break;
+    const int nseq = R * seq_per_row;
+    const int passes = (nseq + S - 1) / S;
+    const double score = ctas * double(nseq) / double(passes * S);
+    if (score >= best - 1e-9) {
+      best = score;
+      best_r = R;
+    }
+  }
+  return best_r;
 }
 
 // lanes per sequence of the register FFT of length n (fft2.cuh plans)
@@ -121,12 +161,6 @@ static void launch_xfwd_st(int NX, XFArgs<T>& a, cudaStream_t st) {
            2 * sizeof(S) * (size_t)R * a.nsrc * NX +
            sizeof(T) * R * a.nf + 2 * sizeof(int) * R + 16;
   };
-  a.R = std::min(32, std::max(rows_per_cta<T>(a.nf, M), ceil_div(256 / lanes(M), a.nf)));
-  while (a.R > 1 && smem_for(a.R) > 100 * 1024) --a.R;
-  const size_t smem = smem_for(a.R);
-  if (smem > SMEM_CAP) throw CudaError(1, "xfwd: shared memory request too large");
-  const long nitems = ceil_div(a.nrows, a.R);
-  if (nitems == 0) return;
   void (*kern)(XFArgs<T>) = nullptr;
   switch (NX) {
 #define XS_CASE(N) \
@@ -136,6 +170,11 @@ static void launch_xfwd_st(int NX, XFArgs<T>& a, cudaStream_t st) {
     default:
       throw CudaError(1, "xfwd: unsupported transform length " + std::to_string(NX));
   }
+  a.R = best_rows((const void*)kern, a.nf, lanes(M), smem_for);
+  const size_t smem = smem_for(a.R);
+  if (smem > SMEM_CAP) throw CudaError(1, "xfwd: shared memory request too large");
+  const long nitems = ceil_div(a.nrows, a.R);
+  if (nitems == 0) return;
   const int grid = int(std::min<long>(nitems, (long)resident_ctas((const void*)kern, 256, smem)));
   kern<<<grid, 256, smem, st>>>(a);
   LES_CHECK_LAUNCH();
@@ -163,12 +202,23 @@ void launch_xfwd(int NX, XFArgs<T> a, cudaStream_t st) {
     hook_after();
     return;
   }
-  a.R = rows_per_cta<T>(a.nf, M);
   a.in_rstride = NX;
   const int SL = slot_stride(M, int(sizeof(cplx<T>)));
-  const size_t smem = sizeof(cplx<T>) * (NX + twm_len(M, false) + (size_t)pad_seqs(a.R * a.nf, M) * SL) +
-                      sizeof(T) * a.R * a.nf +
-                      2 * sizeof(int) * a.R + 16;
+  auto smem_for = [&](int R) {
+    return sizeof(cplx<T>) * (NX + twm_len(M, false) + (size_t)pad_seqs(R * a.nf, M) * SL) + sizeof(T) * R * a.nf +
+           2 * sizeof(int) * R + 16;
+  };
+  void (*kern)(XFArgs<T>) = nullptr;
+  switch (NX) {
+#define XF_CASE(N) \
+  case N: kern = k_xfwd<T, N>; break;
+    LES_LENGTHS(XF_CASE)
+#undef XF_CASE
+    default:
+      throw CudaError(1, "xfwd: unsupported transform length " + std::to_string(NX));
+  }
+  a.R = best_rows((const void*)kern, a.nf, lanes(M), smem_for);
+  const size_t smem = smem_for(a.R);
   if (smem > SMEM_CAP) throw CudaError(1, "xfwd: shared memory request too large");
   const int grid = ceil_div(a.nrows, a.R);
   if (grid == 0) return;
@@ -176,14 +226,7 @@ void launch_xfwd(int NX, XFArgs<T> a, cudaStream_t st) {
   const int nin = (a.op == XF_SCALE || a.op == XF_PRESS) ? a.nf : nin_of_op[a.op];
   const size_t isz = (a.in_f32 ? sizeof(float) : sizeof(T));
   hook_before("xfwd", double(a.nrows) * NX * nin * isz + double(a.nrows) * a.nf * a.nk * sizeof(cplx<T>));
-  switch (NX) {
-#define XF_CASE(N) \
-  case N: k_xfwd<T, N><<<grid, 256, smem, st>>>(a); break;
-    LES_LENGTHS(XF_CASE)
-#undef XF_CASE
-    default:
-      throw CudaError(1, "xfwd: unsupported transform length " + std::to_string(NX));
-  }
+  kern<<<grid, 256, smem, st>>>(a);
   LES_CHECK_LAUNCH();
   hook_after();
 }
@@ -208,16 +251,17 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
     a.nks = a.nk;
     if (TL < W) a.nks += ((TL % W - a.nk % W) % W + W) % W;
   }
+  // a plain store with one staged row per sequence transforms each sequence
+  // in its own staged row (the exchange slot is the row), which leaves room
+  // for more rows per work item
+  a.merged = (a.op == XI_STORE && a.nstage == 0) ? 1 : 0;
+  if (a.merged) a.nks = std::max(a.nks, SL);
+  auto stage_rows = [&](int R) { return a.merged ? pad_seqs(R * a.nin, M) : R * ns; };
   auto smem_for = [&](int R) {
-    return sizeof(cplx<T>) * (NX + twm_len(M, true) + 2 * (size_t)R * ns * a.nks + (size_t)pad_seqs(R * a.nin, M) * SL) +
+    return sizeof(cplx<T>) * (NX + twm_len(M, true) + 2 * (size_t)stage_rows(R) * a.nks +
+                              (a.merged ? 0 : (size_t)pad_seqs(R * a.nin, M) * SL)) +
            2 * sizeof(int) * R + (a.nstage ? sizeof(T) * (a.nk + 2) : 0);
   };
-  a.R = std::min(32, std::max(rows_per_cta<T>(a.nin, M), ceil_div(256 / lanes(M), a.nin)));
-  while (a.R > 1 && smem_for(a.R) > 100 * 1024) --a.R;
-  const size_t smem = smem_for(a.R);
-  if (smem > SMEM_CAP) throw CudaError(1, "xinv: shared memory request too large");
-  const long nitems = ceil_div(a.nrows, a.R);
-  if (nitems == 0) return;
   void (*kern)(XIArgs<T>) = nullptr;
   switch (NX) {
 #define XI_CASE(N) \
@@ -227,6 +271,12 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
     default:
       throw CudaError(1, "xinv: unsupported transform length " + std::to_string(NX));
   }
+  a.R = best_rows((const void*)kern, a.nin, lanes(M), smem_for);
+  a.stage_rows = stage_rows(a.R);
+  const size_t smem = smem_for(a.R);
+  if (smem > SMEM_CAP) throw CudaError(1, "xinv: shared memory request too large");
+  const long nitems = ceil_div(a.nrows, a.R);
+  if (nitems == 0) return;
   const int grid = int(std::min<long>(nitems, (long)resident_ctas((const void*)kern, 256, smem)));
   {
     const size_t osz = (a.out_f32 ? sizeof(float) : sizeof(T));
