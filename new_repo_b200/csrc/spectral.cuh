@@ -607,7 +607,7 @@ enum YPOp : int {
 template <typename T>
 struct YPArgs {
   int op, nin, nout, C, lc;  // C = 1 << lc columns per CTA
-  int SI, SO;                // column strides of the shared input / output staging
+  int SI;                    // column stride of the shared stages (>= both lengths' slots)
   int ncols;           // columns processed
   int ncols1;          // columns stored for the second FILTER2 output
   int nk_in, nk_out, nk_out1;
@@ -706,12 +706,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPA
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* twi = reinterpret_cast<cplx<T>*>(smem_raw);  // twiddle matrices, forward NY
   cplx<T>* two = twi + Twm<NY, false>::len;                 // and inverse NYO
-  const int SI = a.SI;  // >= NY
-  const int SO = a.SO;  // >= NYO
+  const int SI = a.SI;  // >= the slots of NY and NYO
   const int C = a.C;
   cplx<T>* bin0 = two + Twm<NYO, true>::len;  // input stage 0: [nin][C][SI]
   cplx<T>* bin1 = bin0 + a.nin * C * SI;   // input stage 1
-  cplx<T>* bout = bin1 + a.nin * C * SI;   // [C][SO]
+  // the inverse transform, its output layout and the coalesced copy-out use
+  // the first input row of each column of the current stage, free once the
+  // forward transforms hold their values in registers
   twm_build<T, NY, false>(a.tw_in, twi, threadIdx.x, blockDim.x);
   twm_build<T, NYO, true>(a.tw_out, two, threadIdx.x, blockDim.x);
   // persistent CTAs: work item = (column block, plane, group); the columns
@@ -788,7 +789,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPA
       }
     }
   }
-  cplx<T>* sout = bout + c * SO;
+  __syncwarp();  // the column's forward reads are done before its slot is rewritten
+  cplx<T>* sout = bin + c * SI;
   for (int q = 0; q < a.nout; ++q) {
     if constexpr (SAME) {
       // forward output layout (groups FO) == inverse input layout; the
@@ -856,7 +858,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPA
         const int ky0 = threadIdx.x >> a.lc, kstep = blockDim.x >> a.lc;
         const long opitch = second ? a.opitch1 : a.opitch;
         cplx<T>* dst = a.out[grp * a.nout + q] + (long)l * (second ? a.out_pstride1 : a.out_pstride) + kxx;
-        const cplx<T>* srow = bout + cc * SO;
+        const cplx<T>* srow = bin + cc * SI;
         for (int ky = ky0; ky < NYO; ky += kstep) dst[(long)ky * opitch] = srow[ky];
       }
     }

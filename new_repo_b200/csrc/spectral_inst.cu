@@ -298,33 +298,21 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
   if (a.opitch1 == 0) a.opitch1 = a.nk_out1;
   const int TL = lanes(NY);
   if (lanes(NYO) != TL) throw CudaError(1, "ypass: length pair with different lane counts");
-  // column stride of the shared staging buffers: the load and store loops
-  // run c (column) fastest and 32/C rows per warp, so a stride congruent to
-  // 32/C modulo the complex values per 128-byte wavefront spreads a warp
-  // evenly over the banks
+  // column stride of the shared stages: the load and store loops run c
+  // (column) fastest and 32/C rows per warp, so a stride congruent to 32/C
+  // modulo the complex values per 128-byte wavefront spreads a warp evenly
+  // over the banks; room for the padded exchange layout of the longer of the
+  // two transforms (the inverse runs in the first input row of each column)
   const int W = 128 / int(sizeof(cplx<T>));
-  auto stride = [&](int n, int C) {
+  const int NL = std::max(NY, NYO);
+  auto stride = [&](int C) {
     const int target = (32 / C) % W;
-    const int base = n + n / 16;  // room for the FFT's padded exchange layout
+    const int base = NL + NL / 16;
     return base + ((target - base % W) % W + W) % W;
   };
-  auto per_col = [&](int C) {  // two input stages + the output slot
-    return (size_t)(2 * a.nin * stride(NY, C) + stride(NYO, C)) * sizeof(cplx<T>);
+  auto smem_for = [&](int C) {  // twiddle matrices + two stages of nin rows per column
+    return sizeof(cplx<T>) * (twm_len(NY, false) + twm_len(NYO, true) + (size_t)C * 2 * a.nin * stride(C));
   };
-  int lc = 0;  // C = 1 << lc columns per CTA, C * TL <= 256 threads, two CTAs per SM
-  while ((2 << lc) * TL <= 256 && (size_t(2) << lc) * per_col(2 << lc) <= 112 * 1024 && (1 << lc) < a.ncols) ++lc;
-  while ((1 << lc) * TL < 32) ++lc;  // at least one full warp
-  a.lc = lc;
-  a.C = 1 << lc;
-  a.SI = stride(NY, a.C);
-  a.SO = stride(NYO, a.C);
-  const size_t smem = sizeof(cplx<T>) * (twm_len(NY, false) + twm_len(NYO, true)) + (size_t)a.C * per_col(a.C);
-  if (smem > SMEM_CAP) throw CudaError(1, "ypass: shared memory request too large");
-  const int threads = a.C * TL;
-  a.nplanes = nplanes;
-  a.ngroups = ngroups;
-  const long nitems = (long)ceil_div(a.ncols, a.C) * nplanes * ngroups;
-  if (nitems == 0) return;
   const int key = NY * 10000 + NYO;
   void (*kern)(YPArgs<T>) = nullptr;
   switch (key) {
@@ -337,6 +325,40 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
     default:
       throw CudaError(1, "ypass: unsupported length pair " + std::to_string(NY) + "->" + std::to_string(NYO));
   }
+  // columns per CTA (C * TL threads, at least a warp): the most busy warps
+  // per SM -- resident CTAs (shared memory, registers, threads) times the
+  // warps whose columns exist; on a tie the larger C
+  {
+    const int regs = kernel_regs((const void*)kern);
+    double best = -1.0;
+    int best_lc = 0;
+    while ((1 << best_lc) * TL < 32) ++best_lc;  // at least one full warp
+    for (int lc = 0; (1 << lc) * TL <= 256; ++lc) {
+      const int C = 1 << lc, threads = C * TL;
+      if (threads < 32) continue;
+      const size_t sm = smem_for(C);
+      if (sm > SMEM_CAP) break;
+      const int warp_regs = ((regs * 32 + 255) / 256) * 256;
+      const int by_regs = 65536 / (warp_regs * (threads / 32));
+      const int ctas = std::min({int(SM_SMEM / (sm + 1024)), by_regs, 2048 / threads, 32});
+      if (ctas < 1) break;
+      const double busy = ctas * double(threads / 32) * std::min(1.0, double(a.ncols) / C);
+      if (busy >= best - 1e-9) {
+        best = busy;
+        best_lc = lc;
+      }
+    }
+    a.lc = best_lc;
+  }
+  a.C = 1 << a.lc;
+  a.SI = stride(a.C);
+  const size_t smem = smem_for(a.C);
+  if (smem > SMEM_CAP) throw CudaError(1, "ypass: shared memory request too large");
+  const int threads = a.C * TL;
+  a.nplanes = nplanes;
+  a.ngroups = ngroups;
+  const long nitems = (long)ceil_div(a.ncols, a.C) * nplanes * ngroups;
+  if (nitems == 0) return;
   // persistent grid: the CTAs that fit on the device at once
   const int grid = int(std::min<long>(nitems, (long)resident_ctas((const void*)kern, threads, smem)));
   hook_before("ypass", double(nplanes) * ngroups * a.ncols * sizeof(cplx<T>) *
