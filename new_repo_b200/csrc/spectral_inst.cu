@@ -2,6 +2,7 @@
 // transform length (2^a 3^b: the grid sizes 16..512 and their 3/2 padding).
 #include "spectral.cuh"
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <mutex>
 
@@ -327,12 +328,14 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
   }
   // columns per CTA (C * TL threads, at least a warp): the most busy warps
   // per SM -- resident CTAs (shared memory, registers, threads) times the
-  // warps whose columns exist; on a tie the larger C
+  // warps whose columns exist; on a tie the CTA size nearest 128 threads
+  // (measured at 256^3: 128-thread CTAs beat 64 and 256 at equal occupancy)
   {
     const int regs = kernel_regs((const void*)kern);
     double best = -1.0;
     int best_lc = 0;
     while ((1 << best_lc) * TL < 32) ++best_lc;  // at least one full warp
+    auto off128 = [&](int lc) { return std::abs(std::log2(double((1 << lc) * TL) / 128.0)); };
     for (int lc = 0; (1 << lc) * TL <= 256; ++lc) {
       const int C = 1 << lc, threads = C * TL;
       if (threads < 32) continue;
@@ -343,7 +346,7 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
       const int ctas = std::min({int(SM_SMEM / (sm + 1024)), by_regs, 2048 / threads, 32});
       if (ctas < 1) break;
       const double busy = ctas * double(threads / 32) * std::min(1.0, double(a.ncols) / C);
-      if (busy >= best - 1e-9) {
+      if (busy > best + 1e-9 || (busy > best - 1e-9 && off128(lc) < off128(best_lc))) {
         best = busy;
         best_lc = lc;
       }
