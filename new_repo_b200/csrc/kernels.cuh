@@ -27,10 +27,61 @@ __global__ void k_set_bc(T* u, T* v, T* w, const T* lu, const T* lv, const T* lw
 
 // ddz_uv (uvp -> w, k = 1..nz+1) for u, v and ddz_w (w -> uvp, k = 1..nz,
 // top level zero) for w (compute_derivatives.f90:375-441).
+// four consecutive values (16-byte aligned for FP32, 32-byte for FP64)
+__device__ __forceinline__ void ld4(const float* p, float* o) {
+  const float4 x = *reinterpret_cast<const float4*>(p);
+  o[0] = x.x;
+  o[1] = x.y;
+  o[2] = x.z;
+  o[3] = x.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double* o) {
+  const double2 x = reinterpret_cast<const double2*>(p)[0], y = reinterpret_cast<const double2*>(p)[1];
+  o[0] = x.x;
+  o[1] = x.y;
+  o[2] = y.x;
+  o[3] = y.y;
+}
+__device__ __forceinline__ void st4(float* p, const float* v) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double* v) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+
 template <typename T>
 __global__ void k_ddz_vel(const T* u, const T* v, const T* w, T* dudz, T* dvdz, T* dwdz, long plane, int nz,
                           T rdz) {
   const long n = (long)(nz + 1) * plane;
+  if (plane % 4 == 0) {  // four consecutive points (one level) per thread, vector loads and stores
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n / 4; q += (long)gridDim.x * blockDim.x) {
+      const long o = plane + 4 * q;
+      const int k = int(o / plane);
+      T a[4], b[4], r[4];
+      ld4(u + o, a);
+      ld4(u + o - plane, b);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r[i] = rdz * (a[i] - b[i]);
+      st4(dudz + o, r);
+      ld4(v + o, a);
+      ld4(v + o - plane, b);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r[i] = rdz * (a[i] - b[i]);
+      st4(dvdz + o, r);
+      if (k <= nz) {
+        ld4(w + o + plane, a);
+        ld4(w + o, b);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) r[i] = rdz * (a[i] - b[i]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) r[i] = T(0);
+      }
+      st4(dwdz + o, r);
+    }
+    return;
+  }
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const long o = plane + q;  // levels 1..nz+1
     const int k = int(o / plane);
@@ -352,6 +403,32 @@ template <typename T>
 __global__ void k_ab2(T* u, T* v, T* w, const T* rx, const T* ry, const T* rz, const T* fx, const T* fy,
                       const T* fz, long plane, int nz, T dt, T t1, T t2) {
   const long n = (long)(nz + 2) * plane;
+  if (plane % 4 == 0) {  // four consecutive points (one level) per thread
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n / 4; q += (long)gridDim.x * blockDim.x) {
+      const long o = 4 * q;
+      const int k = int(o / plane);
+      T x[4], r[4], f[4];
+      if (k >= 1 && k <= nz) {
+        T* fld[3] = {u, v, w};
+        const T* rr[3] = {rx, ry, rz};
+        const T* ff[3] = {fx, fy, fz};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          ld4(fld[c] + o, x);
+          ld4(rr[c] + o, r);
+          ld4(ff[c] + o, f);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) x[i] = x[i] + dt * (t1 * r[i] + t2 * f[i]);
+          st4(fld[c] + o, x);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) x[i] = T(0);
+        st4(w + o, x);  // w(0) = w(nz+1) = 0
+      }
+    }
+    return;
+  }
   for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n; o += (long)gridDim.x * blockDim.x) {
     const int k = int(o / plane);
     if (k >= 1 && k <= nz) {
@@ -369,6 +446,40 @@ template <typename T>
 __global__ void k_projection(T* u, T* v, T* w, T* rx, T* ry, T* rz, const T* dpdx, const T* dpdy, const T* dpdz,
                              long plane, int nz, T dtt) {
   const long n = (long)(nz + 2) * plane;
+  if (plane % 4 == 0) {  // four consecutive points (one level) per thread
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n / 4; q += (long)gridDim.x * blockDim.x) {
+      const long o = 4 * q;
+      const int k = int(o / plane);
+      T x[4], d[4], r[4];
+      if (k >= 1 && k <= nz) {
+        T* fld[3] = {u, v, w};
+        T* rr[3] = {rx, ry, rz};
+        const T* dd[3] = {dpdx, dpdy, dpdz};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          ld4(dd[c] + o, d);
+          ld4(rr[c] + o, r);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) r[i] = r[i] - d[i];
+          st4(rr[c] + o, r);
+          if (c == 2 && k == 1) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) x[i] = T(0);
+          } else {
+            ld4(fld[c] + o, x);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) x[i] = x[i] - dtt * d[i];
+          }
+          st4(fld[c] + o, x);
+        }
+      } else if (k == nz + 1) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) x[i] = T(0);
+        st4(w + o, x);
+      }
+    }
+    return;
+  }
   for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n; o += (long)gridDim.x * blockDim.x) {
     const int k = int(o / plane);
     if (k >= 1 && k <= nz) {
@@ -602,22 +713,6 @@ __device__ __forceinline__ void diag_block_reduce(DiagAcc& a) {
       o.nan = r[13];
       a.merge(o);
     }
-}
-
-// four consecutive values (16-byte aligned for FP32, 32-byte for FP64)
-__device__ __forceinline__ void ld4(const float* p, float* o) {
-  const float4 x = *reinterpret_cast<const float4*>(p);
-  o[0] = x.x;
-  o[1] = x.y;
-  o[2] = x.z;
-  o[3] = x.w;
-}
-__device__ __forceinline__ void ld4(const double* p, double* o) {
-  const double2 x = reinterpret_cast<const double2*>(p)[0], y = reinterpret_cast<const double2*>(p)[1];
-  o[0] = x.x;
-  o[1] = x.y;
-  o[2] = y.x;
-  o[3] = y.y;
 }
 
 template <typename T>
