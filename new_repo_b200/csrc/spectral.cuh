@@ -691,8 +691,12 @@ __device__ __forceinline__ void yp_issue(const YPArgs<T>& a, long item, int ncb,
   }
 }
 
-template <typename T, int NY, int NYO>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPArgs<T> a) {
+// FWD: forward transform only (YP_FWDKILL), compiled without the inverse so
+// that it keeps fewer registers (more resident warps)
+template <typename T, int NY, int NYO, bool FWD = false>
+__global__ void __launch_bounds__((FWD && sizeof(T) == 8) ? 128 : 256,
+                                  (FWD && sizeof(T) == 8) ? 3 : (sizeof(T) == 4 ? 2 : 1))
+    k_ypass(const YPArgs<T> a) {
   constexpr int TL = Geo<NY>::T;
   static_assert(Geo<NYO>::T == TL, "pad/truncate pairs must share the lanes per sequence");
   constexpr int EI = Geo<NY>::E;
@@ -713,8 +717,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPA
   // the inverse transform, its output layout and the coalesced copy-out use
   // the first input row of each column of the current stage, free once the
   // forward transforms hold their values in registers
+  static_assert(!FWD || NY == NYO, "forward-only y passes keep the length");
   twm_build<T, NY, false>(a.tw_in, twi, threadIdx.x, blockDim.x);
-  twm_build<T, NYO, true>(a.tw_out, two, threadIdx.x, blockDim.x);
+  if constexpr (!FWD) twm_build<T, NYO, true>(a.tw_out, two, threadIdx.x, blockDim.x);
   // persistent CTAs: work item = (column block, plane, group); the columns
   // of the next item are copied into the other input stage asynchronously
   // while this one is transformed
@@ -795,7 +800,18 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPA
     if constexpr (SAME) {
       // forward output layout (groups FO) == inverse input layout; the
       // stress divergence already holds its result in w
-      if (a.op != YP_DIV2) {
+      if constexpr (FWD) {
+        // YP_FWDKILL: the killed forward output goes straight to the slot in
+        // the forward output layout (groups FO)
+#pragma unroll
+        for (int g = 0; g < EI / FO; ++g)
+#pragma unroll
+          for (int r = 0; r < FO; ++r) {
+            const int ky = lt + TL * g + r * (NY / FO);
+            const bool kill = (ky == NY / 2) || (kx == a.nxh) || (kx >= a.ncols);
+            sout[lt + TL * g + r * (NYO / FO)] = kill ? cplx<T>{T(0), T(0)} : f0[g * FO + r];
+          }
+      } else if (a.op != YP_DIV2) {
 #pragma unroll
         for (int g = 0; g < EI / FO; ++g)
 #pragma unroll
@@ -832,12 +848,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_ypass(const YPA
         }
       });
     }
-    if (a.op == YP_FWDKILL) {
-      // no inverse: the op output is in the forward output layout (groups FO)
-#pragma unroll
-      for (int g = 0; g < EO / FO; ++g)
-#pragma unroll
-        for (int r = 0; r < FO; ++r) sout[lt + TL * g + r * (NYO / FO)] = w[g * FO + r];
+    if constexpr (FWD) {
+      // no inverse: stored above
     } else {
       reg_fft<T, NYO, true>(w, sout, lt, two);
       __syncwarp();

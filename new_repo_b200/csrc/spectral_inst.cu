@@ -42,25 +42,31 @@ static int resident_ctas(const void* kern, int threads, size_t smem) {
 }
 
 
-// registers per thread of `kern` on the current device (fixed table, as above)
-static int kernel_regs(const void* kern) {
+// registers per thread and the largest CTA of `kern` on the current device
+// (fixed table, as above)
+struct KernelLimits {
+  int regs, max_threads;
+};
+static KernelLimits kernel_limits(const void* kern) {
   static std::mutex mu;
   static struct {
     int dev;
     const void* kern;
-    int regs;
+    KernelLimits lim;
   } table[128];
   static int used = 0;
   int dev = 0;
   LES_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lock(mu);
   for (int i = 0; i < used; ++i)
-    if (table[i].dev == dev && table[i].kern == kern) return table[i].regs;
+    if (table[i].dev == dev && table[i].kern == kern) return table[i].lim;
   cudaFuncAttributes fa;
   LES_CUDA(cudaFuncGetAttributes(&fa, kern));
-  if (used < 128) table[used++] = {dev, kern, fa.numRegs};
-  return fa.numRegs;
+  const KernelLimits lim{fa.numRegs, fa.maxThreadsPerBlock};
+  if (used < 128) table[used++] = {dev, kern, lim};
+  return lim;
 }
+static int kernel_regs(const void* kern) { return kernel_limits(kern).regs; }
 
 namespace {
 constexpr int SMEM_CAP = 200 * 1024;
@@ -292,6 +298,14 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
   hook_after();
 }
 
+// the y-pass kernel of a length pair; the forward-only variant exists for
+// equal lengths (nullptr otherwise)
+template <typename T, int A, int B>
+static void (*ypass_kernel(bool fwd))(YPArgs<T>) {
+  if constexpr (A == B) return fwd ? k_ypass<T, A, A, true> : k_ypass<T, A, B>;
+  else return fwd ? nullptr : k_ypass<T, A, B>;
+}
+
 template <typename T>
 void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaStream_t st) {
   if (a.ipitch == 0) a.ipitch = a.nk_in;
@@ -315,10 +329,11 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
     return sizeof(cplx<T>) * (twm_len(NY, false) + twm_len(NYO, true) + (size_t)C * 2 * a.nin * stride(C));
   };
   const int key = NY * 10000 + NYO;
+  const bool fwd = (a.op == YP_FWDKILL);
   void (*kern)(YPArgs<T>) = nullptr;
   switch (key) {
 #define YP_CASE(A, B) \
-  case A * 10000 + B: kern = k_ypass<T, A, B>; break;
+  case A * 10000 + B: kern = ypass_kernel<T, A, B>(fwd); break;
     YP_CASE(16, 16) YP_CASE(32, 32) YP_CASE(64, 64) YP_CASE(128, 128) YP_CASE(256, 256) YP_CASE(512, 512)
     YP_CASE(16, 24) YP_CASE(32, 48) YP_CASE(64, 96) YP_CASE(128, 192) YP_CASE(256, 384) YP_CASE(512, 768)
     YP_CASE(24, 16) YP_CASE(48, 32) YP_CASE(96, 64) YP_CASE(192, 128) YP_CASE(384, 256) YP_CASE(768, 512)
@@ -326,17 +341,19 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
     default:
       throw CudaError(1, "ypass: unsupported length pair " + std::to_string(NY) + "->" + std::to_string(NYO));
   }
+  if (!kern) throw CudaError(1, "ypass: a forward-only pass keeps the length");
   // columns per CTA (C * TL threads, at least a warp): the most busy warps
   // per SM -- resident CTAs (shared memory, registers, threads) times the
   // warps whose columns exist; on a tie the CTA size nearest 128 threads
   // (measured at 256^3: 128-thread CTAs beat 64 and 256 at equal occupancy)
   {
-    const int regs = kernel_regs((const void*)kern);
+    const KernelLimits lim = kernel_limits((const void*)kern);
+    const int regs = lim.regs;
     double best = -1.0;
     int best_lc = 0;
     while ((1 << best_lc) * TL < 32) ++best_lc;  // at least one full warp
     auto off128 = [&](int lc) { return std::abs(std::log2(double((1 << lc) * TL) / 128.0)); };
-    for (int lc = 0; (1 << lc) * TL <= 256; ++lc) {
+    for (int lc = 0; (1 << lc) * TL <= std::min(256, lim.max_threads); ++lc) {
       const int C = 1 << lc, threads = C * TL;
       if (threads < 32) continue;
       const size_t sm = smem_for(C);
@@ -383,6 +400,10 @@ static void set_attrs() {
 #undef XA
 #define YA(A, B) \
   LES_CUDA(cudaFuncSetAttribute(k_ypass<T, A, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_CAP));
+#define YF(A) \
+  LES_CUDA(cudaFuncSetAttribute(k_ypass<T, A, A, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_CAP));
+  YF(16) YF(32) YF(64) YF(128) YF(256) YF(512)
+#undef YF
   YA(16, 16) YA(32, 32) YA(64, 64) YA(128, 128) YA(256, 256) YA(512, 512)
   YA(16, 24) YA(32, 48) YA(64, 96) YA(128, 192) YA(256, 384) YA(512, 768)
   YA(24, 16) YA(48, 32) YA(96, 64) YA(192, 128) YA(384, 256) YA(768, 512)
