@@ -182,6 +182,128 @@ __device__ __forceinline__ T strain_norm(const T s[6]) {
   return sqrt(T(2) * (s[0] * s[0] + s[3] * s[3] + s[5] * s[5] + T(2) * (s[1] * s[1] + s[2] * s[2] + s[4] * s[4])));
 }
 
+// sij_at for four consecutive points of one level (16-byte aligned offset),
+// the same arithmetic per point: s[c][i] is component c at point o + i
+template <typename T>
+__device__ __forceinline__ void sij_at4(const SgsArgs<T>& a, long o, int k, T s[6][4]) {
+  const long pl = a.plane;
+  T d[9][4];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) ld4(a.d[j] + o, d[j]);
+  if (k == 1) {
+    T e2[4], e5[4], e6[4], e7[4];
+    ld4(a.d[6] + o + pl, e6);
+    ld4(a.d[7] + o + pl, e7);
+    if (!a.wall) {
+      ld4(a.d[2] + o + pl, e2);
+      ld4(a.d[5] + o + pl, e5);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const T ux = d[0][i], uy = d[1][i];
+      const T uz = a.wall ? d[2][i] : T(0.5) * (d[2][i] + e2[i]);
+      const T vz = a.wall ? d[5][i] : T(0.5) * (d[5][i] + e5[i]);
+      const T vx = d[3][i], vy = d[4][i];
+      const T wx = T(0.5) * (d[6][i] + e6[i]), wy = T(0.5) * (d[7][i] + e7[i]), wz = d[8][i];
+      s[0][i] = ux;
+      s[1][i] = T(0.5) * (uy + vx);
+      s[2][i] = T(0.5) * (uz + wx);
+      s[3][i] = vy;
+      s[4][i] = T(0.5) * (vz + wy);
+      s[5][i] = wz;
+    }
+  } else {
+    T p0[4], p1[4], p3[4], p4[4], p8[4];
+    ld4(a.d[0] + o - pl, p0);
+    ld4(a.d[1] + o - pl, p1);
+    ld4(a.d[3] + o - pl, p3);
+    ld4(a.d[4] + o - pl, p4);
+    ld4(a.d[8] + o - pl, p8);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const T ux = T(0.5) * (d[0][i] + p0[i]), uy = T(0.5) * (d[1][i] + p1[i]), uz = d[2][i];
+      const T vx = T(0.5) * (d[3][i] + p3[i]), vy = T(0.5) * (d[4][i] + p4[i]), vz = d[5][i];
+      const T wx = d[6][i], wy = d[7][i], wz = T(0.5) * (d[8][i] + p8[i]);
+      s[0][i] = ux;
+      s[1][i] = T(0.5) * (uy + vx);
+      s[2][i] = T(0.5) * (uz + wx);
+      s[3][i] = vy;
+      s[4][i] = T(0.5) * (vz + wy);
+      s[5][i] = wz;
+    }
+  }
+}
+
+// k_sgs_tau with four consecutive points per thread (plane a multiple of 4):
+// grid (ceil(plane / 4 / 256), nz + 1)
+template <typename T>
+__global__ void k_sgs_tau4(const SgsArgs<T> a) {
+  const long pl = a.plane;
+  const long p = 4 * (blockIdx.x * (long)blockDim.x + threadIdx.x);
+  if (p >= pl) return;
+  const int k = 1 + blockIdx.y;
+  const long o = (long)k * pl + p;
+  T s[6][4], cs[4], nu[4], d0[4], d1[4], d3[4], d4[4], d8[4], r[4];
+  sij_at4(a, o, k, s);
+  ld4(a.cs + o, cs);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const T si[6] = {s[0][i], s[1][i], s[2][i], s[3][i], s[4][i], s[5][i]};
+    nu[i] = strain_norm(si) * cs[i] * T(a.l2[k]);
+  }
+  st4(a.nu + o, nu);
+  ld4(a.d[0] + o, d0);
+  ld4(a.d[1] + o, d1);
+  ld4(a.d[3] + o, d3);
+  ld4(a.d[4] + o, d4);
+  ld4(a.d[8] + o, d8);
+  if (k == 1) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) r[i] = T(2) * nu[i] * d8[i];
+    st4(a.tzz + o, r);
+    st4(a.tzz + o - pl, r);  // tzz(0) = tzz(1)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) r[i] = T(2) * nu[i] * d0[i];
+    st4(a.txx + o, r);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) r[i] = T(2) * nu[i] * T(0.5) * (d1[i] + d3[i]);
+    st4(a.txy + o, r);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) r[i] = T(2) * nu[i] * d4[i];
+    st4(a.tyy + o, r);
+  } else {
+    if (k <= a.nz) {
+      T s2[6][4], csp[4], c[4];
+      sij_at4(a, o + pl, k + 1, s2);
+      ld4(a.cs + o + pl, csp);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const T si[6] = {s2[0][i], s2[1][i], s2[2][i], s2[3][i], s2[4][i], s2[5][i]};
+        const T nukp = strain_norm(si) * csp[i] * T(a.l2[k + 1]);
+        c[i] = T(0.5) * (nu[i] + nukp);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r[i] = T(2) * c[i] * d0[i];
+      st4(a.txx + o, r);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r[i] = T(2) * c[i] * T(0.5) * (d1[i] + d3[i]);
+      st4(a.txy + o, r);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r[i] = T(2) * c[i] * d4[i];
+      st4(a.tyy + o, r);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r[i] = T(2) * c[i] * d8[i];
+      st4(a.tzz + o, r);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) r[i] = T(2) * nu[i] * s[2][i];
+    st4(a.txz + o, r);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) r[i] = T(2) * nu[i] * s[4][i];
+    st4(a.tyz + o, r);
+  }
+}
+
 // S_ij and |S| on levels 1..nz+1 (written for the dynamic procedure).
 template <typename T>
 __global__ void k_sij(const SgsArgs<T> a) {

@@ -1463,7 +1463,12 @@ class Solver final : public SolverBase {
     } else {
       throw CudaError(1, "Invalid SGS model");
     }
-    KL("k_sgs_tau", 17.0 * (g.nz + 1) * g.plane() * sizeof(T), k_sgs_tau<T><<<dim3(unsigned((g.plane() + 255) / 256), unsigned(g.nz + 1)), 256, 0, st>>>(a));
+    if (g.plane() % 4 == 0)
+      KL("k_sgs_tau", 17.0 * (g.nz + 1) * g.plane() * sizeof(T),
+         k_sgs_tau4<T><<<dim3(unsigned((g.plane() / 4 + 255) / 256), unsigned(g.nz + 1)), 256, 0, st>>>(a));
+    else
+      KL("k_sgs_tau", 17.0 * (g.nz + 1) * g.plane() * sizeof(T),
+         k_sgs_tau<T><<<dim3(unsigned((g.plane() + 255) / 256), unsigned(g.nz + 1)), 256, 0, st>>>(a));
   }
 
   // dynamic-procedure contractions at both test scales (compute_dynamic_mum x2)
