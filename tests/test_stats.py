@@ -41,6 +41,53 @@ def test_oracle_running_sums_cycle(tmp_path):
     assert not S.stat_averages(rs, st, 3, 12, 12, 4, out)
 
 
+# The reference's own reader of these files (matlab_src/load2decomp_RAV.m with
+# the field list of matlab_src/get_data_struct_RAV.m:13-17), restated: the
+# info file is four whitespace-separated integers, the 3D file the fields one
+# after the other as nx*ny*nz doubles in Fortran order, the 2D file u* as
+# nx*ny doubles; means are the sums over all files divided by the summed
+# iteration counts.
+RAV_READER_3D = ("u", "v", "w", "p", "u2", "v2", "w2", "u3", "v3", "w3", "u4", "v4", "w4",
+                 "uv", "uw", "vw", "txx", "tyy", "tzz", "txy", "txz", "tyz", "dudz", "dvdz", "nut", "cs")
+
+
+def _read_rav(folder, steps, nx, ny, nz):
+    sums3, sums2, nt = None, None, 0
+    for jt in steps:
+        info = [int(x) for x in (folder / f"RAV_{jt:09d}_info.txt").read_text().split()]
+        assert info[:3] == [nx, ny, nz]
+        nt += info[3]
+        raw = np.fromfile(folder / f"RAV_{jt:09d}_3D.dat", dtype="<f8")
+        assert raw.size == len(RAV_READER_3D) * nx * ny * nz
+        d3 = {n: raw[q * nx * ny * nz:(q + 1) * nx * ny * nz].reshape((nx, ny, nz), order="F")
+              for q, n in enumerate(RAV_READER_3D)}
+        d2 = np.fromfile(folder / f"RAV_{jt:09d}_2D.dat", dtype="<f8").reshape((nx, ny), order="F")
+        sums3 = d3 if sums3 is None else {n: sums3[n] + d3[n] for n in d3}
+        sums2 = d2 if sums2 is None else sums2 + d2
+    return {n: v / nt for n, v in sums3.items()}, sums2 / nt, nt
+
+
+def test_rav_files_follow_the_reference_reader(tmp_path):
+    assert S.STAT_NAMES == RAV_READER_3D
+    p = O.Params(nx=16, ny=8, nz=4)
+    ops, st = _state(p, 3)
+    rs = S.RunningStats(p)
+    out = str(tmp_path) + "/"
+    us, ws = [], []
+    for jt in range(1, 7):  # two files: RAV_3 (3 iterations) and RAV_6 (3 iterations)
+        st.u = st.u * 1.01  # a changing state
+        st.w = st.w + 0.001
+        us.append(st.u[1:p.nz + 1].copy())
+        ws.append(st.w[1:p.nz + 1].copy())
+        S.stat_averages(rs, st, jt, jt, 0, 3, out)
+    mean3, mean2, nt = _read_rav(tmp_path, (3, 6), p.nx, p.ny, p.nz)
+    assert nt == 6
+    # the reader's (x, y, z) arrays are the transposes of the oracle's (z, y, x)
+    np.testing.assert_allclose(mean3["u"], np.mean(us, axis=0).transpose(2, 1, 0), rtol=1e-14)
+    np.testing.assert_allclose(mean3["w2"], np.mean([w * w for w in ws], axis=0).transpose(2, 1, 0), rtol=1e-14)
+    np.testing.assert_allclose(mean2, st.u_star_avg.T, rtol=1e-14)
+
+
 def test_oracle_tke_quirks(tmp_path):
     p = O.Params(nx=16, ny=16, nz=8)
     ops, st = _state(p, 3)
