@@ -25,6 +25,23 @@ def test_oracle_checkpoint_round_trip(tmp_path):
     assert back.f_coeff_init and back.lagran_init
 
 
+def test_checkpoint_follows_the_reference_reader(tmp_path):
+    """The reference's reader (matlab_src/load2decomp_checkpoint.m), restated:
+    u v w RHSx RHSy RHSz Cs_opt2 [F_LM F_MM F_QN F_NN], each nx*ny*(nz+1)
+    doubles in Fortran order (levels 1..nz+1)."""
+    p = O.Params(nx=16, ny=8, nz=4, dyn_init=5, cs_count=5)
+    _, st = oracle_run(p, 10)
+    path = tmp_path / "checkpoint_000000010"
+    O.write_checkpoint(st, path)
+    raw = np.fromfile(path, dtype="<f8")
+    n = p.nx * p.ny * (p.nz + 1)
+    names = ("u", "v", "w", "rhsx", "rhsy", "rhsz", "cs_opt2", "F_LM", "F_MM", "F_QN", "F_NN")
+    assert raw.size == len(names) * n
+    for q, name in enumerate(names):
+        arr = raw[q * n:(q + 1) * n].reshape((p.nx, p.ny, p.nz + 1), order="F")
+        np.testing.assert_array_equal(arr, getattr(st, name)[1:].transpose(2, 1, 0), err_msg=name)
+
+
 def test_restart_namelist_round_trip(tmp_path):
     from new_repo_b200 import LesError, RunParams
     from new_repo_b200.les import read_parameters_restart, write_parameters_restart
