@@ -667,6 +667,30 @@ __device__ __forceinline__ cplx<T> yp_op(const YPArgs<T>& a, int q, int kx, int 
   }
 }
 
+// yp_op for an op fixed at compile time, with the wavenumbers of the point
+// given: kxv = kkx(kx) of the thread's column (row 0 of the table) and kyv =
+// kky(ky) of the row (column 0).  The tables hold 2 pi / l times the wrapped
+// index, zeroed on the Nyquist row / column only, so away from those the
+// values are the table's; the kills below reproduce the zeros.
+template <typename T, int NY, int OP>
+__device__ __forceinline__ cplx<T> yp_op_c(const YPArgs<T>& a, int q, int kx, int ky, cplx<T> F0, T kxv, T kyv) {
+  const cplx<T> zero = {T(0), T(0)};
+  if constexpr (OP == YP_GRAD) {
+    if (ky == NY / 2 || kx == a.nxh) return zero;
+    if (q == 0) return F0;
+    if (q == 1) return ik_mul(kxv, F0);
+    return ik_mul(kyv, F0);
+  } else if constexpr (OP == YP_GRADY) {
+    if (ky == NY / 2 || kx == a.nxh) return zero;
+    if (q == 0) return F0;
+    return ik_mul(kyv, F0);
+  } else {  // YP_PGRAD: no kill, the Nyquist row / column of the tables are zero
+    if (q == 0) return ik_mul(ky == NY / 2 ? T(0) : kxv, F0);
+    if (q == 1) return ik_mul(kx == a.nxh ? T(0) : kyv, F0);
+    return F0;
+  }
+}
+
 // y pass: start the copies of work item `item` (C columns x NY rows of every
 // input field) into the shared stage `bin` ([nin][C][SI])
 template <typename T, int NY>
@@ -712,7 +736,8 @@ __global__ void __launch_bounds__((FWD && sizeof(T) == 8) ? 128 : 256,
   cplx<T>* two = twi + Twm<NY, false>::len;                 // and inverse NYO
   const int SI = a.SI;  // >= the slots of NY and NYO
   const int C = a.C;
-  cplx<T>* bin0 = two + Twm<NYO, true>::len;  // input stage 0: [nin][C][SI]
+  T* kyrow = reinterpret_cast<T*>(two + Twm<NYO, true>::len);  // kky(ky), column 0 of the table
+  cplx<T>* bin0 = reinterpret_cast<cplx<T>*>(kyrow + ((NY + 3) & ~3));  // input stage 0: [nin][C][SI]
   cplx<T>* bin1 = bin0 + a.nin * C * SI;   // input stage 1
   // the inverse transform, its output layout and the coalesced copy-out use
   // the first input row of each column of the current stage, free once the
@@ -720,6 +745,8 @@ __global__ void __launch_bounds__((FWD && sizeof(T) == 8) ? 128 : 256,
   static_assert(!FWD || NY == NYO, "forward-only y passes keep the length");
   twm_build<T, NY, false>(a.tw_in, twi, threadIdx.x, blockDim.x);
   if constexpr (!FWD) twm_build<T, NYO, true>(a.tw_out, two, threadIdx.x, blockDim.x);
+  if (a.kky)
+    for (int i = threadIdx.x; i < NY; i += blockDim.x) kyrow[i] = a.kky[(long)i * a.lhx];
   // persistent CTAs: work item = (column block, plane, group); the columns
   // of the next item are copied into the other input stage asynchronously
   // while this one is transformed
@@ -774,7 +801,7 @@ __global__ void __launch_bounds__((FWD && sizeof(T) == 8) ? 128 : 256,
             for (int r = 0; r < FO; ++r) {
               const int ky = lt + TL * g + r * (NY / FO);
               const bool kill = (ky == NY / 2) || (kx == a.nxh) || (kx >= a.ncols);
-              w[g * FO + r] = kill ? zero : ik_mul(a.kkx[ky * a.lhx + kx], f0[g * FO + r]);
+              w[g * FO + r] = kill ? zero : ik_mul(a.kkx[kx], f0[g * FO + r]);
             }
           cplx<T>* seq1 = bin + (C + c) * SI;
 #pragma unroll
@@ -788,7 +815,7 @@ __global__ void __launch_bounds__((FWD && sizeof(T) == 8) ? 128 : 256,
             for (int r = 0; r < FO; ++r) {
               const int ky = lt + TL * g + r * (NY / FO);
               const bool kill = (ky == NY / 2) || (kx == a.nxh) || (kx >= a.ncols);
-              if (!kill) w[g * FO + r] = c_add(w[g * FO + r], ik_mul(a.kky[ky * a.lhx + kx], f0[g * FO + r]));
+              if (!kill) w[g * FO + r] = c_add(w[g * FO + r], ik_mul(kyrow[ky], f0[g * FO + r]));
             }
         }
       }
@@ -812,14 +839,36 @@ __global__ void __launch_bounds__((FWD && sizeof(T) == 8) ? 128 : 256,
             sout[lt + TL * g + r * (NYO / FO)] = kill ? cplx<T>{T(0), T(0)} : f0[g * FO + r];
           }
       } else if (a.op != YP_DIV2) {
+        // the derivative ops with the op fixed per loop (no per-element
+        // dispatch) and the wavenumbers from registers / shared memory
+        const T kxv = (kx < a.ncols && a.kkx) ? a.kkx[kx] : T(0);
+        auto fill = [&](auto opc) {
+          constexpr int OP = decltype(opc)::value;
 #pragma unroll
-        for (int g = 0; g < EI / FO; ++g)
+          for (int g = 0; g < EI / FO; ++g)
 #pragma unroll
-          for (int r = 0; r < FO; ++r) {
-            const int ky = lt + TL * g + r * (NY / FO);
-            w[g * FO + r] = (kx < a.ncols) ? yp_op<T, NY>(a, q, kx, ky, f0[g * FO + r], f0[g * FO + r])
-                                           : cplx<T>{T(0), T(0)};
-          }
+            for (int r = 0; r < FO; ++r) {
+              const int ky = lt + TL * g + r * (NY / FO);
+              w[g * FO + r] = (kx < a.ncols) ? yp_op_c<T, NY, OP>(a, q, kx, ky, f0[g * FO + r], kxv, kyrow[ky])
+                                             : cplx<T>{T(0), T(0)};
+            }
+        };
+        if (a.op == YP_GRADY) {
+          fill(std::integral_constant<int, YP_GRADY>{});
+        } else if (a.op == YP_GRAD) {
+          fill(std::integral_constant<int, YP_GRAD>{});
+        } else if (a.op == YP_PGRAD) {
+          fill(std::integral_constant<int, YP_PGRAD>{});
+        } else {
+#pragma unroll
+          for (int g = 0; g < EI / FO; ++g)
+#pragma unroll
+            for (int r = 0; r < FO; ++r) {
+              const int ky = lt + TL * g + r * (NY / FO);
+              w[g * FO + r] = (kx < a.ncols) ? yp_op<T, NY>(a, q, kx, ky, f0[g * FO + r], f0[g * FO + r])
+                                             : cplx<T>{T(0), T(0)};
+            }
+        }
       }
     } else {
       // 3/2 pad or truncate.  Lane lt holds the forward output at ky = lt +

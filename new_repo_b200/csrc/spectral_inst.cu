@@ -325,8 +325,9 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
     const int base = NL + NL / 16;
     return base + ((target - base % W) % W + W) % W;
   };
-  auto smem_for = [&](int C) {  // twiddle matrices + two stages of nin rows per column
-    return sizeof(cplx<T>) * (twm_len(NY, false) + twm_len(NYO, true) + (size_t)C * 2 * a.nin * stride(C));
+  auto smem_for = [&](int C) {  // twiddle matrices, the ky row, two stages of nin rows per column
+    return sizeof(cplx<T>) * (twm_len(NY, false) + twm_len(NYO, true) + (size_t)C * 2 * a.nin * stride(C)) +
+           sizeof(T) * ((NY + 3) & ~3);
   };
   const int key = NY * 10000 + NYO;
   const bool fwd = (a.op == YP_FWDKILL);
