@@ -245,8 +245,8 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
   a.pair_store = (a.out_pstride % 2 == 0);
   for (int f = 0; f < a.nin && f < 16; ++f)
     if (a.out[f] && reinterpret_cast<uintptr_t>(a.out[f]) % (2 * sizeof(T)) != 0) a.pair_store = 0;
-  // enough rows that every thread holds a sequence (256 / lanes sequences),
-  // within ~100 KB of slots and input stages (two CTAs per SM)
+  // sequence slots and two input stages per CTA; rows per work item from
+  // best_rows below
   const int SL = slot_stride(M, int(sizeof(cplx<T>)));
   const int ns = a.nstage ? a.nstage : a.nin;  // staged rows per grid row
   {
