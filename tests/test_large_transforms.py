@@ -67,3 +67,30 @@ def test_press_stag_array_large(gpu, precision):
         e = rel_err(les.download(name), getattr(st, name))
         assert e <= TOL[precision], (precision, name, e)
     les.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("nx,ny", [(16, 128), (128, 16)])
+def test_small_and_asymmetric_plans(gpu, nx, ny, precision):
+    """Single-pass plans (8-24 points: one lane per sequence, many sequences
+    per warp) against multi-pass ones in the other direction."""
+    from new_repo_b200 import LES
+
+    p = O.Params(nx=nx, ny=ny, nz=4)
+    ops = O.Ops(p)
+    st = O.make_state(p, seed=5)
+    O.compute_vel_grad(ops, st)
+    if precision == "mixed":
+        for name in O.FIELDS:
+            a = getattr(st, name)
+            a[...] = a.astype(np.float32).astype(np.float64)
+    les = LES(run_params(p), precision=precision)
+    mirror(les, st)
+    O.grad_velocity_filt(ops, st.v, st.dvdx, st.dvdy)
+    les.grad_velocity_filt("v", "dvdx", "dvdy")
+    O.compute_dealias_convec(p, st, st.rhsx, st.rhsy, st.rhsz)
+    les.compute_dealias_convec("rhsx", "rhsy", "rhsz")
+    for name in ("v", "dvdx", "dvdy", "rhsx", "rhsy", "rhsz"):
+        e = rel_err(les.download(name), getattr(st, name))
+        assert e <= TOL[precision], (nx, ny, precision, name, e)
+    les.close()
