@@ -114,6 +114,15 @@ int les_set_bc_types(les_state* s, const int lbc_typ[3], const int ubc_typ[3]);
 int les_set_lagrangian_init(les_state* s, int f_coeff_init);
 int les_get_lagrangian_init(les_state* s, int* f_coeff_init);
 
+/* Switch an existing state between LES_FP64 and LES_MIXED (the precision
+ * chosen at creation): every field and plane, the boundary-condition types
+ * and the Lagrangian flags move to a new state of the other precision (FP32
+ * fields round to nearest; statistics sums and profiles restart).  Refused
+ * (1) while the learned closure is the SGS model: its normalisation and
+ * training data belong to the state it was trained in.  Replaces the
+ * les_set_precision(mode) of the boundary; the reference runs in FP64 only. */
+int les_set_precision(les_state* s, int precision);
+
 /* --- module entry points ------------------------------------------------ */
 /* compute_derivatives.f90:94-137 grad_velocity_filt(f, dfdx, dfdy) */
 int les_grad_velocity_filt(les_state* s, int f, int dfdx, int dfdy);

@@ -93,6 +93,7 @@ PROTOTYPES = {
     "les_diagnostics_async": [_P, C.c_void_p],
     "les_checkpoint_write": [_P, C.c_char_p],
     "les_checkpoint_read": [_P, C.c_char_p, _I],
+    "les_set_precision": [_P, _I],
     "les_stat_init": [_P],
     "les_stat_averages": [_P, _I, _I, _I, _I, C.c_char_p],
     "les_stat_sums": [_P, _I, _D],

@@ -1,6 +1,8 @@
 // extern "C" boundary of liblesgpu.so (declared in include/lesgpu.h).
 #include <cstring>
+#include <memory>
 #include <string>
+#include <vector>
 
 #include "../../include/lesgpu.h"
 #include "solver.cuh"
@@ -66,6 +68,40 @@ int les_create(const les_params* p, les_state** out) {
       throw;
     }
     *out = st;
+  });
+}
+
+int les_set_precision(les_state* s, int precision) {
+  STATE_OR_FAIL(s);
+  return guard([&] {
+    if (precision != LES_FP64 && precision != LES_MIXED) throw les::CudaError(LES_ERR_INVALID, "Invalid precision");
+    les::SolverBase* old = s->s;
+    if (old->P.precision == precision) return;
+    if (old->P.sgs_model == LES_SGS_MLP)
+      throw les::CudaError(LES_ERR_INVALID, "set the precision before selecting the learned closure");
+    les_params p = old->P;
+    p.precision = precision;
+    std::unique_ptr<les::SolverBase> n(les::make_solver(p));
+    const int nz = p.nz;
+    std::vector<double> buf((size_t)(nz + 2) * p.ny * p.nx);
+    for (int f = 0; f < LES_NFIELDS; ++f) {
+      old->download(f, buf.data(), 0, nz + 1);
+      n->upload(f, buf.data(), 0, nz + 1);
+    }
+    for (int pl = 0; pl < LES_NPLANES; ++pl) {
+      old->download_plane(pl, buf.data());
+      n->upload_plane(pl, buf.data());
+    }
+    for (int c = 0; c < 3; ++c) {
+      n->lbc_t[c] = old->lbc_t[c];
+      n->ubc_t[c] = old->ubc_t[c];
+    }
+    n->f_coeff_init = old->f_coeff_init;
+    n->lagran_init = old->lagran_init;
+    LES_CUDA(cudaStreamSynchronize(n->st));
+    if (les::g_hook == old) les::g_hook = n.get();
+    s->s = n.release();
+    delete old;
   });
 }
 

@@ -528,6 +528,14 @@ class LES:
         check(self.lib.les_diagnostics_async(self._h, C.c_void_p(pinned_ptr)))
 
     # ------------------------------------------------------ learned closure
+    def set_precision(self, precision: str):
+        """Move the state to the other precision ("fp64" / "mixed"): fields,
+        planes, boundary-condition types and Lagrangian flags carry over."""
+        if precision not in capi.PRECISION:
+            raise LesError(capi.LES_ERR_INVALID, f"Invalid precision: {precision!r}")
+        check(self.lib.les_set_precision(self._h, capi.PRECISION[precision]))
+        self.precision = precision
+
     def set_sgs_model(self, name: str):
         """Switch the SGS closure ('cst_Smag', 'dyn_Smag', 'dyn_LagScaleDep', 'mlp')."""
         if name not in capi.SGS_MODELS:
