@@ -564,10 +564,16 @@ __global__ void k_ab2(T* u, T* v, T* w, const T* rx, const T* ry, const T* rz, c
 }
 
 // projection and rhs update (LES_engine.f90:303-331), w(1) = w(nz+1) = 0.
+// The w correction is formed in FP64 whatever T: dp/dz carries the mean
+// vertical pressure gradient (thousands, balancing the mean shear term of
+// the vertical rhs), whose FP32 product with dt would leave the same
+// rounding in every point of a level -- a plane-mean w, i.e. divergence in
+// the (0,0) mode, far above the FP32 rounding of w itself.
 template <typename T>
 __global__ void k_projection(T* u, T* v, T* w, T* rx, T* ry, T* rz, const T* dpdx, const T* dpdy, const T* dpdz,
-                             long plane, int nz, T dtt) {
+                             long plane, int nz, double dtt_d) {
   const long n = (long)(nz + 2) * plane;
+  const T dtt = T(dtt_d);
   if (plane % 4 == 0) {  // four consecutive points (one level) per thread
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n / 4; q += (long)gridDim.x * blockDim.x) {
       const long o = 4 * q;
@@ -587,6 +593,10 @@ __global__ void k_projection(T* u, T* v, T* w, T* rx, T* ry, T* rz, const T* dpd
           if (c == 2 && k == 1) {
 #pragma unroll
             for (int i = 0; i < 4; ++i) x[i] = T(0);
+          } else if (c == 2) {
+            ld4(fld[c] + o, x);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) x[i] = T(double(x[i]) - dtt_d * double(d[i]));
           } else {
             ld4(fld[c] + o, x);
 #pragma unroll
@@ -608,7 +618,7 @@ __global__ void k_projection(T* u, T* v, T* w, T* rx, T* ry, T* rz, const T* dpd
       const T dz_ = dpdz[o];
       u[o] = u[o] - dtt * dpdx[o];
       v[o] = v[o] - dtt * dpdy[o];
-      w[o] = (k == 1) ? T(0) : w[o] - dtt * dz_;
+      w[o] = (k == 1) ? T(0) : T(double(w[o]) - dtt_d * double(dz_));
       rx[o] = rx[o] - dpdx[o];
       ry[o] = ry[o] - dpdy[o];
       rz[o] = rz[o] - dz_;

@@ -1617,7 +1617,7 @@ class Solver final : public SolverBase {
     // dpdz was formed by press_stag_array; this applies LES_engine.f90:303-331
     KL("k_projection", 15.0 * g.nz * g.plane() * sizeof(T), k_projection<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], F[LES_RHSX], F[LES_RHSY],
                                                         F[LES_RHSZ], F[LES_DPDX], F[LES_DPDY], F[LES_DPDZ],
-                                                        g.plane(), g.nz, T(P.dt * tadv1)));
+                                                        g.plane(), g.nz, P.dt * tadv1));
   }
 
   void step(int jt, int jtt) override {
