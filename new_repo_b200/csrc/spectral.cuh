@@ -614,6 +614,7 @@ struct YPArgs {
   int ipitch, opitch, opitch1;  // complex values between rows of in / out / second out (0: the nk)
   int nplanes, ngroups;         // work items: column blocks x planes x groups
   int plane0;
+  int nstage;  // input stages (set by the launcher): 2 = the next item's columns load during this one
   long in_pstride, out_pstride, out_pstride1;
   int nxh, lhx;        // base-grid Nyquist column and row length of kkx/kky/G
   int tt;              // YP_MASK: largest |ky| kept
@@ -738,7 +739,7 @@ __global__ void __launch_bounds__((FWD && sizeof(T) == 8) ? 128 : 256,
   const int C = a.C;
   T* kyrow = reinterpret_cast<T*>(two + Twm<NYO, true>::len);  // kky(ky), column 0 of the table
   cplx<T>* bin0 = reinterpret_cast<cplx<T>*>(kyrow + ((NY + 3) & ~3));  // input stage 0: [nin][C][SI]
-  cplx<T>* bin1 = bin0 + a.nin * C * SI;   // input stage 1
+  cplx<T>* bin1 = bin0 + (a.nstage > 1 ? a.nin * C * SI : 0);  // input stage 1 (stage 0 again when single)
   // the inverse transform, its output layout and the coalesced copy-out use
   // the first input row of each column of the current stage, free once the
   // forward transforms hold their values in registers
@@ -747,9 +748,11 @@ __global__ void __launch_bounds__((FWD && sizeof(T) == 8) ? 128 : 256,
   if constexpr (!FWD) twm_build<T, NYO, true>(a.tw_out, two, threadIdx.x, blockDim.x);
   if (a.kky)
     for (int i = threadIdx.x; i < NY; i += blockDim.x) kyrow[i] = a.kky[(long)i * a.lhx];
-  // persistent CTAs: work item = (column block, plane, group); the columns
-  // of the next item are copied into the other input stage asynchronously
-  // while this one is transformed
+  // persistent CTAs: work item = (column block, plane, group); with two
+  // stages the columns of the next item are copied into the other input
+  // stage asynchronously while this one is transformed, with one stage they
+  // are copied after this item's last read of it (more resident CTAs where
+  // shared memory limits them)
   const int ncb = (a.ncols + C - 1) / C;
   const long nitems = (long)ncb * a.nplanes * a.ngroups;
   if ((long)blockIdx.x < nitems) {
@@ -760,7 +763,7 @@ __global__ void __launch_bounds__((FWD && sizeof(T) == 8) ? 128 : 256,
   for (long item = blockIdx.x; item < nitems; item += gridDim.x) {
   const long next = item + gridDim.x;
   cplx<T>* bin = stage ? bin1 : bin0;
-  if (next < nitems) {
+  if (a.nstage > 1 && next < nitems) {
     yp_issue<T, NY>(a, next, ncb, stage ? bin0 : bin1);
     cp_async_commit();
     cp_async_wait<1>();
@@ -925,7 +928,13 @@ __global__ void __launch_bounds__((FWD && sizeof(T) == 8) ? 128 : 256,
     }
     __syncthreads();
   }
-  stage ^= 1;
+  if (a.nstage > 1) {
+    stage ^= 1;
+  } else if (next < nitems) {
+    // single stage: every thread is past the last read of it (barrier above)
+    yp_issue<T, NY>(a, next, ncb, bin0);
+    cp_async_commit();
+  }
   }
 }
 

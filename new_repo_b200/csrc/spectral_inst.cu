@@ -325,8 +325,8 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
     const int base = NL + NL / 16;
     return base + ((target - base % W) % W + W) % W;
   };
-  auto smem_for = [&](int C) {  // twiddle matrices, the ky row, two stages of nin rows per column
-    return sizeof(cplx<T>) * (twm_len(NY, false) + twm_len(NYO, true) + (size_t)C * 2 * a.nin * stride(C)) +
+  auto smem_for = [&](int C, int ns) {  // twiddle matrices, the ky row, ns stages of nin rows per column
+    return sizeof(cplx<T>) * (twm_len(NY, false) + twm_len(NYO, true) + (size_t)C * ns * a.nin * stride(C)) +
            sizeof(T) * ((NY + 3) & ~3);
   };
   const int key = NY * 10000 + NYO;
@@ -343,37 +343,43 @@ void launch_ypass(int NY, int NYO, YPArgs<T> a, int nplanes, int ngroups, cudaSt
       throw CudaError(1, "ypass: unsupported length pair " + std::to_string(NY) + "->" + std::to_string(NYO));
   }
   if (!kern) throw CudaError(1, "ypass: a forward-only pass keeps the length");
-  // columns per CTA (C * TL threads, at least a warp): the most busy warps
-  // per SM -- resident CTAs (shared memory, registers, threads) times the
-  // warps whose columns exist; on a tie the CTA size nearest 128 threads
-  // (measured at 256^3: 128-thread CTAs beat 64 and 256 at equal occupancy)
+  // columns per CTA (C * TL threads, at least a warp) and input stages: the
+  // most busy warps per SM -- resident CTAs (shared memory, registers,
+  // threads) times the warps whose columns exist; on a tie two stages (the
+  // loads of the next item overlap this one), then the CTA size nearest 128
+  // threads (measured at 256^3: 128-thread CTAs beat 64 and 256 at equal
+  // occupancy).  One stage wins where shared memory, not registers, limits
+  // the resident CTAs (the two-input stress divergence on 512-point columns).
   {
     const KernelLimits lim = kernel_limits((const void*)kern);
     const int regs = lim.regs;
     double best = -1.0;
-    int best_lc = 0;
+    int best_lc = 0, best_ns = 2;
     while ((1 << best_lc) * TL < 32) ++best_lc;  // at least one full warp
     auto off128 = [&](int lc) { return std::abs(std::log2(double((1 << lc) * TL) / 128.0)); };
-    for (int lc = 0; (1 << lc) * TL <= std::min(256, lim.max_threads); ++lc) {
-      const int C = 1 << lc, threads = C * TL;
-      if (threads < 32) continue;
-      const size_t sm = smem_for(C);
-      if (sm > SMEM_CAP) break;
-      const int warp_regs = ((regs * 32 + 255) / 256) * 256;
-      const int by_regs = 65536 / (warp_regs * (threads / 32));
-      const int ctas = std::min({int(SM_SMEM / (sm + 1024)), by_regs, 2048 / threads, 32});
-      if (ctas < 1) break;
-      const double busy = ctas * double(threads / 32) * std::min(1.0, double(a.ncols) / C);
-      if (busy > best + 1e-9 || (busy > best - 1e-9 && off128(lc) < off128(best_lc))) {
-        best = busy;
-        best_lc = lc;
+    for (int ns = 2; ns >= 1; --ns)
+      for (int lc = 0; (1 << lc) * TL <= std::min(256, lim.max_threads); ++lc) {
+        const int C = 1 << lc, threads = C * TL;
+        if (threads < 32) continue;
+        const size_t sm = smem_for(C, ns);
+        if (sm > SMEM_CAP) break;
+        const int warp_regs = ((regs * 32 + 255) / 256) * 256;
+        const int by_regs = 65536 / (warp_regs * (threads / 32));
+        const int ctas = std::min({int(SM_SMEM / (sm + 1024)), by_regs, 2048 / threads, 32});
+        if (ctas < 1) break;
+        const double busy = ctas * double(threads / 32) * std::min(1.0, double(a.ncols) / C);
+        if (busy > best + 1e-9 || (busy > best - 1e-9 && ns == best_ns && off128(lc) < off128(best_lc))) {
+          best = busy;
+          best_lc = lc;
+          best_ns = ns;
+        }
       }
-    }
     a.lc = best_lc;
+    a.nstage = best_ns;
   }
   a.C = 1 << a.lc;
   a.SI = stride(a.C);
-  const size_t smem = smem_for(a.C);
+  const size_t smem = smem_for(a.C, a.nstage);
   if (smem > SMEM_CAP) throw CudaError(1, "ypass: shared memory request too large");
   const int threads = a.C * TL;
   a.nplanes = nplanes;
