@@ -956,6 +956,7 @@ struct XIArgs {
   int ipitch;      // complex values between input rows (>= nk; 0: nk)
   int nks;         // complex values between staged rows in shared memory (set by the launcher)
   int stage_rows;  // staged rows per stage (set by the launcher)
+  int nbuf;        // input stages (set by the launcher): 2 = the next item's rows load during this one
   int merged;      // 1: each sequence is transformed in its own staged row (plain store, nstage 0)
   int nz;
   long in_pstride;
@@ -1019,9 +1020,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
   const int nseq = a.R * a.nin;
   const int npad = seq_pad<M>(nseq);
   const int ns = a.nstage ? a.nstage : a.nin;        // staged rows per grid row
+  // a stage holds an even number of complex values, so the sequence slots
+  // after the stages keep the 16-byte alignment of their four-point accesses
+  // whatever the stage count (FP32 rows of an odd nks)
+  const long stage_len = ((long)a.stage_rows * a.nks + 1) & ~1L;
   cplx<T>* stage0 = twm + Twm<M, true>::len;         // input rows of a work item: [R][ns][nk]
-  cplx<T>* stage1 = stage0 + (long)a.stage_rows * a.nks;
-  cplx<T>* buf = stage1 + (long)a.stage_rows * a.nks;  // sequence slots (none when merged)
+  cplx<T>* stage1 = stage0 + (a.nbuf > 1 ? stage_len : 0L);  // stage 0 again when single
+  cplx<T>* buf = stage0 + a.nbuf * stage_len;        // sequence slots (none when merged)
   int* rowl = reinterpret_cast<int*>(buf + (a.merged ? 0L : (long)npad * SL));  // level of row r (-1: beyond the grid)
   int* rowj = rowl + a.R;
   T* kxs = reinterpret_cast<T*>(rowj + a.R);          // x wavenumbers (nstage > 0)
@@ -1029,8 +1034,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
   twm_build<T, M, true, 2>(a.tw, twm, threadIdx.x, blockDim.x);
   if (a.nstage)
     for (int i = threadIdx.x; i < a.nk; i += blockDim.x) kxs[i] = a.kxr[i];
-  // persistent CTAs over batches of R rows; the spectral rows of the next
-  // batch are copied into the other stage while this one is transformed
+  // persistent CTAs over batches of R rows; with two stages the spectral
+  // rows of the next batch are copied into the other stage while this one
+  // is transformed, with one stage after this batch's last read of it
   const long nitems = (a.nrows + a.R - 1) / a.R;
   if ((long)blockIdx.x < nitems) {
     xi_issue<T>(a, blockIdx.x, stage0);
@@ -1040,7 +1046,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
   for (long item = blockIdx.x; item < nitems; item += gridDim.x) {
   const long next = item + gridDim.x;
   const cplx<T>* stage = stg ? stage1 : stage0;
-  if (next < nitems) {
+  if (a.nbuf > 1 && next < nitems) {
     xi_issue<T>(a, next, stg ? stage0 : stage1);
     cp_async_commit();
     cp_async_wait<1>();
@@ -1240,7 +1246,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
   }
   }  // the combining ops
   __syncthreads();
-  stg ^= 1;
+  if (a.nbuf > 1) {
+    stg ^= 1;
+  } else if (next < nitems) {
+    // single stage: every thread is past the last read of it (barrier above)
+    xi_issue<T>(a, next, stage0);
+    cp_async_commit();
+  }
   }
 }
 

@@ -78,7 +78,7 @@ constexpr size_t SM_SMEM = 228 * 1024;  // shared memory per SM (1 KB of it rese
 // fraction of the 256 / TL slots of each pass that hold a sequence; on a tie
 // the larger count (fewer items).
 template <typename SmemFn>
-int best_rows(const void* kern, int seq_per_row, int TL, SmemFn smem_for, int rmax = 32) {
+int best_rows(const void* kern, int seq_per_row, int TL, SmemFn smem_for, int rmax = 32, double* best_score = nullptr) {
   const int regs = kernel_regs(kern);
   const int warp_regs = ((regs * 32 + 255) / 256) * 256;
   const int by_regs = std::max(1, 65536 / (warp_regs * 8));
@@ -98,6 +98,7 @@ int best_rows(const void* kern, int seq_per_row, int TL, SmemFn smem_for, int rm
       best_r = R;
     }
   }
+  if (best_score) *best_score = best;
   return best_r;
 }
 
@@ -245,8 +246,8 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
   a.pair_store = (a.out_pstride % 2 == 0);
   for (int f = 0; f < a.nin && f < 16; ++f)
     if (a.out[f] && reinterpret_cast<uintptr_t>(a.out[f]) % (2 * sizeof(T)) != 0) a.pair_store = 0;
-  // sequence slots and two input stages per CTA; rows per work item from
-  // best_rows below
+  // sequence slots and one or two input stages per CTA; rows per work item
+  // and stages from best_rows below
   const int SL = slot_stride(M, int(sizeof(cplx<T>)));
   const int ns = a.nstage ? a.nstage : a.nin;  // staged rows per grid row
   {
@@ -264,8 +265,8 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
   a.merged = (a.op == XI_STORE && a.nstage == 0) ? 1 : 0;
   if (a.merged) a.nks = std::max(a.nks, SL);
   auto stage_rows = [&](int R) { return a.merged ? pad_seqs(R * a.nin, M) : R * ns; };
-  auto smem_for = [&](int R) {
-    return sizeof(cplx<T>) * (NX + twm_len(M, true) + 2 * (size_t)stage_rows(R) * a.nks +
+  auto smem_nb = [&](int R, int nb) {
+    return sizeof(cplx<T>) * (NX + twm_len(M, true) + nb * (((size_t)stage_rows(R) * a.nks + 1) & ~size_t(1)) +
                               (a.merged ? 0 : (size_t)pad_seqs(R * a.nin, M) * SL)) +
            2 * sizeof(int) * R + (a.nstage ? sizeof(T) * (a.nk + 2) : 0);
   };
@@ -278,10 +279,24 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
     default:
       throw CudaError(1, "xinv: unsupported transform length " + std::to_string(NX));
   }
-  a.R = best_rows((const void*)kern, a.nin, lanes(M), smem_for);
+  // two stages unless one stage keeps strictly more sequence slots busy
+  // (more resident CTAs where shared memory limits them)
+  {
+    double s2 = -1.0, s1 = -1.0;
+    const int r2 = best_rows((const void*)kern, a.nin, lanes(M), [&](int R) { return smem_nb(R, 2); }, 32, &s2);
+    const int r1 = best_rows((const void*)kern, a.nin, lanes(M), [&](int R) { return smem_nb(R, 1); }, 32, &s1);
+    a.nbuf = (s1 > s2 + 1e-9) ? 1 : 2;
+    a.R = (a.nbuf == 1) ? r1 : r2;
+  }
   a.stage_rows = stage_rows(a.R);
-  const size_t smem = smem_for(a.R);
+  const size_t smem = smem_nb(a.R, a.nbuf);
   if (smem > SMEM_CAP) throw CudaError(1, "xinv: shared memory request too large");
+  {
+    // the combining ops read the sequence slots four reals at a time
+    const size_t stage_len = ((size_t)a.stage_rows * a.nks + 1) & ~size_t(1);
+    const size_t slots = sizeof(cplx<T>) * (NX + twm_len(M, true) + a.nbuf * stage_len);
+    if (!a.merged && slots % 16 != 0) throw CudaError(1, "xinv: sequence slots not 16-byte aligned");
+  }
   const long nitems = ceil_div(a.nrows, a.R);
   if (nitems == 0) return;
   const int grid = int(std::min<long>(nitems, (long)resident_ctas((const void*)kern, 256, smem)));
