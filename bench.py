@@ -200,25 +200,21 @@ def run_ours(args, dist, rank, local, ws):
     les.step(W)
     les.sync()
     barrier(dist, local)
-    les.profile(True)
     n0 = les.launch_count()
     with ClockSampler(local) as clk:
         ms = timed_steps(les, K)
     n1 = les.launch_count()
-    prof = les.profile_report()
-    les.profile(False)
     barrier(dist, local)
     ms = max_over_ranks(dist, ms, local)
     value = npts * K * ws / (ms / 1e3) / 1e6
-    mixed_u = [les.download(n, 1, p.nz) for n in ("u", "v", "w")] if not args.no_fp64 else None
+    # ---- a second timed pass of K steps with per-launch events on the
+    #      state's stream: the dominant kernel's roofline and the per-kernel
+    #      breakdown (the headline above ran without the events) ----
+    les.profile(True)
+    ms_prof = timed_steps(les, K)
+    prof = les.profile_report()
+    les.profile(False)
     status = les.status()
-    if train is not None:
-        train.update(les.mlp_info())
-        prof_chk = les.mlp_check_profile()
-        kmax = int(np.argmax(prof_chk))
-        train["check_profile_max"] = {"level": kmax + 1, "rms_log_error": round(float(prof_chk[kmax]), 4)}
-        train["check_profile_levels_1_12"] = [round(float(x), 4) for x in prof_chk[:12]]
-    # ---- roofline of the dominant kernel (live events of the timed region) ----
     top = max(prof.items(), key=lambda kv: kv[1]["ms"])
     label, rec = top
     avg_ms = rec["ms"] / rec["launches"]
@@ -227,7 +223,8 @@ def run_ours(args, dist, rank, local, ws):
     roof = {"kernel": label, "bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
             "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4), "peak_source": pk_kind,
             "traffic": ncu_traffic(label), "avg_launch_ms": round(avg_ms, 4),
-            "algorithmic_bytes_per_launch": rec["bytes_per_launch"], "share_of_step": round(rec["ms"] / ms, 4)}
+            "algorithmic_bytes_per_launch": rec["bytes_per_launch"], "share_of_step": round(rec["ms"] / ms_prof, 4),
+            "timed_in": f"a second pass of {K} steps with per-launch CUDA events ({ms_prof / K:.4f} ms/step)"}
     # step-level: algorithmic bytes per step (105 F + 28 F / cs_count, F = N * 4 B)
     F = npts * 4.0
     step_bytes = (105.0 + 28.0 / p.cs_count) * F
@@ -237,6 +234,28 @@ def run_ours(args, dist, rank, local, ws):
     step_roof = {"algorithmic_bytes_per_step": step_bytes,
                  "achieved_gbs": round(step_bytes / (ms / K / 1e3) / 1e9, 1),
                  "frac": round(step_bytes / (ms / K / 1e3) / 1e9 / pk["hbm_gbs"], 4)}
+    # ---- untimed continuation to the comparison step (>= 100 steps); the
+    #      closure's LASD check (every 10 updates = 50 steps) also runs at the
+    #      last update of the continuation ----
+    S = max(100, T + W + 2 * K)
+    done = T + W + 2 * K
+    if train is not None:
+        upd = [j for j in range(done + 1, S + 1) if j >= p.dyn_init and j % p.cs_count == 0]
+        if upd:
+            les.step(upd[-1] - done - 1)
+            les.mlp_set_check_every(1)
+            les.step(1)
+            les.mlp_set_check_every(10)
+            done = upd[-1]
+    les.step(S - done)
+    snap = snapshot(les, p) if not args.no_fp64 else None
+    if train is not None:
+        train.update(les.mlp_info())
+        prof_chk = les.mlp_check_profile()
+        kmax = int(np.argmax(prof_chk))
+        train["check_profile_max"] = {"level": kmax + 1, "rms_log_error": round(float(prof_chk[kmax]), 4)}
+        train["check_profile_levels_1_12"] = [round(float(x), 4) for x in prof_chk[:12]]
+        train["check_after_steps"] = S
 
     # ---- end to end through the public API with pinned host buffers ----
     e2e = None
@@ -246,17 +265,20 @@ def run_ours(args, dist, rank, local, ws):
 
     # ---- the same step with the LASD closure (mixed precision) ----
     lasd = None
+    snap_l = None
     if args.closure == "mlp" and not args.no_fp64:
         ll = LES(p, precision="mixed", device=local)
         ll.set_initial_conditions(u0, v0, w0)
         ll.step(T + W)
         ll.sync()
         msl = max_over_ranks(dist, timed_steps(ll, K), local)
+        ll.step(S - (T + W + K))
+        snap_l = snapshot(ll, p)
         ll.close()
         lasd = {"value": round(npts * K * ws / (msl / 1e3) / 1e6, 2), "ms_per_step": round(msl / K, 4),
                 "speedup_of_headline": round(msl / ms, 3)}
 
-    # ---- plain FP64 GPU step (LASD), same seed and step count ----
+    # ---- plain FP64 GPU step (LASD), same seed, compared at step S ----
     fp64 = None
     if not args.no_fp64:
         l64 = LES(p, precision="fp64", device=local)
@@ -264,18 +286,24 @@ def run_ours(args, dist, rank, local, ws):
         l64.step(T + W)
         l64.sync()
         ms64 = timed_steps(l64, K)
-        ref_u = [l64.download(n, 1, p.nz) for n in ("u", "v", "w")]
+        l64.step(S - (T + W + K))
+        snap64 = snapshot(l64, p)
         l64.close()
         ms64 = max_over_ranks(dist, ms64, local)
-        num = sum(float(((a - b) ** 2).sum()) for a, b in zip(mixed_u, ref_u))
-        den = sum(float((b ** 2).sum()) for b in ref_u)
-        prof_m = mixed_u[0].mean(axis=(1, 2))
-        prof_r = ref_u[0].mean(axis=(1, 2))
+        vel = ("u", "v", "w")
+        num = sum(float(((snap[n] - snap64[n]) ** 2).sum()) for n in vel)
+        den = sum(float((snap64[n] ** 2).sum()) for n in vel)
+        prof_m = snap["u"].mean(axis=(1, 2))
+        prof_r = snap64["u"].mean(axis=(1, 2))
         fp64 = {"value": round(npts * K * ws / (ms64 / 1e3) / 1e6, 2), "ms_per_step": round(ms64 / K, 4),
                 "speedup_of_headline": round(ms64 / ms, 3),
                 "velocity_rms_rel_error": float(math.sqrt(num / den)),
                 "mean_profile_drift": float(np.abs(prof_m - prof_r).max() / np.abs(prof_r).max()),
-                "after_steps": T + W + K}
+                "after_steps": S,
+                "per_field_error_of_headline": field_errors(snap, snap64)}
+        if snap_l is not None:
+            lasd["per_field_error_vs_fp64"] = field_errors(snap_l, snap64)
+            lasd["after_steps"] = S
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -301,6 +329,26 @@ def run_ours(args, dist, rank, local, ws):
             "clocks": clk.summary(), "status_bits": status,
         }
         print(json.dumps(line), flush=True)
+
+
+COMPARED = ("u", "v", "w", "p", "cs_opt2", "txz", "rhsx")
+
+
+def snapshot(les, p) -> dict:
+    """Interior levels 1..nz of the fields the precision comparison reports."""
+    return {n: les.download(n, 1, p.nz) for n in COMPARED}
+
+
+def field_errors(a: dict, b: dict) -> dict:
+    """Per field: RMS and max of a - b relative to the RMS / max of b."""
+    import numpy as np
+
+    out = {}
+    for n in COMPARED:
+        d = a[n] - b[n]
+        out[n] = {"rms_rel": float(np.sqrt((d * d).mean() / max((b[n] * b[n]).mean(), 1e-300))),
+                  "max_rel": float(np.abs(d).max() / max(np.abs(b[n]).max(), 1e-300))}
+    return out
 
 
 def train_closure(les, p, T: int, epochs: int = 4, tiles: int = 16) -> dict:

@@ -11,7 +11,8 @@
  *
  * Every function returns 0 on success or a nonzero status that mirrors the
  * reference's decomp_2d_abort codes (1 invalid option, 3 out of memory,
- * 9 numerical failure, 22 I/O); les_last_error() gives the message.  Calls
+ * 9 numerical failure, 22 I/O; 4 for other CUDA errors); les_last_error()
+ * gives the message.  Calls
  * on one state are not re-entrant; each state owns one CUDA stream.
  */
 #ifndef LESGPU_H
@@ -24,6 +25,10 @@ extern "C" {
 #define LES_OK 0
 #define LES_ERR_INVALID 1
 #define LES_ERR_NOMEM 3
+/* any other CUDA error (no reference counterpart: the reference has no
+ * device); les_last_error says whether it is sticky, i.e. a device fault
+ * after which the CUDA context is lost */
+#define LES_ERR_DEVICE 4
 #define LES_ERR_NUMERICAL 9
 #define LES_ERR_IO 22
 
@@ -80,6 +85,10 @@ typedef enum les_field {
   LES_CS_OPT2, LES_NU_T,
   LES_F_LM, LES_F_MM, LES_F_QN, LES_F_NN, LES_BETA,
   LES_U_LAG, LES_V_LAG, LES_W_LAG,
+  /* scalar transport (allocated by les_scalar_init): theta on uvp nodes,
+   * its gradients (d/dz on w nodes), right-hand sides and SGS fluxes
+   * pi_j = nu_theta d_j theta (pi_x, pi_y on uvp nodes, pi_z on w nodes) */
+  LES_THETA, LES_DTDX, LES_DTDY, LES_DTDZ, LES_RHS_T, LES_RHS_T_F, LES_QX, LES_QY, LES_QZ,
   LES_NFIELDS
 } les_field;
 
@@ -165,6 +174,16 @@ int les_step(les_state* s, int jt, int jt_total);
 int les_diagnostics(les_state* s, double out[4]);
 /* Sticky device status bits (NaN seen, zero pivot, ...); cleared on read. */
 int les_get_status(les_state* s, unsigned* bits);
+/* The reference's numerical aborts as a status: check_NaN(jt)
+ * (LES_engine.f90:583-616, called every NaN_check steps, :363-365) and the
+ * zero-pivot abort of the tridiagonal solve (compute_pressure.f90:411-418),
+ * both decomp_2d_abort code 9.  Synchronises the state's stream, reads and
+ * clears the status bits (into *bits, may be NULL) and returns
+ * LES_ERR_NUMERICAL with the reference's message ("I got a NaN" /
+ * "tridiag solver: error bet(i,j)=0, dividing by 0!") when the NaN or pivot
+ * bit was set since the last read, else 0.  The state stays usable: a caller
+ * can reload a checkpoint (les_checkpoint_read) and continue. */
+int les_check_status(les_state* s, unsigned* bits);
 /* Synchronise the state's stream. */
 int les_sync(les_state* s);
 /* Device time of the kernels of the last les_step, per reference profiling
@@ -249,6 +268,54 @@ int les_tke_init(les_state* s, const char* out_path);
 int les_tke_budget(les_state* s, int jt, int tke_period);
 int les_tke_sums(les_state* s, double* out, int* record);
 
+/* ---- scalar transport, buoyancy and momentum forcing ---------------------
+ * The reference's scalar module is a stub (compute_scalars.f90:80-151: the
+ * AB2 update of step_scalars and its ghost values only) and its sponge layer
+ * is built, zeroed and disconnected (sponge_damping.f90:83,
+ * LES_engine.f90:565).  Here theta (uvp nodes, stored as the departure from
+ * a reference value) is advected with the momentum's 3/2-padded (or 2/3
+ * truncated) products, -(u d_x + v d_y) theta - (w d_z theta at k, k+1)/2,
+ * diffuses with the SGS flux pi_j = nu_theta d_j theta (rhs += div pi, the
+ * sign convention of the reference's stresses) and steps with AB2
+ * (step_scalars :111-125).  nu_theta = nu_t / pr_t (LES_SCALAR_SGS_CONST) or
+ * |S| kappa(z) Delta^2 with kappa = Cs^2/Pr_t from the plane-averaged
+ * Germano identity at the 2 Delta test filter (LES_SCALAR_SGS_DYN: the
+ * dynamic Prandtl model, K_j = filt(u_j theta) - filt(u_j) filt(theta),
+ * X_j = Delta^2 (filt(|S| d_j theta) - 4 |S~| d_j theta~), kappa =
+ * max(0, <K.X>/<X.X>), updated every cs_count steps from dyn_init, 0.03/pr_t
+ * before), on the nodes of compute_dynamic_mum.  Boundary conditions: the
+ * wall flux pi_z(1) = -surface_flux and d theta/dz(1) = -surface_flux /
+ * (kappa_vk u* dz/2) (0 where u* = 0), theta(0) = 0 (step_scalars), theta(nz+1)
+ * = theta(nz) + top_gradient dz.  With buoyancy != 0 (g/theta_0) the w
+ * equation gains buoyancy (theta_w - <theta_w>) on w nodes 2..nz, theta_w
+ * the mean of the two uvp levels around the node (the stub's
+ * compute_beta_scalars, :143-148). */
+#define LES_SCALAR_SGS_CONST 0
+#define LES_SCALAR_SGS_DYN 1
+typedef struct les_scalar_params {
+  double surface_flux;  /* kinematic flux at the wall, positive upward */
+  double top_gradient;  /* d theta / dz at the lid */
+  double buoyancy;      /* g / theta_0 in model units; 0 = passive scalar */
+  double pr_t;          /* turbulent Prandtl number (constant model; initial kappa = 0.03 / pr_t) */
+  int sgs;              /* LES_SCALAR_SGS_CONST or LES_SCALAR_SGS_DYN */
+} les_scalar_params;
+/* scalars_module_init (compute_scalars.f90:40-57): allocates the scalar
+ * fields (zero) and turns the scalar on for les_step. */
+int les_scalar_init(les_state* s, const les_scalar_params* sp);
+/* theta (nx, ny, nz) of levels 1..nz, then the ghost values */
+int les_scalar_set_initial(les_state* s, const double* theta);
+/* kappa = Cs^2 / Pr_t per level 0..nz+1 (out[nz+2]) of the scalar SGS model */
+int les_scalar_kappa(les_state* s, double* out, int n);
+/* sponge_damping_init (sponge_damping.f90:42-101) with the layer fraction of
+ * the domain height below the sponge (0.8: the top 20 %) and without the
+ * zeroing of :83; add_sponge_damping (:131-161) then runs at the end of
+ * compute_RHS_adv (the call LES_engine.f90:565 leaves commented out).
+ * fraction <= 0 turns it off. */
+int les_sponge_init(les_state* s, double layer_fraction);
+/* Coriolis forcing of compute_RHS_adv (LES_engine.f90:553-561): rhs_x +=
+ * coriol (v - v_g), rhs_y -= coriol (u - u_g); coriol = 0 turns it off. */
+int les_set_coriolis(les_state* s, double coriol, double ug, double vg);
+
 /* ---- learned SGS closure (no reference counterpart) ---------------------
  * Cs^2 = Cs^2_prev * exp(net(features)) from an 8 -> 64 -> 64 -> 1 GELU network with
  * BF16 weights and FP32 accumulation (tcgen05 tensor cores), evaluated at
@@ -313,7 +380,12 @@ int les_mlp_check_profile(les_state* s, double* out, int n);
  * compute_derivatives.f90 on one field) for a field already on the device:
  * f [nlev][ny][nx] (FP64) is replaced by its Nyquist-filtered version and
  * dfdx, dfdy receive the derivatives (domain lengths lx, ly); the three
- * pointers must be 16-byte aligned (rejected otherwise).  It allocates
+ * pointers must be 16-byte aligned (rejected otherwise).  nx is one of
+ * 16 24 32 48 64 96 128 192 256 384 512 768 and ny one of 16 32 64 128 256
+ * 512 (other sizes are rejected before anything is queued).  Its kernel
+ * launches are not counted by les_profile / les_launch_count of a state used
+ * on the calling thread (the launch observer is per host thread and is
+ * suspended for the duration of the call only).  It allocates
  * nothing: the tables and spectra live in one static device buffer of
  * LES_NOALLOC_SCRATCH_BYTES, for callers that must not change the device
  * memory footprint (an in-situ hook in a coupled run whose memory is fully

@@ -11,7 +11,7 @@ from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "liblesgpu.so"
 
-LES_OK, LES_ERR_INVALID, LES_ERR_NOMEM, LES_ERR_NUMERICAL, LES_ERR_IO = 0, 1, 3, 9, 22
+LES_OK, LES_ERR_INVALID, LES_ERR_NOMEM, LES_ERR_DEVICE, LES_ERR_NUMERICAL, LES_ERR_IO = 0, 1, 3, 4, 9, 22
 SGS_MODELS = {"cst_Smag": 0, "dyn_Smag": 1, "dyn_LagScaleDep": 2, "mlp": 3}
 MLP_NPARAM = 4801
 MLP_NSTATS = 36
@@ -23,7 +23,9 @@ PRECISION = {"fp64": 0, "mixed": 1}
 FIELDS = ("u", "v", "w", "dudx", "dudy", "dudz", "dvdx", "dvdy", "dvdz", "dwdx", "dwdy", "dwdz",
           "p", "dpdx", "dpdy", "dpdz", "rhsx", "rhsy", "rhsz", "rhsx_f", "rhsy_f", "rhsz_f",
           "txx", "txy", "txz", "tyy", "tyz", "tzz", "cs_opt2", "nu_t",
-          "F_LM", "F_MM", "F_QN", "F_NN", "beta", "u_lag", "v_lag", "w_lag")
+          "F_LM", "F_MM", "F_QN", "F_NN", "beta", "u_lag", "v_lag", "w_lag",
+          "theta", "dtdx", "dtdy", "dtdz", "rhs_t", "rhs_t_f", "qx", "qy", "qz")
+SCALAR_SGS = {"const": 0, "dynamic": 1}
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 PLANES = ("lbc_u", "lbc_v", "lbc_w", "ubc_u", "ubc_v", "ubc_w", "bottom_wk_press", "top_wk_press",
           "lbc_z0", "u_star_avg")
@@ -37,6 +39,11 @@ class LesParams(C.Structure):
                 ("sgs_model", C.c_int), ("cs_count", C.c_int), ("dyn_init", C.c_int),
                 ("wall_law", C.c_int), ("wall_model", C.c_int), ("dealias", C.c_int),
                 ("lag_halo", C.c_int), ("precision", C.c_int), ("device", C.c_int)]
+
+
+class ScalarParams(C.Structure):
+    _fields_ = [("surface_flux", C.c_double), ("top_gradient", C.c_double), ("buoyancy", C.c_double),
+                ("pr_t", C.c_double), ("sgs", C.c_int)]
 
 
 class LesError(RuntimeError):
@@ -81,6 +88,12 @@ PROTOTYPES = {
     "les_step": [_P, _I, _I],
     "les_diagnostics": [_P, _D],
     "les_get_status": [_P, C.POINTER(C.c_uint)],
+    "les_check_status": [_P, C.POINTER(C.c_uint)],
+    "les_scalar_init": [_P, C.POINTER(ScalarParams)],
+    "les_scalar_set_initial": [_P, _D],
+    "les_scalar_kappa": [_P, _D, _I],
+    "les_sponge_init": [_P, C.c_double],
+    "les_set_coriolis": [_P, C.c_double, C.c_double, C.c_double],
     "les_sync": [_P],
     "les_timers": [_P, _D],
     "les_profile": [_P, _I],

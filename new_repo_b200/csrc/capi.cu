@@ -82,9 +82,15 @@ int les_set_precision(les_state* s, int precision) {
     les_params p = old->P;
     p.precision = precision;
     std::unique_ptr<les::SolverBase> n(les::make_solver(p));
+    if (old->scalar_on) n->scalar_init(old->SP);
+    if (old->sponge_frac > 0.0) n->sponge_init(old->sponge_frac);
+    n->coriol = old->coriol;
+    n->ug = old->ug;
+    n->vg = old->vg;
     const int nz = p.nz;
     std::vector<double> buf((size_t)(nz + 2) * p.ny * p.nx);
     for (int f = 0; f < LES_NFIELDS; ++f) {
+      if (!old->has_field(f)) continue;
       old->download(f, buf.data(), 0, nz + 1);
       n->upload(f, buf.data(), 0, nz + 1);
     }
@@ -233,6 +239,22 @@ int les_get_status(les_state* s, unsigned* bits) {
   STATE_OR_FAIL(s);
   return guard([&] { *bits = s->s->status(); });
 }
+int les_check_status(les_state* s, unsigned* bits) {
+  STATE_OR_FAIL(s);
+  unsigned b = 0;
+  const int rc = guard([&] { b = s->s->status(); });
+  if (rc != LES_OK) return rc;
+  if (bits) *bits = b;
+  if (b & les::ST_NAN) {
+    g_last_error = "I got a NaN";
+    return LES_ERR_NUMERICAL;
+  }
+  if (b & les::ST_PIVOT) {
+    g_last_error = "tridiag solver: error bet(i,j)=0, dividing by 0!";
+    return LES_ERR_NUMERICAL;
+  }
+  return LES_OK;
+}
 int les_sync(les_state* s) {
   STATE_OR_FAIL(s);
   return guard([&] { LES_CUDA(cudaStreamSynchronize(s->s->st)); });
@@ -286,6 +308,34 @@ int les_set_sgs_model(les_state* s, int model) {
   STATE_OR_FAIL(s);
   return guard([&] { s->s->set_sgs_model(model); });
 }
+int les_scalar_init(les_state* s, const les_scalar_params* sp) {
+  STATE_OR_FAIL(s);
+  if (!sp) return bad_arg("sp");
+  return guard([&] { s->s->scalar_init(*sp); });
+}
+int les_scalar_set_initial(les_state* s, const double* theta) {
+  STATE_OR_FAIL(s);
+  if (!theta) return bad_arg("theta");
+  return guard([&] { s->s->scalar_set_initial(theta); });
+}
+int les_scalar_kappa(les_state* s, double* out, int n) {
+  STATE_OR_FAIL(s);
+  if (!out) return bad_arg("out");
+  return guard([&] { s->s->scalar_kappa(out, n); });
+}
+int les_sponge_init(les_state* s, double fraction) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->sponge_init(fraction); });
+}
+int les_set_coriolis(les_state* s, double coriol, double ug, double vg) {
+  STATE_OR_FAIL(s);
+  return guard([&] {
+    s->s->coriol = coriol;
+    s->s->ug = ug;
+    s->s->vg = vg;
+  });
+}
+
 int les_mlp_init(les_state* s, unsigned seed) {
   STATE_OR_FAIL(s);
   return guard([&] { s->s->mlp_init(seed); });

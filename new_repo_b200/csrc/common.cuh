@@ -52,12 +52,34 @@ struct CudaError : std::runtime_error {
   CudaError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
-#define LES_CUDA(call)                                                              \
-  do {                                                                              \
-    cudaError_t e_ = (call);                                                        \
-    if (e_ != cudaSuccess) {                                                        \
-      throw ::les::CudaError(3, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    }                                                                               \
+// Status of a failed CUDA call: 3 (the reference's out-of-memory code) for an
+// allocation failure, 4 for any other CUDA error.  Errors the CUDA runtime
+// marks as sticky (a device fault: illegal address, launch failure, ...)
+// leave the context unusable; the message says so.
+inline int cuda_status_code(cudaError_t e) { return e == cudaErrorMemoryAllocation ? 3 : 4; }
+inline bool cuda_error_is_sticky(cudaError_t e) {
+  switch (e) {
+    case cudaErrorIllegalAddress: case cudaErrorLaunchFailure: case cudaErrorIllegalInstruction:
+    case cudaErrorMisalignedAddress: case cudaErrorInvalidAddressSpace: case cudaErrorInvalidPc:
+    case cudaErrorHardwareStackError: case cudaErrorAssert: case cudaErrorLaunchTimeout:
+    case cudaErrorECCUncorrectable:
+      return true;
+    default:
+      return false;
+  }
+}
+inline std::string cuda_error_text(const char* call, cudaError_t e) {
+  std::string m = std::string(call) + ": " + cudaGetErrorString(e);
+  if (cuda_error_is_sticky(e)) m += " (sticky device error: the CUDA context is lost; destroy the states and exit)";
+  return m;
+}
+
+#define LES_CUDA(call)                                                                          \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) {                                                                    \
+      throw ::les::CudaError(::les::cuda_status_code(e_), ::les::cuda_error_text(#call, e_));   \
+    }                                                                                           \
   } while (0)
 
 #define LES_CHECK_LAUNCH() LES_CUDA(cudaGetLastError())

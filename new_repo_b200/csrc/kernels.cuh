@@ -137,6 +137,13 @@ struct SgsArgs {
   int wall;
   long plane;
   int nz;
+  // optional scalar SGS flux (q[0] != nullptr): pi_j = nu_theta d_j theta
+  // with nu_theta = |S| (inv_prt Cs^2 l^2 + kapd[k]); pi_z(1) = -qs
+  const T* dt[3];  // d theta / dx, dy (uvp nodes), dz (w nodes)
+  T* q[3];         // pi_x, pi_y (uvp nodes), pi_z (w nodes)
+  const double* kapd;  // Cs^2/Pr_t Delta^2 per level (dynamic model) or nullptr
+  double inv_prt;      // 1 / Pr_t (constant model) or 0
+  double qs;           // surface flux
 };
 
 template <typename T>
@@ -246,12 +253,21 @@ __global__ void k_sgs_tau4(const SgsArgs<T> a) {
   T s[6][4], cs[4], nu[4], d0[4], d1[4], d3[4], d4[4], d8[4], r[4];
   sij_at4(a, o, k, s);
   ld4(a.cs + o, cs);
+  T sn[4];  // |S| at this level
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const T si[6] = {s[0][i], s[1][i], s[2][i], s[3][i], s[4][i], s[5][i]};
-    nu[i] = strain_norm(si) * cs[i] * T(a.l2[k]);
+    sn[i] = strain_norm(si);
+    nu[i] = sn[i] * cs[i] * T(a.l2[k]);
   }
   st4(a.nu + o, nu);
+  const bool scal = a.q[0] != nullptr;
+  T nut[4];  // nu_theta at this level
+  if (scal) {
+    const T kd = a.kapd ? T(a.kapd[k]) : T(0);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) nut[i] = sn[i] * (T(a.inv_prt) * cs[i] * T(a.l2[k]) + kd);
+  }
   ld4(a.d[0] + o, d0);
   ld4(a.d[1] + o, d1);
   ld4(a.d[3] + o, d3);
@@ -271,16 +287,44 @@ __global__ void k_sgs_tau4(const SgsArgs<T> a) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) r[i] = T(2) * nu[i] * d4[i];
     st4(a.tyy + o, r);
+    if (scal) {
+      T t[4];
+      ld4(a.dt[0] + o, t);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r[i] = nut[i] * t[i];
+      st4(a.q[0] + o, r);
+      ld4(a.dt[1] + o, t);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r[i] = nut[i] * t[i];
+      st4(a.q[1] + o, r);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r[i] = -T(a.qs);
+      st4(a.q[2] + o, r);
+    }
   } else {
     if (k <= a.nz) {
-      T s2[6][4], csp[4], c[4];
+      T s2[6][4], csp[4], c[4], ct[4];
       sij_at4(a, o + pl, k + 1, s2);
       ld4(a.cs + o + pl, csp);
+      const T kdp = (scal && a.kapd) ? T(a.kapd[k + 1]) : T(0);
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const T si[6] = {s2[0][i], s2[1][i], s2[2][i], s2[3][i], s2[4][i], s2[5][i]};
-        const T nukp = strain_norm(si) * csp[i] * T(a.l2[k + 1]);
+        const T snp = strain_norm(si);
+        const T nukp = snp * csp[i] * T(a.l2[k + 1]);
         c[i] = T(0.5) * (nu[i] + nukp);
+        if (scal) ct[i] = T(0.5) * (nut[i] + snp * (T(a.inv_prt) * csp[i] * T(a.l2[k + 1]) + kdp));
+      }
+      if (scal) {
+        T t[4];
+        ld4(a.dt[0] + o, t);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) r[i] = ct[i] * t[i];
+        st4(a.q[0] + o, r);
+        ld4(a.dt[1] + o, t);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) r[i] = ct[i] * t[i];
+        st4(a.q[1] + o, r);
       }
 #pragma unroll
       for (int i = 0; i < 4; ++i) r[i] = T(2) * c[i] * d0[i];
@@ -301,6 +345,13 @@ __global__ void k_sgs_tau4(const SgsArgs<T> a) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) r[i] = T(2) * nu[i] * s[4][i];
     st4(a.tyz + o, r);
+    if (scal) {
+      T t[4];
+      ld4(a.dt[2] + o, t);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r[i] = nut[i] * t[i];
+      st4(a.q[2] + o, r);
+    }
   }
 }
 
@@ -923,6 +974,141 @@ __global__ void __launch_bounds__(256) k_diag_final(const double* part, int nblo
     out[2] = a.sum[4].val() / double(plane);
     out[3] = sqrt(a.sum[3].val() / npts);
     if (a.nan != 0.0) atomicOr(status, ST_NAN);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// scalar transport, buoyancy and momentum forcing
+
+// Plane means (FP64, Neumaier) of up to four fields on levels k0..k1: one
+// block per level, out[f * L + k].  Fixed reduction order (per thread, then
+// threads in order), so repeated runs give the same bits.
+template <typename T>
+__global__ void k_plane_means(const T* f0, const T* f1, const T* f2, const T* f3, int nf, double* out, long plane,
+                              int k0, int L) {
+  const int k = k0 + blockIdx.x;
+  const T* fs[4] = {f0, f1, f2, f3};
+  __shared__ double sh[4][2][256];
+  for (int f = 0; f < nf; ++f) {
+    Neu a;
+    const T* x = fs[f] + (long)k * plane;
+    for (long p = threadIdx.x; p < plane; p += blockDim.x) a.add(double(x[p]));
+    sh[f][0][threadIdx.x] = a.s;
+    sh[f][1][threadIdx.x] = a.c;
+  }
+  __syncthreads();
+  if (threadIdx.x < nf) {
+    const int f = threadIdx.x;
+    Neu t;
+    for (int i = 0; i < blockDim.x; ++i) {
+      t.add(sh[f][0][i]);
+      t.add(sh[f][1][i]);
+    }
+    out[f * L + k] = t.val() / double(plane);
+  }
+}
+
+// Plane-averaged least-squares coefficient per level k = 1..nz+1 (one block
+// per level): kapd[k] = max(0, <KX> / <XX>) * scale (FP64 Neumaier sums; 0
+// where <XX> = 0), the reduction of compute_DynSmag.f90:61-245 written to a
+// per-level array.
+template <typename T>
+__global__ void k_level_ratio(const T* KX, const T* XX, double* kapd, long plane, double scale) {
+  const int k = blockIdx.x + 1;
+  __shared__ double sh[4][256];
+  Neu a, b;
+  for (long p = threadIdx.x; p < plane; p += blockDim.x) {
+    a.add(double(KX[(long)k * plane + p]));
+    b.add(double(XX[(long)k * plane + p]));
+  }
+  sh[0][threadIdx.x] = a.s;
+  sh[1][threadIdx.x] = a.c;
+  sh[2][threadIdx.x] = b.s;
+  sh[3][threadIdx.x] = b.c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Neu x, y;
+    for (int i = 0; i < blockDim.x; ++i) {
+      x.add(sh[0][i]);
+      x.add(sh[1][i]);
+      y.add(sh[2][i]);
+      y.add(sh[3][i]);
+    }
+    const double num = x.val() / double(plane), den = y.val() / double(plane);
+    const double c = (den != 0.0) ? num / den : 0.0;
+    kapd[k] = fmax(0.0, c) * scale;
+  }
+}
+
+// Wall value of d theta/dz (level 1): the log law of the prescribed surface
+// flux, -qs / (kappa u* dz/2), zero where u* = 0.
+template <typename T>
+__global__ void k_scalar_wall(T* dtdz1, const T* ustar, long plane, double qs, double half_dz) {
+  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < plane; p += (long)gridDim.x * blockDim.x) {
+    const double us = double(ustar[p]);
+    dtdz1[p] = (us != 0.0) ? T(-qs / (KVONK * us * half_dz)) : T(0);
+  }
+}
+
+// step_scalars (compute_scalars.f90:111-125): theta += dt (t1 rhs + t2 rhs_f)
+// on levels 1..nz (the ghost values follow with k_scalar_bc)
+template <typename T>
+__global__ void k_ab2_scalar(T* th, const T* r, const T* rf, long plane, int nz, T dt, T t1, T t2) {
+  const long n = (long)nz * plane;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long o = plane + q;
+    th[o] = th[o] + dt * (t1 * r[o] + t2 * rf[o]);
+  }
+}
+
+// Ghost values of theta (compute_scalars.f90:127-133 with a lid gradient):
+// theta(0) = 0, theta(nz+1) = theta(nz) + g_top dz.
+template <typename T>
+__global__ void k_scalar_bc(T* th, long plane, int nz, T gdz) {
+  for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < plane; p += (long)gridDim.x * blockDim.x) {
+    th[p] = T(0);
+    th[(long)(nz + 1) * plane + p] = th[(long)nz * plane + p] + gdz;
+  }
+}
+
+// Coriolis (LES_engine.f90:553-561) and the sponge (sponge_damping.f90:131-161)
+// on levels 1..nz.  mean[0*L + k], mean[1*L + k], mean[2*L + k]: plane means
+// of u, v, w; sp[k]: the sponge profile on w nodes (nullptr: none).
+template <typename T>
+__global__ void k_forcing(T* rx, T* ry, T* rz, const T* u, const T* v, const T* w, const double* mean,
+                          const double* sp, long plane, int nz, int L, T f, T ug, T vg) {
+  const long n = (long)nz * plane;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long o = plane + q;
+    const int k = int(o / plane);
+    const T uo = u[o], vo = v[o];
+    T x = rx[o], y = ry[o];
+    if (f != T(0)) {
+      x = x + f * vo - f * vg;
+      y = y - f * uo + f * ug;
+    }
+    if (sp) {
+      const T sh = T(0.5 * (sp[k] + sp[k + 1]));
+      x = x - sh * (uo - T(mean[k]));
+      y = y - sh * (vo - T(mean[L + k]));
+      rz[o] = rz[o] - T(sp[k]) * (w[o] - T(mean[2 * L + k]));
+    }
+    rx[o] = x;
+    ry[o] = y;
+  }
+}
+
+// Buoyancy on w nodes k = 2..nz: rz += beta (theta_w - <theta_w>),
+// theta_w(k) = (theta(k) + theta(k-1)) / 2; tmean = plane means of theta.
+template <typename T>
+__global__ void k_buoyancy(T* rz, const T* th, const double* tmean, long plane, int nz, T beta) {
+  const long n = (long)(nz - 1) * plane;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long o = 2 * plane + q;
+    const int k = int(o / plane);
+    const T tw = T(0.5) * (th[o] + th[o - plane]);
+    const T twm = T(0.5 * (tmean[k] + tmean[k - 1]));
+    rz[o] = rz[o] + beta * (tw - twm);
   }
 }
 

@@ -135,8 +135,13 @@ extern "C" int les_grad_xy_noalloc(double* f, double* dfdx, double* dfdy, int nx
     return fail(LES_ERR_INVALID, "les_grad_xy_noalloc: field pointers must be 16-byte aligned");
   if (nx <= 0 || ny <= 0 || nlev <= 0 || !(lx > 0) || !(ly > 0))
     return fail(LES_ERR_INVALID, "les_grad_xy_noalloc: invalid grid or domain size");
-  if (!supported_length(nx) || !supported_length(ny))
-    return fail(LES_ERR_INVALID, "les_grad_xy_noalloc: nx and ny must be supported FFT lengths (16 .. 768)");
+  // x: every length with a register FFT plan; y: the lengths with an
+  // equal-length y pass (powers of two), checked before anything is queued
+  const bool ny_ok = ny == 16 || ny == 32 || ny == 64 || ny == 128 || ny == 256 || ny == 512;
+  if (!supported_length(nx) || !ny_ok)
+    return fail(LES_ERR_INVALID,
+                "les_grad_xy_noalloc: nx must be one of 16 24 32 48 64 96 128 192 256 384 512 768 and ny one of "
+                "16 32 64 128 256 512");
   const ScratchLayout L = scratch_layout(nx, ny, nlev);
   if (L.total > kScratchBytes) {
     std::snprintf(g_noalloc_error, sizeof(g_noalloc_error),
@@ -145,7 +150,9 @@ extern "C" int les_grad_xy_noalloc(double* f, double* dfdx, double* dfdy, int nx
                   nx, ny, nlev, L.total, kScratchBytes);
     return LES_ERR_INVALID;
   }
-  // launches here are not observed by a solver's profiling hook
+  // launches here are not observed by a solver's profiling hook; the hook is
+  // per host thread, so only states profiled on the calling thread are
+  // affected, and only for the duration of this call
   LaunchHook* saved = g_hook;
   g_hook = nullptr;
   int rc = LES_OK;

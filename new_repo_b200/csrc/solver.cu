@@ -107,13 +107,9 @@ class Solver final : public SolverBase {
     LES_CUDA(cudaSetDevice(p.device));
     LES_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     for (auto& e : ev) LES_CUDA(cudaEventCreate(&e));
-    static bool attrs = false;
-    if (!attrs) {
-      init_spectral_attributes();
-      attrs = true;
-    }
+    init_spectral_attributes();  // once per device (this one is current)
     const long nf = g.field();
-    for (int i = 0; i < LES_NFIELDS; ++i) F[i] = track(dalloc<T>(nf));
+    for (int i = 0; i < LES_THETA; ++i) F[i] = track(dalloc<T>(nf));  // scalar fields: les_scalar_init
     for (int i = 0; i < LES_NPLANES; ++i) PL[i] = track(dalloc<T>(g.plane()));
     build_tables();
     const long se = (long)g.L * std::max((long)g.ny * pitch(g.lhx), (long)g.ny2 * pitch(g.nx / 2));
@@ -367,8 +363,10 @@ class Solver final : public SolverBase {
     LES_CUDA(cudaStreamSynchronize(st));
     for (long i = 0; i < g.plane(); ++i) h[i] = double(tmp[i]);
   }
+  bool has_field(int f) const override { return f >= 0 && f < LES_NFIELDS && F[f] != nullptr; }
   void check_field(int field, int k0, int k1) const {
     if (field < 0 || field >= LES_NFIELDS) throw CudaError(1, "invalid field id");
+    if (!F[field]) throw CudaError(1, "field not allocated (the scalar fields need les_scalar_init)");
     if (k0 < 0 || k1 > g.nz + 1 || k1 < k0) throw CudaError(1, "invalid level range");
   }
 
@@ -961,17 +959,17 @@ class Solver final : public SolverBase {
 
   // ------------------------------------------------ compute_derivatives ----
   // grad_velocity_filt for up to three fields at once
-  void grad_fields(const int* f, const int* dx, const int* dy, int nfld) {
+  void grad_fields(const int* f, const int* dx, const int* dy, int nfld, const char* tag = "grad") {
     T *pf[3], *pdx[3], *pdy[3];
     for (int q = 0; q < nfld; ++q) {
       pf[q] = F[f[q]];
       pdx[q] = F[dx[q]];
       pdy[q] = F[dy[q]];
     }
-    grad_ptrs(pf, pdx, pdy, nfld);
+    grad_ptrs(pf, pdx, pdy, nfld, tag);
   }
-  void grad_ptrs(T* const* f, T* const* dx, T* const* dy, int nfld) {
-    Tag tag_(this, "grad");
+  void grad_ptrs(T* const* f, T* const* dx, T* const* dy, int nfld, const char* tag = "grad") {
+    Tag tag_(this, tag);
     const int L = g.L;
     auto a = xf(XF_SCALE, nfld, 0, L, g.nx, g.ny, g.lhx);
     a.c0 = 1.0 / double(g.nx * g.ny);
@@ -1029,6 +1027,7 @@ class Solver final : public SolverBase {
     Tag tag_(this, "grad");
     KL("k_ddz_vel", 6.0 * (g.nz + 1) * g.plane() * sizeof(T), k_ddz_vel<T><<<grid_for((long)(g.nz + 1) * g.plane()), 256, 0, st>>>(
         F[LES_U], F[LES_V], F[LES_W], F[LES_DUDZ], F[LES_DVDZ], F[LES_DWDZ], g.plane(), g.nz, T(1.0 / dz())));
+    if (scalar_on) scalar_grad();
   }
 
   // stress divergence of up to three equations (compute_derivatives.f90:464-577)
@@ -1036,8 +1035,8 @@ class Solver final : public SolverBase {
     int rhs, tx, ty, tz, stag;
     double pf;
   };
-  void div_eqs(const DivEq* e, int neq, bool layers) {
-    Tag tag_(this, "divstress");
+  void div_eqs(const DivEq* e, int neq, bool layers, const char* tag = "divstress") {
+    Tag tag_(this, tag);
     // forward transforms of the distinct tx, ty fields
     int ids[6];
     int nid = 0;
@@ -1463,8 +1462,22 @@ class Solver final : public SolverBase {
     } else {
       throw CudaError(1, "Invalid SGS model");
     }
+    double sbytes = 17.0;
+    if (scalar_on) {
+      if (SP.sgs == LES_SCALAR_SGS_DYN && jtt >= P.dyn_init && jt % P.cs_count == 0) scalar_dynamic(a);
+      a.dt[0] = F[LES_DTDX];
+      a.dt[1] = F[LES_DTDY];
+      a.dt[2] = F[LES_DTDZ];
+      a.q[0] = F[LES_QX];
+      a.q[1] = F[LES_QY];
+      a.q[2] = F[LES_QZ];
+      a.kapd = SP.sgs == LES_SCALAR_SGS_DYN ? kapd : nullptr;
+      a.inv_prt = SP.sgs == LES_SCALAR_SGS_DYN ? 0.0 : 1.0 / SP.pr_t;
+      a.qs = SP.surface_flux;
+      sbytes += 6.0;
+    }
     if (g.plane() % 4 == 0)
-      KL("k_sgs_tau", 17.0 * (g.nz + 1) * g.plane() * sizeof(T),
+      KL("k_sgs_tau", sbytes * (g.nz + 1) * g.plane() * sizeof(T),
          k_sgs_tau4<T><<<dim3(unsigned((g.plane() / 4 + 255) / 256), unsigned(g.nz + 1)), 256, 0, st>>>(a));
     else
       KL("k_sgs_tau", 17.0 * (g.nz + 1) * g.plane() * sizeof(T),
@@ -1582,6 +1595,220 @@ class Solver final : public SolverBase {
     launch_xinv<T>(g.nx, c, st);
   }
 
+  // ------------------------------------------- scalar transport (theta) ----
+  double* kapd = nullptr;    // Cs^2/Pr_t * Delta^2 per level (dynamic model)
+  double* means = nullptr;   // plane means: 4 x L (u, v, w, theta)
+  double* spong = nullptr;   // sponge profile on w nodes (L)
+  void scalar_init(const les_scalar_params& sp) override {
+    if (!(sp.pr_t > 0.0)) throw CudaError(1, "Invalid scalar parameters: pr_t must be positive");
+    if (sp.sgs != LES_SCALAR_SGS_CONST && sp.sgs != LES_SCALAR_SGS_DYN)
+      throw CudaError(1, "Invalid scalar SGS model");
+    if (g.plane() % 4 != 0) throw CudaError(1, "scalar transport needs nx * ny divisible by 4");
+    SP = sp;
+    const long nf = g.field();
+    for (int i = LES_THETA; i < LES_NFIELDS; ++i) {
+      if (!F[i]) F[i] = track(dalloc<T>(nf));
+      fill(F[i], 0, g.nz + 1, T(0));
+    }
+    if (!kapd) kapd = track(dalloc<double>(g.L));
+    if (!means) means = track(dalloc<double>(4 * g.L));
+    // kappa before the first dynamic update: 0.03 / Pr_t (the LASD start value over Pr_t)
+    const double d2 = delta * delta;
+    std::vector<double> k0(g.L, sp.sgs == LES_SCALAR_SGS_DYN ? 0.03 / sp.pr_t * d2 : 0.0);
+    LES_CUDA(cudaMemcpyAsync(kapd, k0.data(), sizeof(double) * g.L, cudaMemcpyHostToDevice, st));
+    scalar_on = true;
+    scalar_bc();
+    LES_CUDA(cudaStreamSynchronize(st));
+  }
+  void scalar_bc() {
+    KL("k_scalar_bc", 3.0 * g.plane() * sizeof(T),
+       k_scalar_bc<T><<<grid_for(g.plane()), 256, 0, st>>>(F[LES_THETA], g.plane(), g.nz, T(SP.top_gradient * dz())));
+  }
+  void scalar_set_initial(const double* theta) override {
+    if (!scalar_on) throw CudaError(1, "scalar not initialised (les_scalar_init)");
+    upload(LES_THETA, theta, 1, g.nz);
+    scalar_bc();
+    LES_CUDA(cudaStreamSynchronize(st));
+  }
+  void scalar_kappa(double* out, int n) override {
+    if (!scalar_on) throw CudaError(1, "scalar not initialised (les_scalar_init)");
+    if (n < g.L) throw CudaError(1, "kappa output needs nz + 2 values");
+    std::vector<double> h(g.L);
+    LES_CUDA(cudaMemcpyAsync(h.data(), kapd, sizeof(double) * g.L, cudaMemcpyDeviceToHost, st));
+    LES_CUDA(cudaStreamSynchronize(st));
+    const double d2 = delta * delta;
+    for (int k = 0; k < g.L; ++k) out[k] = SP.sgs == LES_SCALAR_SGS_DYN ? h[k] / d2 : 0.0;
+  }
+  void sponge_init(double frac) override {
+    // sponge_damping.f90:61-80 on w nodes z = (k-1) dz, without the zeroing of :83
+    sponge_frac = frac > 0.0 ? frac : 0.0;
+    if (sponge_frac <= 0.0) return;
+    if (sponge_frac >= 1.0) throw CudaError(1, "sponge layer fraction must be below 1");
+    std::vector<double> h(g.L, 0.0);
+    const double lz = P.lz, z_d = sponge_frac * lz;
+    for (int k = 1; k <= g.nz + 1; ++k) {
+      const double z = (1 + k - 2.0) * dz();
+      if (z >= z_d && z <= lz) h[k] = 3.9 * 0.5 * (1.0 - std::cos(PI * (z - z_d) / (lz - z_d)));
+    }
+    h[g.nz + 1] = h[g.nz];
+    if (!spong) spong = track(dalloc<double>(g.L));
+    if (!means) means = track(dalloc<double>(4 * g.L));
+    LES_CUDA(cudaMemcpy(spong, h.data(), sizeof(double) * g.L, cudaMemcpyHostToDevice));
+  }
+
+  // gradients of theta (after compute_vel_grad: the wall law's u* is current)
+  void scalar_grad() {
+    Tag tag_(this, "scalar");
+    const int f = LES_THETA, dx = LES_DTDX, dy = LES_DTDY;
+    grad_fields(&f, &dx, &dy, 1, "scalar");
+    KL("k_ddz", 2.0 * (g.nz + 1) * g.plane() * sizeof(T),
+       k_ddz<T><<<grid_for((long)(g.nz + 1) * g.plane()), 256, 0, st>>>(F[LES_DTDZ], F[LES_THETA], g.plane(), g.nz,
+                                                                       T(1.0 / dz()), 0));
+    KL("k_scalar_wall", 2.0 * g.plane() * sizeof(T),
+       k_scalar_wall<T><<<grid_for(g.plane()), 256, 0, st>>>(lev(F[LES_DTDZ], 1), PL[LES_U_STAR_AVG], g.plane(),
+                                                             SP.surface_flux, 0.5 * dz()));
+  }
+
+  // dynamic Prandtl model: plane-averaged Cs^2/Pr_t at the 2 Delta filter
+  void scalar_dynamic(SgsArgs<T>& a) {
+    Tag tag_(this, "scalar");
+    const int nlev = g.nz + 1;
+    const long n1 = (long)nlev * g.plane();
+    SgsArgs<T> ab = a;
+    KL("k_sij", 16.0 * n1 * sizeof(T), k_sij<T><<<grid_for(n1), 256, 0, st>>>(ab));
+    auto x = xf(XF_SCDYN, 19, 1, nlev, g.nx, g.ny, nk2);
+    x.in[0] = F[LES_U];
+    x.in[1] = F[LES_V];
+    x.in[2] = F[LES_W];
+    x.in[3] = F[LES_THETA];
+    for (int q = 0; q < 6; ++q) x.in[4 + q] = sc[1 + q];
+    x.in[10] = sc[0];
+    x.in[11] = F[LES_DTDX];
+    x.in[12] = F[LES_DTDY];
+    x.in[13] = F[LES_DTDZ];
+    for (int q = 0; q < 19; ++q) x.out[q] = spec[q];
+    x.fluct = mixed() ? 1 : 0;
+    launch_xfwd<T>(g.nx, x, st);
+    auto y = yp(YP_FILTER1, 1, 1, nk2, nk2, g.ny, nk2, g.ny, 1);
+    y.G0 = gt;
+    for (int q = 0; q < 19; ++q) {
+      y.in[q] = spec[q];
+      y.out[q] = spec[q];
+    }
+    launch_ypass<T>(g.ny, g.ny, y, nlev, 19, st);
+    auto z = xi(XI_SCDYN, 19, 1, nlev, g.nx, g.ny, nk2);
+    z.c0 = delta * delta;
+    z.c1 = 4.0;
+    for (int q = 0; q < 19; ++q) z.in[q] = spec[q];
+    z.out[0] = sc[7];
+    z.out[1] = sc[8];
+    launch_xinv<T>(g.nx, z, st);
+    KL("k_level_ratio", 2.0 * n1 * sizeof(T),
+       k_level_ratio<T><<<nlev, 256, 0, st>>>(sc[7], sc[8], kapd, g.plane(), delta * delta));
+  }
+
+  // scalar convective term into rhs_t (levels 1..nz); the padded -u, -v, -w
+  // of the momentum's convective term are still in fine[0..2]
+  void scalar_convec() {
+    Tag tag_(this, "scalar");
+    const int nz = g.nz;
+    const bool padd = (P.dealias == LES_DEALIAS_PADD);
+    const int nkin = padd ? g.nx / 2 : int(std::ceil(double(float(g.nx)) / 3.0)) - 1;
+    const int FNX = padd ? g.nx2 : g.nx;
+    const int FNY = padd ? g.ny2 : g.ny;
+    auto a = xf(XF_SCALE, 3, 1, nz + 1, g.nx, g.ny, nkin);
+    a.c0 = 1.0 / double(g.nx * g.ny);
+    a.in[0] = F[LES_DTDX];
+    a.in[1] = F[LES_DTDY];
+    a.in[2] = F[LES_DTDZ];
+    for (int q = 0; q < 3; ++q) a.out[q] = spec[q];
+    launch_xfwd<T>(g.nx, a, st);
+    if (padd) {
+      auto b = yp(YP_PAD, 1, 1, nkin, nkin, g.ny, nkin, g.ny2, 1);
+      for (int q = 0; q < 3; ++q) {
+        b.in[q] = spec[q];
+        b.out[q] = spec[6 + q];
+      }
+      launch_ypass<T>(g.ny, g.ny2, b, nz + 1, 3, st);
+    } else {
+      auto b = yp(YP_MASK, 1, 1, nkin, nkin, g.ny, nkin, g.ny, 1);
+      b.tt = int(std::ceil(double(float(g.ny)) / 3.0)) - 2;
+      for (int q = 0; q < 3; ++q) {
+        b.in[q] = spec[q];
+        b.out[q] = spec[6 + q];
+      }
+      launch_ypass<T>(g.ny, g.ny, b, nz + 1, 3, st);
+    }
+    auto c = xi(XI_STORE, 3, 1, nz + 1, FNX, FNY, nkin);
+    for (int q = 0; q < 3; ++q) {
+      c.in[q] = spec[6 + q];
+      c.out[q] = fine[3 + q];
+      c.lo[q] = 0;
+      c.hi[q] = nz + 1;
+    }
+    launch_xinv<T>(FNX, c, st);
+    const int nkout = padd ? g.nx / 2 : int(std::ceil(double(float(2 * g.lhx)) / 3.0)) - 1;
+    auto d = xf(XF_PROD_SC, 1, 1, nz, FNX, FNY, nkout);
+    d.c0 = padd ? 1.0 / double(g.nx2 * g.ny2) : 1.0 / double(g.nx * g.ny);
+    for (int q = 0; q < 6; ++q) d.in[q] = fine[q];
+    d.out[0] = spec[0];
+    launch_xfwd<T>(FNX, d, st);
+    if (padd) {
+      auto e = yp(YP_TRUNC, 1, 1, nkout, nkout, g.ny2, nkout, g.ny, 1);
+      e.in[0] = spec[0];
+      e.out[0] = spec[3];
+      launch_ypass<T>(g.ny2, g.ny, e, nz, 1, st);
+    } else {
+      auto e = yp(YP_MASK, 1, 1, nkout, nkout, g.ny, nkout, g.ny, 1);
+      e.tt = int(std::ceil(double(float(2 * g.lhy)) / 3.0)) - 2;
+      e.in[0] = spec[0];
+      e.out[0] = spec[3];
+      launch_ypass<T>(g.ny, g.ny, e, nz, 1, st);
+    }
+    auto h = xi(XI_STORE, 1, 1, nz, g.nx, g.ny, nkout);
+    h.in[0] = spec[3];
+    h.out[0] = F[LES_RHS_T];
+    h.lo[0] = 1;
+    h.hi[0] = nz;
+    launch_xinv<T>(g.nx, h, st);
+  }
+
+  // after the momentum right-hand side: forcing, scalar rhs, buoyancy
+  void rhs_extras() {
+    const int L = g.L;
+    if (coriol != 0.0 || sponge_frac > 0.0) {
+      Tag tag_(this, "forcing");
+      if (sponge_frac > 0.0)
+        KL("k_plane_means", 3.0 * g.nz * g.plane() * sizeof(T),
+           k_plane_means<T><<<g.nz, 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], nullptr, 3, means, g.plane(), 1, L));
+      KL("k_forcing", 7.0 * g.nz * g.plane() * sizeof(T),
+         k_forcing<T><<<grid_for((long)g.nz * g.plane()), 256, 0, st>>>(
+             F[LES_RHSX], F[LES_RHSY], F[LES_RHSZ], F[LES_U], F[LES_V], F[LES_W], means,
+             sponge_frac > 0.0 ? spong : nullptr, g.plane(), g.nz, L, T(coriol), T(ug), T(vg)));
+    }
+    if (!scalar_on) return;
+    {
+      Tag tag_(this, "scalar");
+      // rhs_t_f = rhs_t (buffer exchange, as the momentum's)
+      copy(lev(F[LES_RHS_T], 0), lev(F[LES_RHS_T_F], 0), g.plane());
+      copy(lev(F[LES_RHS_T], g.nz + 1), lev(F[LES_RHS_T_F], g.nz + 1), g.plane());
+      std::swap(F[LES_RHS_T], F[LES_RHS_T_F]);
+    }
+    scalar_convec();
+    {
+      DivEq e{LES_RHS_T, LES_QX, LES_QY, LES_QZ, 1, 0.0};
+      div_eqs(&e, 1, false, "scalar");
+    }
+    if (SP.buoyancy != 0.0) {
+      Tag tag_(this, "scalar");
+      KL("k_plane_means", double(L) * g.plane() * sizeof(T),
+         k_plane_means<T><<<L, 256, 0, st>>>(F[LES_THETA], nullptr, nullptr, nullptr, 1, means + 3 * L, g.plane(), 0, L));
+      KL("k_buoyancy", 3.0 * (g.nz - 1) * g.plane() * sizeof(T),
+         k_buoyancy<T><<<grid_for((long)(g.nz - 1) * g.plane()), 256, 0, st>>>(F[LES_RHSZ], F[LES_THETA], means + 3 * L,
+                                                                               g.plane(), g.nz, T(SP.buoyancy)));
+    }
+  }
+
   // -------------------------------------------------------- LES_engine ----
   void compute_rhs_adv() override {
     // LES_engine.f90:516-527: rhs_f(1:nz) = rhs(1:nz); rhs = convective term.
@@ -1603,6 +1830,7 @@ class Solver final : public SolverBase {
                   {LES_RHSY, LES_TXY, LES_TYY, LES_TYZ, 1, P.pfy},
                   {LES_RHSZ, LES_TXZ, LES_TYZ, LES_TZZ, 0, 0.0}};
     div_eqs(e, 3, true);
+    rhs_extras();
   }
 
   void ab2(double tadv1, double tadv2) override {
@@ -1610,6 +1838,13 @@ class Solver final : public SolverBase {
     KL("k_ab2", 12.0 * g.nz * g.plane() * sizeof(T), k_ab2<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_U], F[LES_V], F[LES_W], F[LES_RHSX], F[LES_RHSY],
                                                  F[LES_RHSZ], F[LES_RHSX_F], F[LES_RHSY_F], F[LES_RHSZ_F],
                                                  g.plane(), g.nz, T(P.dt), T(tadv1), T(tadv2)));
+    if (scalar_on)
+    {
+      KL("k_ab2_scalar", 4.0 * g.nz * g.plane() * sizeof(T),
+         k_ab2_scalar<T><<<grid_for((long)g.nz * g.plane()), 256, 0, st>>>(
+             F[LES_THETA], F[LES_RHS_T], F[LES_RHS_T_F], g.plane(), g.nz, T(P.dt), T(tadv1), T(tadv2)));
+      scalar_bc();
+    }
   }
 
   void projection(double tadv1) override {

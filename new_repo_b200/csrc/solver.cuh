@@ -139,6 +139,16 @@ struct SolverBase : LaunchHook {
   virtual void tke_init(const char* out_path) = 0;
   virtual void tke_budget(int jt, int tke_period) = 0;
   virtual void tke_sums(double* out, int* record) = 0;
+  // scalar transport, buoyancy, sponge, Coriolis
+  bool scalar_on = false;
+  les_scalar_params SP{};
+  double sponge_frac = 0.0;
+  double coriol = 0.0, ug = 0.0, vg = 0.0;
+  virtual void scalar_init(const les_scalar_params& sp) = 0;
+  virtual void scalar_set_initial(const double* theta) = 0;
+  virtual void scalar_kappa(double* out, int n) = 0;
+  virtual void sponge_init(double frac) = 0;
+  virtual bool has_field(int f) const = 0;
   // timing events on the state's stream
   cudaEvent_t slots[16] = {};
   void record_event(int i) {

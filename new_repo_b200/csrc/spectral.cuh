@@ -54,6 +54,8 @@ enum XFOp : int {
   XF_PROD = 2,    // fine-grid u x omega products (inputs on the padded grid)
   XF_LASD = 3,    // the 21 test-filter inputs of the dynamic procedure
   XF_PRESS = 4,   // field f = c0 * (in[f] / c1)   (compute_pressure.f90:138-140)
+  XF_PROD_SC = 5, // fine-grid scalar advection -(u . grad theta) (inputs on the padded grid)
+  XF_SCDYN = 6,   // the 19 test-filter inputs of the dynamic Prandtl model
 };
 
 template <typename T>
@@ -73,8 +75,8 @@ struct XFArgs {
   long in_pstride; // elements per plane of the input grid
   long in_rstride; // elements per row of the input grid (== NX)
   double c0, c1;
-  const T* in[12];
-  const float* inf[12];  // FP32 inputs of an FP64 transform (in_f32 = 1)
+  const T* in[16];
+  const float* inf[16];  // FP32 inputs of an FP64 transform (in_f32 = 1)
   int in_f32;
   cplx<T>* out[MAXIN];
   long out_pstride;  // rows_pp * nk
@@ -238,6 +240,61 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
         vst(v + 1 * vs, c * (ub0 * o30 + T(0.5) * (wb0 * (-o10) + wbu * (-o1u))));
         vst(v + 2 * vs, c * T(0.5) * ((ub0 + vld<V>(ub, dn)) * (-o20) + (vb0 + vld<V>(vb, dn)) * o10));
       }
+      break;
+    }
+    case XF_PROD_SC: {
+      // scalar advection on the fine grid, uvp level l: inputs ub, vb, wb
+      // (padded -u, -v, -w), tx, ty (padded d theta/dx, dy, uvp nodes) and
+      // tz (padded d theta/dz, w nodes): ub tx + vb ty + (wb tz at l, l+1)/2
+      const T c = T(a.c0);
+      const long up = off + a.in_pstride;
+      const V r = vld<V>(a.in[0], off) * vld<V>(a.in[3], off) + vld<V>(a.in[1], off) * vld<V>(a.in[4], off) +
+                  T(0.5) * (vld<V>(a.in[2], off) * vld<V>(a.in[5], off) + vld<V>(a.in[2], up) * vld<V>(a.in[5], up));
+      vst(v, c * r);
+      break;
+    }
+    case XF_SCDYN: {
+      // dynamic Prandtl model on the nodes of compute_dynamic_mum
+      // (compute_LagScaleDep.f90:501-520: level 1 on uvp nodes with w(2)/4,
+      // levels >= 2 on w nodes).  Inputs: 0 u, 1 v, 2 w, 3 theta, 4..9 S_ij,
+      // 10 |S|, 11 d theta/dx, 12 d theta/dy, 13 d theta/dz (w nodes).
+      // Outputs: u, v, w, theta, u theta, v theta, w theta, S_ij (6),
+      // d_j theta (3), |S| d_j theta (3).
+      const long pl = a.in_pstride;
+      auto at_w = [&](const T* f, long o) -> V {
+        return l == 1 ? vld<V>(f, o) : T(0.5) * (vld<V>(f, o) + vld<V>(f, o - pl));
+      };
+      V uf = at_w(a.in[0], off), vf = at_w(a.in[1], off), tf = at_w(a.in[3], off);
+      V wf = l == 1 ? T(0.25) * vld<V>(a.in[2], off + pl) : vld<V>(a.in[2], off);
+      if (a.fluct) {
+        // K_j = filt(u_j theta) - filt(u_j) filt(theta) does not change when
+        // per-level constants are removed from u_j and theta (the filter
+        // keeps the mean); FP32 keeps the fluctuations
+        const long o0 = (long)l * pl;
+        auto at_w0 = [&](const T* f) -> T { return l == 1 ? f[o0] : T(0.5) * (f[o0] + f[o0 - pl]); };
+        const T w0 = l == 1 ? T(0.25) * a.in[2][o0 + pl] : a.in[2][o0];
+        uf = uf - vsplat<V>(at_w0(a.in[0]));
+        vf = vf - vsplat<V>(at_w0(a.in[1]));
+        tf = tf - vsplat<V>(at_w0(a.in[3]));
+        wf = wf - vsplat<V>(w0);
+      }
+      vst(v + 0 * vs, uf);
+      vst(v + 1 * vs, vf);
+      vst(v + 2 * vs, wf);
+      vst(v + 3 * vs, tf);
+      vst(v + 4 * vs, uf * tf);
+      vst(v + 5 * vs, vf * tf);
+      vst(v + 6 * vs, wf * tf);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) vst(v + (7 + q) * vs, vld<V>(a.in[4 + q], off));
+      const V S = vld<V>(a.in[10], off);
+      const V tx = at_w(a.in[11], off), ty = at_w(a.in[12], off), tz = vld<V>(a.in[13], off);
+      vst(v + 13 * vs, tx);
+      vst(v + 14 * vs, ty);
+      vst(v + 15 * vs, tz);
+      vst(v + 16 * vs, S * tx);
+      vst(v + 17 * vs, S * ty);
+      vst(v + 18 * vs, S * tz);
       break;
     }
     case XF_LASD: {
@@ -944,6 +1001,7 @@ enum XIOp : int {
   XI_DIV = 2,    // rhs += x + dz(tz) + pf ; pressure-BC layers of the w equation
   XI_LASD = 3,   // 21 filtered fields -> L:M and M:M
   XI_WALL = 4,   // filtered u1, v1 -> u*, Neumann ghost value, wall stress
+  XI_SCDYN = 5,  // 19 filtered fields of the dynamic Prandtl model -> K.X and X.X
 };
 
 template <typename T>
@@ -1213,6 +1271,26 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
         const T b33 = cst * (x[20 * XS] - tf2 * sft * s33);
         a.out[0][off] = a11 * b11 + a22 * b22 + a33 * b33 + T(2) * (a12 * b12 + a13 * b13 + a23 * b23);
         a.out[1][off] = b11 * b11 + b22 * b22 + b33 * b33 + T(2) * (b12 * b12 + b13 * b13 + b23 * b23);
+        break;
+      }
+      case XI_SCDYN: {
+        // K_j = filt(u_j theta) - filt(u_j) filt(theta),
+        // X_j = Delta^2 (filt(|S| d_j theta) - alpha^2 |S~| filt(d_j theta));
+        // c0 = Delta^2, c1 = alpha^2
+        const T uf = x[0], vf = x[XS], wf = x[2 * XS], tf = x[3 * XS];
+        const T k1 = x[4 * XS] - uf * tf;
+        const T k2 = x[5 * XS] - vf * tf;
+        const T k3 = x[6 * XS] - wf * tf;
+        const T s11 = x[7 * XS], s12 = x[8 * XS], s13 = x[9 * XS];
+        const T s22 = x[10 * XS], s23 = x[11 * XS], s33 = x[12 * XS];
+        const T sft = sqrt(T(2) * (s11 * s11 + s22 * s22 + s33 * s33 +
+                                   T(2) * (s12 * s12 + s13 * s13 + s23 * s23)));
+        const T d2 = T(a.c0), tf2 = T(a.c1);
+        const T x1 = d2 * (x[16 * XS] - tf2 * sft * x[13 * XS]);
+        const T x2 = d2 * (x[17 * XS] - tf2 * sft * x[14 * XS]);
+        const T x3 = d2 * (x[18 * XS] - tf2 * sft * x[15 * XS]);
+        a.out[0][off] = k1 * x1 + k2 * x2 + k3 * x3;
+        a.out[1][off] = x1 * x1 + x2 * x2 + x3 * x3;
         break;
       }
       case XI_WALL: {

@@ -197,7 +197,7 @@ void launch_xfwd(int NX, XFArgs<T> a, cudaStream_t st) {
   const bool staged = a.op == XF_PRESS || (a.op == XF_SCALE && a.nf <= 3);
   if (staged) {
     a.in_rstride = NX;
-    static const int nin_of_op[] = {0, 9, 6, 10, 0};
+    static const int nin_of_op[] = {0, 9, 6, 10, 0, 6, 14};
     const int nin = (a.op == XF_SCALE || a.op == XF_PRESS) ? a.nf : nin_of_op[a.op];
     const size_t isz = (a.in_f32 ? sizeof(float) : sizeof(T));
     hook_before("xfwd", double(a.nrows) * NX * nin * isz + double(a.nrows) * a.nf * a.nk * sizeof(cplx<T>));
@@ -230,7 +230,7 @@ void launch_xfwd(int NX, XFArgs<T> a, cudaStream_t st) {
   if (smem > SMEM_CAP) throw CudaError(1, "xfwd: shared memory request too large");
   const int grid = ceil_div(a.nrows, a.R);
   if (grid == 0) return;
-  static const int nin_of_op[] = {0, 9, 6, 10, 0};
+  static const int nin_of_op[] = {0, 9, 6, 10, 0, 6, 14};
   const int nin = (a.op == XF_SCALE || a.op == XF_PRESS) ? a.nf : nin_of_op[a.op];
   const size_t isz = (a.in_f32 ? sizeof(float) : sizeof(T));
   hook_before("xfwd", double(a.nrows) * NX * nin * isz + double(a.nrows) * a.nf * a.nk * sizeof(cplx<T>));
@@ -304,7 +304,7 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
     const size_t osz = (a.out_f32 ? sizeof(float) : sizeof(T));
     int nout = a.nin, rmw = 0;
     if (a.op == XI_DIV) { nout = a.nin; rmw = 2 * a.nin; }
-    else if (a.op == XI_LASD) nout = 2;
+    else if (a.op == XI_LASD || a.op == XI_SCDYN) nout = 2;
     else if (a.op == XI_WALL) nout = 7;
     hook_before("xinv", double(a.nrows) * ns * a.nk * sizeof(cplx<T>) + double(a.nrows) * NX * (nout + rmw) * osz);
   }
@@ -432,9 +432,21 @@ static void set_attrs() {
 #undef YA
 }
 
+// cudaFuncSetAttribute applies to the current device only: done once per
+// device ordinal (fixed table and a mutex, no heap allocation), so states on
+// several devices of one process, and threads creating them at once, all
+// launch with the shared-memory limit raised
 void init_spectral_attributes() {
+  static std::mutex mu;
+  static bool done[256] = {};
+  int dev = 0;
+  LES_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) throw CudaError(1, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[dev]) return;
   set_attrs<float>();
   set_attrs<double>();
+  done[dev] = true;
 }
 
 template void launch_xfwd<float>(int, XFArgs<float>, cudaStream_t);

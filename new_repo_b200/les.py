@@ -96,6 +96,8 @@ class RunParams:
     start_tke: int = 0
     tke_period: int = 100
     spectra_flag: bool = False
+    # LES_engine.f90:81 (a parameter there): check_NaN every nan_check steps
+    nan_check: int = 20
 
     lx: float = field(init=False, default=0.0)
     ly: float = field(init=False, default=0.0)
@@ -334,6 +336,42 @@ class LES:
         check(self.lib.les_download_plane(self._h, PLANE_ID[name], _dptr(out)))
         return out
 
+    # ------------------------------------------------- scalar and forcing
+    def scalar_init(self, surface_flux: float = 0.0, top_gradient: float = 0.0, buoyancy: float = 0.0,
+                    pr_t: float = 0.4, sgs: str = "dynamic"):
+        """scalars_module_init (compute_scalars.f90:40-57): theta on uvp nodes
+        with the SGS flux of the constant- or dynamic-Prandtl model, a wall
+        flux, a lid gradient and (buoyancy = g/theta_0 != 0) buoyancy in the
+        w equation; see les_scalar_init in lesgpu.h."""
+        if sgs not in capi.SCALAR_SGS:
+            raise LesError(capi.LES_ERR_INVALID, f"Invalid scalar SGS model {sgs!r}")
+        sp = capi.ScalarParams(float(surface_flux), float(top_gradient), float(buoyancy), float(pr_t),
+                               capi.SCALAR_SGS[sgs])
+        check(self.lib.les_scalar_init(self._h, C.byref(sp)))
+
+    def scalar_set_initial(self, theta):
+        """theta (nz, ny, nx) on levels 1..nz; the ghost values follow."""
+        a = np.ascontiguousarray(theta, dtype=np.float64)
+        p = self.params
+        if a.shape != (p.nz, p.ny, p.nx):
+            raise LesError(capi.LES_ERR_INVALID, "theta must be (nz, ny, nx)")
+        check(self.lib.les_scalar_set_initial(self._h, _dptr(a)))
+
+    def scalar_kappa(self) -> np.ndarray:
+        """Cs^2/Pr_t per level 0..nz+1 of the dynamic Prandtl model (0 for the constant one)."""
+        out = np.zeros(self.params.nz + 2)
+        check(self.lib.les_scalar_kappa(self._h, _dptr(out), out.size))
+        return out
+
+    def sponge_init(self, layer_fraction: float):
+        """sponge_damping_init (sponge_damping.f90:42-101, no zeroing): damping
+        above layer_fraction * lz, applied at the end of compute_RHS_adv."""
+        check(self.lib.les_sponge_init(self._h, float(layer_fraction)))
+
+    def set_coriolis(self, coriol: float, ug: float = 0.0, vg: float = 0.0):
+        """Coriolis forcing of compute_RHS_adv (LES_engine.f90:553-561)."""
+        check(self.lib.les_set_coriolis(self._h, float(coriol), float(ug), float(vg)))
+
     def set_initial_conditions(self, u, v, w):
         a = [np.ascontiguousarray(x, dtype=np.float64) for x in (u, v, w)]
         check(self.lib.les_set_initial_conditions(self._h, *map(_dptr, a)))
@@ -407,6 +445,8 @@ class LES:
             self.jt += 1
             self.jt_total += 1
             check(self.lib.les_step(self._h, self.jt, self.jt_total))
+            if p.nan_check > 0 and self.jt % p.nan_check == 0:  # LES_engine.f90:363-365
+                self.check_status()
             if p.stat_flag and self.jt_total > p.start_stats:
                 self.stat_averages()
             if p.spectra_flag:
@@ -481,6 +521,15 @@ class LES:
     def status(self) -> int:
         v = C.c_uint()
         check(self.lib.les_get_status(self._h, C.byref(v)))
+        return int(v.value)
+
+    def check_status(self) -> int:
+        """check_NaN (LES_engine.f90:583-616) and the tridiagonal pivot abort
+        (compute_pressure.f90:411-418): LesError(9) with the reference's
+        message when either happened since the last read; otherwise the
+        status bits (read and cleared)."""
+        v = C.c_uint()
+        check(self.lib.les_check_status(self._h, C.byref(v)))
         return int(v.value)
 
     def sync(self):

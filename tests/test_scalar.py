@@ -1,0 +1,271 @@
+"""Scalar transport, dynamic Prandtl model, buoyancy, sponge and Coriolis
+forcing: the CUDA library against the FP64 oracle (oracle/scalar_oracle.py).
+
+Parity unpinned: the reference's scalar module is a stub and its sponge is
+zeroed (see the oracle's header); the oracle is written from the equations
+and pinned here by known answers (an exactly dealiased band-limited product,
+the sponge profile's end values, a uniform scalar that nothing moves).
+Tolerances as for the momentum: FP64 <= 1e-12 per operator, mixed precision
+<= 1e-5 per operator on FP32-rounded inputs; 10-step FP64 horizons <= 1e-10
+for resolved fields.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import les_oracle as O
+from oracle import scalar_oracle as S
+from tests.helpers import mirror, rel_err, run_params
+
+TOL = {"fp64": 1e-12, "mixed": 1e-5}
+
+
+# ------------------------------------------------------------------ CPU
+def test_scalar_convection_of_band_limited_fields_is_exact():
+    """u = U sin(y), v = w = 0, theta = sin(3x): the advection term
+    -u d_x theta = -3 U sin(y) cos(3x) is band-limited, so the padded (and
+    the 2/3-truncated) product is exact."""
+    p = O.Params(nx=16, ny=16, nz=4)
+    st = O.State(p)
+    sp = S.ScalarParams()
+    S.scalar_init(p, st, sp)
+    x = np.arange(p.nx) * p.dx
+    y = np.arange(p.ny) * p.dy
+    U = 1.7
+    st.u[:] = U * np.sin(y)[None, :, None]
+    st.v[:] = 0.0
+    st.w[:] = 0.0
+    st.dtdx[:] = 3.0 * np.cos(3.0 * x)[None, None, :]
+    st.dtdy[:] = 0.0
+    st.dtdz[:] = 0.0
+    for dealias in ("padd", "trunc"):
+        q = p.with_(dealias=dealias)
+        out = S.scalar_convec(q, st)
+        want = -U * np.sin(y)[None, :, None] * 3.0 * np.cos(3.0 * x)[None, None, :]
+        assert np.abs(out[1:p.nz + 1] - want).max() < 1e-13, dealias
+
+
+def test_sponge_profile_end_values():
+    """sponge_damping.f90:61-80: zero below z_d, half of cfrdmp = 3.9 half
+    way to the lid, the level below the lid at its cosine value, and that
+    value copied to nz+1 (the lid node itself would be 3.9)."""
+    p = O.Params(nx=16, ny=16, nz=40)
+    s = S.sponge_profile(p, 0.8)
+    z = (np.arange(p.nz + 2) - 1.0) * p.dz
+    assert np.all(s[1:][z[1:] < 0.8 - 1e-12] == 0.0)
+    k_top = p.nz  # z = (nz - 1) dz
+    assert s[p.nz + 1] == s[p.nz]
+    mid = int(round(0.9 / p.dz)) + 1
+    assert abs(s[mid] - 3.9 * 0.5) < 1e-12
+    assert abs(s[k_top] - 3.9 * 0.5 * (1.0 - math.cos(math.pi * (1.0 - p.dz - 0.8) / 0.2))) < 1e-12
+
+
+def test_uniform_scalar_stays_uniform():
+    """theta = const with zero wall flux and lid gradient: every term of the
+    scalar equation vanishes (gradients, fluxes, advection)."""
+    p = O.Params(nx=16, ny=16, nz=8, sgs_model="cst_Smag")
+    ops = O.Ops(p)
+    st = O.make_state(p, seed=1)
+    S.scalar_init(p, st, S.ScalarParams(dynamic=False), theta=np.full((p.nz, p.ny, p.nx), 2.5))
+    for _ in range(3):
+        S.les_step(ops, st)
+    assert np.abs(st.theta[1:p.nz + 1] - 2.5).max() < 1e-12
+
+
+# ------------------------------------------------------------------ GPU
+def _setup(p, sp, precision="fp64", seed=2, fc=None, steps=0, theta=None):
+    """Oracle state with the scalar after `steps` oracle steps, mirrored into
+    a library state with the same scalar and forcing settings."""
+    from new_repo_b200 import LES
+
+    ops = O.Ops(p)
+    st = O.make_state(p, seed=seed)
+    th = S.linear_profile(p, seed=seed) if theta is None else theta
+    S.scalar_init(p, st, sp, theta=th)
+    fc = fc or S.Forcing()
+    for _ in range(steps):
+        S.les_step(ops, st, fc)
+    if precision == "mixed":
+        for n in O.FIELDS + O.PLANES + S.SCALAR_FIELDS:
+            a = getattr(st, n)
+            a[...] = a.astype(np.float32).astype(np.float64)
+    les = LES(run_params(p), precision=precision)
+    les.scalar_init(surface_flux=sp.surface_flux, top_gradient=sp.top_gradient, buoyancy=sp.buoyancy,
+                    pr_t=sp.pr_t, sgs="dynamic" if sp.dynamic else "const")
+    if fc.sponge_fraction > 0.0:
+        les.sponge_init(fc.sponge_fraction)
+    if fc.coriol != 0.0:
+        les.set_coriolis(fc.coriol, fc.ug, fc.vg)
+    mirror(les, st)
+    for n in S.SCALAR_FIELDS:
+        les.upload(n, getattr(st, n))
+    return ops, st, les, fc
+
+
+def _check(les, st, names, tol, label, levels=slice(1, None)):
+    for n in names:
+        a = les.download(n)[levels]
+        b = getattr(st, n)[levels]
+        e = rel_err(a, b)
+        assert e <= tol, f"{label}: {n} rel err {e:.3e} > {tol:.0e}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_scalar_gradients(gpu, precision):
+    p = O.Params(nx=32, ny=32, nz=16)
+    sp = S.ScalarParams(surface_flux=0.05, top_gradient=1.0)
+    ops, st, les, _ = _setup(p, sp, precision)
+    O.obukhov(ops, st)
+    O.wallstress(ops, st)
+    O.compute_vel_grad(ops, st)
+    S.scalar_grad(ops, st)
+    les.obukhov()
+    les.wallstress()
+    les.compute_vel_grad()
+    _check(les, st, ("theta", "dtdx", "dtdy", "dtdz"), TOL[precision], "scalar gradients", slice(0, None))
+    les.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("model,jt", [("const", 3), ("dynamic", 3), ("dynamic", 10)])
+def test_scalar_sgs_flux(gpu, model, jt, precision):
+    """pi_j of the constant and dynamic Prandtl models; jt = 10 runs the
+    dynamic procedure (cs_count 5), jt = 3 keeps the initial coefficient."""
+    p = O.Params(nx=32, ny=32, nz=16, sgs_model="cst_Smag")
+    sp = S.ScalarParams(surface_flux=0.05, top_gradient=1.0, dynamic=(model == "dynamic"))
+    ops, st, les, _ = _setup(p, sp, precision)
+    O.obukhov(ops, st)
+    O.wallstress(ops, st)
+    O.compute_vel_grad(ops, st)
+    S.scalar_grad(ops, st)
+    if precision == "mixed":
+        for n in O.FIELDS + O.PLANES + S.SCALAR_FIELDS:
+            a = getattr(st, n)
+            a[...] = a.astype(np.float32).astype(np.float64)
+    mirror(les, st)
+    for n in S.SCALAR_FIELDS:
+        les.upload(n, getattr(st, n))
+    O.sgs_stress(ops, st, jt, jt)
+    S.scalar_sgs(ops, st, jt, jt)
+    les.sgs_stress(jt, jt)
+    _check(les, st, ("qx", "qy", "qz", "nu_t"), TOL[precision], f"scalar flux {model} jt={jt}")
+    if model == "dynamic":
+        k = les.scalar_kappa()
+        e = np.abs(k[1:] - st.kappa[1:]).max() / np.abs(st.kappa[1:]).max()
+        assert e <= TOL[precision], f"kappa rel err {e:.3e}"
+        if jt == 10:
+            assert np.all(k[1:] >= 0.0) and np.any(k[1:] != 0.03 / sp.pr_t)
+    les.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("dealias", ["padd", "trunc"])
+def test_scalar_rhs_with_buoyancy_sponge_coriolis(gpu, dealias, precision):
+    """compute_RHS_adv with the scalar: the scalar's convective term and
+    flux divergence, buoyancy in rhs_z, the sponge and Coriolis terms."""
+    p = O.Params(nx=32, ny=32, nz=20, dealias=dealias)
+    sp = S.ScalarParams(surface_flux=0.24, top_gradient=10.0, buoyancy=30.0)
+    fc = S.Forcing(sponge_fraction=0.8, coriol=0.5, ug=1.0, vg=-0.3)
+    th = S.inversion_profile(p, seed=3)
+    ops, st, les, fc = _setup(p, sp, precision, fc=fc, steps=2, theta=th)
+    O.obukhov(ops, st)
+    O.wallstress(ops, st)
+    O.compute_vel_grad(ops, st)
+    S.scalar_grad(ops, st)
+    O.sgs_stress(ops, st, 3, 3)
+    S.scalar_sgs(ops, st, 3, 3)
+    if precision == "mixed":
+        for n in O.FIELDS + O.PLANES + S.SCALAR_FIELDS:
+            a = getattr(st, n)
+            a[...] = a.astype(np.float32).astype(np.float64)
+    mirror(les, st)
+    for n in S.SCALAR_FIELDS:
+        les.upload(n, getattr(st, n))
+    O.compute_rhs_adv(ops, st)
+    S.forcing(p, st, fc)
+    S.scalar_rhs(ops, st)
+    S.buoyancy(p, st)
+    les.compute_RHS_adv()
+    _check(les, st, ("rhs_t", "rhsx", "rhsy", "rhsz"), TOL[precision], f"rhs {dealias}", slice(1, p.nz + 1))
+    les.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["passive", "convective"])
+def test_scalar_ten_step_horizon(gpu, case):
+    """10 full steps from the same fields: the config-2 passive scalar
+    (linear profile, dynamic Prandtl, LASD momentum) and a convective case
+    (heat flux, inversion, buoyancy, sponge, Coriolis)."""
+    from new_repo_b200 import LES
+
+    if case == "passive":
+        p = O.Params(nx=32, ny=32, nz=16)
+        sp = S.ScalarParams(top_gradient=1.0)
+        fc = S.Forcing()
+        th = S.linear_profile(p, seed=0)
+    else:
+        p = O.Params(nx=32, ny=32, nz=20, sgs_model="cst_Smag")
+        sp = S.ScalarParams(surface_flux=0.24, top_gradient=10.0, buoyancy=30.0, dynamic=True)
+        fc = S.Forcing(sponge_fraction=0.8, coriol=0.5, ug=1.0)
+        th = S.inversion_profile(p, seed=0)
+    ops = O.Ops(p)
+    st = O.make_state(p, seed=0)
+    S.scalar_init(p, st, sp, theta=th)
+    les = LES(run_params(p))
+    les.set_initial_conditions(*O.log_law_fields(p, seed=0))
+    les.scalar_init(surface_flux=sp.surface_flux, top_gradient=sp.top_gradient, buoyancy=sp.buoyancy,
+                    pr_t=sp.pr_t, sgs="dynamic" if sp.dynamic else "const")
+    les.scalar_set_initial(th)
+    if fc.sponge_fraction:
+        les.sponge_init(fc.sponge_fraction)
+    if fc.coriol:
+        les.set_coriolis(fc.coriol, fc.ug, fc.vg)
+    for n in range(10):
+        d_o = S.les_step(ops, st, fc)
+        les.step()
+        d_g = les.diagnostics()
+        assert np.allclose(d_g, d_o, rtol=1e-9, atol=1e-13), (n, d_g, d_o)
+    flipped = rel_err(les.download("cs_opt2")[1:], st.cs_opt2[1:]) > 1e-12
+    tol = 1e-8 if flipped else 1e-10
+    for n in ("u", "v", "w", "theta", "dtdz"):
+        e = rel_err(les.download(n)[1:-1], getattr(st, n)[1:-1])
+        assert e <= tol, f"{case}: {n} {e:.3e}"
+    k = les.scalar_kappa()
+    assert np.abs(k[1:] - st.kappa[1:]).max() <= 1e-8 * max(np.abs(st.kappa[1:]).max(), 1e-30)
+    assert les.status() == 0
+    les.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_scalar_production_plans(gpu, precision):
+    """The scalar's padded advection, dynamic filter and fluxes on 256-point
+    plans (a few levels)."""
+    p = O.Params(nx=256, ny=256, nz=4, dt=1e-4, sgs_model="cst_Smag")
+    sp = S.ScalarParams(surface_flux=0.1, top_gradient=1.0, buoyancy=10.0)
+    ops, st, les, fc = _setup(p, sp, precision)
+    O.obukhov(ops, st)
+    O.wallstress(ops, st)
+    O.compute_vel_grad(ops, st)
+    S.scalar_grad(ops, st)
+    if precision == "mixed":
+        for n in O.FIELDS + O.PLANES + S.SCALAR_FIELDS:
+            a = getattr(st, n)
+            a[...] = a.astype(np.float32).astype(np.float64)
+    mirror(les, st)
+    for n in S.SCALAR_FIELDS:
+        les.upload(n, getattr(st, n))
+    O.sgs_stress(ops, st, 5, 5)
+    S.scalar_sgs(ops, st, 5, 5)
+    les.sgs_stress(5, 5)
+    _check(les, st, ("qx", "qy", "qz"), TOL[precision], "fluxes 256")
+    O.compute_rhs_adv(ops, st)
+    S.scalar_rhs(ops, st)
+    S.buoyancy(p, st)
+    les.compute_RHS_adv()
+    _check(les, st, ("rhs_t", "rhsz"), TOL[precision], "rhs 256", slice(1, p.nz + 1))
+    les.close()

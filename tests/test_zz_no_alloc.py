@@ -3,11 +3,18 @@ solver entry point les_grad_velocity_filt on the same fields, two calls in a
 row.  Tolerance: FP64 parity bar, max|a - b| / max|b| <= 1e-12 per output
 (the two paths run the same kernels; only the twiddle tables are computed on
 a different processor).
+
+Shapes: a square-free case, an x length with a radix-3 factor (96), and at
+128x128 the largest level count whose spectra still fit the static buffer
+(the last spectrum ends at the buffer's edge); one case runs on a stream the
+caller created.
 """
 import ctypes as C
 
 import numpy as np
 import pytest
+
+SCRATCH = 32 << 20  # LES_NOALLOC_SCRATCH_BYTES
 
 
 def _lib():
@@ -16,30 +23,69 @@ def _lib():
     return capi, capi.load()
 
 
+def _scratch_bytes(nx, ny, nlev):
+    """Bytes of the static buffer a call uses: two wavenumber tables, two
+    twiddle tables and three FP64 spectra, each rounded up to 256 bytes."""
+    a = lambda b: (b + 255) // 256 * 256  # noqa: E731
+    lhx = nx // 2 + 1
+    return 2 * a(8 * ny * lhx) + a(16 * nx) + a(16 * ny) + 3 * a(16 * nlev * ny * lhx)
+
+
+def _max_levels(nx, ny):
+    n = 1
+    while _scratch_bytes(nx, ny, n + 1) <= SCRATCH:
+        n += 1
+    return n
+
+
 def test_noalloc_rejects_sizes_beyond_the_static_buffer():
-    """The size check runs before any CUDA call, so it needs no GPU; the
+    """The size checks run before any CUDA call, so they need no GPU; the
     pointers are never dereferenced."""
     capi, lib = _lib()
     fake = C.c_void_p(256)
-    rc = lib.les_grad_xy_noalloc(fake, fake, fake, 768, 768, 64, 1.0, 1.0, None)
+    rc = lib.les_grad_xy_noalloc(fake, fake, fake, 768, 512, 64, 1.0, 1.0, None)
     assert rc == capi.LES_ERR_INVALID
     msg = lib.les_noalloc_last_error().decode()
     assert "needs" in msg and "LES_NOALLOC_SCRATCH_BYTES" in msg
+    # one level past the largest that fits at 128x128
+    n = _max_levels(128, 128)
+    assert lib.les_grad_xy_noalloc(fake, fake, fake, 128, 128, n + 1, 1.0, 1.0, None) == capi.LES_ERR_INVALID
+    assert "needs" in lib.les_noalloc_last_error().decode()
     rc = lib.les_grad_xy_noalloc(None, fake, fake, 64, 64, 8, 1.0, 1.0, None)
     assert rc == capi.LES_ERR_INVALID
 
 
+@pytest.mark.parametrize("ny", [24, 768, 96, 20])
+def test_noalloc_rejects_y_lengths_without_a_y_pass(ny):
+    """ny must have an equal-length y pass (powers of two 16..512): checked
+    before anything is queued, so no GPU is needed."""
+    capi, lib = _lib()
+    fake = C.c_void_p(256)
+    rc = lib.les_grad_xy_noalloc(fake, fake, fake, 64, ny, 2, 1.0, 1.0, None)
+    assert rc == capi.LES_ERR_INVALID
+    assert "ny one of" in lib.les_noalloc_last_error().decode()
+
+
+CASES = [(64, 32, 16, False), (96, 64, 8, False), (128, 128, None, False), (64, 32, 16, True)]
+
+
 @pytest.mark.gpu
-def test_noalloc_matches_grad_velocity_filt_twice(gpu):
+@pytest.mark.parametrize("nx,ny,nlev,own_stream", CASES)
+def test_noalloc_matches_grad_velocity_filt_twice(gpu, nx, ny, nlev, own_stream):
     import torch
 
     from new_repo_b200 import LES, RunParams
 
     capi, lib = _lib()
-    p = RunParams(nx=64, ny=32, nz=14, dt=1e-4, sgs_model="cst_Smag")
+    if nlev is None:
+        nlev = _max_levels(nx, ny)
+        assert _scratch_bytes(nx, ny, nlev) > SCRATCH - 3 * 16 * ny * (nx // 2 + 1)
+    p = RunParams(nx=nx, ny=ny, nz=nlev - 2, dt=1e-4, sgs_model="cst_Smag")
     les = LES(p, precision="fp64")
     L = p.nz + 2
-    rng = np.random.default_rng(0)
+    rng = np.random.default_rng(nx + ny + nlev)
+    stream = torch.cuda.Stream() if own_stream else None
+    handle = C.c_void_p(stream.cuda_stream) if own_stream else None
     for call in range(2):
         f = rng.standard_normal((L, p.ny, p.nx))
         les.upload("u", f)
@@ -48,11 +94,13 @@ def test_noalloc_matches_grad_velocity_filt_twice(gpu):
         dev = [torch.from_numpy(f.copy()).cuda(), torch.full_like(torch.from_numpy(f), 7.0).cuda(),
                torch.full_like(torch.from_numpy(f), -7.0).cuda()]
         torch.cuda.synchronize()
-        rc = lib.les_grad_xy_noalloc(*(C.c_void_p(t.data_ptr()) for t in dev), p.nx, p.ny, L, p.lx, p.ly, None)
+        rc = lib.les_grad_xy_noalloc(*(C.c_void_p(t.data_ptr()) for t in dev), p.nx, p.ny, L, p.lx, p.ly, handle)
         assert rc == capi.LES_OK, lib.les_noalloc_last_error().decode()
+        if own_stream:
+            stream.synchronize()
         torch.cuda.synchronize()
         for name, t, r in zip(("filtered f", "dfdx", "dfdy"), dev, ref):
             a = t.cpu().numpy()
             err = np.abs(a - r).max() / np.abs(r).max()
-            assert err <= 1e-12, f"call {call}: {name} rel err {err:.2e}"
+            assert err <= 1e-12, f"{nx}x{ny}x{nlev} call {call}: {name} rel err {err:.2e}"
     les.close()
