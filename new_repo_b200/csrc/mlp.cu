@@ -114,7 +114,14 @@ __device__ __forceinline__ void raw_features(const MlpFeatIn<T>& a, long o, int 
   const float vs = s11 * w1 * w1 + s22 * w2 * w2 + s33 * w3 * w3 +
                    2.0f * (s12 * w1 * w2 + s13 * w1 * w3 + s23 * w2 * w3);
   t[6] = copysignf(log1pf(fabsf(vs)), vs);
-  t[7] = a.log_delta_z0;
+  if (a.dtdz) {
+    // gradient Richardson number g/theta_0 (d theta/dz) / |d u_h/dz|^2 at this
+    // node (level 1: the wall value of d theta/dz), signed log1p
+    const float ri = a.beta * float(a.dtdz[o]) / (uz * uz + vz * vz + 1e-12f);
+    t[7] = copysignf(log1pf(fabsf(ri)), ri);
+  } else {
+    t[7] = a.log_delta_z0;
+  }
 }
 
 // order-preserving float -> int map (for atomic min / max of floats)

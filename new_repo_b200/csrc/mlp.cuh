@@ -36,6 +36,10 @@ struct MlpFeatIn {
   int nz;
   int wall;
   float dz, delta, log_delta_z0;
+  // buoyant runs: d theta/dz (w nodes) and g/theta_0; feature 7 is then the
+  // gradient Richardson number instead of the constant log(Delta/z0)
+  const T* dtdz = nullptr;
+  float beta = 0.0f;
 };
 
 struct MlpDevice {

@@ -417,6 +417,10 @@ class Solver final : public SolverBase {
     a.dz = float(dz());
     a.delta = float(delta);
     a.log_delta_z0 = float(std::log(delta / P.z0));
+    if (scalar_on && SP.buoyancy != 0.0) {
+      a.dtdz = F[LES_DTDZ];
+      a.beta = float(SP.buoyancy);
+    }
     return a;
   }
   void set_sgs_model(int m) override {

@@ -114,7 +114,7 @@ def grad(p, x, t, bf16_ops=True):
     return g, loss
 
 
-def raw_features(d, cs_prev, k, dz, delta, log_delta_z0, wall):
+def raw_features(d, cs_prev, k, dz, delta, log_delta_z0, wall, dtdz=None, beta=0.0):
     """The 8 transformed features at level k (mlp.cu raw_features).
 
     ``d`` maps 'dudx' .. 'dwdz' to (nz+2, ny, nx) arrays, ``cs_prev`` is the
@@ -123,7 +123,9 @@ def raw_features(d, cs_prev, k, dz, delta, log_delta_z0, wall):
     w nodes (uvp quantities averaged down).  Features: log1p |S|,
     log1p S:S, log1p Omega:Omega, signed log1p tr(S^3), log1p(z / Delta),
     log max(Cs^2_prev, 1e-6), signed log1p of the vortex stretching
-    w_i S_ij w_j, log(Delta / z0).
+    w_i S_ij w_j, log(Delta / z0) -- or, for a buoyant run (``dtdz`` the
+    scalar's vertical gradient on w nodes, ``beta`` = g/theta_0), the signed
+    log1p of the gradient Richardson number beta dtdz / (uz^2 + vz^2 + 1e-12).
     """
     f = {key: np.asarray(a, np.float32) for key, a in d.items()}
     h = np.float32(0.5)
@@ -162,7 +164,11 @@ def raw_features(d, cs_prev, k, dz, delta, log_delta_z0, wall):
     w1, w2, w3 = -2 * o23, 2 * o13, -2 * o12
     vs = s11 * w1 * w1 + s22 * w2 * w2 + s33 * w3 * w3 + 2 * (s12 * w1 * w2 + s13 * w1 * w3 + s23 * w2 * w3)
     out[..., 6] = np.copysign(np.log1p(np.abs(vs)), vs)
-    out[..., 7] = np.float32(log_delta_z0)
+    if dtdz is not None:
+        ri = np.float32(beta) * np.asarray(dtdz, np.float32)[k] / (uz * uz + vz * vz + np.float32(1e-12))
+        out[..., 7] = np.copysign(np.log1p(np.abs(ri)), ri)
+    else:
+        out[..., 7] = np.float32(log_delta_z0)
     return out.reshape(-1, 8)
 
 

@@ -132,14 +132,16 @@ def _fields(les):
     return {n: les.download(n) for n in names}
 
 
-def _oracle_cs(les, p, stats, cs_prev):
-    """Cs^2 and the in-range mask of every level 1..nz+1 from the oracle's features."""
+def _oracle_cs(les, p, stats, cs_prev, beta=0.0):
+    """Cs^2 and the in-range mask of every level 1..nz+1 from the oracle's
+    features (beta != 0: the buoyant run's Richardson-number feature)."""
     rp = les.params
     d = _fields(les)
+    dtdz = les.download("dtdz") if beta else None
     delta = (rp.dx * rp.dy * rp.dz) ** (1.0 / 3.0)
     cs, ok = [], []
     for k in range(1, rp.nz + 2):
-        t = M.raw_features(d, cs_prev, k, rp.dz, delta, np.log(delta / rp.z0), 1)
+        t = M.raw_features(d, cs_prev, k, rp.dz, delta, np.log(delta / rp.z0), 1, dtdz=dtdz, beta=beta)
         xn = (t - stats[M.S_MU:M.S_MU + 8]) / stats[M.S_SD:M.S_SD + 8]
         cs.append(M.cs_from_output(M.forward(p, xn.astype(np.float32)), stats, t[:, 5]))
         ok.append(M.in_range(xn, stats))
@@ -147,14 +149,24 @@ def _oracle_cs(les, p, stats, cs_prev):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("buoyant", [False, True])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_mlp_inference_in_step_matches_oracle(gpu, precision):
+def test_mlp_inference_in_step_matches_oracle(gpu, precision, buoyant):
     """Features from the state's gradients, normalisation and the tcgen05
-    forward pass inside sgs_stress, against the oracle on the same fields."""
+    forward pass inside sgs_stress, against the oracle on the same fields;
+    buoyant: a heated, stratified run whose eighth feature is the gradient
+    Richardson number."""
+    from oracle import les_oracle as O
+    from oracle import scalar_oracle as S
     from new_repo_b200 import log_law_noise
 
     les = _les(precision=precision)
     les.set_initial_conditions(*log_law_noise(les.params, seed=3))
+    beta = 30.0 if buoyant else 0.0
+    if buoyant:
+        les.scalar_init(surface_flux=0.24, top_gradient=10.0, buoyancy=beta)
+        rp = les.params
+        les.scalar_set_initial(S.inversion_profile(O.Params(nx=rp.nx, ny=rp.ny, nz=rp.nz), seed=3, z_inv=0.3))
     p = _params(7, scale=0.5)
     st = _stats()
     les.mlp_set_params(np.concatenate([p, st]))
@@ -166,7 +178,7 @@ def test_mlp_inference_in_step_matches_oracle(gpu, precision):
     cs_prev = les.download("cs_opt2")
     les.sgs_stress(10, 10)
     cs = les.download("cs_opt2")[1:les.params.nz + 2]
-    cso, _ = _oracle_cs(les, p, st, cs_prev)
+    cso, _ = _oracle_cs(les, p, st, cs_prev, beta)
     cso = cso.reshape(cs.shape)
     e = np.abs(np.log(cs) - np.log(cso))
     assert e.max() <= 2e-2 and np.median(e) <= 3e-4, (e.max(), np.median(e))

@@ -262,7 +262,11 @@ def test_scalar_production_plans(gpu, precision):
     O.sgs_stress(ops, st, 5, 5)
     S.scalar_sgs(ops, st, 5, 5)
     les.sgs_stress(5, 5)
-    _check(les, st, ("qx", "qy", "qz"), TOL[precision], "fluxes 256")
+    # jt = 5 runs the dynamic procedure: K_j = filt(u_j theta) - filt(u_j)
+    # filt(theta) cancels ~3 digits (u ~ 20, theta ~ 1, K ~ 1e-2), so the
+    # coefficient, and the fluxes built from it, carry ~1e3 ulp of FP64
+    # rounding in either implementation (measured 1.2e-12 on 256-point plans)
+    _check(les, st, ("qx", "qy", "qz"), 5e-12 if precision == "fp64" else TOL[precision], "fluxes 256")
     O.compute_rhs_adv(ops, st)
     S.scalar_rhs(ops, st)
     S.buoyancy(p, st)
