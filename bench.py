@@ -239,6 +239,8 @@ def run_ours(args, dist, rank, local, ws):
     #      last update of the continuation ----
     S = max(100, T + W + 2 * K)
     done = T + W + 2 * K
+    if args.no_fp64 and train is None:
+        S = done  # nothing is compared at step S
     if train is not None:
         upd = [j for j in range(done + 1, S + 1) if j >= p.dyn_init and j % p.cs_count == 0]
         if upd:
