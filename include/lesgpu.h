@@ -147,6 +147,16 @@ int les_div_stress(les_state* s, int rhs, int tx, int ty, int tz, int stag);
 int les_compute_dealias_convec(les_state* s, int cx, int cy, int cz);
 /* compute_pressure.f90:116-242 press_stag_array(tadv1) */
 int les_press_stag_array(les_state* s, double tadv1);
+/* compute_pressure.f90:116-242 press_stag_array(tadv1) in increment form,
+ * for the state les_ab2_advance(tadv1, tadv2) just left: u* / (dt tadv1) =
+ * u^n / (dt tadv1) + rhs + (tadv2/tadv1) rhs_f, whose divergence is formed
+ * from this step's dudx + dvdy + dwdz (les_compute_vel_grad before the
+ * advance) and the transforms of rhs, rhs_f; the same pressure in exact
+ * arithmetic, without the cancellation of transforming u* (values ~ u
+ * against increments ~ dt rhs), so the transforms run in the state's
+ * precision.  les_step uses it in LES_MIXED.  Preconditions: rhs, rhs_f and
+ * the gradients unchanged since the advance, w(nz+1) = 0. */
+int les_press_from_increment(les_state* s, double tadv1, double tadv2);
 /* compute_wall_law.f90:198-254 obukhov(u_star_avg, wall_model) */
 int les_obukhov(les_state* s);
 /* compute_wall_law.f90:107-185 wallstress(lbc_u, lbc_v, wall_model) */

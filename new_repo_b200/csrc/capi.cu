@@ -187,6 +187,11 @@ int les_press_stag_array(les_state* s, double tadv1) {
   STATE_OR_FAIL(s);
   return guard([&] { s->s->press_stag_array(tadv1); });
 }
+int les_press_from_increment(les_state* s, double tadv1, double tadv2) {
+  STATE_OR_FAIL(s);
+  if (!(tadv1 != 0.0)) return bad_arg("tadv1");
+  return guard([&] { s->s->press_from_increment(tadv1, tadv2); });
+}
 int les_obukhov(les_state* s) {
   STATE_OR_FAIL(s);
   return guard([&] { s->s->obukhov(); });

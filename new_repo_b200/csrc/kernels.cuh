@@ -695,18 +695,24 @@ __global__ void k_p_finish(T* p, const double* pmean, long plane, int nz) {
 // 448-493, matrix of build_matrix :544-619), always in FP64.
 // O: type of the pressure spectrum written (FP32 in mixed precision, whose
 // inverse transforms run in FP32); its rows are opitch values apart
+// G (optional): a fourth spectrum added to the right-hand side of every
+// interior row (the divergence of u^n over dt tadv1 when Hx, Hy, Hz hold the
+// AB2 increment only)
 template <typename T, typename O = T>
 __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restrict__ Hy,
-                          const cplx<T>* __restrict__ Hz, const cplx<T>* __restrict__ bot,
+                          const cplx<T>* __restrict__ Hz, const cplx<T>* __restrict__ G,
+                          const cplx<T>* __restrict__ bot,
                           const cplx<T>* __restrict__ top, const double* __restrict__ kkx,
                           const double* __restrict__ kky, cplx<O>* __restrict__ phat, cplx<double>* __restrict__ xs,
                           double* __restrict__ gam, double* pmean, unsigned* status, int lhx, int ny, int nz,
-                          double dz, int drop_mean, int opitch) {
+                          double dz, int drop_mean, int opitch, int ipitch) {
   const int kx = blockIdx.x * blockDim.x + threadIdx.x;
   const int ky = blockIdx.y;
   if (kx >= lhx) return;
-  const long col = (long)ky * lhx + kx;
+  const long col = (long)ky * lhx + kx;  // tables and the FP64 sweep scratch
   const long sp = (long)ny * lhx;
+  const long icol = (long)ky * ipitch + kx;  // input spectra (rows ipitch apart)
+  const long isp = (long)ny * ipitch;
   const long ocol = (long)ky * opitch + kx;
   const long osp = (long)ny * opitch;
   if (kx == lhx - 1 || ky == ny / 2) {
@@ -720,7 +726,7 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
   // row 1: bottom Neumann closure (p1 - p0 = dz * bottom layer) or p0 = 0
   cplx<double> r;
   if (mean) r = {0.0, 0.0};
-  else r = {double(bot[col].x) * dz, double(bot[col].y) * dz};
+  else r = {double(bot[icol].x) * dz, double(bot[icol].y) * dz};
   double bet = mean ? 1.0 : -1.0;
   double cprev = mean ? 0.0 : 1.0;
   cplx<double> x = {r.x / bet, r.y / bet};
@@ -732,22 +738,23 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
   // thread per (kx, ky), too few warps to hide DRAM latency otherwise).
   // Hz(k+1) of one level is Hz(k) of the next.
   constexpr int TB = 4;
-  cplx<T> hz = Hz[sp + col];
-  cplx<T> cx[TB], cy[TB], cz[TB];
-  auto load_fwd = [&](int k0, cplx<T>* ax, cplx<T>* ay, cplx<T>* az) {
+  cplx<T> hz = Hz[isp + icol];
+  cplx<T> cx[TB], cy[TB], cz[TB], cg[TB];
+  auto load_fwd = [&](int k0, cplx<T>* ax, cplx<T>* ay, cplx<T>* az, cplx<T>* agg) {
 #pragma unroll
     for (int j = 0; j < TB; ++j) {
       const int k = k0 + j;
-      const long o = (long)k * sp + col;
+      const long o = (long)k * isp + icol;
       ax[j] = (k <= nz) ? Hx[o] : cplx<T>{T(0), T(0)};
       ay[j] = (k <= nz) ? Hy[o] : cplx<T>{T(0), T(0)};
-      az[j] = (k < nz) ? Hz[o + sp] : cplx<T>{T(0), T(0)};
+      az[j] = (k < nz) ? Hz[o + isp] : cplx<T>{T(0), T(0)};
+      agg[j] = (G && k <= nz) ? G[o] : cplx<T>{T(0), T(0)};
     }
   };
-  load_fwd(1, cx, cy, cz);
+  load_fwd(1, cx, cy, cz, cg);
   for (int k0 = 1; k0 <= nz; k0 += TB) {
-    cplx<T> nx_[TB], ny_[TB], nz_[TB];
-    load_fwd(k0 + TB, nx_, ny_, nz_);
+    cplx<T> nx_[TB], ny_[TB], nz_[TB], ng_[TB];
+    load_fwd(k0 + TB, nx_, ny_, nz_, ng_);
 #pragma unroll
     for (int j = 0; j < TB; ++j) {
       const int k = k0 + j;
@@ -757,6 +764,10 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
         const double sx = kxv * double(hx.x) + kyv * double(hy.x);
         const double sy = kxv * double(hx.y) + kyv * double(hy.y);
         r = {-sy + (double(hzp.x) - double(hz.x)) / dz, sx + (double(hzp.y) - double(hz.y)) / dz};
+        if (G) {
+          r.x += double(cg[j].x);
+          r.y += double(cg[j].y);
+        }
         const double g = cprev / bet;
         bet = b_in - a_in * g;
         bad |= (bet == 0.0);
@@ -772,11 +783,12 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
       cx[j] = nx_[j];
       cy[j] = ny_[j];
       cz[j] = nz_[j];
+      cg[j] = ng_[j];
     }
   }
   {  // top row: -p(nz) + p(nz+1) = dz * top layer
     const long o = (long)(nz + 1) * sp + col;
-    r = {double(top[col].x) * dz, double(top[col].y) * dz};
+    r = {double(top[icol].x) * dz, double(top[icol].y) * dz};
     const double g = cprev / bet;
     bet = 1.0 - (-1.0) * g;
     bad |= (bet == 0.0);

@@ -1323,8 +1323,8 @@ class Solver final : public SolverBase {
       // kept apart in FP64); the inverse transforms of p run in FP32 -- only
       // the forward right-hand side needs FP64, where div u* cancels
       KL("k_tridiag", 96.0 * double(g.L) * g.ny * g.lhx,
-         k_tridiag<S, T><<<tg, 64, 0, st>>>(sp[2], sp[3], sp[4], bot, top, kkxd, kkyd, spec[0], xs, gam, pmean, dstatus,
-                                            g.lhx, g.ny, nz, dz(), 1, pitch(g.lhx)));
+         k_tridiag<S, T><<<tg, 64, 0, st>>>(sp[2], sp[3], sp[4], nullptr, bot, top, kkxd, kkyd, spec[0], xs, gam, pmean, dstatus,
+                                            g.lhx, g.ny, nz, dz(), 1, pitch(g.lhx), g.lhx));
       auto e = yp(YP_PGRAD, 1, 3, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 0);
       e.in[0] = spec[0];
       e.out[0] = spec[1];
@@ -1350,8 +1350,8 @@ class Solver final : public SolverBase {
          k_p_finish<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_P], pmean, g.plane(), nz));
       return;
     }
-    KL("k_tridiag", 112.0 * double(g.L) * g.ny * g.lhx, k_tridiag<S><<<tg, 64, 0, st>>>(sp[2], sp[3], sp[4], bot, top, kkxd, kkyd, sp[5], xs, gam,
-                                   mixed() ? pmean : nullptr, dstatus, g.lhx, g.ny, nz, dz(), mixed() ? 1 : 0, g.lhx));
+    KL("k_tridiag", 112.0 * double(g.L) * g.ny * g.lhx, k_tridiag<S><<<tg, 64, 0, st>>>(sp[2], sp[3], sp[4], nullptr, bot, top, kkxd, kkyd, sp[5], xs, gam,
+                                   mixed() ? pmean : nullptr, dstatus, g.lhx, g.ny, nz, dz(), mixed() ? 1 : 0, g.lhx, g.lhx));
     // compute_press_grad: i kx p^, i ky p^, p^ -> dpdx, dpdy (1..nz), p (0..nz+1)
     auto e = yp_s<S>(YP_PGRAD, 1, 3, 0);
     e.in[0] = sp[5];
@@ -1379,6 +1379,84 @@ class Solver final : public SolverBase {
   }
   double press_tadv1_ = 1.0;
   void dpdz_only();
+
+  // press_stag_array on the state an AB2 advance left, with the right-hand
+  // side formed from the increment: u* / (dt t1) = u^n / (dt t1) + r +
+  // (t2/t1) r_f, and the spectral divergence of u^n is FFT(dudx + dvdy +
+  // dwdz) of this step's gradients (the same Nyquist-killed derivatives the
+  // reference's transform of u* forms), so rhs(k) = i kx H^x + i ky H^y +
+  // (H^z(k+1) - H^z(k))/dz + FFT(div u^n)/(dt t1) with H the increments.
+  // The pressure is the same in exact arithmetic; in FP32 no large value
+  // cancels (u* ~ 20 against an increment of dt rhs ~ 1e-3), so the
+  // transforms run in the state's precision.  Needs w(nz+1) = 0.
+  void press_from_increment(double tadv1, double tadv2) override {
+    Tag tag_(this, "press");
+    const int nz = g.nz;
+    const double c = 1.0 / double(g.nx * g.ny);
+    KL("k_scale", 2.0 * g.plane() * sizeof(T), k_scale<T><<<grid_for(g.plane()), 256, 0, st>>>(PL[LES_BOTTOM_WK_PRESS], g.plane(), T(c)));
+    cplx<T>* bot = spec[8];
+    cplx<T>* top = spec[9];
+    {
+      auto a = xf(XF_SCALE, 1, 0, 1, g.nx, g.ny, g.lhx);
+      a.c0 = 1.0;
+      a.in[0] = PL[LES_BOTTOM_WK_PRESS];
+      a.out[0] = bot;
+      launch_xfwd<T>(g.nx, a, st);
+      a.c0 = c;
+      a.in[0] = PL[LES_TOP_WK_PRESS];
+      a.out[0] = top;
+      launch_xfwd<T>(g.nx, a, st);
+      auto b = yp(YP_FWDKILL, 1, 1, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 0);
+      b.in[0] = bot;
+      b.out[0] = bot;
+      b.in[1] = top;
+      b.out[1] = top;
+      launch_ypass<T>(g.ny, g.ny, b, 1, 2, st);
+    }
+    auto a = xf(XF_PRESS_INC, 4, 1, nz, g.nx, g.ny, g.lhx);
+    a.c0 = c;
+    a.c1 = tadv2 / tadv1;
+    a.c2 = 1.0 / (P.dt * tadv1);
+    const int ins[9] = {LES_RHSX, LES_RHSY, LES_RHSZ, LES_RHSX_F, LES_RHSY_F, LES_RHSZ_F, LES_DUDX, LES_DVDY, LES_DWDZ};
+    for (int q = 0; q < 9; ++q) a.in[q] = F[ins[q]];
+    for (int q = 0; q < 4; ++q) a.out[q] = spec[2 + q];
+    launch_xfwd<T>(g.nx, a, st);
+    auto b = yp(YP_FWDKILL, 1, 1, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 1);
+    for (int q = 0; q < 4; ++q) {
+      b.in[q] = spec[2 + q];
+      b.out[q] = spec[2 + q];
+    }
+    launch_ypass<T>(g.ny, g.ny, b, nz, 4, st);
+    dim3 tg(ceil_div(g.lhx, 64), g.ny);
+    KL("k_tridiag", (4.0 * 2 * sizeof(T) + 2 * sizeof(T) + 24.0) * double(g.L) * g.ny * g.lhx,
+       k_tridiag<T, T><<<tg, 64, 0, st>>>(spec[2], spec[3], spec[4], spec[5], bot, top, kkxd, kkyd, spec[0], xs, gam,
+                                          mixed() ? pmean : nullptr, dstatus, g.lhx, g.ny, nz, dz(), mixed() ? 1 : 0,
+                                          pitch(g.lhx), pitch(g.lhx)));
+    auto e = yp(YP_PGRAD, 1, 3, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 0);
+    e.in[0] = spec[0];
+    e.out[0] = spec[1];
+    e.out[1] = spec[2];
+    e.out[2] = spec[0];
+    launch_ypass<T>(g.ny, g.ny, e, g.L, 1, st);
+    auto h = xi(XI_STORE, 3, 0, g.L, g.nx, g.ny, g.lhx);
+    h.in[0] = spec[1];
+    h.in[1] = spec[2];
+    h.in[2] = spec[0];
+    h.out[0] = F[LES_DPDX];
+    h.out[1] = F[LES_DPDY];
+    h.out[2] = F[LES_P];
+    h.lo[0] = 1;
+    h.hi[0] = nz;
+    h.lo[1] = 1;
+    h.hi[1] = nz;
+    h.lo[2] = 0;
+    h.hi[2] = nz + 1;
+    launch_xinv<T>(g.nx, h, st);
+    dpdz_only();
+    KL("k_p_finish", (mixed() ? 2.0 * g.field() : double(g.plane())) * sizeof(T),
+       k_p_finish<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_P], mixed() ? pmean : nullptr, g.plane(), nz));
+  }
+
 
   // ---------------------------------------------------- compute_wall_law ----
   void wall_layer() {
@@ -1877,7 +1955,10 @@ class Solver final : public SolverBase {
       t2 = 1.0 - t1;
     }
     ab2(t1, t2);
-    press_stag_array(t1);
+    // mixed precision: the right-hand side from the increment (FP32
+    // transforms, no cancellation); FP64: the reference's formulation
+    if (mixed()) press_from_increment(t1, t2);
+    else press_stag_array(t1);
     LES_CUDA(cudaEventRecord(ev[4], st));
     projection(t1);
     set_bc();

@@ -56,6 +56,7 @@ enum XFOp : int {
   XF_PRESS = 4,   // field f = c0 * (in[f] / c1)   (compute_pressure.f90:138-140)
   XF_PROD_SC = 5, // fine-grid scalar advection -(u . grad theta) (inputs on the padded grid)
   XF_SCDYN = 6,   // the 19 test-filter inputs of the dynamic Prandtl model
+  XF_PRESS_INC = 7,  // pressure right-hand side from the AB2 increment and div u^n
 };
 
 template <typename T>
@@ -74,7 +75,7 @@ struct XFArgs {
   T* refout[MAXIN];
   long in_pstride; // elements per plane of the input grid
   long in_rstride; // elements per row of the input grid (== NX)
-  double c0, c1;
+  double c0, c1, c2;
   const T* in[16];
   const float* inf[16];  // FP32 inputs of an FP64 transform (in_f32 = 1)
   int in_f32;
@@ -251,6 +252,19 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
       const V r = vld<V>(a.in[0], off) * vld<V>(a.in[3], off) + vld<V>(a.in[1], off) * vld<V>(a.in[4], off) +
                   T(0.5) * (vld<V>(a.in[2], off) * vld<V>(a.in[5], off) + vld<V>(a.in[2], up) * vld<V>(a.in[5], up));
       vst(v, c * r);
+      break;
+    }
+    case XF_PRESS_INC: {
+      // u* = u^n + dt (t1 r + t2 r_f), so u* / (dt t1) = u^n / (dt t1) + r +
+      // (t2/t1) r_f: the increment parts (inputs 0..5: rx ry rz rfx rfy rfz)
+      // and the divergence of u^n (inputs 6..8: dudx dvdy dwdz, uvp nodes)
+      // over dt t1 as a fourth field; c0 = 1/(nx ny), c1 = t2/t1,
+      // c2 = 1/(dt t1).  Nothing large cancels in any of the four.
+      const T c = T(a.c0), r21 = T(a.c1), idt = T(a.c2);
+      vst(v + 0 * vs, c * (vld<V>(a.in[0], off) + r21 * vld<V>(a.in[3], off)));
+      vst(v + 1 * vs, c * (vld<V>(a.in[1], off) + r21 * vld<V>(a.in[4], off)));
+      vst(v + 2 * vs, c * (vld<V>(a.in[2], off) + r21 * vld<V>(a.in[5], off)));
+      vst(v + 3 * vs, (c * idt) * ((vld<V>(a.in[6], off) + vld<V>(a.in[7], off)) + vld<V>(a.in[8], off)));
       break;
     }
     case XF_SCDYN: {

@@ -197,7 +197,7 @@ void launch_xfwd(int NX, XFArgs<T> a, cudaStream_t st) {
   const bool staged = a.op == XF_PRESS || (a.op == XF_SCALE && a.nf <= 3);
   if (staged) {
     a.in_rstride = NX;
-    static const int nin_of_op[] = {0, 9, 6, 10, 0, 6, 14};
+    static const int nin_of_op[] = {0, 9, 6, 10, 0, 6, 14, 9};
     const int nin = (a.op == XF_SCALE || a.op == XF_PRESS) ? a.nf : nin_of_op[a.op];
     const size_t isz = (a.in_f32 ? sizeof(float) : sizeof(T));
     hook_before("xfwd", double(a.nrows) * NX * nin * isz + double(a.nrows) * a.nf * a.nk * sizeof(cplx<T>));
@@ -230,7 +230,7 @@ void launch_xfwd(int NX, XFArgs<T> a, cudaStream_t st) {
   if (smem > SMEM_CAP) throw CudaError(1, "xfwd: shared memory request too large");
   const int grid = ceil_div(a.nrows, a.R);
   if (grid == 0) return;
-  static const int nin_of_op[] = {0, 9, 6, 10, 0, 6, 14};
+  static const int nin_of_op[] = {0, 9, 6, 10, 0, 6, 14, 9};
   const int nin = (a.op == XF_SCALE || a.op == XF_PRESS) ? a.nf : nin_of_op[a.op];
   const size_t isz = (a.in_f32 ? sizeof(float) : sizeof(T));
   hook_before("xfwd", double(a.nrows) * NX * nin * isz + double(a.nrows) * a.nf * a.nk * sizeof(cplx<T>));

@@ -410,6 +410,12 @@ class LES:
     def press_stag_array(self, tadv1: float):
         check(self.lib.les_press_stag_array(self._h, float(tadv1)))
 
+    def press_from_increment(self, tadv1: float, tadv2: float | None = None):
+        """press_stag_array in increment form for the state les_ab2_advance
+        left (see les_press_from_increment in lesgpu.h)."""
+        tadv2 = 1.0 - float(tadv1) if tadv2 is None else float(tadv2)
+        check(self.lib.les_press_from_increment(self._h, float(tadv1), tadv2))
+
     def obukhov(self):
         check(self.lib.les_obukhov(self._h))
 

@@ -216,3 +216,52 @@ def test_mixed_ten_step_horizon(gpu, grid):
         assert e <= HORIZON_TOL[group], f"{n}: {e:.2e} > {HORIZON_TOL[group]:.0e} ({report})"
     assert les.status() == 0
     les.close()
+
+
+def _advance(p, seed=9, tadv1=1.5):
+    """An oracle state just before press_stag_array: the part of
+    LES_engine.f90:189-283 that precedes it, on a state with a previous rhs."""
+    ops = O.Ops(p)
+    st = O.make_state(p, seed=seed)
+    for _ in range(2):
+        O.les_step(ops, st)
+    st.jt_total += 1
+    O.obukhov(ops, st)
+    O.wallstress(ops, st)
+    O.compute_vel_grad(ops, st)
+    O.sgs_stress(ops, st, st.jt_total, st.jt_total)
+    O.compute_rhs_adv(ops, st)
+    k = slice(1, p.nz + 1)
+    for f, r, rf in ((st.u, st.rhsx, st.rhsx_f), (st.v, st.rhsy, st.rhsy_f), (st.w, st.rhsz, st.rhsz_f)):
+        f[k] = f[k] + p.dt * (tadv1 * r[k] + (1.0 - tadv1) * rf[k])
+    st.w[0] = 0.0
+    st.w[p.nz + 1] = 0.0
+    return ops, st
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("grid", [dict(nx=32, ny=32, nz=32), dict(nx=256, ny=256, nz=4)])
+def test_press_from_increment(gpu, grid, precision):
+    """les_press_from_increment (the mixed step's pressure solve) against the
+    oracle's press_stag_array on the same advanced state.  FP64: the same
+    pressure to 1e-12 (the formulations differ only in rounding).  Mixed:
+    FP32 inputs and transforms against the FP64 oracle on the unrounded
+    state, 1e-5 -- the error of the path itself, the rounding of u* to FP32
+    included (the direct formulation transforms that rounding divided by dt)."""
+    p = O.Params(dt=2e-4, **grid)
+    ops, st = _advance(p)
+    les = _les(p, precision)
+    gst = st.copy()
+    if precision == "mixed":
+        _round_f32(gst)
+    mirror(les, gst)
+    O.press_stag_array(ops, st, 1.5)
+    les.press_from_increment(1.5)
+    for name in ("p", "dpdx", "dpdy", "dpdz"):
+        a, b = les.download(name), getattr(st, name)
+        if name == "p":
+            a, b = a[:-1], b[:-1]
+        e = rel_err(a, b)
+        assert e <= TOL[precision], (grid, precision, name, e)
+    assert les.status() == 0
+    les.close()
