@@ -55,7 +55,20 @@ def parse():
     ap.add_argument("--wall-levels", type=int, default=8,
                     help="levels next to the wall that keep the LASD procedure under the learned closure")
     ap.add_argument("--train-batch-tiles", type=int, default=16, help="training batch = 128 x this")
-    return ap.parse_args()
+    ap.add_argument("--case", default="abl", choices=["abl", "scalar", "cbl"],
+                    help="abl: the headline (neutral channel, 256^3); scalar: config 2 (FP64, passive scalar "
+                         "with the dynamic Prandtl model, 128^3); cbl: config 5 (convective boundary layer, "
+                         "512x512x256: heat flux, inversion, buoyancy, sponge)")
+    a = ap.parse_args()
+    CASES = {"abl": {}, "scalar": dict(n=128, precision="fp64", closure="lasd", no_fp64=True),
+             "cbl": dict(n=512, nz=256)}
+    for k, v in CASES[a.case].items():
+        if k in ("n", "nz") and getattr(a, k) not in (None, 256):
+            continue  # explicit grid sizes win
+        setattr(a, k, v)
+    if not hasattr(a, "precision"):
+        a.precision = "mixed"
+    return a
 
 
 # ----------------------------------------------------------------- helpers
@@ -160,6 +173,27 @@ def barrier(dist, local):
             dist.barrier()
 
 
+def setup_case(les, p, args, seed: int):
+    """Initial state of a bench case: the log-law velocity with seeded noise,
+    and for the scalar cases theta, its model and the forcing."""
+    from new_repo_b200 import inversion_noise, log_law_noise, scalar_linear_noise
+
+    les.set_initial_conditions(*log_law_noise(p, seed=seed))
+    if args.case == "scalar":
+        # config 2: passive scalar on a linear profile (+-0.01 noise), zero wall
+        # flux, the profile's gradient at the lid, dynamic Prandtl model
+        les.scalar_init(surface_flux=0.0, top_gradient=1.0, buoyancy=0.0, sgs="dynamic")
+        les.scalar_set_initial(scalar_linear_noise(p, seed=seed))
+    elif args.case == "cbl":
+        # config 5: surface heat flux 0.24, inversion of 0.01 K/m above z = 0.5
+        # (10 K per unit height with z_i = 1000 m), +-0.1 K noise below z = 0.1,
+        # buoyancy g z_i / (theta_0 u*^2) with theta_0 = 300 K, sponge in the
+        # top 20 % (sponge_damping.f90 profile)
+        les.scalar_init(surface_flux=0.24, top_gradient=10.0, buoyancy=9.81 * 1000.0 / 300.0, sgs="dynamic")
+        les.scalar_set_initial(inversion_noise(p, seed=seed))
+        les.sponge_init(0.8)
+
+
 def run_params(n: int, nz: int | None = None):
     from new_repo_b200 import RunParams
 
@@ -186,12 +220,11 @@ def run_ours(args, dist, rank, local, ws):
     p = run_params(args.n, args.nz)
     npts = p.nx * p.ny * p.nz
     K, W = args.steps, max(args.warmup, 3)
-    u0, v0, w0 = log_law_noise(p, seed=rank)
     out = {}
 
     # ---- headline: mixed precision, learned closure trained on the GPU ----
-    les = LES(p, precision="mixed", device=local)
-    les.set_initial_conditions(u0, v0, w0)
+    les = LES(p, precision=args.precision, device=local)
+    setup_case(les, p, args, rank)
     T = args.train_steps if args.closure == "mlp" else 0
     train = train_closure(les, p, T, args.train_epochs, args.train_batch_tiles) if T else None
     if T:
@@ -226,7 +259,7 @@ def run_ours(args, dist, rank, local, ws):
             "algorithmic_bytes_per_launch": rec["bytes_per_launch"], "share_of_step": round(rec["ms"] / ms_prof, 4),
             "timed_in": f"a second pass of {K} steps with per-launch CUDA events ({ms_prof / K:.4f} ms/step)"}
     # step-level: algorithmic bytes per step (105 F + 28 F / cs_count, F = N * 4 B)
-    F = npts * 4.0
+    F = npts * (8.0 if args.precision == "fp64" else 4.0)
     step_bytes = (105.0 + 28.0 / p.cs_count) * F
     prof_top = sorted(({"kernel": k, "ms_per_step": round(v["ms"] / K, 4), "launches_per_step": v["launches"] / K,
                         "gbs": round(v["bytes_per_launch"] * v["launches"] / (v["ms"] / 1e3) / 1e9, 1)}
@@ -270,7 +303,7 @@ def run_ours(args, dist, rank, local, ws):
     snap_l = None
     if args.closure == "mlp" and not args.no_fp64:
         ll = LES(p, precision="mixed", device=local)
-        ll.set_initial_conditions(u0, v0, w0)
+        setup_case(ll, p, args, rank)
         ll.step(T + W)
         ll.sync()
         msl = max_over_ranks(dist, timed_steps(ll, K), local)
@@ -284,7 +317,7 @@ def run_ours(args, dist, rank, local, ws):
     fp64 = None
     if not args.no_fp64:
         l64 = LES(p, precision="fp64", device=local)
-        l64.set_initial_conditions(u0, v0, w0)
+        setup_case(l64, p, args, rank)
         l64.step(T + W)
         l64.sync()
         ms64 = timed_steps(l64, K)
@@ -315,15 +348,22 @@ def run_ours(args, dist, rank, local, ws):
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
             "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 (fields, FFTs, convection, SGS) + f64 (pressure solve, mean mode, diagnostics)",
-            "data": "synthetic: log-law profile + seeded uniform +-0.1 noise (counter-based hash)",
+            "dtype": ("f64" if args.precision == "fp64" else
+                      "f32 (fields, FFTs, convection, SGS) + f64 (pressure solve, mean mode, diagnostics)"),
+            "data": "synthetic: log-law profile + seeded uniform +-0.1 noise (counter-based hash)"
+                    + {"abl": "", "scalar": "; scalar: linear profile + seeded +-0.01 noise",
+                       "cbl": "; temperature: inversion above z = 0.5 + seeded +-0.1 K noise below z = 0.1"}[args.case],
             "config": {"workload": f"LES time step {p.nx}x{p.ny}x{p.nz}, 3/2 dealiasing, "
                                    + (f"learned SGS closure above level {args.wall_levels} (LASD on the "
                                       f"{args.wall_levels} wall levels, LASD fallback/check)" if T else "LASD SGS")
                                    + " (cs_count 5, closure update every 5th step), log-law wall, "
-                                     "FP32+FP64-pressure",
-                       "grid": [p.nx, p.ny, p.nz], "dt": p.dt_nd, "sgs_model": "mlp" if T else p.sgs_model,
-                       "precision": "mixed", "parallelism": f"replicas x{ws}",
+                                   + ("FP64" if args.precision == "fp64" else "FP32+FP64-pressure")
+                                   + {"abl": "", "scalar": ", passive scalar with the dynamic Prandtl model",
+                                      "cbl": ", convective boundary layer: surface heat flux 0.24, capping "
+                                             "inversion, buoyancy, top-20 % sponge, dynamic Prandtl model"}[args.case],
+                       "case": args.case, "grid": [p.nx, p.ny, p.nz], "dt": p.dt_nd,
+                       "sgs_model": "mlp" if T else p.sgs_model,
+                       "precision": args.precision, "parallelism": f"replicas x{ws}",
                        "l2": "inputs larger than L2 (>= 9 GB of fields per step)"},
             "roofline": roof, "step_roofline": step_roof, "profile_top": prof_top,
             "e2e": e2e, "gpu_launches": n1 - n0, "fp64_gpu": fp64, "lasd_mixed": lasd, "closure_training": train,

@@ -154,8 +154,9 @@ int les_press_stag_array(les_state* s, double tadv1);
  * advance) and the transforms of rhs, rhs_f; the same pressure in exact
  * arithmetic, without the cancellation of transforming u* (values ~ u
  * against increments ~ dt rhs), so the transforms run in the state's
- * precision.  les_step uses it in LES_MIXED.  Preconditions: rhs, rhs_f and
- * the gradients unchanged since the advance, w(nz+1) = 0. */
+ * precision (the kx = ky = 0 column from FP64 plane means).  les_step keeps
+ * the reference's formulation.  Preconditions: rhs, rhs_f and the gradients
+ * unchanged since the advance, w(nz+1) = 0. */
 int les_press_from_increment(les_state* s, double tadv1, double tadv2);
 /* compute_wall_law.f90:198-254 obukhov(u_star_avg, wall_model) */
 int les_obukhov(les_state* s);

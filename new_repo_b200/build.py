@@ -62,10 +62,14 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
             if l:
                 print(l)
     if not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
-        cmd = [cc, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"]
+        # link to a temporary name and rename: a process loading the library
+        # meanwhile sees the old file or the new one, never a partial one
+        tmp = LIB.with_name(LIB.name + ".tmp")
+        cmd = [cc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
+        os.replace(tmp, LIB)
     return LIB
 
 

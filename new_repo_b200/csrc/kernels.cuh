@@ -453,14 +453,16 @@ __device__ __forceinline__ T ff_at(const T* F, int i, int j, int k, const LagGeo
 template <typename T>
 __global__ void k_lag_interp(const T* ul, const T* vl, const T* wl, const T* F0, const T* F1, const T* F2,
                              const T* F3, T* N0, T* N1, T* N2, T* N3, LagGeom g) {
+  // grid: (plane / blockDim.x, nlev); one point per thread, level
+  // blockIdx.y + 1, and one 32-bit division for the (i, j) of the point
   const long pl = g.plane;
-  const long n = (long)g.nlev * pl;
   const T cs = T(g.cs);
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
-    const long o = pl + q;
-    const int k = int(o / pl);
-    const int jj = int((o % pl) / g.nx);
-    const int i = int(o % g.nx) + 1;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < pl) {
+    const int k = blockIdx.y + 1;
+    const long o = (long)k * pl + p;
+    const int jj = p / g.nx;
+    const int i = p - jj * g.nx + 1;
     const int j = jj + 1;
     T uu, vv;
     if (k == 1) {
@@ -474,7 +476,7 @@ __global__ void k_lag_interp(const T* ul, const T* vl, const T* wl, const T* F0,
     const T yp = -vv * T(g.dt) * cs / T(g.dy);
     T zp;
     if (k <= 2) {
-      const long o2 = 2 * pl + (o % pl);
+      const long o2 = 2 * pl + p;
       const T w2 = wl[o2] / cs;
       T z2 = -w2 * T(g.dt) * cs / T(g.dz);
       z2 = z2 + fmin(z2, T(0));
@@ -516,7 +518,7 @@ __global__ void k_lasd_update(T* FLM, T* FMM, T* FQN, T* FNN, const T* LM, const
   const long n = (long)(nlev < 0 ? nz + 1 : nlev) * plane;  // levels 1..nlev
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const long o = plane + q;
-    const int k = int(o / plane);
+    const bool top = q >= (long)nz * plane;  // level nz + 1 (o = plane + q)
     double flm, fmm, fqn, fnn;
     const double lm = LM[o], mm = MM[o], qn = QN[o], nn = NN[o];
     if (init) {
@@ -564,7 +566,7 @@ __global__ void k_lasd_update(T* FLM, T* FMM, T* FQN, T* FNN, const T* LM, const
     const double c4 = f32max_tiny(double(T(fqn)) / double(T(fnn)));
     double b = (beta_pow == 1.0) ? (c4 / c2) : pow(c4 / c2, beta_pow);
     b = double(fmaxf(float(b), 0.125f));
-    if (k == nz + 1) b = 1.0;
+    if (top) b = 1.0;
     beta[o] = T(b);
     cs[o] = T(f32max_tiny(c2 / b));
   }
@@ -697,7 +699,11 @@ __global__ void k_p_finish(T* p, const double* pmean, long plane, int nz) {
 // inverse transforms run in FP32); its rows are opitch values apart
 // G (optional): a fourth spectrum added to the right-hand side of every
 // interior row (the divergence of u^n over dt tadv1 when Hx, Hy, Hz hold the
-// AB2 increment only)
+// AB2 increment only).  pm (optional, with G): FP64 plane means per level
+// (pm[f * pm_L + k]: f = 0 rz, 1 rfz, 2 dudx, 3 dvdy, 4 dwdz) from which
+// the kx = ky = 0 column forms its right-hand side,
+// (hz(k+1) - hz(k)) / dz + (dudx + dvdy + dwdz) idt with hz = rz + r21 rfz,
+// instead of the FP32 spectra's mean coefficients.
 template <typename T, typename O = T>
 __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restrict__ Hy,
                           const cplx<T>* __restrict__ Hz, const cplx<T>* __restrict__ G,
@@ -705,7 +711,8 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
                           const cplx<T>* __restrict__ top, const double* __restrict__ kkx,
                           const double* __restrict__ kky, cplx<O>* __restrict__ phat, cplx<double>* __restrict__ xs,
                           double* __restrict__ gam, double* pmean, unsigned* status, int lhx, int ny, int nz,
-                          double dz, int drop_mean, int opitch, int ipitch) {
+                          double dz, int drop_mean, int opitch, int ipitch, const double* pm = nullptr,
+                          double pm_r21 = 0.0, double pm_idt = 0.0, int pm_L = 0) {
   const int kx = blockIdx.x * blockDim.x + threadIdx.x;
   const int ky = blockIdx.y;
   if (kx >= lhx) return;
@@ -767,6 +774,11 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
         if (G) {
           r.x += double(cg[j].x);
           r.y += double(cg[j].y);
+        }
+        if (pm && mean) {
+          const double hk = pm[k] + pm_r21 * pm[pm_L + k];
+          const double hkp = (k < nz) ? pm[k + 1] + pm_r21 * pm[pm_L + k + 1] : 0.0;
+          r = {(hkp - hk) / dz + ((pm[2 * pm_L + k] + pm[3 * pm_L + k]) + pm[4 * pm_L + k]) * pm_idt, 0.0};
         }
         const double g = cprev / bet;
         bet = b_in - a_in * g;
@@ -992,15 +1004,15 @@ __global__ void __launch_bounds__(256) k_diag_final(const double* part, int nblo
 // ---------------------------------------------------------------------------
 // scalar transport, buoyancy and momentum forcing
 
-// Plane means (FP64, Neumaier) of up to four fields on levels k0..k1: one
-// block per level, out[f * L + k].  Fixed reduction order (per thread, then
-// threads in order), so repeated runs give the same bits.
+// Plane means (FP64, Neumaier) of up to six fields on levels k0..k0 +
+// gridDim.x - 1: one block per level, out[f * L + k].  Fixed reduction order
+// (per thread, then threads in order), so repeated runs give the same bits.
 template <typename T>
 __global__ void k_plane_means(const T* f0, const T* f1, const T* f2, const T* f3, int nf, double* out, long plane,
-                              int k0, int L) {
+                              int k0, int L, const T* f4 = nullptr, const T* f5 = nullptr) {
   const int k = k0 + blockIdx.x;
-  const T* fs[4] = {f0, f1, f2, f3};
-  __shared__ double sh[4][2][256];
+  const T* fs[6] = {f0, f1, f2, f3, f4, f5};
+  __shared__ double sh[6][2][256];
   for (int f = 0; f < nf; ++f) {
     Neu a;
     const T* x = fs[f] + (long)k * plane;

@@ -1427,11 +1427,19 @@ class Solver final : public SolverBase {
       b.out[q] = spec[2 + q];
     }
     launch_ypass<T>(g.ny, g.ny, b, nz, 4, st);
+    // the mean mode's right-hand side from FP64 plane means: the plane mean of
+    // rhs_z carries the mean vertical pressure gradient (thousands at the
+    // wall), which an FP32 transform would round
+    if (!means) means = track(dalloc<double>(6 * g.L));
+    KL("k_plane_means", 5.0 * nz * g.plane() * sizeof(T),
+       k_plane_means<T><<<nz, 256, 0, st>>>(F[LES_RHSZ], F[LES_RHSZ_F], F[LES_DUDX], F[LES_DVDY], 5, means, g.plane(), 1,
+                                            g.L, F[LES_DWDZ]));
     dim3 tg(ceil_div(g.lhx, 64), g.ny);
     KL("k_tridiag", (4.0 * 2 * sizeof(T) + 2 * sizeof(T) + 24.0) * double(g.L) * g.ny * g.lhx,
        k_tridiag<T, T><<<tg, 64, 0, st>>>(spec[2], spec[3], spec[4], spec[5], bot, top, kkxd, kkyd, spec[0], xs, gam,
                                           mixed() ? pmean : nullptr, dstatus, g.lhx, g.ny, nz, dz(), mixed() ? 1 : 0,
-                                          pitch(g.lhx), pitch(g.lhx)));
+                                          pitch(g.lhx), pitch(g.lhx), means, tadv2 / tadv1, 1.0 / (P.dt * tadv1),
+                                          g.L));
     auto e = yp(YP_PGRAD, 1, 3, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 0);
     e.in[0] = spec[0];
     e.out[0] = spec[1];
@@ -1630,7 +1638,7 @@ class Solver final : public SolverBase {
     if (f_coeff_init) {
       LagGeom geo{g.nx, g.ny, nz, g.plane(), P.lag_halo, P.dt, P.lx / double(g.nx), P.ly / double(g.ny), dz(),
                   double(P.cs_count), nlev};
-      KL("k_lag_interp", 11.0 * n1 * sizeof(T), k_lag_interp<T><<<grid_for(n1), 256, 0, st>>>(F[LES_U_LAG], F[LES_V_LAG], F[LES_W_LAG], F[LES_F_LM],
+      KL("k_lag_interp", 11.0 * n1 * sizeof(T), k_lag_interp<T><<<dim3(unsigned((g.plane() + 255) / 256), unsigned(nlev)), 256, 0, st>>>(F[LES_U_LAG], F[LES_V_LAG], F[LES_W_LAG], F[LES_F_LM],
                                                    F[LES_F_MM], F[LES_F_QN], F[LES_F_NN], sc[11], sc[12], sc[13],
                                                    sc[14], geo));
       if (nlev == nz + 1) {
@@ -1679,7 +1687,7 @@ class Solver final : public SolverBase {
 
   // ------------------------------------------- scalar transport (theta) ----
   double* kapd = nullptr;    // Cs^2/Pr_t * Delta^2 per level (dynamic model)
-  double* means = nullptr;   // plane means: 4 x L (u, v, w, theta)
+  double* means = nullptr;   // plane means: 6 x L (forcing: u, v, w, theta; pressure: five rhs fields)
   double* spong = nullptr;   // sponge profile on w nodes (L)
   void scalar_init(const les_scalar_params& sp) override {
     if (!(sp.pr_t > 0.0)) throw CudaError(1, "Invalid scalar parameters: pr_t must be positive");
@@ -1693,7 +1701,7 @@ class Solver final : public SolverBase {
       fill(F[i], 0, g.nz + 1, T(0));
     }
     if (!kapd) kapd = track(dalloc<double>(g.L));
-    if (!means) means = track(dalloc<double>(4 * g.L));
+    if (!means) means = track(dalloc<double>(6 * g.L));
     // kappa before the first dynamic update: 0.03 / Pr_t (the LASD start value over Pr_t)
     const double d2 = delta * delta;
     std::vector<double> k0(g.L, sp.sgs == LES_SCALAR_SGS_DYN ? 0.03 / sp.pr_t * d2 : 0.0);
@@ -1734,7 +1742,7 @@ class Solver final : public SolverBase {
     }
     h[g.nz + 1] = h[g.nz];
     if (!spong) spong = track(dalloc<double>(g.L));
-    if (!means) means = track(dalloc<double>(4 * g.L));
+    if (!means) means = track(dalloc<double>(6 * g.L));
     LES_CUDA(cudaMemcpy(spong, h.data(), sizeof(double) * g.L, cudaMemcpyHostToDevice));
   }
 
@@ -1955,10 +1963,11 @@ class Solver final : public SolverBase {
       t2 = 1.0 - t1;
     }
     ab2(t1, t2);
-    // mixed precision: the right-hand side from the increment (FP32
-    // transforms, no cancellation); FP64: the reference's formulation
-    if (mixed()) press_from_increment(t1, t2);
-    else press_stag_array(t1);
+    // the reference's formulation (FP64 transforms of u* in mixed precision);
+    // press_from_increment forms the same pressure in FP32 without the
+    // cancellation, but its FP32 four-field y pass measured slower than the
+    // FP64 three-field one at 256^3 (0.47 against 0.36 ms per step)
+    press_stag_array(t1);
     LES_CUDA(cudaEventRecord(ev[4], st));
     projection(t1);
     set_bc();

@@ -244,6 +244,27 @@ def log_law_noise(p: RunParams, seed: int = 0, amp: float = 0.1):
     return u, v, w
 
 
+def scalar_linear_noise(p: RunParams, seed: int = 0, amp: float = 0.01, gradient: float = 1.0):
+    """Passive-scalar initial field (nz, ny, nx): gradient * z at the uvp
+    heights plus uniform noise in [-amp, amp) (the velocity's hash, stream 3)."""
+    z = (np.arange(1, p.nz + 1) - 0.5) * p.dz
+    th = gradient * z[:, None, None] + np.zeros((p.nz, p.ny, p.nx))
+    return th + amp * _hash_uniform(seed, 3, th.shape)
+
+
+def inversion_noise(p: RunParams, seed: int = 0, z_inv: float = 0.5, lapse: float = 10.0, amp: float = 0.1,
+                    z_noise: float = 0.1):
+    """Convective-boundary-layer temperature as the departure from theta_0
+    (nz, ny, nx): 0 up to z_inv, lapse * (z - z_inv) above (0.01 K/m with
+    z_i = 1000 m is 10 K per unit height), uniform noise in [-amp, amp) K
+    below z_noise (hash stream 3)."""
+    z = (np.arange(1, p.nz + 1) - 0.5) * p.dz
+    base = np.where(z > z_inv, lapse * (z - z_inv), 0.0)
+    th = base[:, None, None] + np.zeros((p.nz, p.ny, p.nx))
+    noise = amp * _hash_uniform(seed, 3, th.shape)
+    return th + np.where((z < z_noise)[:, None, None], noise, 0.0)
+
+
 def _hash_uniform(seed: int, fid: int, shape):
     n = int(np.prod(shape))
     x = np.arange(n, dtype=np.uint64)
