@@ -55,6 +55,10 @@ def parse():
     ap.add_argument("--wall-levels", type=int, default=8,
                     help="levels next to the wall that keep the LASD procedure under the learned closure")
     ap.add_argument("--train-batch-tiles", type=int, default=16, help="training batch = 128 x this")
+    ap.add_argument("--train-protocol", default="short", choices=["short", "long"],
+                    help="short: pairs of the first --train-steps LASD steps (default); long: the learned-closure "
+                         "configuration's protocol, ~5e7 (invariant, Cs^2) pairs (10 %% held out) drawn evenly "
+                         "from 2000 LASD steps")
     ap.add_argument("--case", default="abl", choices=["abl", "scalar", "cbl"],
                     help="abl: the headline (neutral channel, 256^3); scalar: config 2 (FP64, passive scalar "
                          "with the dynamic Prandtl model, 128^3); cbl: config 5 (convective boundary layer, "
@@ -226,7 +230,10 @@ def run_ours(args, dist, rank, local, ws):
     les = LES(p, precision=args.precision, device=local)
     setup_case(les, p, args, rank)
     T = args.train_steps if args.closure == "mlp" else 0
-    train = train_closure(les, p, T, args.train_epochs, args.train_batch_tiles) if T else None
+    if T and args.train_protocol == "long":
+        T = 2000
+    train = (train_closure(les, p, T, args.train_epochs, args.train_batch_tiles,
+                           target_pairs=5e7 if args.train_protocol == "long" else None) if T else None)
     if T:
         les.mlp_set_wall_levels(args.wall_levels)
         train["wall_levels"] = args.wall_levels
@@ -393,19 +400,28 @@ def field_errors(a: dict, b: dict) -> dict:
     return out
 
 
-def train_closure(les, p, T: int, epochs: int = 4, tiles: int = 16) -> dict:
+def train_closure(les, p, T: int, epochs: int = 4, tiles: int = 16, target_pairs: float | None = None) -> dict:
     """Untimed: T LASD steps; the (features, log Cs^2) pairs of consecutive
-    update steps (one point in 8, every point of the 8 lowest levels, the
-    two wall levels 4 times; the first update only records the coefficient)
-    train the closure on the GPU; the state then continues with the learned
-    closure."""
+    update steps (the first update only records the coefficient) train the
+    closure on the GPU; the state then continues with the learned closure.
+    Short protocol: one point in 8, every point of the 8 lowest levels, the
+    two wall levels 4 times.  With target_pairs: one point in a stride that
+    spreads ~target_pairs (train + 10 % validation) evenly over the updates."""
     les.mlp_init(0)
-    les.mlp_reset_data(1 << 24)
+    nupd = sum(1 for j in range(1, T + 1) if j >= p.dyn_init and j % p.cs_count == 0) - 1
+    if target_pairs:
+        npts = p.nx * p.ny * (p.nz + 1)
+        stride = max(1, int(math.ceil(nupd * npts / target_pairs)))
+        collect = dict(stride=stride, dense_levels=0, wall_repeat=1)
+        les.mlp_reset_data(int(target_pairs * 1.02))
+    else:
+        collect = dict(stride=8, dense_levels=8, wall_repeat=4)
+        les.mlp_reset_data(1 << 24)
     t0 = time.perf_counter()
     for _ in range(T):
         les.step(1)
         if les.jt_total >= p.dyn_init and les.jt_total % p.cs_count == 0:  # consecutive updates
-            les.mlp_collect(stride=8, seed=les.jt_total, dense_levels=8, wall_repeat=4)
+            les.mlp_collect(seed=les.jt_total, **collect)
     les.sync()
     t1 = time.perf_counter()
     ntr, nva = les.mlp_counts()
@@ -414,7 +430,7 @@ def train_closure(les, p, T: int, epochs: int = 4, tiles: int = 16) -> dict:
     les.sync()
     t2 = time.perf_counter()
     les.set_sgs_model("mlp")
-    return {"lasd_steps": T, "train_pairs": ntr, "validation_pairs": nva, "epochs": epochs,
+    return {"lasd_steps": T, "collect": collect, "train_pairs": ntr, "validation_pairs": nva, "epochs": epochs,
             "batch": tiles * 128, "train_loss": [round(float(x), 4) for x in losses],
             "validation_loss": round(val, 4), "collect_s": round(t1 - t0, 3), "train_s": round(t2 - t1, 3)}
 

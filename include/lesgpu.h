@@ -158,6 +158,19 @@ int les_press_stag_array(les_state* s, double tadv1);
  * the reference's formulation.  Preconditions: rhs, rhs_f and the gradients
  * unchanged since the advance, w(nz+1) = 0. */
 int les_press_from_increment(les_state* s, double tadv1, double tadv2);
+/* z-slab decomposition of the pressure solve, emulated on this GPU: with
+ * nslabs > 1 the tridiagonal systems of press_stag_array (and of les_step)
+ * are solved by the partition method over nslabs blocks of rows, the blocks
+ * a z-slab rank holding levels b nz/G + 1 .. (b+1) nz/G would own: each
+ * block eliminates its rows with the right-hand side and the two unit
+ * couplings to its neighbours, the 2 nslabs boundary unknowns of every
+ * (kx, ky) column solve a 2 x 2 block-tridiagonal system, and each block
+ * back-substitutes.  Replaces the Y <-> Z transposes around
+ * tridiag_solver_parallel (compute_pressure.f90:265,290) of the reference's
+ * pencil decomposition; the same solution up to rounding.  nslabs = 1 (the
+ * default) is the single sweep.  Errors: 1 unless 1 <= nslabs <= 64 and nz
+ * is a multiple of nslabs with at least two levels per slab. */
+int les_set_pressure_slabs(les_state* s, int nslabs);
 /* compute_wall_law.f90:198-254 obukhov(u_star_avg, wall_model) */
 int les_obukhov(les_state* s);
 /* compute_wall_law.f90:107-185 wallstress(lbc_u, lbc_v, wall_model) */

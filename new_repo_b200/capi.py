@@ -77,6 +77,7 @@ PROTOTYPES = {
     "les_compute_dealias_convec": [_P, _I, _I, _I],
     "les_press_stag_array": [_P, C.c_double],
     "les_press_from_increment": [_P, C.c_double, C.c_double],
+    "les_set_pressure_slabs": [_P, _I],
     "les_obukhov": [_P],
     "les_wallstress": [_P],
     "les_sgs_stress": [_P, _I, _I],

@@ -187,6 +187,10 @@ int les_press_stag_array(les_state* s, double tadv1) {
   STATE_OR_FAIL(s);
   return guard([&] { s->s->press_stag_array(tadv1); });
 }
+int les_set_pressure_slabs(les_state* s, int nslabs) {
+  STATE_OR_FAIL(s);
+  return guard([&] { s->s->set_pressure_slabs(nslabs); });
+}
 int les_press_from_increment(les_state* s, double tadv1, double tadv2) {
   STATE_OR_FAIL(s);
   if (!(tadv1 != 0.0)) return bad_arg("tadv1");

@@ -1136,4 +1136,204 @@ __global__ void k_buoyancy(T* rz, const T* th, const double* tmean, long plane, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// pressure systems of a z-slab decomposition: the partition method.  Slab b
+// of G owns rows [s_b, e_b] of every (kx, ky) column (rows 0..nz+1: the
+// bottom closure row, nz interior rows, the top row; slab b holds levels
+// b m + 1 .. (b+1) m, m = nz/G, plus row 0 on the first and row nz+1 on
+// the last slab).  k_tri_slab_local eliminates a slab's rows with three
+// right-hand sides (r, and the unit couplings -a e_first, -c e_last to the
+// neighbouring slabs' boundary unknowns) into y, u, v; k_tri_slab_reduced
+// solves the 2G boundary unknowns of each column (2 x 2 block Thomas);
+// k_tri_slab_back forms x = y + u x_left + v x_right.  Same matrix,
+// right-hand side and outputs as k_tridiag (compute_pressure.f90:256-305,
+// 448-493, 544-619); only the elimination order differs.
+struct SlabRows {
+  int G, m, nz;
+  __host__ __device__ int start(int b) const { return b == 0 ? 0 : b * m + 1; }
+  __host__ __device__ int end(int b) const { return b < G - 1 ? (b + 1) * m : nz + 1; }
+  __host__ __device__ int of_row(int k) const { return k == 0 ? 0 : min((k - 1) / m, G - 1); }
+};
+
+// row k of a column: coefficients (a, b, c) and the right-hand side
+template <typename T>
+__device__ __forceinline__ void tri_row(int k, int nz, bool mean, double a_in, double b_in, double dz, double kxv,
+                                        double kyv, const cplx<T>* Hx, const cplx<T>* Hy, const cplx<T>* Hz,
+                                        const cplx<T>* bot, const cplx<T>* top, long icol, long isp, double& a,
+                                        double& b, double& c, cplx<double>& r) {
+  if (k == 0) {
+    a = 0.0;
+    b = mean ? 1.0 : -1.0;
+    c = mean ? 0.0 : 1.0;
+    r = mean ? cplx<double>{0.0, 0.0} : cplx<double>{double(bot[icol].x) * dz, double(bot[icol].y) * dz};
+  } else if (k == nz + 1) {
+    a = -1.0;
+    b = 1.0;
+    c = 0.0;
+    r = {double(top[icol].x) * dz, double(top[icol].y) * dz};
+  } else {
+    a = a_in;
+    b = b_in;
+    c = a_in;
+    const long o = (long)k * isp + icol;
+    const cplx<T> hx = Hx[o], hy = Hy[o], hz = Hz[o];
+    const cplx<T> hzp = (k < nz) ? Hz[o + isp] : cplx<T>{T(0), T(0)};
+    const double sx = kxv * double(hx.x) + kyv * double(hy.x);
+    const double sy = kxv * double(hx.y) + kyv * double(hy.y);
+    r = {-sy + (double(hzp.x) - double(hz.x)) / dz, sx + (double(hzp.y) - double(hz.y)) / dz};
+  }
+}
+
+// grid (ceil(lhx/64), ny, G), 64 threads: one (column, slab) per thread.
+// ys (complex), uu, vv: the slab's solutions at its rows; gam: scratch.
+template <typename T>
+__global__ void k_tri_slab_local(const cplx<T>* __restrict__ Hx, const cplx<T>* __restrict__ Hy,
+                                 const cplx<T>* __restrict__ Hz, const cplx<T>* __restrict__ bot,
+                                 const cplx<T>* __restrict__ top, const double* __restrict__ kkx,
+                                 const double* __restrict__ kky, cplx<double>* __restrict__ ys,
+                                 double* __restrict__ uu, double* __restrict__ vv, double* __restrict__ gam,
+                                 unsigned* status, int lhx, int ny, int nz, double dz, int ipitch, SlabRows sr) {
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ky = blockIdx.y;
+  const int sb = blockIdx.z;
+  if (kx >= lhx || kx == lhx - 1 || ky == ny / 2) return;  // Nyquist columns: zero (k_tri_slab_back)
+  const long col = (long)ky * lhx + kx, sp = (long)ny * lhx;
+  const long icol = (long)ky * ipitch + kx, isp = (long)ny * ipitch;
+  const bool mean = (kx == 0 && ky == 0);
+  const double a_in = 1.0 / (dz * dz);
+  const double kxv = kkx[col], kyv = kky[col];
+  const double b_in = -((kxv * kxv + kyv * kyv) + 2.0 / (dz * dz));
+  const int s = sr.start(sb), e = sr.end(sb);
+  double a, b, c;
+  cplx<double> r;
+  tri_row<T>(s, nz, mean, a_in, b_in, dz, kxv, kyv, Hx, Hy, Hz, bot, top, icol, isp, a, b, c, r);
+  double bet = b;
+  bool bad = (bet == 0.0);
+  cplx<double> y = {r.x / bet, r.y / bet};
+  double u = (sb > 0 ? -a : 0.0) / bet;
+  double cprev = c;
+  double v = (e == s && sb < sr.G - 1) ? -c / bet : 0.0;
+  ys[(long)s * sp + col] = y;
+  uu[(long)s * sp + col] = u;
+  vv[(long)s * sp + col] = v;
+  for (int k = s + 1; k <= e; ++k) {
+    tri_row<T>(k, nz, mean, a_in, b_in, dz, kxv, kyv, Hx, Hy, Hz, bot, top, icol, isp, a, b, c, r);
+    const double g = cprev / bet;
+    bet = b - a * g;
+    bad |= (bet == 0.0);
+    const double rv = (k == e && sb < sr.G - 1) ? -c : 0.0;
+    y = {(r.x - a * y.x) / bet, (r.y - a * y.y) / bet};
+    u = (0.0 - a * u) / bet;
+    v = (rv - a * v) / bet;
+    const long o = (long)k * sp + col;
+    gam[o] = g;
+    ys[o] = y;
+    uu[o] = u;
+    vv[o] = v;
+    cprev = c;
+  }
+  for (int k = e - 1; k >= s; --k) {
+    const long o = (long)k * sp + col;
+    const double g = gam[o + sp];
+    y = {ys[o].x - g * y.x, ys[o].y - g * y.y};
+    u = uu[o] - g * u;
+    v = vv[o] - g * v;
+    ys[o] = y;
+    uu[o] = u;
+    vv[o] = v;
+  }
+  if (bad) atomicOr(status, ST_PIVOT);
+}
+
+// one column per thread: the boundary unknowns X_s^b, X_e^b of every slab
+// (block Thomas over 2 x 2 blocks), written as the neighbours' values each
+// slab needs: xlr[(col G + b) 2 + 0] = X_e^{b-1}, [.. + 1] = X_s^{b+1}
+constexpr int MAX_SLABS = 64;
+__global__ void k_tri_slab_reduced(const cplx<double>* __restrict__ ys, const double* __restrict__ uu,
+                                   const double* __restrict__ vv, cplx<double>* __restrict__ xlr, unsigned* status,
+                                   int lhx, int ny, SlabRows sr) {
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ky = blockIdx.y;
+  if (kx >= lhx || kx == lhx - 1 || ky == ny / 2) return;
+  const long col = (long)ky * lhx + kx, sp = (long)ny * lhx;
+  const int G = sr.G;
+  // forward elimination; keep the modified blocks (first column only
+  // changes) and right-hand sides
+  double p00[MAX_SLABS], p10[MAX_SLABS];
+  cplx<double> y0[MAX_SLABS], y1[MAX_SLABS];
+  bool bad = false;
+  for (int b = 0; b < G; ++b) {
+    const long os = (long)sr.start(b) * sp + col, oe = (long)sr.end(b) * sp + col;
+    const double us = uu[os], ue = uu[oe];
+    cplx<double> a0 = ys[os], a1 = ys[oe];
+    double b00 = 1.0, b10 = 0.0;
+    if (b > 0) {
+      // p01 = 0, p11 = 1 for every modified block
+      const double det = p00[b - 1];
+      bad |= (det == 0.0);
+      const double i10 = -p10[b - 1] / det, i11 = p00[b - 1] / det;
+      const long ops = (long)sr.start(b - 1) * sp + col, ope = (long)sr.end(b - 1) * sp + col;
+      const double w0 = i10 * (-vv[ops]) + i11 * (-vv[ope]);
+      const cplx<double> z = {i10 * y0[b - 1].x + i11 * y1[b - 1].x, i10 * y0[b - 1].y + i11 * y1[b - 1].y};
+      b00 = b00 + us * w0;
+      b10 = b10 + ue * w0;
+      a0 = {a0.x + us * z.x, a0.y + us * z.y};
+      a1 = {a1.x + ue * z.x, a1.y + ue * z.y};
+    }
+    p00[b] = b00;
+    p10[b] = b10;
+    y0[b] = a0;
+    y1[b] = a1;
+  }
+  cplx<double> xs_next = {0.0, 0.0};  // X_s^{b+1}
+  for (int b = G - 1; b >= 0; --b) {
+    cplx<double> r0 = y0[b], r1 = y1[b];
+    if (b < G - 1) {
+      const double vs = vv[(long)sr.start(b) * sp + col], ve = vv[(long)sr.end(b) * sp + col];
+      r0 = {r0.x + vs * xs_next.x, r0.y + vs * xs_next.y};
+      r1 = {r1.x + ve * xs_next.x, r1.y + ve * xs_next.y};
+    }
+    const double det = p00[b];  // p01 = 0, p11 = 1
+    bad |= (det == 0.0);
+    const cplx<double> Xs = {r0.x / det, r0.y / det};
+    const cplx<double> Xe = {(-p10[b] * r0.x + p00[b] * r1.x) / det, (-p10[b] * r0.y + p00[b] * r1.y) / det};
+    // slab b + 1 needs X_e^b as its left value, slab b - 1 needs X_s^b
+    if (b + 1 < G) xlr[(col * G + b + 1) * 2 + 0] = Xe;
+    if (b > 0) xlr[(col * G + b - 1) * 2 + 1] = Xs;
+    xs_next = Xs;
+  }
+  xlr[(col * G + 0) * 2 + 0] = {0.0, 0.0};
+  xlr[(col * G + G - 1) * 2 + 1] = {0.0, 0.0};
+  if (bad) atomicOr(status, ST_PIVOT);
+}
+
+// grid (ceil(lhx/64), ny, nz + 2): x = y + u x_left + v x_right into phat
+// (the outputs of k_tridiag: phat(nz+1) = 0; the mean mode kept apart in
+// FP64 as pmean with drop_mean)
+template <typename O>
+__global__ void k_tri_slab_back(const cplx<double>* __restrict__ ys, const double* __restrict__ uu,
+                                const double* __restrict__ vv, const cplx<double>* __restrict__ xlr,
+                                cplx<O>* __restrict__ phat, double* pmean, int lhx, int ny, int nz, int drop_mean,
+                                int opitch, SlabRows sr) {
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ky = blockIdx.y;
+  const int k = blockIdx.z;
+  if (kx >= lhx) return;
+  const long col = (long)ky * lhx + kx, sp = (long)ny * lhx;
+  const long oo = (long)k * ny * opitch + (long)ky * opitch + kx;
+  if (kx == lhx - 1 || ky == ny / 2 || k == nz + 1) {
+    phat[oo] = cplx<O>{O(0), O(0)};
+    if (kx == 0 && ky == 0 && pmean && k == nz + 1) pmean[k] = 0.0;
+    return;
+  }
+  const bool mean = (kx == 0 && ky == 0);
+  const int b = sr.of_row(k);
+  const long o = (long)k * sp + col;
+  const cplx<double> xl = xlr[(col * sr.G + b) * 2 + 0], xr = xlr[(col * sr.G + b) * 2 + 1];
+  const double u = uu[o], v = vv[o];
+  const cplx<double> x = {ys[o].x + u * xl.x + v * xr.x, ys[o].y + u * xl.y + v * xr.y};
+  if (mean && pmean) pmean[k] = x.x;
+  phat[oo] = (mean && drop_mean) ? cplx<O>{O(0), O(0)} : cplx<O>{O(x.x), O(x.y)};
+}
+
 }  // namespace les

@@ -347,6 +347,18 @@ __device__ __forceinline__ void put_row64(unsigned char* tile, int row, const fl
     *reinterpret_cast<uint4*>(tile + kmaj_off(row, 8 * c, 1024)) = q;
   }
 }
+// write 16 values as columns 16 c .. 16 c + 15 of row `row` of a K-major (sbo 1024) BF16 tile
+__device__ __forceinline__ void put16(unsigned char* tile, int row, int c, const float* v) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    uint4 q;
+    q.x = pack_bf16x2(v[8 * h + 0], v[8 * h + 1]);
+    q.y = pack_bf16x2(v[8 * h + 2], v[8 * h + 3]);
+    q.z = pack_bf16x2(v[8 * h + 4], v[8 * h + 5]);
+    q.w = pack_bf16x2(v[8 * h + 6], v[8 * h + 7]);
+    *reinterpret_cast<uint4*>(tile + kmaj_off(row, 16 * c + 8 * h, 1024)) = q;
+  }
+}
 __device__ __forceinline__ float tile_val(const unsigned char* tile, int row, int k, int sbo) {
   const uint16_t b = *reinterpret_cast<const uint16_t*>(tile + kmaj_off(row, k, sbo));
   return __uint_as_float(uint32_t(b) << 16);
@@ -491,15 +503,87 @@ __global__ void __launch_bounds__(TILE) k_mlp_infer(const MlpFeatIn<T> a, T* cs,
 
 // ------------------------------------------------------------- training ----
 // One launch: each CTA loops over tiles of samples [tile*128, +128) < n,
-// forward + backward; per-thread gradient accumulators are added to
-// m.grad once per CTA.  Gradient of L = mean_i (y_i - t_i)^2 with inv_n = 1/n.
+// forward + backward.  Gradient of L = mean_i (y_i - t_i)^2 with inv_n = 1/n.
+//
+// The weight gradients are one more tensor-core GEMM per tile, accumulated
+// in TMEM over all of a CTA's tiles and added to m.grad once per CTA:
+// D[128 x 192] += AW[128 x 128] . BW[192 x 128]^T (K = the 128 samples),
+// with AW rows 0..63 = h1^T, 64..71 = x^T, 72 = ones, 73 = dy, rest zero and
+// BW rows 0..63 = g2^T, 64..127 = delta1^T, 128..191 = h2^T, so that
+// D[k][n] = dW2, D[64 + f][64 + k] = dW1, D[72][n] = db2, D[72][64 + k] =
+// db1, D[73][128 + i] = dw3 (db3 = sum dy on the CUDA cores).  Operands are
+// BF16 (the oracle rounds the same values), accumulation FP32.  The
+// transposed tiles are built from the K-major sample-row tiles by 8 x 8
+// transposes of core matrices (16-byte loads and stores, byte permutes).
+constexpr int AW_ROWS = 128, BW_ROWS = 192, W_SBO = 2048;  // K = 128 samples: 16 chunks of 128 B per row group
+constexpr uint32_t IDESC_W = tc::idesc_bf16_f32(128, 192);
+constexpr uint32_t TM_Z1 = 0, TM_Z2 = 64, TM_D1 = 128, TM_W = 256;  // TMEM columns
+
 struct TrainSmem {
   MlpSmem s;
-  float red[TILE][65];  // h2, then delta1 (fp32 rows)
-  float g2f[TILE][65];  // g2 (fp32 rows)
-  float xf[TILE][8];
-  float dy[TILE];
+  alignas(1024) unsigned char AW[AW_ROWS / 8 * W_SBO];   // 32 KB
+  alignas(1024) unsigned char BW[BW_ROWS / 8 * W_SBO];   // 48 KB
+  alignas(1024) unsigned char T64[TILE * 64 * 2];        // 16 KB sample-row staging (h2, delta1)
+  float dsum[TILE / 32];
+  uint64_t wbar;
 };
+
+// 8 x 8 transpose of 16-bit elements: in[r] = row r (8 values in a uint4),
+// out[c] = column c
+__device__ __forceinline__ void transpose8x8(const uint4* in, uint4* out) {
+  uint32_t w[8][4];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    w[r][0] = in[r].x;
+    w[r][1] = in[r].y;
+    w[r][2] = in[r].z;
+    w[r][3] = in[r].w;
+  }
+  uint32_t o[8][4];  // o[c][p]: column c, rows 2p and 2p + 1
+#pragma unroll
+  for (int c = 0; c < 8; ++c)
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+      o[c][p] = __byte_perm(w[2 * p][c >> 1], w[2 * p + 1][c >> 1], (c & 1) ? 0x7632 : 0x5410);
+#pragma unroll
+  for (int c = 0; c < 8; ++c) out[c] = make_uint4(o[c][0], o[c][1], o[c][2], o[c][3]);
+}
+
+// core matrix (sample group sg, feature chunk fc) of a sample-row K-major tile
+// (sbo_src) -> core matrix (feature group row0 / 8 + fc, sample chunk sg) of a
+// transposed tile (sbo W_SBO)
+__device__ __forceinline__ void transpose_block(const unsigned char* src, int sbo_src, unsigned char* dst, int row0,
+                                                int sg, int fc) {
+  uint4 in[8], out[8];
+  const unsigned char* sp = src + sg * sbo_src + fc * 128;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) in[r] = *reinterpret_cast<const uint4*>(sp + 16 * r);
+  transpose8x8(in, out);
+  unsigned char* dp = dst + (row0 / 8 + fc) * W_SBO + sg * 128;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) *reinterpret_cast<uint4*>(dp + 16 * c) = out[c];
+}
+
+// the weight-gradient GEMM of one tile into TMEM columns TM_W.. (thread 0);
+// waits (bounded) so the next tile may overwrite AW / BW
+__device__ __forceinline__ bool tc_weights(TrainSmem& TS, uint32_t& wphase, unsigned* status, bool first) {
+  MlpSmem& S = TS.s;
+  if (threadIdx.x == 0) {
+    tc::fence_after_sync();
+    const uint32_t aw = tc::smem_u32(TS.AW), bw = tc::smem_u32(TS.BW);
+#pragma unroll
+    for (int ks = 0; ks < 8; ++ks)
+      tc::mma_bf16(S.tmem + TM_W, tc::smem_desc(aw + 256 * ks, 128, W_SBO), tc::smem_desc(bw + 256 * ks, 128, W_SBO),
+                   IDESC_W, (!first || ks > 0) ? 1u : 0u);
+    tc::mma_commit(&TS.wbar);
+    S.ok = tc::mbar_wait(&TS.wbar, wphase) ? 1 : 0;
+    if (!S.ok) atomicOr(status, 16u);
+  }
+  wphase ^= 1u;
+  __syncthreads();
+  tc::fence_after_sync();
+  return S.ok != 0;
+}
 
 __global__ void __launch_bounds__(TILE) k_mlp_train(MlpDevice m, const float* X, const float* Tg, long n,
                                                     float inv_n, float* y_out, float* loss, unsigned* status,
@@ -508,17 +592,22 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(MlpDevice m, const float* X,
   TrainSmem& TS = *reinterpret_cast<TrainSmem*>(smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023));
   MlpSmem& S = TS.s;
   load_images(S, m.img, m.params, m.stats);
-  if (threadIdx.x == 0) S.ok = 1;
-  tc_setup(S, 256);
+  if (threadIdx.x == 0) {
+    S.ok = 1;
+    tc::mbar_init(&TS.wbar, 1);
+  }
   const int tid = threadIdx.x;
-  // gradient ownership: dW2 entries k = tid/2, n in [32*(tid%2), +32); dW1
-  // entries f = tid/16, k in [4*(tid%16), +4); biases / w3 by tid < 64
-  float aw2[32], aw1[4];
-  for (int i = 0; i < 32; ++i) aw2[i] = 0.0f;
-  for (int i = 0; i < 4; ++i) aw1[i] = 0.0f;
-  float ab1 = 0.0f, ab2 = 0.0f, aw3 = 0.0f, ab3 = 0.0f, aloss = 0.0f;
-  uint32_t phase = 0;
+  // AW rows 72..127: row 72 ones, the rest zero (row 73 is rewritten per tile)
+  for (int i = tid; i < (AW_ROWS - 72) * TILE; i += TILE) {
+    const int r = 72 + i / TILE, c = i % TILE;
+    *reinterpret_cast<uint16_t*>(TS.AW + kmaj_off(r, c, W_SBO)) = bf16_bits(r == 72 ? 1.0f : 0.0f);
+  }
+  tc_setup(S, 512);  // z1, z2, delta1 (64 columns each) and the 192 weight-gradient columns
+  float ab3 = 0.0f, aloss = 0.0f;
+  uint32_t phase = 0, wphase = 0;
+  bool first = true, wfail = false;
   const long ntiles = (n + TILE - 1) / TILE;
+  const int sg = tid >> 3, fc = tid & 7;  // this thread's core matrix of the 64-wide tiles
   for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const long q = tile * TILE + tid;
     const bool valid = q < n;
@@ -527,104 +616,116 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(MlpDevice m, const float* X,
     for (int i = 0; i < 8; ++i) x[i] = valid ? X[src * 8 + i] : 0.0f;
     const float tg = valid ? Tg[src] : 0.0f;
     put_features(S, tid, x);
-    for (int i = 0; i < 8; ++i) TS.xf[tid][i] = tile_val(S.A1, tid, i, 256);  // bf16-rounded inputs
     tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
-    if (!tc_stage(S, phase, status, 0, 0)) break;
-    float z1[64], h[64];
-    tmem_row64(S.tmem, 0, z1);
+    if (tid < 16) transpose_block(S.A1, 256, TS.AW, 64, tid, 0);  // x^T -> AW rows 64..71
+    if (!tc_stage(S, phase, status, 0, TM_Z1)) break;
+    // the layer outputs stay in TMEM (z1 at TM_Z1, z2 at TM_Z2) and are read
+    // back 16 columns at a time where they are needed, so that no 64-value
+    // row is live across a stage
+    const uint32_t lane = uint32_t((tid / 32) * 32) << 16;
+#pragma unroll 1
+    for (int c = 0; c < 4; ++c) {  // h1 = gelu(z1 + b1)
+      float v[16];
+      tc::tmem_ld16(S.tmem + lane + TM_Z1 + 16 * c, v);
+      tc::tmem_wait_ld();
 #pragma unroll
-    for (int i = 0; i < 64; ++i) {
-      z1[i] += S.b1[i];
-      h[i] = gelu(z1[i]);
+      for (int i = 0; i < 16; ++i) v[i] = gelu(v[i] + S.b1[16 * c + i]);
+      put16(S.A2, tid, c, v);
     }
-    put_row64(S.A2, tid, h);
     tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
-    if (!tc_stage(S, phase, status, 1, 64)) break;
-    tmem_row64(S.tmem, 64, h);  // z2 (without bias)
+    transpose_block(S.A2, 1024, TS.AW, 0, sg, fc);  // h1^T -> AW rows 0..63 (the BF16 values layer 2 uses)
+    if (!tc_stage(S, phase, status, 1, TM_Z2)) break;
     float y = S.b3;
-    for (int i = 0; i < 64; ++i) {
-      h[i] += S.b2[i];  // z2
-      y += S.w3[i] * gelu(h[i]);
+#pragma unroll 1
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      tc::tmem_ld16(S.tmem + lane + TM_Z2 + 16 * c, v);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) y += S.w3[16 * c + i] * gelu(v[i] + S.b2[16 * c + i]);
     }
     if (y_out && valid) y_out[q] = y;
     const float dy = valid ? 2.0f * (y - tg) * inv_n : 0.0f;
     if (valid) aloss += (y - tg) * (y - tg) * inv_n;
-    TS.dy[tid] = dy;
-    float g2[64];
-    for (int i = 0; i < 64; ++i) {
-      TS.red[tid][i] = gelu(h[i]);          // h2
-      g2[i] = dy * S.w3[i] * gelu_grad(h[i]);
-      TS.g2f[tid][i] = g2[i];
+#pragma unroll 1
+    for (int c = 0; c < 4; ++c) {  // h2 and g2 = dy w3 gelu'(z2)
+      float v[16], h2[16], g2[16];
+      tc::tmem_ld16(S.tmem + lane + TM_Z2 + 16 * c, v);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const float z2 = v[i] + S.b2[16 * c + i];
+        h2[i] = gelu(z2);
+        g2[i] = dy * S.w3[16 * c + i] * gelu_grad(z2);
+      }
+      put16(S.G2, tid, c, g2);
+      put16(TS.T64, tid, c, h2);
     }
-    put_row64(S.G2, tid, g2);
+    *reinterpret_cast<uint16_t*>(TS.AW + kmaj_off(73, tid, W_SBO)) = bf16_bits(dy);
+    {  // db3: sum of dy over the tile
+      float d = dy;
+      for (int off = 16; off > 0; off >>= 1) d += __shfl_down_sync(0xffffffffu, d, off);
+      if ((tid & 31) == 0) TS.dsum[tid >> 5] = d;
+    }
     tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
-    // dw3, db3, db2 (row reductions over the tile)
-    if (tid < 64) {
-      float s3 = 0.0f, s2 = 0.0f;
-      for (int r = 0; r < TILE; ++r) {
-        s3 += TS.dy[r] * TS.red[r][tid];
-        s2 += TS.g2f[r][tid];
-      }
-      aw3 += s3;
-      ab2 += s2;
-    } else if (tid == 64) {
-      float s = 0.0f;
-      for (int r = 0; r < TILE; ++r) s += TS.dy[r];
-      ab3 += s;
-    }
-    // dW2[k][n] = sum_r h1[r][k] g2[r][n] (h1 as the BF16 values layer 2 used)
-    {
-      const int kk = tid >> 1, n0 = (tid & 1) * 32;
-      for (int r = 0; r < TILE; ++r) {
-        const float hv = tile_val(S.A2, r, kk, 1024);
+    if (tid == 0) ab3 += (TS.dsum[0] + TS.dsum[1]) + (TS.dsum[2] + TS.dsum[3]);
+    transpose_block(S.G2, 1024, TS.BW, 0, sg, fc);     // g2^T -> BW rows 0..63
+    transpose_block(TS.T64, 1024, TS.BW, 128, sg, fc); // h2^T -> BW rows 128..191
+    if (!tc_stage(S, phase, status, 2, TM_D1)) break;
+    // delta1 = (g2 . W2^T) * gelu'(z1); h2's transpose finished before the
+    // stage's barrier, so T64 is free
+#pragma unroll 1
+    for (int c = 0; c < 4; ++c) {
+      float d1[16], z1[16];
+      tc::tmem_ld16(S.tmem + lane + TM_D1 + 16 * c, d1);
+      tc::tmem_ld16(S.tmem + lane + TM_Z1 + 16 * c, z1);
+      tc::tmem_wait_ld();
 #pragma unroll
-        for (int i = 0; i < 32; ++i) aw2[i] += hv * TS.g2f[r][n0 + i];
-      }
+      for (int i = 0; i < 16; ++i) d1[i] *= gelu_grad(z1[i] + S.b1[16 * c + i]);
+      put16(TS.T64, tid, c, d1);
     }
-    if (!tc_stage(S, phase, status, 2, 128)) break;
-    // delta1 = (g2 . W2^T) * gelu'(z1)
-    float d1[64];
-    tmem_row64(S.tmem, 128, d1);
-    for (int i = 0; i < 64; ++i) TS.red[tid][i] = d1[i] * gelu_grad(z1[i]);
     __syncthreads();
-    if (tid < 64) {
-      float s = 0.0f;
-      for (int r = 0; r < TILE; ++r) s += TS.red[r][tid];
-      ab1 += s;
-    }
-    {
-      const int f = tid >> 4, k0 = (tid & 15) * 4;
-      for (int r = 0; r < TILE; ++r) {
-        const float xv = TS.xf[r][f];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) aw1[i] += xv * TS.red[r][k0 + i];
-      }
-    }
+    transpose_block(TS.T64, 1024, TS.BW, 64, sg, fc);  // delta1^T -> BW rows 64..127
+    tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
-  }
-  tc_teardown(S, 256, phase);
-  {
-    const int kk = tid >> 1, n0 = (tid & 1) * 32;
-    for (int i = 0; i < 32; ++i) atomicAdd(&m.grad[MLP_O_W2 + kk * MLP_H + n0 + i], aw2[i]);
-    const int f = tid >> 4, k0 = (tid & 15) * 4;
-    for (int i = 0; i < 4; ++i) atomicAdd(&m.grad[MLP_O_W1 + f * MLP_H + k0 + i], aw1[i]);
-    if (tid < 64) {
-      atomicAdd(&m.grad[MLP_O_B1 + tid], ab1);
-      atomicAdd(&m.grad[MLP_O_B2 + tid], ab2);
-      atomicAdd(&m.grad[MLP_O_W3 + tid], aw3);
+    if (!tc_weights(TS, wphase, status, first)) {
+      wfail = true;
+      break;
     }
-    if (tid == 64) atomicAdd(&m.grad[MLP_O_B3], ab3);
-    // loss: warp reduce then one atomic per warp
-    for (int off = 16; off > 0; off >>= 1) aloss += __shfl_down_sync(0xffffffffu, aloss, off);
-    if ((tid & 31) == 0 && loss) atomicAdd(loss, aloss);
+    first = false;
   }
+  // the weight gradients: thread r reads TMEM lane r (D row r); every warp
+  // runs the same loads (tcgen05.ld is warp-collective)
+  if (!first && S.ok) {
+    float v[64];
+    tmem_row64(S.tmem, TM_W, v);
+    if (tid < 64)
+      for (int i = 0; i < 64; ++i) atomicAdd(&m.grad[MLP_O_W2 + tid * MLP_H + i], v[i]);  // dW2[tid][.]
+    else if (tid == 72)
+      for (int i = 0; i < 64; ++i) atomicAdd(&m.grad[MLP_O_B2 + i], v[i]);
+    tmem_row64(S.tmem, TM_W + 64, v);
+    if (tid >= 64 && tid < 72)
+      for (int i = 0; i < 64; ++i) atomicAdd(&m.grad[MLP_O_W1 + (tid - 64) * MLP_H + i], v[i]);  // dW1
+    else if (tid == 72)
+      for (int i = 0; i < 64; ++i) atomicAdd(&m.grad[MLP_O_B1 + i], v[i]);
+    tmem_row64(S.tmem, TM_W + 128, v);
+    if (tid == 73)
+      for (int i = 0; i < 64; ++i) atomicAdd(&m.grad[MLP_O_W3 + i], v[i]);
+  }
+  // a weight GEMM whose wait ran out may still be in flight: wait (bounded)
+  // for it before the TMEM is freed
+  if (tid == 0 && !S.ok && wfail) tc::mbar_wait(&TS.wbar, wphase ^ 1u);
+  tc_teardown(S, 512, phase);
+  if (tid == 0) atomicAdd(&m.grad[MLP_O_B3], ab3);
+  for (int off = 16; off > 0; off >>= 1) aloss += __shfl_down_sync(0xffffffffu, aloss, off);
+  if ((tid & 31) == 0 && loss) atomicAdd(loss, aloss);
 }
 
 __global__ void k_mlp_adam(float* p, const float* g, float* mm, float* vv, int step, float lr) {

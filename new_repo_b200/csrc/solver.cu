@@ -1322,9 +1322,12 @@ class Solver final : public SolverBase {
       // mixed precision: p^ leaves the FP64 solve as FP32 (its mean mode is
       // kept apart in FP64); the inverse transforms of p run in FP32 -- only
       // the forward right-hand side needs FP64, where div u* cancels
-      KL("k_tridiag", 96.0 * double(g.L) * g.ny * g.lhx,
-         k_tridiag<S, T><<<tg, 64, 0, st>>>(sp[2], sp[3], sp[4], nullptr, bot, top, kkxd, kkyd, spec[0], xs, gam, pmean, dstatus,
-                                            g.lhx, g.ny, nz, dz(), 1, pitch(g.lhx), g.lhx));
+      if (pslabs > 1)
+        slab_solve<S, T>(sp[2], sp[3], sp[4], bot, top, spec[0], pmean, 1, pitch(g.lhx), g.lhx);
+      else
+        KL("k_tridiag", 96.0 * double(g.L) * g.ny * g.lhx,
+           k_tridiag<S, T><<<tg, 64, 0, st>>>(sp[2], sp[3], sp[4], nullptr, bot, top, kkxd, kkyd, spec[0], xs, gam, pmean, dstatus,
+                                              g.lhx, g.ny, nz, dz(), 1, pitch(g.lhx), g.lhx));
       auto e = yp(YP_PGRAD, 1, 3, g.lhx, g.lhx, g.ny, g.lhx, g.ny, 0);
       e.in[0] = spec[0];
       e.out[0] = spec[1];
@@ -1350,8 +1353,11 @@ class Solver final : public SolverBase {
          k_p_finish<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_P], pmean, g.plane(), nz));
       return;
     }
-    KL("k_tridiag", 112.0 * double(g.L) * g.ny * g.lhx, k_tridiag<S><<<tg, 64, 0, st>>>(sp[2], sp[3], sp[4], nullptr, bot, top, kkxd, kkyd, sp[5], xs, gam,
-                                   mixed() ? pmean : nullptr, dstatus, g.lhx, g.ny, nz, dz(), mixed() ? 1 : 0, g.lhx, g.lhx));
+    if (pslabs > 1)
+      slab_solve<S, S>(sp[2], sp[3], sp[4], bot, top, sp[5], mixed() ? pmean : nullptr, mixed() ? 1 : 0, g.lhx, g.lhx);
+    else
+      KL("k_tridiag", 112.0 * double(g.L) * g.ny * g.lhx, k_tridiag<S><<<tg, 64, 0, st>>>(sp[2], sp[3], sp[4], nullptr, bot, top, kkxd, kkyd, sp[5], xs, gam,
+                                     mixed() ? pmean : nullptr, dstatus, g.lhx, g.ny, nz, dz(), mixed() ? 1 : 0, g.lhx, g.lhx));
     // compute_press_grad: i kx p^, i ky p^, p^ -> dpdx, dpdy (1..nz), p (0..nz+1)
     auto e = yp_s<S>(YP_PGRAD, 1, 3, 0);
     e.in[0] = sp[5];
@@ -1379,6 +1385,43 @@ class Solver final : public SolverBase {
   }
   double press_tadv1_ = 1.0;
   void dpdz_only();
+  // z-slab emulation of the pressure solve: the systems solved by the
+  // partition method over pslabs row blocks, as pslabs z-slab ranks would
+  // (k_tri_slab_*); 1 = the single sweep of k_tridiag
+  int pslabs = 1;
+  double *slab_u = nullptr, *slab_v = nullptr;
+  cplx<double>* slab_x = nullptr;
+  int slab_x_cap = 1;
+  void set_pressure_slabs(int G) override {
+    if (G < 1 || G > MAX_SLABS || g.nz % G != 0 || g.nz / G < 2)
+      throw CudaError(1, "pressure slabs: 1 <= G <= 64, nz a multiple of G with at least two levels per slab");
+    pslabs = G;
+    if (G > 1 && !slab_u) {
+      const long n = (long)g.L * g.ny * g.lhx;
+      slab_u = track(dalloc<double>(n));
+      slab_v = track(dalloc<double>(n));
+    }
+    if (G > slab_x_cap) {
+      slab_x = track(dalloc<cplx<double>>((long)g.ny * g.lhx * G * 2));
+      slab_x_cap = G;
+    }
+  }
+  template <typename S, typename O>
+  void slab_solve(const cplx<S>* Hx, const cplx<S>* Hy, const cplx<S>* Hz, const cplx<S>* bot, const cplx<S>* top,
+                  cplx<O>* phat, double* pm, int drop_mean, int opitch, int ipitch) {
+    const SlabRows sr{pslabs, g.nz / pslabs, g.nz};
+    const double cols = double(g.ny) * g.lhx;
+    KL("k_tri_slab_local", cols * g.L * (3.0 * 2 * sizeof(S) + 40.0),
+       k_tri_slab_local<S><<<dim3(ceil_div(g.lhx, 64), g.ny, pslabs), 64, 0, st>>>(
+           Hx, Hy, Hz, bot, top, kkxd, kkyd, xs, slab_u, slab_v, gam, dstatus, g.lhx, g.ny, g.nz, dz(), ipitch, sr));
+    KL("k_tri_slab_reduced", cols * pslabs * (2 * 32.0 + 32.0),
+       k_tri_slab_reduced<<<dim3(ceil_div(g.lhx, 64), g.ny), 64, 0, st>>>(xs, slab_u, slab_v, slab_x, dstatus, g.lhx,
+                                                                          g.ny, sr));
+    KL("k_tri_slab_back", cols * g.L * (32.0 + 2 * sizeof(O)),
+       k_tri_slab_back<O><<<dim3(ceil_div(g.lhx, 64), g.ny, g.L), 64, 0, st>>>(xs, slab_u, slab_v, slab_x, phat, pm,
+                                                                               g.lhx, g.ny, g.nz, drop_mean, opitch, sr));
+  }
+
 
   // press_stag_array on the state an AB2 advance left, with the right-hand
   // side formed from the increment: u* / (dt t1) = u^n / (dt t1) + r +

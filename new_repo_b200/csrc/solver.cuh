@@ -96,6 +96,7 @@ struct SolverBase : LaunchHook {
   virtual void dealias_convec(int cx, int cy, int cz) = 0;
   virtual void press_stag_array(double tadv1) = 0;
   virtual void press_from_increment(double tadv1, double tadv2) = 0;
+  virtual void set_pressure_slabs(int G) = 0;
   virtual void obukhov() = 0;
   virtual void wallstress() = 0;
   virtual void sgs_stress(int jt, int jtt) = 0;

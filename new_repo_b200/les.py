@@ -431,6 +431,11 @@ class LES:
     def press_stag_array(self, tadv1: float):
         check(self.lib.les_press_stag_array(self._h, float(tadv1)))
 
+    def set_pressure_slabs(self, nslabs: int):
+        """Solve the pressure systems by the partition method over nslabs
+        z-slabs (the decomposed solve emulated on one GPU); 1 = single sweep."""
+        check(self.lib.les_set_pressure_slabs(self._h, int(nslabs)))
+
     def press_from_increment(self, tadv1: float, tadv2: float | None = None):
         """press_stag_array in increment form for the state les_ab2_advance
         left (see les_press_from_increment in lesgpu.h)."""

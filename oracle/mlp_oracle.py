@@ -102,15 +102,19 @@ def grad(p, x, t, bf16_ops=True):
     loss = float(np.mean(r * r))
     dy = 2.0 * r / n
     g2 = dy[:, None] * w3[None, :] * gelu_grad(z2)
-    g = np.zeros(NP)
-    g[O_W3:O_B3] = h2.T @ dy
-    g[O_B3] = dy.sum()
-    g[O_B2:O_W3] = g2.sum(0)
-    g[O_W2:O_B2] = (h1.T @ g2).ravel()
     g2e = bf16(g2.astype(np.float32)).astype(np.float64) if bf16_ops else g2
     d1 = (g2e @ W2e.T) * gelu_grad(z1)
-    g[O_B1:O_W2] = d1.sum(0)
-    g[O_W1:O_B1] = (x64.T @ d1).ravel()
+    # the weight gradients are a BF16 GEMM on the GPU (FP32 accumulation):
+    # g2, delta1, h2 and dy enter it rounded to BF16; db3 is an FP32 sum
+    rb = (lambda a: bf16(a.astype(np.float32)).astype(np.float64)) if bf16_ops else (lambda a: a)
+    d1e, h2e, dye = rb(d1), rb(h2), rb(dy)
+    g = np.zeros(NP)
+    g[O_W3:O_B3] = h2e.T @ dye
+    g[O_B3] = dy.sum()
+    g[O_B2:O_W3] = g2e.sum(0)
+    g[O_W2:O_B2] = (h1.T @ g2e).ravel()
+    g[O_B1:O_W2] = d1e.sum(0)
+    g[O_W1:O_B1] = (x64.T @ d1e).ravel()
     return g, loss
 
 
