@@ -336,6 +336,15 @@ int les_scalar_kappa(les_state* s, double* out, int n);
  * compute_RHS_adv (the call LES_engine.f90:565 leaves commented out).
  * fraction <= 0 turns it off. */
 int les_sponge_init(les_state* s, double layer_fraction);
+/* Optional upper bound on the dynamic SGS coefficient Cs^2 of the LASD update,
+ * the plane-averaged dynamic Smagorinsky model and the learned closure
+ * (0, the default, applies none: the reference has no upper clip,
+ * compute_LagScaleDep.f90:651-707).  A stabiliser for grids whose lid
+ * region is nearly laminar: there the Lagrangian averages' ratio
+ * F_LM/F_MM of tiny test-filtered strains can grow without bound and the
+ * explicit SGS diffusion then loses stability (seen at 512 x 512 x 256 from
+ * the synthetic initial field within ~100 steps). */
+int les_set_cs2_max(les_state* s, double cs2_max);
 /* Coriolis forcing of compute_RHS_adv (LES_engine.f90:553-561): rhs_x +=
  * coriol (v - v_g), rhs_y -= coriol (u - u_g); coriol = 0 turns it off. */
 int les_set_coriolis(les_state* s, double coriol, double ug, double vg);

@@ -96,6 +96,7 @@ PROTOTYPES = {
     "les_scalar_kappa": [_P, _D, _I],
     "les_sponge_init": [_P, C.c_double],
     "les_set_coriolis": [_P, C.c_double, C.c_double, C.c_double],
+    "les_set_cs2_max": [_P, C.c_double],
     "les_sync": [_P],
     "les_timers": [_P, _D],
     "les_profile": [_P, _I],

@@ -85,6 +85,7 @@ int les_set_precision(les_state* s, int precision) {
     if (old->scalar_on) n->scalar_init(old->SP);
     if (old->sponge_frac > 0.0) n->sponge_init(old->sponge_frac);
     n->coriol = old->coriol;
+    n->cs2_max = old->cs2_max;
     n->ug = old->ug;
     n->vg = old->vg;
     const int nz = p.nz;
@@ -335,6 +336,11 @@ int les_scalar_kappa(les_state* s, double* out, int n) {
 int les_sponge_init(les_state* s, double fraction) {
   STATE_OR_FAIL(s);
   return guard([&] { s->s->sponge_init(fraction); });
+}
+int les_set_cs2_max(les_state* s, double cs2_max) {
+  STATE_OR_FAIL(s);
+  if (!(cs2_max >= 0.0)) return bad_arg("cs2_max");
+  return guard([&] { s->s->cs2_max = cs2_max; });
 }
 int les_set_coriolis(les_state* s, double coriol, double ug, double vg) {
   STATE_OR_FAIL(s);

@@ -514,7 +514,7 @@ __device__ __forceinline__ double f32max_tiny(double x) {
 template <typename T>
 __global__ void k_lasd_update(T* FLM, T* FMM, T* FQN, T* FNN, const T* LM, const T* MM, const T* QN, const T* NN,
                               T* cs, T* beta, int init, long plane, int nz, double opftdelta, double lagran_dt,
-                              double beta_pow, const T* cs_init = nullptr, int nlev = -1) {
+                              double beta_pow, const T* cs_init = nullptr, int nlev = -1, double cs_max = 0.0) {
   const long n = (long)(nlev < 0 ? nz + 1 : nlev) * plane;  // levels 1..nlev
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const long o = plane + q;
@@ -568,7 +568,8 @@ __global__ void k_lasd_update(T* FLM, T* FMM, T* FQN, T* FNN, const T* LM, const
     b = double(fmaxf(float(b), 0.125f));
     if (top) b = 1.0;
     beta[o] = T(b);
-    cs[o] = T(f32max_tiny(c2 / b));
+    const double cv = f32max_tiny(c2 / b);
+    cs[o] = T(cs_max > 0.0 ? fmin(cv, cs_max) : cv);  // optional upper clip (off: the reference)
   }
 }
 

@@ -493,7 +493,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_infer(const MlpFeatIn<T> a, T* cs,
       float lc = lprev + S.stats[MLP_S_YMU] + S.stats[MLP_S_YSD] * y;
       lc = fminf(fmaxf(lc, S.stats[MLP_S_MU + 5] + S.stats[MLP_S_SD + 5] * S.stats[MLP_S_MIN + 5]),
                  S.stats[MLP_S_MU + 5] + S.stats[MLP_S_SD + 5] * S.stats[MLP_S_MAX + 5]);
-      cs[o] = T(fminf(fmaxf(expf(lc), 1e-24f), 1.0f));
+      cs[o] = T(fminf(fmaxf(expf(lc), 1e-24f), a.cs_max));
     }
     tc::fence_before_sync();
     __syncthreads();

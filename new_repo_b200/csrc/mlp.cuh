@@ -40,6 +40,7 @@ struct MlpFeatIn {
   // gradient Richardson number instead of the constant log(Delta/z0)
   const T* dtdz = nullptr;
   float beta = 0.0f;
+  float cs_max = 1.0f;  // upper clip of the coefficient
 };
 
 struct MlpDevice {

@@ -417,6 +417,7 @@ class Solver final : public SolverBase {
     a.dz = float(dz());
     a.delta = float(delta);
     a.log_delta_z0 = float(std::log(delta / P.z0));
+    a.cs_max = cs2_max > 0.0 ? float(std::min(cs2_max, 1.0)) : 1.0f;
     if (scalar_on && SP.buoyancy != 0.0) {
       a.dtdz = F[LES_DTDZ];
       a.beta = float(SP.buoyancy);
@@ -649,7 +650,7 @@ class Solver final : public SolverBase {
       KL("k_lasd_update", 14.0 * n1 * sizeof(T),
          k_lasd_update<T><<<grid_for(n1), 256, 0, st>>>(sc[0], sc[12], sc[13], sc[14], sc[7], sc[8], sc[9], sc[10],
                                                        sc[11], sc[1], 1, g.plane(), g.nz, 1.5 * delta,
-                                                       P.dt * double(P.cs_count), beta_pow, cs_prev));
+                                                       P.dt * double(P.cs_count), beta_pow, cs_prev, -1, cs2_max));
       std::vector<double> prof(g.L, 0.0);
       mlp_blend<T>(F[LES_CS_OPT2], sc[11], md, g.nz, check, derr, prof.data(), st);
       if (check) {
@@ -1697,7 +1698,7 @@ class Solver final : public SolverBase {
     KL("k_lasd_update", 14.0 * n1 * sizeof(T), k_lasd_update<T><<<grid_for(n1), 256, 0, st>>>(F[LES_F_LM], F[LES_F_MM], F[LES_F_QN], F[LES_F_NN], sc[7],
                                                   sc[8], sc[9], sc[10], F[LES_CS_OPT2], F[LES_BETA],
                                                   f_coeff_init ? 0 : 1, g.plane(), nz, 1.5 * delta,
-                                                  P.dt * double(P.cs_count), beta_pow, nullptr, nlev));
+                                                  P.dt * double(P.cs_count), beta_pow, nullptr, nlev, cs2_max));
     f_coeff_init = true;
     lagran_init = true;
     for (int q : {LES_U_LAG, LES_V_LAG, LES_W_LAG}) fill(F[q], 0, std::min(nlev, nz + 1), T(0));
@@ -2150,7 +2151,7 @@ void Solver<T>::wall_plain() {
 
 // plane-averaged dynamic Smagorinsky (compute_DynSmag.f90:61-245)
 template <typename T>
-__global__ void k_plane_ratio(const T* LM, const T* MM, T* cs, long plane, int nz) {
+__global__ void k_plane_ratio(const T* LM, const T* MM, T* cs, long plane, int nz, double cs_max) {
   // one block per level k = 1..nz+1; Neumaier sums in FP64
   const int k = blockIdx.x + 1;
   __shared__ double s[4][256];
@@ -2176,6 +2177,7 @@ __global__ void k_plane_ratio(const T* LM, const T* MM, T* cs, long plane, int n
     const double num = x.val() / double(plane), den = y.val() / double(plane);
     double c = (den != 0.0) ? num / den : 0.0;
     res = fmax(0.0, c);
+    if (cs_max > 0.0) res = fmin(res, cs_max);  // optional upper clip (off: the reference)
   }
   __syncthreads();
   for (long p = threadIdx.x; p < plane; p += blockDim.x) cs[(long)k * plane + p] = T(res);
@@ -2189,7 +2191,7 @@ void Solver<T>::dynsmag(SgsArgs<T>& a, int jt, int jtt) {
   }
   if (jt % P.cs_count != 0) return;
   dynamic_mum(a, false);
-  KL("k_plane_ratio", 3.0 * (g.nz + 1) * g.plane() * sizeof(T), k_plane_ratio<T><<<g.nz + 1, 256, 0, st>>>(sc[7], sc[8], F[LES_CS_OPT2], g.plane(), g.nz));
+  KL("k_plane_ratio", 3.0 * (g.nz + 1) * g.plane() * sizeof(T), k_plane_ratio<T><<<g.nz + 1, 256, 0, st>>>(sc[7], sc[8], F[LES_CS_OPT2], g.plane(), g.nz, cs2_max));
 }
 
 std::string SolverBase::profile_report() {

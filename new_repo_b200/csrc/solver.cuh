@@ -145,6 +145,7 @@ struct SolverBase : LaunchHook {
   bool scalar_on = false;
   les_scalar_params SP{};
   double sponge_frac = 0.0;
+  double cs2_max = 0.0;  // optional upper clip of the dynamic coefficients (0: none, the reference)
   double coriol = 0.0, ug = 0.0, vg = 0.0;
   virtual void scalar_init(const les_scalar_params& sp) = 0;
   virtual void scalar_set_initial(const double* theta) = 0;

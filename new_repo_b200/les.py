@@ -389,6 +389,10 @@ class LES:
         above layer_fraction * lz, applied at the end of compute_RHS_adv."""
         check(self.lib.les_sponge_init(self._h, float(layer_fraction)))
 
+    def set_cs2_max(self, cs2_max: float):
+        """Upper clip of the dynamic Cs^2 (0 = none, the reference's behaviour)."""
+        check(self.lib.les_set_cs2_max(self._h, float(cs2_max)))
+
     def set_coriolis(self, coriol: float, ug: float = 0.0, vg: float = 0.0):
         """Coriolis forcing of compute_RHS_adv (LES_engine.f90:553-561)."""
         check(self.lib.les_set_coriolis(self._h, float(coriol), float(ug), float(vg)))
