@@ -298,6 +298,22 @@ def test_mlp_training_gain_over_constant_coefficient(gpu):
     print(f"rms log error vs LASD: mlp {e_mlp:.3f}, best constant {e_mean:.3f}, cs0=0.16 {e_smag:.3f}; "
           f"val loss {val:.3f}")
     assert e_mlp < 0.8 * e_mean and e_mlp < e_smag
+    # time saved: the SGS update of a dynamic-update step (gradients given)
+    # with the closure against the LASD procedure, device time, same fields
+    def update_ms(model, reps=5):
+        les.set_sgs_model(model)
+        les.sgs_stress(les.jt, les.jt_total)  # warm
+        les.sync()
+        les.event_record(0)
+        for _ in range(reps):
+            les.sgs_stress(les.jt, les.jt_total)
+        les.event_record(1)
+        return les.event_elapsed(0, 1) / reps
+
+    t_lasd = update_ms("dyn_LagScaleDep")
+    t_mlp = update_ms("mlp")
+    print(f"SGS update at a dynamic step (64x64x32): LASD {t_lasd:.3f} ms, learned closure {t_mlp:.3f} ms")
+    assert t_mlp < t_lasd
     les.close()
 
 

@@ -121,36 +121,36 @@ def test_distributed_slabs_gloo(world):
 @pytest.mark.parametrize("G", [2, 4, 8])
 def test_pressure_slabs_match_single_sweep(gpu, G, precision):
     """les_set_pressure_slabs(G): press_stag_array with the partitioned
-    solve against the single sweep on the same state, and against the
-    oracle; FP64 1e-12, mixed (both paths FP32 fields) 1e-12 between the two
-    GPU solves and 1e-5 against the oracle."""
+    solve on the state an AB2 advance leaves (u* with its divergence), against
+    the single sweep and the oracle.  FP64: 1e-12 to both.  Mixed: the two
+    GPU solves differ only where the FP32 pressure spectrum rounds the
+    slightly different FP64 solutions apart (1e-6), 1e-5 against the oracle
+    on the same FP32-rounded inputs."""
     from new_repo_b200 import LES
     from tests.helpers import mirror, rel_err, run_params
+    from tests.test_production_plans import _advance, _round_f32
 
     p = O.Params(nx=32, ny=32, nz=64, dt=2e-4)
-    ops = O.Ops(p)
-    st = O.make_state(p, seed=4)
-    for _ in range(2):
-        O.les_step(ops, st)
+    ops, st = _advance(p)
+    gst = st.copy()
     if precision == "mixed":
-        for n in O.FIELDS + O.PLANES:
-            a = getattr(st, n)
-            a[...] = a.astype(np.float32).astype(np.float64)
+        _round_f32(gst)
     outs = {}
     for g in (1, G):
         les = LES(run_params(p), precision=precision)
-        mirror(les, st)
+        mirror(les, gst)
         les.set_pressure_slabs(g)
         les.press_stag_array(1.5)
         outs[g] = {n: les.download(n) for n in ("p", "dpdx", "dpdy", "dpdz")}
         assert les.status() == 0
         les.close()
-    O.press_stag_array(ops, st, 1.5)
+    ost = gst.copy()  # the oracle on the same (FP32-representable in mixed) inputs
+    O.press_stag_array(ops, ost, 1.5)
     for n in ("p", "dpdx", "dpdy", "dpdz"):
-        a, b, o = outs[G][n], outs[1][n], getattr(st, n)
+        a, b, o = outs[G][n], outs[1][n], getattr(ost, n)
         if n == "p":
             a, b, o = a[:-1], b[:-1], o[:-1]
-        assert rel_err(a, b) <= 1e-12, (G, precision, n, rel_err(a, b))
+        assert rel_err(a, b) <= (1e-12 if precision == "fp64" else 1e-6), (G, precision, n, rel_err(a, b))
         assert rel_err(a, o) <= (1e-12 if precision == "fp64" else 1e-5), (G, precision, n, rel_err(a, o))
 
 
