@@ -700,12 +700,12 @@ __global__ void k_p_finish(T* p, const double* pmean, long plane, int nz) {
 // inverse transforms run in FP32); its rows are opitch values apart
 // G (optional): a fourth spectrum added to the right-hand side of every
 // interior row (the divergence of u^n over dt tadv1 when Hx, Hy, Hz hold the
-// AB2 increment only).  pm (optional, with G): FP64 plane means per level
+// AB2 increment only; compiled in with INC).  pm (with G): FP64 plane means per level
 // (pm[f * pm_L + k]: f = 0 rz, 1 rfz, 2 dudx, 3 dvdy, 4 dwdz) from which
 // the kx = ky = 0 column forms its right-hand side,
 // (hz(k+1) - hz(k)) / dz + (dudx + dvdy + dwdz) idt with hz = rz + r21 rfz,
 // instead of the FP32 spectra's mean coefficients.
-template <typename T, typename O = T>
+template <typename T, typename O = T, bool INC = false>
 __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restrict__ Hy,
                           const cplx<T>* __restrict__ Hz, const cplx<T>* __restrict__ G,
                           const cplx<T>* __restrict__ bot,
@@ -756,7 +756,7 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
       ax[j] = (k <= nz) ? Hx[o] : cplx<T>{T(0), T(0)};
       ay[j] = (k <= nz) ? Hy[o] : cplx<T>{T(0), T(0)};
       az[j] = (k < nz) ? Hz[o + isp] : cplx<T>{T(0), T(0)};
-      agg[j] = (G && k <= nz) ? G[o] : cplx<T>{T(0), T(0)};
+      if constexpr (INC) agg[j] = (k <= nz) ? G[o] : cplx<T>{T(0), T(0)};
     }
   };
   load_fwd(1, cx, cy, cz, cg);
@@ -772,11 +772,11 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
         const double sx = kxv * double(hx.x) + kyv * double(hy.x);
         const double sy = kxv * double(hx.y) + kyv * double(hy.y);
         r = {-sy + (double(hzp.x) - double(hz.x)) / dz, sx + (double(hzp.y) - double(hz.y)) / dz};
-        if (G) {
+        if constexpr (INC) {
           r.x += double(cg[j].x);
           r.y += double(cg[j].y);
         }
-        if (pm && mean) {
+        if (INC && mean) {
           const double hk = pm[k] + pm_r21 * pm[pm_L + k];
           const double hkp = (k < nz) ? pm[k + 1] + pm_r21 * pm[pm_L + k + 1] : 0.0;
           r = {(hkp - hk) / dz + ((pm[2 * pm_L + k] + pm[3 * pm_L + k]) + pm[4 * pm_L + k]) * pm_idt, 0.0};
@@ -796,7 +796,7 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
       cx[j] = nx_[j];
       cy[j] = ny_[j];
       cz[j] = nz_[j];
-      cg[j] = ng_[j];
+      if constexpr (INC) cg[j] = ng_[j];
     }
   }
   {  // top row: -p(nz) + p(nz+1) = dz * top layer

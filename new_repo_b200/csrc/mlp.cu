@@ -64,7 +64,7 @@ __device__ __forceinline__ uint16_t bf16_bits(float x) {
 }
 
 // raw (transformed, not normalised) features at level k, offset o
-template <typename T>
+template <typename T, bool RI = true>
 __device__ __forceinline__ void raw_features(const MlpFeatIn<T>& a, long o, int k, float* t) {
   const long pl = a.plane;
   float ux, uy, uz, vx, vy, vz, wx, wy, wz;
@@ -114,7 +114,7 @@ __device__ __forceinline__ void raw_features(const MlpFeatIn<T>& a, long o, int 
   const float vs = s11 * w1 * w1 + s22 * w2 * w2 + s33 * w3 * w3 +
                    2.0f * (s12 * w1 * w2 + s13 * w1 * w3 + s23 * w2 * w3);
   t[6] = copysignf(log1pf(fabsf(vs)), vs);
-  if (a.dtdz) {
+  if (RI && a.dtdz) {
     // gradient Richardson number g/theta_0 (d theta/dz) / |d u_h/dz|^2 at this
     // node (level 1: the wall value of d theta/dz), signed log1p
     const float ri = a.beta * float(a.dtdz[o]) / (uz * uz + vz * vz + 1e-12f);
@@ -432,8 +432,10 @@ __device__ __forceinline__ void tc_teardown(S_t& S, uint32_t ncols, uint32_t pha
 }
 
 // ------------------------------------------------------------ inference ----
-template <typename T>
-__global__ void __launch_bounds__(TILE) k_mlp_infer(const MlpFeatIn<T> a, T* cs, MlpDevice m, unsigned* status) {
+// RI: buoyant runs (feature 7 = the gradient Richardson number); the
+// neutral variant is compiled without it (fewer registers, one more CTA per SM)
+template <typename T, bool RI>
+__global__ void __launch_bounds__(TILE, 5) k_mlp_infer(const MlpFeatIn<T> a, T* cs, MlpDevice m, unsigned* status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   InferSmem& S = *reinterpret_cast<InferSmem*>(smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023));
   load_images(S, m.img, m.params, m.stats);
@@ -456,7 +458,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_infer(const MlpFeatIn<T> a, T* cs,
       o = a.plane + q;
       const int k = int(o / a.plane);
       float t[8];
-      raw_features(a, o, k, t);
+      raw_features<T, RI>(a, o, k, t);
       int out = 0;  // bit i: feature i outside the training range (margin: 0.25 sd + 5 % of the range)
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
@@ -798,14 +800,17 @@ void mlp_infer(const MlpFeatIn<T>& in, T* cs, MlpDevice& m, unsigned* status, cu
   const long ntiles = (n + TILE - 1) / TILE;
   const int grid = int(std::min<long>(ntiles, 148L * 5));  // 5 CTAs per SM fit (registers)
   hook_before("k_mlp_infer", double(n) * 11 * sizeof(T));
-  k_mlp_infer<T><<<grid, TILE, infer_smem(), st>>>(in, cs, m, status);
+  if (in.dtdz) k_mlp_infer<T, true><<<grid, TILE, infer_smem(), st>>>(in, cs, m, status);
+  else k_mlp_infer<T, false><<<grid, TILE, infer_smem(), st>>>(in, cs, m, status);
   LES_CHECK_LAUNCH();
   hook_after();
 }
 
 void init_mlp_attributes() {
-  LES_CUDA(cudaFuncSetAttribute(k_mlp_infer<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem()));
-  LES_CUDA(cudaFuncSetAttribute(k_mlp_infer<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem()));
+  LES_CUDA(cudaFuncSetAttribute(k_mlp_infer<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem()));
+  LES_CUDA(cudaFuncSetAttribute(k_mlp_infer<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem()));
+  LES_CUDA(cudaFuncSetAttribute(k_mlp_infer<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem()));
+  LES_CUDA(cudaFuncSetAttribute(k_mlp_infer<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem()));
   LES_CUDA(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem()));
 }
 

@@ -1480,7 +1480,7 @@ class Solver final : public SolverBase {
                                             g.L, F[LES_DWDZ]));
     dim3 tg(ceil_div(g.lhx, 64), g.ny);
     KL("k_tridiag", (4.0 * 2 * sizeof(T) + 2 * sizeof(T) + 24.0) * double(g.L) * g.ny * g.lhx,
-       k_tridiag<T, T><<<tg, 64, 0, st>>>(spec[2], spec[3], spec[4], spec[5], bot, top, kkxd, kkyd, spec[0], xs, gam,
+       k_tridiag<T, T, true><<<tg, 64, 0, st>>>(spec[2], spec[3], spec[4], spec[5], bot, top, kkxd, kkyd, spec[0], xs, gam,
                                           mixed() ? pmean : nullptr, dstatus, g.lhx, g.ny, nz, dz(), mixed() ? 1 : 0,
                                           pitch(g.lhx), pitch(g.lhx), means, tadv2 / tadv1, 1.0 / (P.dt * tadv1),
                                           g.L));

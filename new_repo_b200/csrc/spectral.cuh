@@ -155,6 +155,25 @@ template <typename V, typename S>
 __device__ __forceinline__ V vld(const S* p, long o) {
   return VLd<V, S>::ld(p, o);
 }
+// the same through the read-only data path (ld.global.nc): for inputs that
+// no thread of the kernel writes; the compiler may then schedule these
+// loads across shared-memory stores
+template <typename V, typename S>
+__device__ __forceinline__ V vldg(const S* p, long o) {
+  if constexpr (std::is_same<V, V4<float>>::value && std::is_same<S, float>::value) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(p + o));
+    return {{q.x, q.y, q.z, q.w}};
+  } else if constexpr (std::is_same<V, V4<double>>::value && std::is_same<S, double>::value) {
+    const double2 q0 = __ldg(reinterpret_cast<const double2*>(p + o));
+    const double2 q1 = __ldg(reinterpret_cast<const double2*>(p + o + 2));
+    return {{q0.x, q0.y, q1.x, q1.y}};
+  } else if constexpr (std::is_same<V, V4<double>>::value && std::is_same<S, float>::value) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(p + o));
+    return {{double(q.x), double(q.y), double(q.z), double(q.w)}};
+  } else {
+    return V(__ldg(p + o));
+  }
+}
 template <typename T>
 __device__ __forceinline__ void vst(T* p, T x) {
   *p = x;
@@ -180,13 +199,13 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
   switch (a.op) {
     case XF_SCALE: {
       for (int f = 0; f < a.nf; ++f)
-        vst(v + f * vs, T(a.c0) * (a.in_f32 ? vld<V>(a.inf[f], off) : vld<V>(a.in[f], off)));
+        vst(v + f * vs, T(a.c0) * (a.in_f32 ? vldg<V>(a.inf[f], off) : vldg<V>(a.in[f], off)));
       break;
     }
     case XF_PRESS: {
       // compute_pressure.f90:138-140
       for (int f = 0; f < a.nf; ++f) {
-        const V x = a.in_f32 ? vld<V>(a.inf[f], off) : vld<V>(a.in[f], off);
+        const V x = a.in_f32 ? vldg<V>(a.inf[f], off) : vldg<V>(a.in[f], off);
         vst(v + f * vs, T(a.c0) * (x / T(a.c1)));
       }
       break;
@@ -194,9 +213,9 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
     case XF_CONV_IN: {
       // compute_convective_padd.f90:133-165
       const T c = T(a.c0);
-      vst(v + 0 * vs, -c * vld<V>(a.in[0], off));
-      vst(v + 1 * vs, -c * vld<V>(a.in[1], off));
-      vst(v + 2 * vs, -c * vld<V>(a.in[2], off));
+      vst(v + 0 * vs, -c * vldg<V>(a.in[0], off));
+      vst(v + 1 * vs, -c * vldg<V>(a.in[1], off));
+      vst(v + 2 * vs, -c * vldg<V>(a.in[2], off));
       const T* dwdy = a.in[3];
       const T* dvdz = a.in[4];
       const T* dudz = a.in[5];
@@ -208,13 +227,13 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
         vst(v + 4 * vs, vsplat<V>(T(0)));
       } else if (a.wall && l == 1) {
         const long up = off + a.in_pstride;
-        vst(v + 3 * vs, c * (T(0.5) * (vld<V>(dwdy, off) + vld<V>(dwdy, up)) - vld<V>(dvdz, off)));
-        vst(v + 4 * vs, c * (vld<V>(dudz, off) - T(0.5) * (vld<V>(dwdx, off) + vld<V>(dwdx, up))));
+        vst(v + 3 * vs, c * (T(0.5) * (vldg<V>(dwdy, off) + vldg<V>(dwdy, up)) - vldg<V>(dvdz, off)));
+        vst(v + 4 * vs, c * (vldg<V>(dudz, off) - T(0.5) * (vldg<V>(dwdx, off) + vldg<V>(dwdx, up))));
       } else {
-        vst(v + 3 * vs, c * (vld<V>(dwdy, off) - vld<V>(dvdz, off)));
-        vst(v + 4 * vs, c * (vld<V>(dudz, off) - vld<V>(dwdx, off)));
+        vst(v + 3 * vs, c * (vldg<V>(dwdy, off) - vldg<V>(dvdz, off)));
+        vst(v + 4 * vs, c * (vldg<V>(dudz, off) - vldg<V>(dwdx, off)));
       }
-      vst(v + 5 * vs, c * (vld<V>(dvdx, off) - vld<V>(dudy, off)));
+      vst(v + 5 * vs, c * (vldg<V>(dvdx, off) - vldg<V>(dudy, off)));
       break;
     }
     case XF_PROD: {
@@ -229,17 +248,17 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
       const T* o3 = a.in[5];
       const long up = off + a.in_pstride;
       const long dn = off - a.in_pstride;
-      const V vb0 = vld<V>(vb, off), o30 = vld<V>(o3, off), ub0 = vld<V>(ub, off);
-      const V wbu = vld<V>(wb, up), o2u = vld<V>(o2, up), o1u = vld<V>(o1, up);
+      const V vb0 = vldg<V>(vb, off), o30 = vldg<V>(o3, off), ub0 = vldg<V>(ub, off);
+      const V wbu = vldg<V>(wb, up), o2u = vldg<V>(o2, up), o1u = vldg<V>(o1, up);
       if (l == 1) {
         vst(v + 0 * vs, c * (-vb0 * o30 + T(0.5) * wbu * o2u));
         vst(v + 1 * vs, c * (ub0 * o30 + T(0.5) * wbu * (-o1u)));
         vst(v + 2 * vs, vsplat<V>(T(0)));
       } else {
-        const V wb0 = vld<V>(wb, off), o20 = vld<V>(o2, off), o10 = vld<V>(o1, off);
+        const V wb0 = vldg<V>(wb, off), o20 = vldg<V>(o2, off), o10 = vldg<V>(o1, off);
         vst(v + 0 * vs, c * (-vb0 * o30 + T(0.5) * (wbu * o2u + wb0 * o20)));
         vst(v + 1 * vs, c * (ub0 * o30 + T(0.5) * (wb0 * (-o10) + wbu * (-o1u))));
-        vst(v + 2 * vs, c * T(0.5) * ((ub0 + vld<V>(ub, dn)) * (-o20) + (vb0 + vld<V>(vb, dn)) * o10));
+        vst(v + 2 * vs, c * T(0.5) * ((ub0 + vldg<V>(ub, dn)) * (-o20) + (vb0 + vldg<V>(vb, dn)) * o10));
       }
       break;
     }
@@ -249,8 +268,8 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
       // tz (padded d theta/dz, w nodes): ub tx + vb ty + (wb tz at l, l+1)/2
       const T c = T(a.c0);
       const long up = off + a.in_pstride;
-      const V r = vld<V>(a.in[0], off) * vld<V>(a.in[3], off) + vld<V>(a.in[1], off) * vld<V>(a.in[4], off) +
-                  T(0.5) * (vld<V>(a.in[2], off) * vld<V>(a.in[5], off) + vld<V>(a.in[2], up) * vld<V>(a.in[5], up));
+      const V r = vldg<V>(a.in[0], off) * vldg<V>(a.in[3], off) + vldg<V>(a.in[1], off) * vldg<V>(a.in[4], off) +
+                  T(0.5) * (vldg<V>(a.in[2], off) * vldg<V>(a.in[5], off) + vldg<V>(a.in[2], up) * vldg<V>(a.in[5], up));
       vst(v, c * r);
       break;
     }
@@ -261,10 +280,10 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
       // over dt t1 as a fourth field; c0 = 1/(nx ny), c1 = t2/t1,
       // c2 = 1/(dt t1).  Nothing large cancels in any of the four.
       const T c = T(a.c0), r21 = T(a.c1), idt = T(a.c2);
-      vst(v + 0 * vs, c * (vld<V>(a.in[0], off) + r21 * vld<V>(a.in[3], off)));
-      vst(v + 1 * vs, c * (vld<V>(a.in[1], off) + r21 * vld<V>(a.in[4], off)));
-      vst(v + 2 * vs, c * (vld<V>(a.in[2], off) + r21 * vld<V>(a.in[5], off)));
-      vst(v + 3 * vs, (c * idt) * ((vld<V>(a.in[6], off) + vld<V>(a.in[7], off)) + vld<V>(a.in[8], off)));
+      vst(v + 0 * vs, c * (vldg<V>(a.in[0], off) + r21 * vldg<V>(a.in[3], off)));
+      vst(v + 1 * vs, c * (vldg<V>(a.in[1], off) + r21 * vldg<V>(a.in[4], off)));
+      vst(v + 2 * vs, c * (vldg<V>(a.in[2], off) + r21 * vldg<V>(a.in[5], off)));
+      vst(v + 3 * vs, (c * idt) * ((vldg<V>(a.in[6], off) + vldg<V>(a.in[7], off)) + vldg<V>(a.in[8], off)));
       break;
     }
     case XF_SCDYN: {
@@ -276,10 +295,10 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
       // d_j theta (3), |S| d_j theta (3).
       const long pl = a.in_pstride;
       auto at_w = [&](const T* f, long o) -> V {
-        return l == 1 ? vld<V>(f, o) : T(0.5) * (vld<V>(f, o) + vld<V>(f, o - pl));
+        return l == 1 ? vldg<V>(f, o) : T(0.5) * (vldg<V>(f, o) + vldg<V>(f, o - pl));
       };
       V uf = at_w(a.in[0], off), vf = at_w(a.in[1], off), tf = at_w(a.in[3], off);
-      V wf = l == 1 ? T(0.25) * vld<V>(a.in[2], off + pl) : vld<V>(a.in[2], off);
+      V wf = l == 1 ? T(0.25) * vldg<V>(a.in[2], off + pl) : vldg<V>(a.in[2], off);
       if (a.fluct) {
         // K_j = filt(u_j theta) - filt(u_j) filt(theta) does not change when
         // per-level constants are removed from u_j and theta (the filter
@@ -300,9 +319,9 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
       vst(v + 5 * vs, vf * tf);
       vst(v + 6 * vs, wf * tf);
 #pragma unroll
-      for (int q = 0; q < 6; ++q) vst(v + (7 + q) * vs, vld<V>(a.in[4 + q], off));
-      const V S = vld<V>(a.in[10], off);
-      const V tx = at_w(a.in[11], off), ty = at_w(a.in[12], off), tz = vld<V>(a.in[13], off);
+      for (int q = 0; q < 6; ++q) vst(v + (7 + q) * vs, vldg<V>(a.in[4 + q], off));
+      const V S = vldg<V>(a.in[10], off);
+      const V tx = at_w(a.in[11], off), ty = at_w(a.in[12], off), tz = vldg<V>(a.in[13], off);
       vst(v + 13 * vs, tx);
       vst(v + 14 * vs, ty);
       vst(v + 15 * vs, tz);
@@ -318,14 +337,14 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
       const T* w = a.in[2];
       V uf, vf, wf;
       if (l == 1) {
-        uf = vld<V>(u, off);
-        vf = vld<V>(vv, off);
-        wf = T(0.25) * vld<V>(w, off + a.in_pstride);
+        uf = vldg<V>(u, off);
+        vf = vldg<V>(vv, off);
+        wf = T(0.25) * vldg<V>(w, off + a.in_pstride);
       } else {
         const long dn = off - a.in_pstride;
-        uf = T(0.5) * (vld<V>(u, off) + vld<V>(u, dn));
-        vf = T(0.5) * (vld<V>(vv, off) + vld<V>(vv, dn));
-        wf = vld<V>(w, off);
+        uf = T(0.5) * (vldg<V>(u, off) + vldg<V>(u, dn));
+        vf = T(0.5) * (vldg<V>(vv, off) + vldg<V>(vv, dn));
+        wf = vldg<V>(w, off);
       }
       if (a.fluct) {
         // L_ij = filt(u_i u_j) - filt(u_i) filt(u_j) is unchanged when a
@@ -354,10 +373,10 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
       vst(v + 6 * vs, vf * vf);  // A22
       vst(v + 7 * vs, vf * wf);  // A23
       vst(v + 8 * vs, wf * wf);  // A33
-      const V S = vld<V>(a.in[9], off);
+      const V S = vldg<V>(a.in[9], off);
 #pragma unroll
       for (int q = 0; q < 6; ++q) {  // s11 s12 s13 s22 s23 s33
-        const V sq = vld<V>(a.in[3 + q], off);
+        const V sq = vldg<V>(a.in[3 + q], off);
         vst(v + (9 + q) * vs, sq);
         vst(v + (15 + q) * vs, S * sq);
       }
