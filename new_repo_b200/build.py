@@ -16,7 +16,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 BUILD = HERE.parent / "_build"
 LIB = HERE / "liblesgpu.so"
-SOURCES = ["spectral_inst.cu", "solver.cu", "capi.cu", "mlp.cu", "noalloc.cu"]
+SOURCES = ["spectral_inst.cu", "spectral_xfwd.cu", "spectral_xinv.cu", "spectral_ypass.cu", "solver.cu", "capi.cu", "mlp.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fno-strict-aliasing",
          "--expt-relaxed-constexpr", "-I", str(HERE.parent / "include")]

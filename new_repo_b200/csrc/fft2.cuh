@@ -88,6 +88,53 @@ template <typename T>
 __device__ __forceinline__ cplx<T> c_mulc(cplx<T> a, cplx<T> b) {
   return {a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y};
 }
+// a + s b for a real s
+template <typename T>
+__device__ __forceinline__ cplx<T> c_axpy(cplx<T> a, T s, cplx<T> b) { return {a.x + s * b.x, a.y + s * b.y}; }
+template <typename T>
+__device__ __forceinline__ cplx<T> c_scl(cplx<T> a, T s) { return {a.x * s, a.y * s}; }
+// componentwise a * s + b (s a pair of reals, e.g. the sign pattern (1, -1)
+// of a conjugate sum)
+template <typename T>
+__device__ __forceinline__ cplx<T> c_fma(cplx<T> a, cplx<T> s, cplx<T> b) {
+  return {a.x * s.x + b.x, a.y * s.y + b.y};
+}
+
+// FP32 complex adds on the packed FP32x2 instructions of sm_100: one
+// instruction for both components, with the rounding of the scalar add,
+// multiply or fused multiply-add per component (results are bit-identical
+// to the scalar forms).  Complex multiplies stay scalar: their packed form
+// needs the components of one operand duplicated and swapped, and the moves
+// that takes cost more than the packed multiply saves.
+__device__ __forceinline__ float2 f2_of(cplx<float> a) { return make_float2(a.x, a.y); }
+__device__ __forceinline__ cplx<float> c_of(float2 a) { return {a.x, a.y}; }
+__device__ __forceinline__ float2 f2_sub(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;"
+      : "=l"(r)
+      : "l"(*reinterpret_cast<unsigned long long*>(&a)), "l"(*reinterpret_cast<unsigned long long*>(&b)));
+  return *reinterpret_cast<float2*>(&r);
+}
+template <>
+__device__ __forceinline__ cplx<float> c_add<float>(cplx<float> a, cplx<float> b) {
+  return c_of(__fadd2_rn(f2_of(a), f2_of(b)));
+}
+template <>
+__device__ __forceinline__ cplx<float> c_sub<float>(cplx<float> a, cplx<float> b) {
+  return c_of(f2_sub(f2_of(a), f2_of(b)));
+}
+template <>
+__device__ __forceinline__ cplx<float> c_axpy<float>(cplx<float> a, float s, cplx<float> b) {
+  return c_of(__ffma2_rn(make_float2(s, s), f2_of(b), f2_of(a)));
+}
+template <>
+__device__ __forceinline__ cplx<float> c_scl<float>(cplx<float> a, float s) {
+  return c_of(__fmul2_rn(f2_of(a), make_float2(s, s)));
+}
+template <>
+__device__ __forceinline__ cplx<float> c_fma<float>(cplx<float> a, cplx<float> s, cplx<float> b) {
+  return c_of(__ffma2_rn(f2_of(a), f2_of(s), f2_of(b)));
+}
 
 // ------------------------------------------------------ register DFTs ----
 template <typename T, int R, bool INV>
@@ -102,8 +149,8 @@ struct RegDFT {
       const T s3 = T(0.86602540378443864676372317075294);  // sqrt(3)/2
       const cplx<T> a = v[0];
       const cplx<T> t1 = c_add(v[1], v[2]), t2 = c_sub(v[1], v[2]);
-      const cplx<T> m = {a.x - T(0.5) * t1.x, a.y - T(0.5) * t1.y};
-      const cplx<T> st = {s3 * t2.x, s3 * t2.y};
+      const cplx<T> m = c_axpy(a, T(-0.5), t1);
+      const cplx<T> st = c_scl(t2, s3);
       const cplx<T> ist = INV ? cplx<T>{-st.y, st.x} : cplx<T>{st.y, -st.x};
       v[0] = c_add(a, t1);
       v[1] = c_add(m, ist);
@@ -129,7 +176,14 @@ struct RegDFT {
         static_for<R2>([&](auto k2c) {
           constexpr int k2 = decltype(k2c)::value;
           constexpr int m = (n1 * k2) % R;
-          if constexpr (m != 0) {
+          if constexpr (4 * m == R) {
+            // W_R^(R/4) = -i (forward) or +i (inverse): a swap
+            t[k2] = INV ? cplx<T>{-t[k2].y, t[k2].x} : cplx<T>{t[k2].y, -t[k2].x};
+          } else if constexpr (2 * m == R) {
+            t[k2] = {-t[k2].x, -t[k2].y};
+          } else if constexpr (4 * m == 3 * R) {
+            t[k2] = INV ? cplx<T>{t[k2].y, -t[k2].x} : cplx<T>{-t[k2].y, t[k2].x};
+          } else if constexpr (m != 0) {
             constexpr CS w = TwCE<m, R>::v;
             const cplx<T> tw = {T(w.c), INV ? T(w.s) : T(-w.s)};
             t[k2] = c_mul(t[k2], tw);

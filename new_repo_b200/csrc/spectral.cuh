@@ -47,6 +47,28 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// r2c split of a length-2M real row transformed as M complex values Z:
+// X_k = (Z_k + conj Z_{M-k}) / 2 + W^k (Z_k - conj Z_{M-k}) / (2i), with
+// wh = W^k / 2 (W = exp(-2 pi i / 2M)).  The sums with the sign pairs are
+// packed FP32x2 instructions in single precision.
+template <typename T>
+__device__ __forceinline__ cplx<T> r2c_split(cplx<T> zk, cplx<T> zm, cplx<T> wh) {
+  const cplx<T> sp = c_fma(zm, cplx<T>{T(1), T(-1)}, zk);  // Z_k + conj Z_{M-k}
+  const cplx<T> dp = c_fma(zm, cplx<T>{T(-1), T(1)}, zk);  // Z_k - conj Z_{M-k}
+  const cplx<T> q = {dp.y * wh.x + dp.x * wh.y, dp.y * wh.y - dp.x * wh.x};  // dp wh / i
+  return c_fma(sp, cplx<T>{T(0.5), T(0.5)}, q);
+}
+// c2r split, the inverse of the above without the halving:
+// Z_m = (X_m + conj X_{M-m}) + i W^{-m} (X_m - conj X_{M-m}).
+template <typename T>
+__device__ __forceinline__ cplx<T> c2r_split(cplx<T> xk, cplx<T> xm, cplx<T> w) {
+  const cplx<T> s1 = c_fma(xm, cplx<T>{T(1), T(-1)}, xk);
+  const cplx<T> d1 = c_fma(xm, cplx<T>{T(-1), T(1)}, xk);
+  // t = d1 conj(w), held swapped as (t.y, t.x); Z = s1 + i t
+  const cplx<T> ts = {d1.y * w.x - d1.x * w.y, d1.x * w.x + d1.y * w.y};
+  return c_fma(ts, cplx<T>{T(-1), T(1)}, s1);
+}
+
 // ---------------------------------------------------------------- xfwd ----
 enum XFOp : int {
   XF_SCALE = 0,   // field f = c0 * in[f]
@@ -410,7 +432,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd(const XFAr
   T* refs = reinterpret_cast<T*>(buf + (long)npad * SL);  // R * nf per-row references
   int* rowl = reinterpret_cast<int*>(refs + a.R * a.nf);  // level of row r (-1: beyond the grid)
   int* rowj = rowl + a.R;
-  for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
+  for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = c_scl(a.tw[i], T(0.5));  // W^k / 2 for the split
   twm_build<T, M, false, 2>(a.tw, twm, threadIdx.x, blockDim.x);
   const long g0 = (long)blockIdx.x * a.R;
   for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
@@ -483,12 +505,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd(const XFAr
         const int j = rowj[r];
         cplx<T>* orow = a.out[f] + (long)l * a.out_pstride + (long)j * a.opitch;
         for (int k = lane_t; k < a.nk; k += TL) {
-          // X_k = E_k + W^k O_k, E = (Z_k + conj Z_{M-k})/2, O = (Z_k - conj Z_{M-k})/(2i)
-          const cplx<T> zk = seq[k == M ? 0 : k];
-          const cplx<T> zm = seq[(M - k) % M];
-          const cplx<T> e = {T(0.5) * (zk.x + zm.x), T(0.5) * (zk.y - zm.y)};
-          const cplx<T> o = {T(0.5) * (zk.y + zm.y), T(-0.5) * (zk.x - zm.x)};
-          orow[k] = c_add(e, c_mul(o, tw[k]));
+          orow[k] = r2c_split(seq[k == M ? 0 : k], seq[(M - k) % M], tw[k]);
         }
       }
     }
@@ -582,7 +599,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd_st(const X
   T* refs = reinterpret_cast<T*>(buf + (long)npad * SL);
   int* rowl = reinterpret_cast<int*>(refs + a.R * a.nf);
   int* rowj = rowl + a.R;
-  for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
+  for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = c_scl(a.tw[i], T(0.5));  // W^k / 2 for the split
   twm_build<T, M, false, 2>(a.tw, twm, threadIdx.x, blockDim.x);
   const long nitems = (a.nrows + a.R - 1) / a.R;
   if ((long)blockIdx.x < nitems) {
@@ -666,11 +683,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd_st(const X
           const int j = rowj[r];
           cplx<T>* orow = a.out[f] + (long)l * a.out_pstride + (long)j * a.opitch;
           for (int k = lane_t; k < a.nk; k += TL) {
-            const cplx<T> zk = seq[k == M ? 0 : k];
-            const cplx<T> zm = seq[(M - k) % M];
-            const cplx<T> e = {T(0.5) * (zk.x + zm.x), T(0.5) * (zk.y - zm.y)};
-            const cplx<T> o = {T(0.5) * (zk.y + zm.y), T(-0.5) * (zk.x - zm.x)};
-            orow[k] = c_add(e, c_mul(o, tw[k]));
+            orow[k] = r2c_split(seq[k == M ? 0 : k], seq[(M - k) % M], tw[k]);
           }
         }
       }
@@ -1191,10 +1204,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
             xk.y = T(0);
             xm.y = T(0);
           }
-          const cplx<T> s1 = {xk.x + xm.x, xk.y - xm.y};
-          const cplx<T> d1 = {xk.x - xm.x, xk.y + xm.y};
-          const cplx<T> t = c_mulc(d1, tw[m]);
-          z = {s1.x - t.y, s1.y + t.x};
+          z = c2r_split(xk, xm, tw[m]);
         }
         v[gg * RI + rr] = z;
       }
