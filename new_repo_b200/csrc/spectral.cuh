@@ -1187,48 +1187,82 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
     const int fs = a.nstage ? a.src[f] : f;
     const bool dxf = a.nstage && a.dx[f];
     const cplx<T>* row = valid ? stage + (long)(r * ns + fs) * a.nks : nullptr;  // the staged spectral row
+    // The per-sequence choices (d/dx, whether every mode below M is present)
+    // are made once here, not inside the unrolled element loop: with nk >= M
+    // the partner X_{M-m} exists for every element but m = 0, which only the
+    // first element of lane 0 can hold.
+    auto split = [&](auto dx_c, auto full_c) {
+      constexpr bool DX = decltype(dx_c)::value;
+      constexpr bool FULL = decltype(full_c)::value;
 #pragma unroll
-    for (int gg = 0; gg < E / RI; ++gg)
+      for (int gg = 0; gg < E / RI; ++gg)
 #pragma unroll
-      for (int rr = 0; rr < RI; ++rr) {
-        const int m = lane_t + TL * gg + rr * (M / RI);
-        cplx<T> z = {T(0), T(0)};
-        if (valid) {
-          cplx<T> xk = (m < a.nk) ? row[m] : cplx<T>{T(0), T(0)};
-          cplx<T> xm = (M - m < a.nk) ? row[M - m] : cplx<T>{T(0), T(0)};
-          if (dxf) {  // d/dx: i kx X (compute_derivatives.f90:94-137)
-            xk = (m < a.nk) ? ik_mul(kxs[m], xk) : xk;
-            xm = (M - m < a.nk) ? ik_mul(kxs[M - m], xm) : xm;
+        for (int rr = 0; rr < RI; ++rr) {
+          const int m = lane_t + TL * gg + rr * (M / RI);
+          const bool first = (gg == 0 && rr == 0);  // the only element that can hold m = 0
+          cplx<T> xk, xm;
+          if constexpr (FULL) {
+            xk = row[m];
+            xm = (first && m == 0 && a.nk == M) ? cplx<T>{T(0), T(0)} : row[M - m];
+          } else {
+            xk = (m < a.nk) ? row[m] : cplx<T>{T(0), T(0)};
+            xm = (M - m < a.nk) ? row[M - m] : cplx<T>{T(0), T(0)};
           }
-          if (m == 0) {
+          if constexpr (DX) {  // d/dx: i kx X (compute_derivatives.f90:94-137)
+            if constexpr (FULL) {
+              xk = ik_mul(kxs[m], xk);
+              if (!(first && m == 0 && a.nk == M)) xm = ik_mul(kxs[M - m], xm);
+            } else {
+              xk = (m < a.nk) ? ik_mul(kxs[m], xk) : xk;
+              xm = (M - m < a.nk) ? ik_mul(kxs[M - m], xm) : xm;
+            }
+          }
+          if (first && m == 0) {
             xk.y = T(0);
             xm.y = T(0);
           }
-          z = c2r_split(xk, xm, tw[m]);
+          v[gg * RI + rr] = c2r_split(xk, xm, tw[m]);
         }
-        v[gg * RI + rr] = z;
-      }
+    };
+    if (!valid) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) v[i] = cplx<T>{T(0), T(0)};
+    } else if (a.nk >= M) {
+      if (dxf) split(std::true_type{}, std::true_type{});
+      else split(std::false_type{}, std::true_type{});
+    } else {
+      if (dxf) split(std::true_type{}, std::false_type{});
+      else split(std::false_type{}, std::false_type{});
+    }
     reg_fft<T, M, true>(v, seq, lane_t, twm);
     if (direct) {
       if (valid && l >= a.lo[f] && l <= a.hi[f]) {
         const T ref = a.refin[f] ? a.refin[f][l] : T(0);
+        const cplx<T> ref2 = {ref, ref};
         const long off = (long)l * a.out_pstride + (long)j * NX;
+        // the store form is chosen once per sequence (outside the unrolled loop)
+        auto store = [&](auto form_c) {
+          constexpr int FORM = decltype(form_c)::value;
 #pragma unroll
-        for (int gg = 0; gg < E / RO; ++gg)
+          for (int gg = 0; gg < E / RO; ++gg)
 #pragma unroll
-          for (int rr = 0; rr < RO; ++rr) {
-            const int m = lane_t + TL * gg + rr * (M / RO);
-            const cplx<T> z = v[gg * RO + rr];
-            if (a.out_f32) {
-              *reinterpret_cast<float2*>(a.outf[f] + off + 2 * m) = make_float2(float(z.x + ref), float(z.y + ref));
-            } else if (a.pair_store) {
-              // one 8-byte (FP32) / 16-byte (FP64) store per output pair
-              *reinterpret_cast<cplx<T>*>(a.out[f] + off + 2 * m) = cplx<T>{z.x + ref, z.y + ref};
-            } else {
-              a.out[f][off + 2 * m] = z.x + ref;
-              a.out[f][off + 2 * m + 1] = z.y + ref;
+            for (int rr = 0; rr < RO; ++rr) {
+              const int m = lane_t + TL * gg + rr * (M / RO);
+              const cplx<T> z = c_add(v[gg * RO + rr], ref2);
+              if constexpr (FORM == 0) {
+                *reinterpret_cast<float2*>(a.outf[f] + off + 2 * m) = make_float2(float(z.x), float(z.y));
+              } else if constexpr (FORM == 1) {
+                // one 8-byte (FP32) / 16-byte (FP64) store per output pair
+                *reinterpret_cast<cplx<T>*>(a.out[f] + off + 2 * m) = z;
+              } else {
+                a.out[f][off + 2 * m] = z.x;
+                a.out[f][off + 2 * m + 1] = z.y;
+              }
             }
-          }
+        };
+        if (a.out_f32) store(std::integral_constant<int, 0>{});
+        else if (a.pair_store) store(std::integral_constant<int, 1>{});
+        else store(std::integral_constant<int, 2>{});
       }
     } else {
       __syncwarp();
