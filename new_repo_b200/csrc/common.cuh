@@ -39,12 +39,21 @@ __device__ __forceinline__ cplx<T> ik_mul(T k, cplx<T> a) {
   return {T(0) * a.x - k * a.y, T(0) * a.y + k * a.x};
 }
 
+// Quotient and remainder of non-negative offsets below 2^32 (every field and
+// fine-grid buffer of a supported grid; the state checks its sizes when it is
+// created) in 32-bit unsigned arithmetic: a 64-bit division is a long
+// software sequence on the GPU, and these sit in per-row and per-point paths.
+__device__ __forceinline__ int udiv32(long n, long d) { return int(unsigned(n) / unsigned(d)); }
+__device__ __forceinline__ int umod32(long n, long d) { return int(unsigned(n) % unsigned(d)); }
+
 // Device status bits (read back by les_get_status).
 enum StatusBits : unsigned {
   ST_NAN = 1u << 0,          // NaN in the velocity (LES_engine.f90:583-616)
   ST_PIVOT = 1u << 1,        // zero pivot in the tridiagonal solve (compute_pressure.f90:411-418)
   ST_MLP_RANGE = 1u << 2,    // learned closure saw inputs outside its training range
   ST_BAD_ARG = 1u << 3,      // kernel argument check failed
+  ST_MLP_WAIT = 1u << 4,     // a closure kernel's tensor-core wait ran out
+  ST_COPY_WAIT = 1u << 5,    // a spectral pass's bulk-copy wait ran out
 };
 
 struct CudaError : std::runtime_error {

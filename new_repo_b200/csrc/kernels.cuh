@@ -57,7 +57,7 @@ __global__ void k_ddz_vel(const T* u, const T* v, const T* w, T* dudz, T* dvdz, 
   if (plane % 4 == 0) {  // four consecutive points (one level) per thread, vector loads and stores
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n / 4; q += (long)gridDim.x * blockDim.x) {
       const long o = plane + 4 * q;
-      const int k = int(o / plane);
+      const int k = udiv32(o, plane);
       T a[4], b[4], r[4];
       ld4(u + o, a);
       ld4(u + o - plane, b);
@@ -84,7 +84,7 @@ __global__ void k_ddz_vel(const T* u, const T* v, const T* w, T* dudz, T* dvdz, 
   }
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const long o = plane + q;  // levels 1..nz+1
-    const int k = int(o / plane);
+    const int k = udiv32(o, plane);
     dudz[o] = rdz * (u[o] - u[o - plane]);
     dvdz[o] = rdz * (v[o] - v[o - plane]);
     dwdz[o] = (k <= nz) ? rdz * (w[o + plane] - w[o]) : T(0);
@@ -96,7 +96,7 @@ __global__ void k_ddz(T* out, const T* f, long plane, int nz, T rdz, int w_to_uv
   const long n = (long)(nz + 1) * plane;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const long o = plane + q;
-    const int k = int(o / plane);
+    const int k = udiv32(o, plane);
     if (w_to_uvp) out[o] = (k <= nz) ? rdz * (f[o + plane] - f[o]) : T(0);
     else out[o] = rdz * (f[o] - f[o - plane]);
   }
@@ -361,7 +361,7 @@ __global__ void k_sij(const SgsArgs<T> a) {
   const long n = (long)(a.nz + 1) * a.plane;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const long o = a.plane + q;
-    const int k = int(o / a.plane);
+    const int k = udiv32(o, a.plane);
     T s[6];
     sij_at(a, o, k, s);
 #pragma unroll
@@ -582,7 +582,7 @@ __global__ void k_ab2(T* u, T* v, T* w, const T* rx, const T* ry, const T* rz, c
   if (plane % 4 == 0) {  // four consecutive points (one level) per thread
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n / 4; q += (long)gridDim.x * blockDim.x) {
       const long o = 4 * q;
-      const int k = int(o / plane);
+      const int k = udiv32(o, plane);
       T x[4], r[4], f[4];
       if (k >= 1 && k <= nz) {
         T* fld[3] = {u, v, w};
@@ -606,7 +606,7 @@ __global__ void k_ab2(T* u, T* v, T* w, const T* rx, const T* ry, const T* rz, c
     return;
   }
   for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n; o += (long)gridDim.x * blockDim.x) {
-    const int k = int(o / plane);
+    const int k = udiv32(o, plane);
     if (k >= 1 && k <= nz) {
       u[o] = u[o] + dt * (t1 * rx[o] + t2 * fx[o]);
       v[o] = v[o] + dt * (t1 * ry[o] + t2 * fy[o]);
@@ -631,7 +631,7 @@ __global__ void k_projection(T* u, T* v, T* w, T* rx, T* ry, T* rz, const T* dpd
   if (plane % 4 == 0) {  // four consecutive points (one level) per thread
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n / 4; q += (long)gridDim.x * blockDim.x) {
       const long o = 4 * q;
-      const int k = int(o / plane);
+      const int k = udiv32(o, plane);
       T x[4], d[4], r[4];
       if (k >= 1 && k <= nz) {
         T* fld[3] = {u, v, w};
@@ -667,7 +667,7 @@ __global__ void k_projection(T* u, T* v, T* w, T* rx, T* ry, T* rz, const T* dpd
     return;
   }
   for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n; o += (long)gridDim.x * blockDim.x) {
-    const int k = int(o / plane);
+    const int k = udiv32(o, plane);
     if (k >= 1 && k <= nz) {
       const T dz_ = dpdz[o];
       u[o] = u[o] - dtt * dpdx[o];
@@ -687,7 +687,7 @@ template <typename T>
 __global__ void k_p_finish(T* p, const double* pmean, long plane, int nz) {
   const long n = (long)(nz + 2) * plane;
   for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n; o += (long)gridDim.x * blockDim.x) {
-    const int k = int(o / plane);
+    const int k = udiv32(o, plane);
     if (k == nz + 1) p[o] = T(BOGUS);
     else if (pmean) p[o] = T(double(p[o]) + pmean[k]);
   }
@@ -1105,7 +1105,7 @@ __global__ void k_forcing(T* rx, T* ry, T* rz, const T* u, const T* v, const T* 
   const long n = (long)nz * plane;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const long o = plane + q;
-    const int k = int(o / plane);
+    const int k = udiv32(o, plane);
     const T uo = u[o], vo = v[o];
     T x = rx[o], y = ry[o];
     if (f != T(0)) {
@@ -1130,7 +1130,7 @@ __global__ void k_buoyancy(T* rz, const T* th, const double* tmean, long plane, 
   const long n = (long)(nz - 1) * plane;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const long o = 2 * plane + q;
-    const int k = int(o / plane);
+    const int k = udiv32(o, plane);
     const T tw = T(0.5) * (th[o] + th[o - plane]);
     const T twm = T(0.5 * (tmean[k] + tmean[k - 1]));
     rz[o] = rz[o] + beta * (tw - twm);

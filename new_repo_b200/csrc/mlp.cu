@@ -159,7 +159,7 @@ __global__ void k_mlp_collect(const MlpFeatIn<T> a, const T* cs, MlpDevice m, in
   }
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const long o = a.plane + q;
-    const int k = int(o / a.plane);
+    const int k = udiv32(o, a.plane);
     float t[8];
     raw_features(a, o, k, t);  // every point: the range covers the whole state
 #pragma unroll
@@ -456,7 +456,7 @@ __global__ void __launch_bounds__(TILE, 5) k_mlp_infer(const MlpFeatIn<T> a, T* 
     long o = 0;
     if (valid) {
       o = a.plane + q;
-      const int k = int(o / a.plane);
+      const int k = udiv32(o, a.plane);
       float t[8];
       raw_features<T, RI>(a, o, k, t);
       int out = 0;  // bit i: feature i outside the training range (margin: 0.25 sd + 5 % of the range)
@@ -467,7 +467,7 @@ __global__ void __launch_bounds__(TILE, 5) k_mlp_infer(const MlpFeatIn<T> a, T* 
         const float margin = 0.25f + 0.05f * (mx - mn);
         if ((x[i] < mn - margin) || (x[i] > mx + margin)) out |= 1 << i;
       }
-      if (out && k > a.wall_levels) atomicOr(&m.colflag[q % a.plane], out);
+      if (out && k > a.wall_levels) atomicOr(&m.colflag[umod32(q, a.plane)], out);
       lprev = t[5];
     }
     put_features(S, threadIdx.x, x);

@@ -104,6 +104,9 @@ class Solver final : public SolverBase {
     if (!supported_length(p.nx) || !supported_length(p.ny) || !supported_length(g.nx2) ||
         !supported_length(g.ny2) || p.nz < 2)
       throw CudaError(1, "grid size not supported (nx, ny in {16,32,64,128,256,512}, nz >= 2)");
+    // the kernels index fields and the padded fine grid with 32-bit offsets
+    if ((long)(p.nz + 2) * g.nx2 * g.ny2 >= (1L << 32))
+      throw CudaError(1, "grid too large: (nz + 2) * (3 nx / 2) * (3 ny / 2) must stay below 2^32 points");
     LES_CUDA(cudaSetDevice(p.device));
     LES_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     for (auto& e : ev) LES_CUDA(cudaEventCreate(&e));
@@ -329,6 +332,7 @@ class Solver final : public SolverBase {
     a.in_pstride = (long)rows_pp * a.ipitch;
     a.out_pstride = (long)rows_pp * NX;
     a.tw = twiddles(NX);
+    a.status = dstatus;
     return a;
   }
 
@@ -1246,6 +1250,7 @@ class Solver final : public SolverBase {
     a.in_pstride = (long)g.ny * g.lhx;
     a.out_pstride = (long)g.ny * g.nx;
     a.tw = twiddles64(g.nx);
+    a.status = dstatus;
     return a;
   }
   template <typename S>

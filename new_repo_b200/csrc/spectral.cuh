@@ -24,6 +24,7 @@
 
 #include "common.cuh"
 #include "fft2.cuh"
+#include "tc05.cuh"
 
 namespace les {
 
@@ -45,6 +46,21 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// ---- bulk global -> shared copies (cp.async.bulk, completion on an mbarrier) ----
+// One instruction moves a whole contiguous row: both addresses 16-byte
+// aligned, the size a multiple of 16.  No multicast: the destination is this
+// CTA's shared memory only.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(tc::smem_u32(dst)), "l"(src), "r"(bytes), "r"(tc::smem_u32(mbar))
+               : "memory");
+}
+// the one arrival of a stage's mbarrier, announcing the bytes its copies bring
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(mbar)), "r"(bytes)
+               : "memory");
 }
 
 // r2c split of a length-2M real row transformed as M complex values Z:
@@ -437,16 +453,16 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd(const XFAr
   const long g0 = (long)blockIdx.x * a.R;
   for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
     const long g = g0 + r;
-    rowl[r] = (g < a.nrows) ? a.plane0 + int(g / a.rows_pp) : -1;
-    rowj[r] = (g < a.nrows) ? int(g % a.rows_pp) : 0;
+    rowl[r] = (g < a.nrows) ? a.plane0 + udiv32(g, a.rows_pp) : -1;
+    rowj[r] = (g < a.nrows) ? umod32(g, a.rows_pp) : 0;
   }
   __syncthreads();
   if (a.use_ref) {
     for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
       const long g = g0 + r;
       if (g >= a.nrows) continue;
-      const int l = a.plane0 + int(g / a.rows_pp);
-      const int j = int(g % a.rows_pp);
+      const int l = a.plane0 + udiv32(g, a.rows_pp);
+      const int j = umod32(g, a.rows_pp);
       xf_load<T, T>(a, l, 0, 0, refs + r * a.nf, 1);
       for (int f = 0; f < a.nf; ++f) {
         if (!a.refout[f]) refs[r * a.nf + f] = T(0);
@@ -498,7 +514,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd(const XFAr
       for (int r = 0; r < RO; ++r) seq[lane_t + TL * g + r * (M / RO)] = v[g * RO + r];
     __syncwarp();
     if (s < nseq) {
-      const int r = s / a.nf;
+      const int r = udiv32(s, a.nf);
       const int f = s - r * a.nf;
       const int l = rowl[r];
       if (l >= 0) {
@@ -558,14 +574,14 @@ __device__ __forceinline__ void xf_issue(const XFArgs<T>& a, long item, S* stage
   constexpr int PIECES = NX * int(sizeof(S)) / 16;
   const int nrow = a.R * a.nsrc;
   for (int s = warp; s < nrow; s += nwarps) {
-    const int r = s / a.nsrc;
+    const int r = udiv32(s, a.nsrc);
     const int q = s - r * a.nsrc;
     const long g = item * a.R + r;
-    const int l = a.plane0 + int(g / a.rows_pp);
+    const int l = a.plane0 + udiv32(g, a.rows_pp);
     const bool valid = g < a.nrows && (!a.scond[q] || (a.wall && l == 1));
     const S* base = reinterpret_cast<const S*>(std::is_same<S, T>::value ? (const void*)a.in[a.sf[q]]
                                                                           : (const void*)a.inf[a.sf[q]]);
-    const S* row = valid ? base + (long)(l + a.sdl[q]) * a.in_pstride + (g % a.rows_pp) * a.in_rstride : base;
+    const S* row = valid ? base + (long)(l + a.sdl[q]) * a.in_pstride + long(umod32(g, a.rows_pp)) * a.in_rstride : base;
     S* dst = stage + (long)s * NX;
     for (int k = lane; k < PIECES; k += 32)
       cp_async<16>(reinterpret_cast<unsigned char*>(dst) + 16 * k,
@@ -620,8 +636,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd_st(const X
     const long g0 = item * a.R;
     for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
       const long g = g0 + r;
-      rowl[r] = (g < a.nrows) ? a.plane0 + int(g / a.rows_pp) : -1;
-      rowj[r] = (g < a.nrows) ? int(g % a.rows_pp) : 0;
+      rowl[r] = (g < a.nrows) ? a.plane0 + udiv32(g, a.rows_pp) : -1;
+      rowj[r] = (g < a.nrows) ? umod32(g, a.rows_pp) : 0;
     }
     __syncthreads();
     if (a.use_ref) {  // per-level references: the (0,0) value of each field (from global)
@@ -676,7 +692,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd_st(const X
         for (int r = 0; r < RO; ++r) seq[lane_t + TL * g + r * (M / RO)] = v[g * RO + r];
       __syncwarp();
       if (s < nseq) {
-        const int r = s / a.nf;
+        const int r = udiv32(s, a.nf);
         const int f = s - r * a.nf;
         const int l = rowl[r];
         if (l >= 0) {
@@ -800,9 +816,9 @@ __device__ __forceinline__ cplx<T> yp_op_c(const YPArgs<T>& a, int q, int kx, in
 template <typename T, int NY>
 __device__ __forceinline__ void yp_issue(const YPArgs<T>& a, long item, int ncb, cplx<T>* bin) {
   const int C = a.C, SI = a.SI;
-  const int col0 = int(item % ncb) * C;
-  const int l = a.plane0 + int((item / ncb) % a.nplanes);
-  const int grp = int(item / ((long)ncb * a.nplanes));
+  const int col0 = umod32(item, ncb) * C;
+  const int l = a.plane0 + umod32(udiv32(item, ncb), a.nplanes);
+  const int grp = udiv32(item, (long)ncb * a.nplanes);
   // thread -> fixed column c, rows ky0, ky0 + kstep, ...: the addresses
   // advance by constant strides (blockDim.x is a multiple of C)
   const int c = threadIdx.x & (C - 1);
@@ -874,9 +890,9 @@ __global__ void __launch_bounds__((FWD && sizeof(T) == 8) ? 128 : 256,
     cp_async_wait<0>();
   }
   __syncthreads();
-  const int col0 = int(item % ncb) * C;
-  const int l = a.plane0 + int((item / ncb) % a.nplanes);
-  const int grp = int(item / ((long)ncb * a.nplanes));
+  const int col0 = umod32(item, ncb) * C;
+  const int l = a.plane0 + umod32(udiv32(item, ncb), a.nplanes);
+  const int grp = udiv32(item, (long)ncb * a.nplanes);
   const int c = threadIdx.x / TL;
   const int lt = threadIdx.x % TL;
   const int kx = col0 + c;
@@ -1085,6 +1101,10 @@ struct XIArgs {
   // set by the launcher: every output (and the plane stride) admits stores of
   // whole (x_2m, x_2m+1) pairs
   int pair_store;
+  // set by the launcher: stage the spectral rows with bulk copies (every
+  // input and stage row 16-byte aligned); else per-thread cp.async copies
+  int bulk;
+  unsigned* status;  // device status word (ST_COPY_WAIT), may be null
 };
 
 // x inverse pass: start the copies of the spectral rows of batch `item`
@@ -1103,9 +1123,56 @@ __device__ __forceinline__ void xi_issue(const XIArgs<T>& a, long item, cplx<T>*
     const bool valid = g < a.nrows;
     const cplx<T>* base = a.in[f];
     const cplx<T>* row =
-        valid ? base + (long)(a.plane0 + int(g / a.rows_pp)) * a.in_pstride + (g % a.rows_pp) * a.ipitch : base;
+        valid ? base + (long)(a.plane0 + udiv32(g, a.rows_pp)) * a.in_pstride + long(umod32(g, a.rows_pp)) * a.ipitch : base;
     cplx<T>* dst = stage + (long)s * a.nks;
     for (int m = lane; m < a.nk; m += 32) cp_async<int(sizeof(cplx<T>))>(dst + m, valid ? row + m : base, valid);
+  }
+}
+
+// the same with bulk copies, issued by warp 0: lane 0 announces the bytes
+// of every valid row's aligned part, then each lane copies whole rows; a
+// row whose addresses are not 16-byte aligned (none when the launcher set
+// a.bulk) and the last value of an odd FP32 row go by plain loads and stores
+// (visible after the barrier that follows the wait)
+template <typename T>
+__device__ __forceinline__ void xi_issue_bulk(const XIArgs<T>& a, long item, cplx<T>* stage, uint64_t* mbar) {
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
+  const int ns = a.nstage ? a.nstage : a.nin;
+  const long rows_left = a.nrows - item * a.R;
+  const int nvalid = int(rows_left < a.R ? rows_left : a.R);
+  const unsigned rb = unsigned(a.nk * sizeof(cplx<T>));
+  const unsigned rbulk = rb & ~15u;
+  auto aligned = [&](int s) {
+    const int r = udiv32(s, ns), f = s - r * ns;
+    const long g = item * a.R + r;
+    const cplx<T>* row = a.in[f] + (long)(a.plane0 + udiv32(g, a.rows_pp)) * a.in_pstride +
+                         long(umod32(g, a.rows_pp)) * a.ipitch;
+    const cplx<T>* dst = stage + (long)s * a.nks;
+    return ((reinterpret_cast<uintptr_t>(row) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0;
+  };
+  const int nrow = nvalid * ns;
+  unsigned mine = 0;
+  for (int s = lane; s < nrow; s += 32)
+    if (rbulk && aligned(s)) mine += rbulk;
+  for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+  // the barrier's one arrival carries every byte the copies below bring (an
+  // item always has a valid row, so the phase completes)
+  if (lane == 0) mbar_expect_tx(mbar, mine);
+  __syncwarp();
+  tc::fence_async_smem();  // earlier generic reads of this stage come first
+  for (int s = lane; s < nrow; s += 32) {
+    const int r = udiv32(s, ns), f = s - r * ns;
+    const long g = item * a.R + r;
+    const cplx<T>* row = a.in[f] + (long)(a.plane0 + udiv32(g, a.rows_pp)) * a.in_pstride +
+                         long(umod32(g, a.rows_pp)) * a.ipitch;
+    cplx<T>* dst = stage + (long)s * a.nks;
+    int m0 = 0;
+    if (rbulk && aligned(s)) {
+      bulk_g2s(dst, row, rbulk, mbar);
+      m0 = int(rbulk / sizeof(cplx<T>));
+    }
+    for (int m = m0; m < a.nk; ++m) dst[m] = row[m];
   }
 }
 
@@ -1134,23 +1201,44 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
   int* rowl = reinterpret_cast<int*>(buf + (a.merged ? 0L : (long)npad * SL));  // level of row r (-1: beyond the grid)
   int* rowj = rowl + a.R;
   T* kxs = reinterpret_cast<T*>(rowj + a.R);          // x wavenumbers (nstage > 0)
+  // one mbarrier per input stage (bulk staging)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(
+      (reinterpret_cast<uintptr_t>(kxs + (a.nstage ? a.nk + 2 : 0)) + 7) & ~uintptr_t(7));
   for (int i = threadIdx.x; i < NX; i += blockDim.x) tw[i] = a.tw[i];
   twm_build<T, M, true, 2>(a.tw, twm, threadIdx.x, blockDim.x);
   if (a.nstage)
     for (int i = threadIdx.x; i < a.nk; i += blockDim.x) kxs[i] = a.kxr[i];
+  if (a.bulk) {
+    if (threadIdx.x == 0) {
+      tc::mbar_init(&bars[0], 1);
+      tc::mbar_init(&bars[1], 1);
+      tc::fence_mbar_init();
+    }
+    __syncthreads();
+  }
+  unsigned phase = 0;  // bit b: parity of the next completion of bars[b]
   // persistent CTAs over batches of R rows; with two stages the spectral
   // rows of the next batch are copied into the other stage while this one
   // is transformed, with one stage after this batch's last read of it
   const long nitems = (a.nrows + a.R - 1) / a.R;
   if ((long)blockIdx.x < nitems) {
-    xi_issue<T>(a, blockIdx.x, stage0);
-    cp_async_commit();
+    if (a.bulk) {
+      xi_issue_bulk<T>(a, blockIdx.x, stage0, &bars[0]);
+    } else {
+      xi_issue<T>(a, blockIdx.x, stage0);
+      cp_async_commit();
+    }
   }
   int stg = 0;
   for (long item = blockIdx.x; item < nitems; item += gridDim.x) {
   const long next = item + gridDim.x;
   const cplx<T>* stage = stg ? stage1 : stage0;
-  if (a.nbuf > 1 && next < nitems) {
+  bool late = false;  // this thread's wait for the item's rows ran out
+  if (a.bulk) {
+    if (a.nbuf > 1 && next < nitems) xi_issue_bulk<T>(a, next, stg ? stage0 : stage1, &bars[stg ^ 1]);
+    late = !tc::mbar_wait(&bars[stg], (phase >> stg) & 1u);
+    phase ^= 1u << stg;
+  } else if (a.nbuf > 1 && next < nitems) {
     xi_issue<T>(a, next, stg ? stage0 : stage1);
     cp_async_commit();
     cp_async_wait<1>();
@@ -1160,10 +1248,18 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
   const long g0 = item * a.R;
   for (int r = threadIdx.x; r < a.R; r += blockDim.x) {
     const long g = g0 + r;
-    rowl[r] = (g < a.nrows) ? a.plane0 + int(g / a.rows_pp) : -1;
-    rowj[r] = (g < a.nrows) ? int(g % a.rows_pp) : 0;
+    rowl[r] = (g < a.nrows) ? a.plane0 + udiv32(g, a.rows_pp) : -1;
+    rowj[r] = (g < a.nrows) ? umod32(g, a.rows_pp) : 0;
   }
-  __syncthreads();
+  if (__syncthreads_or(late)) {
+    // the copies did not complete within the limit: record it, give the
+    // copies in flight a last bounded wait (they write this CTA's shared
+    // memory) and leave, every thread of the CTA together
+    if (threadIdx.x == 0 && a.status) atomicOr(a.status, unsigned(ST_COPY_WAIT));
+    tc::mbar_wait(&bars[stg], (phase >> stg) & 1u ^ 1u);
+    if (a.nbuf > 1 && next < nitems) tc::mbar_wait(&bars[stg ^ 1], (phase >> (stg ^ 1)) & 1u);
+    return;
+  }
   // a plain store writes straight from registers; the other ops combine
   // fields per point through shared memory
   const bool direct = (a.op == XI_STORE);
@@ -1171,7 +1267,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
   for (int base = 0; base < npad; base += blockDim.x / TL) {
     const int s = base + threadIdx.x / TL;
     if (base + (threadIdx.x / 32) * (32 / TL) >= npad) break;  // whole warp beyond the slots
-    const int r = s / a.nin;
+    const int r = udiv32(s, a.nin);
     const int f = s - r * a.nin;
     const bool valid = (s < nseq) && (rowl[r < a.R ? r : 0] >= 0);
     int l = 0, j = 0;
@@ -1224,7 +1320,31 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
           v[gg * RI + rr] = c2r_split(xk, xm, tw[m]);
         }
     };
-    if (!valid) {
+    if constexpr (sizeof(T) == 8) {
+      // FP64: one generic loop (the specialised copies cost the double
+      // precision kernels register spills at their 128-register budget)
+#pragma unroll
+      for (int gg = 0; gg < E / RI; ++gg)
+#pragma unroll
+        for (int rr = 0; rr < RI; ++rr) {
+          const int m = lane_t + TL * gg + rr * (M / RI);
+          cplx<T> z = {T(0), T(0)};
+          if (valid) {
+            cplx<T> xk = (m < a.nk) ? row[m] : cplx<T>{T(0), T(0)};
+            cplx<T> xm = (M - m < a.nk) ? row[M - m] : cplx<T>{T(0), T(0)};
+            if (dxf) {  // d/dx: i kx X (compute_derivatives.f90:94-137)
+              xk = (m < a.nk) ? ik_mul(kxs[m], xk) : xk;
+              xm = (M - m < a.nk) ? ik_mul(kxs[M - m], xm) : xm;
+            }
+            if (m == 0) {
+              xk.y = T(0);
+              xm.y = T(0);
+            }
+            z = c2r_split(xk, xm, tw[m]);
+          }
+          v[gg * RI + rr] = z;
+        }
+    } else if (!valid) {
 #pragma unroll
       for (int i = 0; i < E; ++i) v[i] = cplx<T>{T(0), T(0)};
     } else if (a.nk >= M) {
@@ -1405,8 +1525,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIAr
     stg ^= 1;
   } else if (next < nitems) {
     // single stage: every thread is past the last read of it (barrier above)
-    xi_issue<T>(a, next, stage0);
-    cp_async_commit();
+    if (a.bulk) {
+      xi_issue_bulk<T>(a, next, stage0, &bars[0]);
+    } else {
+      xi_issue<T>(a, next, stage0);
+      cp_async_commit();
+    }
   }
   }
 }

@@ -32,10 +32,21 @@ void launch_xinv(int NX, XIArgs<T> a, cudaStream_t st) {
   a.merged = (a.op == XI_STORE && a.nstage == 0) ? 1 : 0;
   if (a.merged) a.nks = std::max(a.nks, SL);
   auto stage_rows = [&](int R) { return a.merged ? pad_seqs(R * a.nin, M) : R * ns; };
+  // bulk staging: one cp.async.bulk per staged row needs 16-byte aligned
+  // rows in global memory (pitch and plane stride) and in the stages (stage
+  // base and row stride); the kernel checks every row's addresses again and
+  // copies a row that fails with plain loads
+  {
+    const size_t cs = sizeof(cplx<T>);
+    a.bulk = ((cs * a.ipitch) % 16 == 0 && (cs * a.in_pstride) % 16 == 0 && (cs * a.nks) % 16 == 0 &&
+              (cs * (NX + twm_len(M, true))) % 16 == 0 && a.nk * cs >= 16)
+                 ? 1
+                 : 0;
+  }
   auto smem_nb = [&](int R, int nb) {
     return sizeof(cplx<T>) * (NX + twm_len(M, true) + nb * (((size_t)stage_rows(R) * a.nks + 1) & ~size_t(1)) +
                               (a.merged ? 0 : (size_t)pad_seqs(R * a.nin, M) * SL)) +
-           2 * sizeof(int) * R + (a.nstage ? sizeof(T) * (a.nk + 2) : 0);
+           2 * sizeof(int) * R + (a.nstage ? sizeof(T) * (a.nk + 2) : 0) + (a.bulk ? 2 * sizeof(uint64_t) + 8 : 0);
   };
   void (*kern)(XIArgs<T>) = nullptr;
   switch (NX) {

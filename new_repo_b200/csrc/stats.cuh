@@ -232,7 +232,7 @@ __global__ void k_tke_cpress(const T* __restrict__ p, const T* __restrict__ u, c
                              const T* __restrict__ w, const T* __restrict__ cs, T* __restrict__ c, long plane, int nz) {
   const long n = (long)(nz + 2) * plane;
   for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n; o += (long)gridDim.x * blockDim.x) {
-    const long k = o / plane;
+    const long k = udiv32(o, plane);
     if (k == 0) {
       c[o] = cs[o + plane];
     } else if (k == nz + 1) {
