@@ -196,7 +196,11 @@ int les_step(les_state* s, int jt, int jt_total);
 /* running_diagnostics.f90:80-136 of the last step: cfl, mke, u_star, rms div u
  * (FP64, compensated sums). */
 int les_diagnostics(les_state* s, double out[4]);
-/* Sticky device status bits (NaN seen, zero pivot, ...); cleared on read. */
+/* Sticky device status bits, cleared on read: 1 NaN in the velocity, 2 zero
+ * pivot in the tridiagonal solve, 4 closure inputs outside the training range,
+ * 8 kernel argument check failed, 16 a closure kernel's tensor-core wait ran
+ * out, 32 a spectral pass's bulk-copy wait ran out (the pass left its CTA's
+ * work undone). */
 int les_get_status(les_state* s, unsigned* bits);
 /* The reference's numerical aborts as a status: check_NaN(jt)
  * (LES_engine.f90:583-616, called every NaN_check steps, :363-365) and the

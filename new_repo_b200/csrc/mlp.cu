@@ -53,6 +53,16 @@ __device__ __forceinline__ float gelu(float x) {
   const float hx = 0.5f * x;
   return fmaf(hx, t, hx);
 }
+// the same on a pair of values with the packed FP32x2 instructions of sm_100
+// (per component the rounding of the scalar form: results are bit-identical)
+__device__ __forceinline__ float2 gelu2(float2 x) {
+  const float2 x2 = __fmul2_rn(x, x);
+  const float2 p = __ffma2_rn(make_float2(GELU_C0 * GELU_C1, GELU_C0 * GELU_C1), x2, make_float2(GELU_C0, GELU_C0));
+  const float2 u = __fmul2_rn(x, p);
+  const float2 t = make_float2(tanh_fast(u.x), tanh_fast(u.y));
+  const float2 hx = __fmul2_rn(make_float2(0.5f, 0.5f), x);
+  return __ffma2_rn(hx, t, hx);
+}
 __device__ __forceinline__ float gelu_grad(float x) {
   const float t = tanh_fast(GELU_C0 * fmaf(GELU_C1 * x, x * x, x));
   return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * GELU_C0 * fmaf(3.0f * GELU_C1, x * x, 1.0f);
@@ -475,19 +485,43 @@ __global__ void __launch_bounds__(TILE, 5) k_mlp_infer(const MlpFeatIn<T> a, T* 
     tc::fence_before_sync();
     __syncthreads();
     if (!tc_stage(S, phase, status, 0, 0)) break;
-    float h[64];
-    tmem_row64(S.tmem, 0, h);
+    // bias and GELU two values at a time (packed FP32x2; the epilogues are
+    // issue bound), 16 TMEM columns at a time (fewer live registers)
+    const uint32_t tlane = uint32_t((threadIdx.x / 32) * 32) << 16;
 #pragma unroll
-    for (int i = 0; i < 64; ++i) h[i] = gelu(h[i] + S.b1[i]);
-    put_row64(S.A2, threadIdx.x, h);
+    for (int c = 0; c < 4; ++c) {
+      float h[16];
+      tc::tmem_ld16(S.tmem + tlane + uint32_t(16 * c), h);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 16; i += 2) {
+        const float2 z = gelu2(
+            __fadd2_rn(make_float2(h[i], h[i + 1]), make_float2(S.b1[16 * c + i], S.b1[16 * c + i + 1])));
+        h[i] = z.x;
+        h[i + 1] = z.y;
+      }
+      put16(S.A2, threadIdx.x, c, h);
+    }
     tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     if (!tc_stage(S, phase, status, 1, 0)) break;
-    tmem_row64(S.tmem, 0, h);
-    float y = S.b3;
+    // output layer: even and odd hidden units summed in the two lanes of a
+    // packed accumulator, then added
+    float2 y2 = make_float2(S.b3, 0.0f);
 #pragma unroll
-    for (int i = 0; i < 64; ++i) y += S.w3[i] * gelu(h[i] + S.b2[i]);
+    for (int c = 0; c < 4; ++c) {
+      float h[16];
+      tc::tmem_ld16(S.tmem + tlane + uint32_t(16 * c), h);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 16; i += 2) {
+        const int k = 16 * c + i;
+        const float2 g = gelu2(__fadd2_rn(make_float2(h[i], h[i + 1]), make_float2(S.b2[k], S.b2[k + 1])));
+        y2 = __ffma2_rn(make_float2(S.w3[k], S.w3[k + 1]), g, y2);
+      }
+    }
+    float y = y2.x + y2.y;
     if (valid) {
       // no extrapolation: the change is clamped to the trained range, the
       // coefficient to the range of the previous coefficients seen in training

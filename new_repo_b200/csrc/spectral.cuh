@@ -85,6 +85,24 @@ __device__ __forceinline__ cplx<T> c2r_split(cplx<T> xk, cplx<T> xm, cplx<T> w) 
   return c_fma(ts, cplx<T>{T(-1), T(1)}, s1);
 }
 
+// r2c split and store of the first nk modes of a sequence whose FFT output
+// Z sits in natural order in its slot: lane t writes modes k = t + TL i
+// (i <= E: mode M, the Nyquist bin, falls on lane 0 at i = E), an unrolled
+// loop with compile-time offsets; Z_M is Z_0 and the partner of mode 0 is
+// Z_0 itself
+template <typename T, int M, int TL, int E>
+__device__ __forceinline__ void xf_split_store(const cplx<T>* seq, const cplx<T>* tw, cplx<T>* orow, int t, int nk) {
+#pragma unroll
+  for (int i = 0; i <= E; ++i) {
+    const int k = t + TL * i;
+    if (k < nk) {
+      if (i == 0) orow[k] = r2c_split(seq[k], seq[k == 0 ? 0 : M - k], tw[k]);
+      else if (i < E) orow[k] = r2c_split(seq[k], seq[M - k], tw[k]);
+      else orow[k] = r2c_split(seq[0], seq[0], tw[M]);  // k = M (t = 0)
+    }
+  }
+}
+
 // ---------------------------------------------------------------- xfwd ----
 enum XFOp : int {
   XF_SCALE = 0,   // field f = c0 * in[f]
@@ -229,31 +247,34 @@ __device__ __forceinline__ V vsplat(T x) {
   else return V{{x, x, x, x}};
 }
 
-// Values of every field at level l, row j, columns i (one point for V = T,
-// four for V = V4<T>; i a multiple of 4 then), stored at v + f * vs.
-template <typename T, typename V>
-__device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i, T* v, int vs) {
+// Values of every field of op OP at level l, row j, columns i (one point for
+// V = T, four for V = V4<T>; i a multiple of 4 then), stored at v + f * vs,
+// minus sub[f] when SUB (the per-level references of the mixed-precision
+// transforms).  The op is a template parameter so that a pass's load loop
+// is compiled per op, with no dispatch per point.
+template <typename T, typename V, int OP, bool SUB>
+__device__ __forceinline__ void xf_load_op(const XFArgs<T>& a, int l, int j, int i, T* v, int vs, const T* sub) {
   const long off = (long)l * a.in_pstride + (long)j * a.in_rstride + i;
-  switch (a.op) {
-    case XF_SCALE: {
+  auto put = [&](int f, const V& x) {
+    if constexpr (SUB) vst(v + f * vs, x - vsplat<V>(sub[f]));
+    else vst(v + f * vs, x);
+  };
+  {
+    if constexpr (OP == XF_SCALE) {
       for (int f = 0; f < a.nf; ++f)
-        vst(v + f * vs, T(a.c0) * (a.in_f32 ? vldg<V>(a.inf[f], off) : vldg<V>(a.in[f], off)));
-      break;
-    }
-    case XF_PRESS: {
+        put(f, T(a.c0) * (a.in_f32 ? vldg<V>(a.inf[f], off) : vldg<V>(a.in[f], off)));
+    } else if constexpr (OP == XF_PRESS) {
       // compute_pressure.f90:138-140
       for (int f = 0; f < a.nf; ++f) {
         const V x = a.in_f32 ? vldg<V>(a.inf[f], off) : vldg<V>(a.in[f], off);
-        vst(v + f * vs, T(a.c0) * (x / T(a.c1)));
+        put(f, T(a.c0) * (x / T(a.c1)));
       }
-      break;
-    }
-    case XF_CONV_IN: {
+    } else if constexpr (OP == XF_CONV_IN) {
       // compute_convective_padd.f90:133-165
       const T c = T(a.c0);
-      vst(v + 0 * vs, -c * vldg<V>(a.in[0], off));
-      vst(v + 1 * vs, -c * vldg<V>(a.in[1], off));
-      vst(v + 2 * vs, -c * vldg<V>(a.in[2], off));
+      put(0, -c * vldg<V>(a.in[0], off));
+      put(1, -c * vldg<V>(a.in[1], off));
+      put(2, -c * vldg<V>(a.in[2], off));
       const T* dwdy = a.in[3];
       const T* dvdz = a.in[4];
       const T* dudz = a.in[5];
@@ -261,20 +282,18 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
       const T* dvdx = a.in[7];
       const T* dudy = a.in[8];
       if (a.wall && l == 0) {
-        vst(v + 3 * vs, vsplat<V>(T(0)));
-        vst(v + 4 * vs, vsplat<V>(T(0)));
+        put(3, vsplat<V>(T(0)));
+        put(4, vsplat<V>(T(0)));
       } else if (a.wall && l == 1) {
         const long up = off + a.in_pstride;
-        vst(v + 3 * vs, c * (T(0.5) * (vldg<V>(dwdy, off) + vldg<V>(dwdy, up)) - vldg<V>(dvdz, off)));
-        vst(v + 4 * vs, c * (vldg<V>(dudz, off) - T(0.5) * (vldg<V>(dwdx, off) + vldg<V>(dwdx, up))));
+        put(3, c * (T(0.5) * (vldg<V>(dwdy, off) + vldg<V>(dwdy, up)) - vldg<V>(dvdz, off)));
+        put(4, c * (vldg<V>(dudz, off) - T(0.5) * (vldg<V>(dwdx, off) + vldg<V>(dwdx, up))));
       } else {
-        vst(v + 3 * vs, c * (vldg<V>(dwdy, off) - vldg<V>(dvdz, off)));
-        vst(v + 4 * vs, c * (vldg<V>(dudz, off) - vldg<V>(dwdx, off)));
+        put(3, c * (vldg<V>(dwdy, off) - vldg<V>(dvdz, off)));
+        put(4, c * (vldg<V>(dudz, off) - vldg<V>(dwdx, off)));
       }
-      vst(v + 5 * vs, c * (vldg<V>(dvdx, off) - vldg<V>(dudy, off)));
-      break;
-    }
-    case XF_PROD: {
+      put(5, c * (vldg<V>(dvdx, off) - vldg<V>(dudy, off)));
+    } else if constexpr (OP == XF_PROD) {
       // compute_convective_padd.f90:180-249 on the fine grid; inputs are
       // ub, vb, wb, o1, o2, o3 (padded -c*u, -c*v, -c*w and vorticity).
       const T c = T(a.c0);
@@ -289,18 +308,16 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
       const V vb0 = vldg<V>(vb, off), o30 = vldg<V>(o3, off), ub0 = vldg<V>(ub, off);
       const V wbu = vldg<V>(wb, up), o2u = vldg<V>(o2, up), o1u = vldg<V>(o1, up);
       if (l == 1) {
-        vst(v + 0 * vs, c * (-vb0 * o30 + T(0.5) * wbu * o2u));
-        vst(v + 1 * vs, c * (ub0 * o30 + T(0.5) * wbu * (-o1u)));
-        vst(v + 2 * vs, vsplat<V>(T(0)));
+        put(0, c * (-vb0 * o30 + T(0.5) * wbu * o2u));
+        put(1, c * (ub0 * o30 + T(0.5) * wbu * (-o1u)));
+        put(2, vsplat<V>(T(0)));
       } else {
         const V wb0 = vldg<V>(wb, off), o20 = vldg<V>(o2, off), o10 = vldg<V>(o1, off);
-        vst(v + 0 * vs, c * (-vb0 * o30 + T(0.5) * (wbu * o2u + wb0 * o20)));
-        vst(v + 1 * vs, c * (ub0 * o30 + T(0.5) * (wb0 * (-o10) + wbu * (-o1u))));
-        vst(v + 2 * vs, c * T(0.5) * ((ub0 + vldg<V>(ub, dn)) * (-o20) + (vb0 + vldg<V>(vb, dn)) * o10));
+        put(0, c * (-vb0 * o30 + T(0.5) * (wbu * o2u + wb0 * o20)));
+        put(1, c * (ub0 * o30 + T(0.5) * (wb0 * (-o10) + wbu * (-o1u))));
+        put(2, c * T(0.5) * ((ub0 + vldg<V>(ub, dn)) * (-o20) + (vb0 + vldg<V>(vb, dn)) * o10));
       }
-      break;
-    }
-    case XF_PROD_SC: {
+    } else if constexpr (OP == XF_PROD_SC) {
       // scalar advection on the fine grid, uvp level l: inputs ub, vb, wb
       // (padded -u, -v, -w), tx, ty (padded d theta/dx, dy, uvp nodes) and
       // tz (padded d theta/dz, w nodes): ub tx + vb ty + (wb tz at l, l+1)/2
@@ -308,23 +325,19 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
       const long up = off + a.in_pstride;
       const V r = vldg<V>(a.in[0], off) * vldg<V>(a.in[3], off) + vldg<V>(a.in[1], off) * vldg<V>(a.in[4], off) +
                   T(0.5) * (vldg<V>(a.in[2], off) * vldg<V>(a.in[5], off) + vldg<V>(a.in[2], up) * vldg<V>(a.in[5], up));
-      vst(v, c * r);
-      break;
-    }
-    case XF_PRESS_INC: {
+      put(0, c * r);
+    } else if constexpr (OP == XF_PRESS_INC) {
       // u* = u^n + dt (t1 r + t2 r_f), so u* / (dt t1) = u^n / (dt t1) + r +
       // (t2/t1) r_f: the increment parts (inputs 0..5: rx ry rz rfx rfy rfz)
       // and the divergence of u^n (inputs 6..8: dudx dvdy dwdz, uvp nodes)
       // over dt t1 as a fourth field; c0 = 1/(nx ny), c1 = t2/t1,
       // c2 = 1/(dt t1).  Nothing large cancels in any of the four.
       const T c = T(a.c0), r21 = T(a.c1), idt = T(a.c2);
-      vst(v + 0 * vs, c * (vldg<V>(a.in[0], off) + r21 * vldg<V>(a.in[3], off)));
-      vst(v + 1 * vs, c * (vldg<V>(a.in[1], off) + r21 * vldg<V>(a.in[4], off)));
-      vst(v + 2 * vs, c * (vldg<V>(a.in[2], off) + r21 * vldg<V>(a.in[5], off)));
-      vst(v + 3 * vs, (c * idt) * ((vldg<V>(a.in[6], off) + vldg<V>(a.in[7], off)) + vldg<V>(a.in[8], off)));
-      break;
-    }
-    case XF_SCDYN: {
+      put(0, c * (vldg<V>(a.in[0], off) + r21 * vldg<V>(a.in[3], off)));
+      put(1, c * (vldg<V>(a.in[1], off) + r21 * vldg<V>(a.in[4], off)));
+      put(2, c * (vldg<V>(a.in[2], off) + r21 * vldg<V>(a.in[5], off)));
+      put(3, (c * idt) * ((vldg<V>(a.in[6], off) + vldg<V>(a.in[7], off)) + vldg<V>(a.in[8], off)));
+    } else if constexpr (OP == XF_SCDYN) {
       // dynamic Prandtl model on the nodes of compute_dynamic_mum
       // (compute_LagScaleDep.f90:501-520: level 1 on uvp nodes with w(2)/4,
       // levels >= 2 on w nodes).  Inputs: 0 u, 1 v, 2 w, 3 theta, 4..9 S_ij,
@@ -349,26 +362,24 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
         tf = tf - vsplat<V>(at_w0(a.in[3]));
         wf = wf - vsplat<V>(w0);
       }
-      vst(v + 0 * vs, uf);
-      vst(v + 1 * vs, vf);
-      vst(v + 2 * vs, wf);
-      vst(v + 3 * vs, tf);
-      vst(v + 4 * vs, uf * tf);
-      vst(v + 5 * vs, vf * tf);
-      vst(v + 6 * vs, wf * tf);
+      put(0, uf);
+      put(1, vf);
+      put(2, wf);
+      put(3, tf);
+      put(4, uf * tf);
+      put(5, vf * tf);
+      put(6, wf * tf);
 #pragma unroll
-      for (int q = 0; q < 6; ++q) vst(v + (7 + q) * vs, vldg<V>(a.in[4 + q], off));
+      for (int q = 0; q < 6; ++q) put(7 + q, vldg<V>(a.in[4 + q], off));
       const V S = vldg<V>(a.in[10], off);
       const V tx = at_w(a.in[11], off), ty = at_w(a.in[12], off), tz = vldg<V>(a.in[13], off);
-      vst(v + 13 * vs, tx);
-      vst(v + 14 * vs, ty);
-      vst(v + 15 * vs, tz);
-      vst(v + 16 * vs, S * tx);
-      vst(v + 17 * vs, S * ty);
-      vst(v + 18 * vs, S * tz);
-      break;
-    }
-    case XF_LASD: {
+      put(13, tx);
+      put(14, ty);
+      put(15, tz);
+      put(16, S * tx);
+      put(17, S * ty);
+      put(18, S * tz);
+    } else if constexpr (OP == XF_LASD) {
       // compute_LagScaleDep.f90:501-584: u_ft, A_ij, S_ij, |S| S_ij
       const T* u = a.in[0];
       const T* vv = a.in[1];
@@ -402,24 +413,39 @@ __device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i,
         vf = vf - vsplat<V>(v0);
         wf = wf - vsplat<V>(w0);
       }
-      vst(v + 0 * vs, uf);
-      vst(v + 1 * vs, vf);
-      vst(v + 2 * vs, wf);
-      vst(v + 3 * vs, uf * uf);  // A11
-      vst(v + 4 * vs, uf * vf);  // A12
-      vst(v + 5 * vs, uf * wf);  // A13
-      vst(v + 6 * vs, vf * vf);  // A22
-      vst(v + 7 * vs, vf * wf);  // A23
-      vst(v + 8 * vs, wf * wf);  // A33
+      put(0, uf);
+      put(1, vf);
+      put(2, wf);
+      put(3, uf * uf);  // A11
+      put(4, uf * vf);  // A12
+      put(5, uf * wf);  // A13
+      put(6, vf * vf);  // A22
+      put(7, vf * wf);  // A23
+      put(8, wf * wf);  // A33
       const V S = vldg<V>(a.in[9], off);
 #pragma unroll
       for (int q = 0; q < 6; ++q) {  // s11 s12 s13 s22 s23 s33
         const V sq = vldg<V>(a.in[3 + q], off);
-        vst(v + (9 + q) * vs, sq);
-        vst(v + (15 + q) * vs, S * sq);
+        put(9 + q, sq);
+        put(15 + q, S * sq);
       }
-      break;
     }
+  }
+}
+
+// the same with the op chosen at run time (the per-row references)
+template <typename T, typename V>
+__device__ __forceinline__ void xf_load(const XFArgs<T>& a, int l, int j, int i, T* v, int vs) {
+  switch (a.op) {
+    case XF_SCALE: xf_load_op<T, V, XF_SCALE, false>(a, l, j, i, v, vs, nullptr); break;
+    case XF_CONV_IN: xf_load_op<T, V, XF_CONV_IN, false>(a, l, j, i, v, vs, nullptr); break;
+    case XF_PROD: xf_load_op<T, V, XF_PROD, false>(a, l, j, i, v, vs, nullptr); break;
+    case XF_LASD: xf_load_op<T, V, XF_LASD, false>(a, l, j, i, v, vs, nullptr); break;
+    case XF_PRESS: xf_load_op<T, V, XF_PRESS, false>(a, l, j, i, v, vs, nullptr); break;
+    case XF_PROD_SC: xf_load_op<T, V, XF_PROD_SC, false>(a, l, j, i, v, vs, nullptr); break;
+    case XF_SCDYN: xf_load_op<T, V, XF_SCDYN, false>(a, l, j, i, v, vs, nullptr); break;
+    case XF_PRESS_INC: xf_load_op<T, V, XF_PRESS_INC, false>(a, l, j, i, v, vs, nullptr); break;
+    default: break;
   }
 }
 
@@ -475,23 +501,35 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd(const XFAr
   // s = r*nf + f holds the packed row z_m = x_{2m} + i x_{2m+1}, i.e. the
   // real row itself viewed as complex.
   T* xr = reinterpret_cast<T*>(buf);
-  for (int idx = threadIdx.x; idx < a.R * (NX / 4); idx += blockDim.x) {
-    const int r = idx / (NX / 4);
-    const int i = 4 * (idx - r * (NX / 4));
-    T* dst = xr + (long)(r * a.nf) * XS + i;
-    const int l = rowl[r];
-    if (l >= 0) {
-      const int j = rowj[r];
-      xf_load<T, V4<T>>(a, l, j, i, dst, XS);
-      if (a.use_ref)
-        for (int f = 0; f < a.nf; ++f) {
-          const T rf = refs[r * a.nf + f];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) dst[f * XS + q] -= rf;
-        }
-    } else {
-      for (int f = 0; f < a.nf; ++f) vst(dst + f * XS, vsplat<V4<T>>(T(0)));
+  // the load loop is compiled per op and per reference mode (no dispatch
+  // per point); references are subtracted in registers before the store
+  auto load_rows = [&](auto op_c, auto ref_c) {
+    constexpr int OP = decltype(op_c)::value;
+    constexpr bool REF = decltype(ref_c)::value;
+    for (int idx = threadIdx.x; idx < a.R * (NX / 4); idx += blockDim.x) {
+      const int r = idx / (NX / 4);
+      const int i = 4 * (idx - r * (NX / 4));
+      T* dst = xr + (long)(r * a.nf) * XS + i;
+      const int l = rowl[r];
+      if (l >= 0) xf_load_op<T, V4<T>, OP, REF>(a, l, rowj[r], i, dst, XS, refs + r * a.nf);
+      else
+        for (int f = 0; f < a.nf; ++f) vst(dst + f * XS, vsplat<V4<T>>(T(0)));
     }
+  };
+  auto load_op = [&](auto op_c) {
+    if (a.use_ref) load_rows(op_c, std::true_type{});
+    else load_rows(op_c, std::false_type{});
+  };
+  switch (a.op) {
+    case XF_SCALE: load_op(std::integral_constant<int, XF_SCALE>{}); break;
+    case XF_CONV_IN: load_op(std::integral_constant<int, XF_CONV_IN>{}); break;
+    case XF_PROD: load_op(std::integral_constant<int, XF_PROD>{}); break;
+    case XF_LASD: load_op(std::integral_constant<int, XF_LASD>{}); break;
+    case XF_PRESS: load_op(std::integral_constant<int, XF_PRESS>{}); break;
+    case XF_PROD_SC: load_op(std::integral_constant<int, XF_PROD_SC>{}); break;
+    case XF_SCDYN: load_op(std::integral_constant<int, XF_SCDYN>{}); break;
+    case XF_PRESS_INC: load_op(std::integral_constant<int, XF_PRESS_INC>{}); break;
+    default: break;
   }
   for (int idx = nseq * SL + threadIdx.x; idx < npad * SL; idx += blockDim.x) buf[idx] = cplx<T>{T(0), T(0)};
   __syncthreads();
@@ -520,9 +558,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd(const XFAr
       if (l >= 0) {
         const int j = rowj[r];
         cplx<T>* orow = a.out[f] + (long)l * a.out_pstride + (long)j * a.opitch;
-        for (int k = lane_t; k < a.nk; k += TL) {
-          orow[k] = r2c_split(seq[k == M ? 0 : k], seq[(M - k) % M], tw[k]);
-        }
+        xf_split_store<T, M, TL, E>(seq, tw, orow, lane_t, a.nk);
       }
     }
   }
@@ -698,9 +734,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd_st(const X
         if (l >= 0) {
           const int j = rowj[r];
           cplx<T>* orow = a.out[f] + (long)l * a.out_pstride + (long)j * a.opitch;
-          for (int k = lane_t; k < a.nk; k += TL) {
-            orow[k] = r2c_split(seq[k == M ? 0 : k], seq[(M - k) % M], tw[k]);
-          }
+          xf_split_store<T, M, TL, E>(seq, tw, orow, lane_t, a.nk);
         }
       }
     }
@@ -819,19 +853,22 @@ __device__ __forceinline__ void yp_issue(const YPArgs<T>& a, long item, int ncb,
   const int col0 = umod32(item, ncb) * C;
   const int l = a.plane0 + umod32(udiv32(item, ncb), a.nplanes);
   const int grp = udiv32(item, (long)ncb * a.nplanes);
-  // thread -> fixed column c, rows ky0, ky0 + kstep, ...: the addresses
-  // advance by constant strides (blockDim.x is a multiple of C)
+  // thread -> fixed column c, rows ky0 + TL i: the CTA has C x TL threads,
+  // so every thread copies NY / TL rows at a compile-time count and the
+  // addresses advance by constant strides (an unrolled loop)
+  constexpr int TL = Geo<NY>::T;
   const int c = threadIdx.x & (C - 1);
   const int ky0 = threadIdx.x >> a.lc;
-  const int kstep = blockDim.x >> a.lc;
   const int kx = col0 + c;
   const bool valid = kx < a.ncols;
+  const long step = (long)TL * a.ipitch;
   for (int q = 0; q < a.nin; ++q) {
     const cplx<T>* base = a.in[grp * a.nin + q];
-    const cplx<T>* src = base + (long)l * a.in_pstride + kx;
-    cplx<T>* dst = bin + (q * C + c) * SI;
-    for (int ky = ky0; ky < NY; ky += kstep)
-      cp_async<int(sizeof(cplx<T>))>(dst + ky, valid ? src + (long)ky * a.ipitch : base, valid);
+    const cplx<T>* src = valid ? base + (long)l * a.in_pstride + kx + (long)ky0 * a.ipitch : base;
+    cplx<T>* dst = bin + (q * C + c) * SI + ky0;
+#pragma unroll
+    for (int i = 0; i < NY / TL; ++i)
+      cp_async<int(sizeof(cplx<T>))>(dst + TL * i, valid ? src + i * step : base, valid);
   }
 }
 
@@ -1034,15 +1071,18 @@ __global__ void __launch_bounds__((FWD && sizeof(T) == 8) ? 128 : 256,
     const bool second = (a.op == YP_FILTER2 && q == 1);
     const int lim = second ? a.ncols1 : a.ncols;
     {
-      // thread -> fixed column cc, rows ky0 + kstep i (as in yp_issue)
+      // thread -> fixed column cc, rows ky0 + TL i (as in yp_issue)
       const int cc = threadIdx.x & (C - 1);
       const int kxx = col0 + cc;
       if (kxx < lim) {
-        const int ky0 = threadIdx.x >> a.lc, kstep = blockDim.x >> a.lc;
+        const int ky0 = threadIdx.x >> a.lc;
         const long opitch = second ? a.opitch1 : a.opitch;
-        cplx<T>* dst = a.out[grp * a.nout + q] + (long)l * (second ? a.out_pstride1 : a.out_pstride) + kxx;
-        const cplx<T>* srow = bin + cc * SI;
-        for (int ky = ky0; ky < NYO; ky += kstep) dst[(long)ky * opitch] = srow[ky];
+        cplx<T>* dst = a.out[grp * a.nout + q] + (long)l * (second ? a.out_pstride1 : a.out_pstride) + kxx +
+                       (long)ky0 * opitch;
+        const cplx<T>* srow = bin + cc * SI + ky0;
+        const long step = (long)TL * opitch;
+#pragma unroll
+        for (int i = 0; i < NYO / TL; ++i) dst[i * step] = srow[TL * i];
       }
     }
     __syncthreads();
