@@ -496,49 +496,54 @@ def run_e2e(les, p, K: int, local: int):
 
 # --------------------------------------------------------- CPU baseline
 def cpu_sample(n: int):
-    """The FP64 oracle on the host cores: one plain step and one dynamic-update
-    step of an n x n x 32 slab of the workload, amortised over cs_count = 5."""
+    """The compiled FP64 oracle (oracle/cpu_step.cpp, OpenMP on every host
+    core) on one plain step and one dynamic-update step of an n x n x 32 slab
+    of the workload, amortised over cs_count = 5."""
+    from oracle import cpu_step as CS
     from oracle import les_oracle as O
 
     cores = os.cpu_count() or 1
-    O.set_workers(cores)
     p = O.Params(nx=n, ny=n, nz=32, dt=1e-4, dyn_init=1, cs_count=2)
-    ops = O.Ops(p)
-    st = O.make_state(p)
+    cs = CS.CpuStep(p, threads=cores)
+    cs.mirror(O.make_state(p))
     t = []
     for _ in range(4):  # plain, F-initialising update, plain, interpolating update
         t0 = time.perf_counter()
-        O.les_step(ops, st)
+        cs.step()
         t.append(time.perf_counter() - t0)
+    cs.close()
     t_plain = 0.5 * (t[0] + t[2])
     t_upd = t[3]
     per_step = (4 * t_plain + t_upd) / 5.0
     pts = p.nx * p.ny * p.nz
     return {"value": round(pts / per_step / 1e6, 4), "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"numpy/scipy FP64 oracle, {n}x{n}x32 slab: plain step {t_plain:.2f} s, "
-                      f"dynamic-update step {t_upd:.2f} s, amortised 4:1 (cs_count 5)"}
+            "sample": f"C++ FP64 port of the oracle (oracle/cpu_step.cpp, OpenMP, {cores} threads), "
+                      f"{n}x{n}x32 slab: plain step {t_plain:.3f} s, dynamic-update step {t_upd:.3f} s, "
+                      f"amortised 4:1 (cs_count 5)"}
 
 
 # -------------------------------------------------------- reference arm
 def run_reference(args, dist, rank, ws):
+    """The reference's algorithm on the host cores: the compiled FP64 port
+    (oracle/cpu_step.cpp, OpenMP on every core) stepping an n x n x 32 slab of
+    the workload (one eighth of the 256^3 grid's levels)."""
     if rank != 0:
         return
+    from oracle import cpu_step as CS
     from oracle import les_oracle as O
 
     cores = os.cpu_count() or 1
-    O.set_workers(cores)
     n = args.n
-    nz = 8
+    nz = 32
     p = O.Params(nx=n, ny=n, nz=nz, dt=1e-4, dyn_init=5, cs_count=5)
-    ops = O.Ops(p)
-    st = O.make_state(p)
+    cs = CS.CpuStep(p, threads=cores)
+    cs.mirror(O.make_state(p))
     W, K = max(args.warmup, 3), args.steps
-    for _ in range(W):
-        O.les_step(ops, st)
+    cs.step(W)
     t0 = time.perf_counter()
-    for _ in range(K):
-        O.les_step(ops, st)
+    cs.step(K)
     dt = time.perf_counter() - t0
+    cs.close()
     pts = p.nx * p.ny * p.nz
     v = pts * K / dt / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": ws,
@@ -547,9 +552,10 @@ def run_reference(args, dist, rank, ws):
             "config": {"workload": f"LES time step, {n}x{n}x{nz} slab of the {n}^3 workload per sample step",
                        "grid": [n, n, nz]},
             "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"one full time step of a {n}x{n}x{nz} slab per step (FP64 oracle, "
-                                       f"scipy pocketfft with {cores} workers); the Fortran reference cannot "
-                                       "be built here (no Fortran compiler, MPI, FFTW or 2DECOMP&FFT)"},
+                             "sample": f"full time steps of a {n}x{n}x{nz} slab (LASD update every 5th step), "
+                                       f"C++ FP64 port of the oracle with OpenMP on {cores} threads; the Fortran "
+                                       "reference cannot be built here (no Fortran compiler, MPI, FFTW or "
+                                       "2DECOMP&FFT)"},
             "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
