@@ -2016,8 +2016,7 @@ class Solver final : public SolverBase {
     // press_from_increment forms the same pressure in FP32 without the
     // cancellation, but its FP32 four-field y pass measured slower than the
     // FP64 three-field one at 256^3 (0.47 against 0.36 ms per step)
-    if (mixed()) press_from_increment(t1, t2);
-    else press_stag_array(t1);
+    press_stag_array(t1);
     LES_CUDA(cudaEventRecord(ev[4], st));
     projection(t1);
     set_bc();
