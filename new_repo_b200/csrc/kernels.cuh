@@ -107,6 +107,24 @@ __global__ void k_fill(T* f, long n, T val) {
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) f[q] = val;
 }
 
+// up to 8 plane-sized copies or fills in one launch (blockIdx.y = the op):
+// the ghost-level writes of a step, which would otherwise each be a launch
+template <typename T>
+struct PlaneOps {
+  T* dst[8];
+  const T* src[8];  // null: fill with val[op]
+  T val[8];
+};
+template <typename T>
+__global__ void k_plane_ops(const PlaneOps<T> ops, long n) {
+  const int op = blockIdx.y;
+  T* d = ops.dst[op];
+  const T* s = ops.src[op];
+  const T v = ops.val[op];
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+    d[q] = s ? s[q] : v;
+}
+
 template <typename T>
 __global__ void k_scale(T* f, long n, T c) {
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) f[q] = c * f[q];

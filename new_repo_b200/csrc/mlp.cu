@@ -445,7 +445,7 @@ __device__ __forceinline__ void tc_teardown(S_t& S, uint32_t ncols, uint32_t pha
 // RI: buoyant runs (feature 7 = the gradient Richardson number); the
 // neutral variant is compiled without it (fewer registers, one more CTA per SM)
 template <typename T, bool RI>
-__global__ void __launch_bounds__(TILE, 5) k_mlp_infer(const MlpFeatIn<T> a, T* cs, MlpDevice m, unsigned* status) {
+__global__ void __launch_bounds__(TILE, 6) k_mlp_infer(const MlpFeatIn<T> a, T* cs, MlpDevice m, unsigned* status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   InferSmem& S = *reinterpret_cast<InferSmem*>(smem_raw + ((1024 - (tc::smem_u32(smem_raw) & 1023)) & 1023));
   load_images(S, m.img, m.params, m.stats);
@@ -832,7 +832,7 @@ void mlp_infer(const MlpFeatIn<T>& in, T* cs, MlpDevice& m, unsigned* status, cu
   LES_CUDA(cudaMemsetAsync(m.colflag, 0, sizeof(int) * m.plane, st));
   const long n = (long)(in.nz + 1) * in.plane;
   const long ntiles = (n + TILE - 1) / TILE;
-  const int grid = int(std::min<long>(ntiles, 148L * 5));  // 5 CTAs per SM fit (registers)
+  const int grid = int(std::min<long>(ntiles, 148L * 6));  // 6 CTAs per SM fit (79 registers, 32 KB, 64 TMEM columns each)
   hook_before("k_mlp_infer", double(n) * 11 * sizeof(T));
   if (in.dtdz) k_mlp_infer<T, true><<<grid, TILE, infer_smem(), st>>>(in, cs, m, status);
   else k_mlp_infer<T, false><<<grid, TILE, infer_smem(), st>>>(in, cs, m, status);

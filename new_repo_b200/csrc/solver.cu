@@ -268,6 +268,21 @@ class Solver final : public SolverBase {
     const long n = (long)(k1 - k0 + 1) * g.plane();
     KL("k_fill", double(n) * sizeof(T), k_fill<T><<<grid_for(n), 256, 0, st>>>(lev(f, k0), n, v));
   }
+  // plane-sized copies / fills batched into one launch (src null: fill)
+  void plane_ops(int nops, T* const* dst, const T* const* src, const T* val) {
+    PlaneOps<T> o;
+    std::memset(&o, 0, sizeof(o));
+    for (int i = 0; i < nops; ++i) {
+      o.dst[i] = dst[i];
+      o.src[i] = src ? src[i] : nullptr;
+      o.val[i] = val ? val[i] : T(0);
+    }
+    const long n = g.plane();
+    double bytes = 0.0;
+    for (int i = 0; i < nops; ++i) bytes += (o.src[i] ? 2.0 : 1.0) * n * sizeof(T);
+    dim3 grid(unsigned(std::min<long>(ceil_div(n, 256L), 148)), unsigned(nops));
+    KL("k_plane_ops", bytes, k_plane_ops<T><<<grid, 256, 0, st>>>(o, n));
+  }
   void copy(T* dst, const T* src, long n) {
     KL("k_copy", 2.0 * n * sizeof(T), k_copy<T><<<grid_for(n), 256, 0, st>>>(dst, src, n));
   }
@@ -1178,13 +1193,18 @@ class Solver final : public SolverBase {
     }
     launch_xinv<T>(g.nx, h, st);
     // ghost levels of the outputs (compute_convective_padd.f90:251-259)
-    for (int q = 0; q < 3; ++q) {
-      if (padd) {
-        fill(F[outs[q]], 0, 0, T(BOGUS));
-        fill(F[outs[q]], nz + 1, nz + 1, T(BOGUS));
+    if (padd) {
+      T* dst[6];
+      T val[6];
+      for (int q = 0; q < 3; ++q) {
+        dst[2 * q] = lev(F[outs[q]], 0);
+        dst[2 * q + 1] = lev(F[outs[q]], nz + 1);
+        val[2 * q] = val[2 * q + 1] = T(BOGUS);
       }
+      plane_ops(6, dst, nullptr, val);
+    } else {
+      trunc_ghosts(outs);
     }
-    if (!padd) trunc_ghosts(outs);
   }
 
   // compute_convective_trunc leaves its vorticity scratch in the ghost levels
@@ -1958,11 +1978,16 @@ class Solver final : public SolverBase {
     {
       Tag tag_(this, "convec");
       const int r[3] = {LES_RHSX, LES_RHSY, LES_RHSZ}, rf[3] = {LES_RHSX_F, LES_RHSY_F, LES_RHSZ_F};
+      T* dst[6];
+      const T* src[6];
       for (int q = 0; q < 3; ++q) {
-        copy(lev(F[r[q]], 0), lev(F[rf[q]], 0), g.plane());
-        copy(lev(F[r[q]], g.nz + 1), lev(F[rf[q]], g.nz + 1), g.plane());
-        std::swap(F[r[q]], F[rf[q]]);
+        dst[2 * q] = lev(F[r[q]], 0);
+        src[2 * q] = lev(F[rf[q]], 0);
+        dst[2 * q + 1] = lev(F[r[q]], g.nz + 1);
+        src[2 * q + 1] = lev(F[rf[q]], g.nz + 1);
       }
+      plane_ops(6, dst, src, nullptr);
+      for (int q = 0; q < 3; ++q) std::swap(F[r[q]], F[rf[q]]);
     }
     dealias_convec(LES_RHSX, LES_RHSY, LES_RHSZ);
     DivEq e[3] = {{LES_RHSX, LES_TXX, LES_TXY, LES_TXZ, 1, P.pfx},
