@@ -457,7 +457,7 @@ __host__ __device__ constexpr int seq_pad(int nseq) {
 }
 
 template <typename T, int NX>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd(const XFArgs<T> a) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (NX <= 256 ? 4 : 3) : 2) k_xfwd(const XFArgs<T> a) {
   constexpr int M = NX / 2;
   constexpr int TL = Geo<M>::T;
   constexpr int E = Geo<M>::E;
@@ -632,7 +632,7 @@ __device__ __forceinline__ void xf_issue(const XFArgs<T>& a, long item, S* stage
 // the input rows of the next batch copied into the other shared stage with
 // cp.async while the current batch is transformed.  S: input element type.
 template <typename T, int NX, typename S>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xfwd_st(const XFArgs<T> a) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (NX <= 256 ? 4 : 3) : 2) k_xfwd_st(const XFArgs<T> a) {
   constexpr int M = NX / 2;
   constexpr int TL = Geo<M>::T;
   constexpr int E = Geo<M>::E;
@@ -1217,7 +1217,7 @@ __device__ __forceinline__ void xi_issue_bulk(const XIArgs<T>& a, long item, cpl
 }
 
 template <typename T, int NX>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_xinv(const XIArgs<T> a) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (NX <= 256 ? 4 : 3) : 2) k_xinv(const XIArgs<T> a) {
   constexpr int M = NX / 2;
   constexpr int TL = Geo<M>::T;
   constexpr int E = Geo<M>::E;
