@@ -463,7 +463,9 @@ def ncu_traffic(label: str):
 def run_e2e(les, p, K: int, local: int):
     """K steps through the public API with the velocity state held in
     page-locked host memory (the drop-in boundary: the host arrays stay
-    authoritative): per step H2D u,v,w -> les_step -> D2H u,v,w + diagnostics."""
+    authoritative): per step H2D u,v,w -> les_step -> D2H u,v,w + diagnostics,
+    one les_step_host call per step (the copies back of a step and the copies
+    in of the next overlap, one per direction of the host link)."""
     import torch
 
     L = p.nz + 2
@@ -476,14 +478,8 @@ def run_e2e(les, p, K: int, local: int):
     les.sync()
     les.event_record(2)
     t0 = time.perf_counter()
-    for _ in range(K):
-        for h, n in zip(host, names):
-            les.upload_async(n, h.data_ptr())
-        les.step(1)
-        les.diagnostics_async(diag.data_ptr())
-        for h, n in zip(host, names):
-            les.download_async(n, h.data_ptr())
-    les.event_record(3)
+    les.step_host(host[0].data_ptr(), host[1].data_ptr(), host[2].data_ptr(), diag.data_ptr(), n=K)
+    les.event_record(3)  # ordered after the last copies back
     les.sync()
     wall = time.perf_counter() - t0
     ms = les.event_elapsed(2, 3)

@@ -13,10 +13,12 @@
  * reference's decomp_2d_abort codes (1 invalid option, 3 out of memory,
  * 9 numerical failure, 22 I/O; 4 for other CUDA errors); les_last_error()
  * gives the message.  Calls
- * on one state are not re-entrant; each state owns one CUDA stream.
+ * on one state are not re-entrant; each state owns one CUDA stream (and two
+ * copy streams once les_step_host is used).
  */
 #ifndef LESGPU_H
 #define LESGPU_H
+#include <stddef.h>
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -238,6 +240,23 @@ int les_event_elapsed(les_state* s, int a, int b, double* ms);
 int les_upload_async(les_state* s, int field, const double* pinned, int k0, int k1);
 int les_download_async(les_state* s, int field, double* pinned, int k0, int k1);
 int les_diagnostics_async(les_state* s, double* pinned_out4);
+/* One time step of the LES_engine.f90:189-360 loop body with the velocity
+ * state held in host memory, as a caller whose arrays stay authoritative
+ * (the reference's u, v, w of system.f90:21-43) would step it: copies
+ * u, v, w (FP64, levels 0..nz+1, the les_upload layout) to the device,
+ * runs les_step(jt, jt_total), and copies the new u, v, w and the step's
+ * four diagnostics (les_diagnostics order; diag_out4 may be NULL) back into
+ * the same arrays.  Asynchronous: the call returns once the work is queued,
+ * and the arrays must be neither read nor written until les_sync (or any
+ * other entry point, which orders itself after these copies).  Successive
+ * calls overlap the copies back of one step with the copies in of the next,
+ * per chunk of levels, one in each direction of the host link; page-locked
+ * arrays are needed for that overlap (pageable ones work, serialised). */
+int les_step_host(les_state* s, int jt, int jt_total, double* u, double* v, double* w, double* diag_out4);
+/* Page-lock (and release) caller-allocated host memory, e.g. the Fortran
+ * u, v, w handed to les_step_host, so that its copies can overlap. */
+int les_host_register(void* p, size_t bytes);
+int les_host_unregister(void* p);
 
 /* Checkpoint file of write_checkpoint_file / read_checkpoint_file
  * (IO_checkpoint.f90:119-256) on one rank, byte for byte: native FP64

@@ -38,9 +38,12 @@ int bad_arg(const char* what) {
 }
 }  // namespace
 
-#define STATE_OR_FAIL(s)            \
+// Every entry point but les_step_host first orders the state's stream after
+// the copies back of an earlier les_step_host (a no-op without one).
+#define STATE_OR_FAIL(s)                     \
   if (!(s) || !(s)->s) return bad_state(); \
-  les::g_hook = (s)->s
+  les::g_hook = (s)->s;                    \
+  (s)->s->join_copies()
 
 extern "C" {
 
@@ -312,6 +315,20 @@ int les_download_async(les_state* s, int field, double* pinned, int k0, int k1) 
 int les_diagnostics_async(les_state* s, double* pinned_out4) {
   STATE_OR_FAIL(s);
   return guard([&] { s->s->diagnostics_async(pinned_out4); });
+}
+int les_host_register(void* p, size_t bytes) {
+  if (!p || bytes == 0) return bad_arg("p, bytes");
+  return guard([&] { LES_CUDA(cudaHostRegister(p, bytes, cudaHostRegisterDefault)); });
+}
+int les_host_unregister(void* p) {
+  if (!p) return bad_arg("p");
+  return guard([&] { LES_CUDA(cudaHostUnregister(p)); });
+}
+int les_step_host(les_state* s, int jt, int jt_total, double* u, double* v, double* w, double* diag_out4) {
+  if (!s || !s->s) return bad_state();
+  if (!u || !v || !w) return bad_arg("u, v, w");
+  les::g_hook = s->s;
+  return guard([&] { s->s->step_host(jt, jt_total, u, v, w, diag_out4); });
 }
 
 int les_set_sgs_model(les_state* s, int model) {

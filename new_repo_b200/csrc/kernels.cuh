@@ -136,6 +136,19 @@ __global__ void k_convert(D* dst, const S* src, long n) {
     dst[q] = D(src[q]);
 }
 
+// The three velocity fields in one launch: blockIdx.y selects the field.
+template <typename D, typename S>
+struct Convert3 {
+  D* dst[3];
+  const S* src[3];
+};
+template <typename D, typename S>
+__global__ void k_convert3(const Convert3<D, S> a, long n) {
+  D* __restrict__ d = a.dst[blockIdx.y];
+  const S* __restrict__ s = a.src[blockIdx.y];
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) d[q] = D(s[q]);
+}
+
 template <typename T>
 __global__ void k_copy(T* dst, const T* src, long n) {
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) dst[q] = src[q];

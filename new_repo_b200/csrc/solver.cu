@@ -137,10 +137,16 @@ class Solver final : public SolverBase {
   }
 
   ~Solver() override {
-    if (st) cudaStreamSynchronize(st);
+    for (cudaStream_t s : {sh2d, sd2h, st})
+      if (s) cudaStreamSynchronize(s);
     for (void* q : allocs) cudaFree(q);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : {ev_go, ev_in, ev_done, ev_copies})
+      if (e) cudaEventDestroy(e);
+    for (auto e : ev_out) cudaEventDestroy(e);
+    for (cudaStream_t s : {sh2d, sd2h})
+      if (s) cudaStreamDestroy(s);
     if (st) cudaStreamDestroy(st);
   }
 
@@ -942,6 +948,89 @@ class Solver final : public SolverBase {
   void diagnostics_async(double* h) override {
     diagnostics_launch();
     LES_CUDA(cudaMemcpyAsync(h, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+
+  // ------------------------------------------- step with host velocity ----
+  // Copies in on sh2d, the step on st, copies back on sd2h, per chunk of
+  // ~16 MB of levels.  The copy in of a chunk waits for the previous call's
+  // copy back of the same chunk (same host memory; in FP64 also the same
+  // device levels), so that one call's copies back and the next call's
+  // copies in run at the same time, one in each direction of the link.
+  // Mixed precision stages the FP64 values in device buffers (one set per
+  // direction) and converts on st.
+  cudaStream_t sh2d = nullptr, sd2h = nullptr;
+  cudaEvent_t ev_go = nullptr, ev_in = nullptr, ev_done = nullptr;
+  std::vector<cudaEvent_t> ev_out;  // per (field, chunk): copy back done
+  bool out_recorded = false;
+  double* stage_in[3] = {};
+  double* stage_out[3] = {};
+  int chunk_lev = 0, nchunk = 0;
+
+  void setup_host_pipe() {
+    LES_CUDA(cudaStreamCreateWithFlags(&sh2d, cudaStreamNonBlocking));
+    LES_CUDA(cudaStreamCreateWithFlags(&sd2h, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&ev_go, &ev_in, &ev_done, &ev_copies})
+      LES_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    const long pb = g.plane() * (long)sizeof(double);
+    chunk_lev = int(std::max(1L, (16L << 20) / pb));
+    nchunk = (g.L + chunk_lev - 1) / chunk_lev;
+    ev_out.assign(3 * nchunk, nullptr);
+    for (auto& e : ev_out) LES_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    if (mixed())
+      for (int q = 0; q < 3; ++q) {
+        stage_in[q] = track(dalloc<double>(g.field()));
+        stage_out[q] = track(dalloc<double>(g.field()));
+      }
+  }
+
+  void step_host(int jt, int jtt, double* u, double* v, double* w, double* diag4) override {
+    if (!sh2d) setup_host_pipe();
+    double* h[3] = {u, v, w};
+    const int fid[3] = {LES_U, LES_V, LES_W};
+    auto dev = [&](int q) -> double* {
+      if constexpr (std::is_same<T, double>::value) return F[fid[q]];
+      else return stage_in[q];
+    };
+    auto dev_out = [&](int q) -> const double* {
+      if constexpr (std::is_same<T, double>::value) return F[fid[q]];
+      else return stage_out[q];
+    };
+    // the copies in follow everything queued on st before this call
+    LES_CUDA(cudaEventRecord(ev_go, st));
+    LES_CUDA(cudaStreamWaitEvent(sh2d, ev_go, 0));
+    for (int q = 0; q < 3; ++q)
+      for (int c = 0; c < nchunk; ++c) {
+        const int k0 = c * chunk_lev, k1 = std::min(g.L, k0 + chunk_lev);
+        if (out_recorded) LES_CUDA(cudaStreamWaitEvent(sh2d, ev_out[q * nchunk + c], 0));
+        LES_CUDA(cudaMemcpyAsync(dev(q) + k0 * g.plane(), h[q] + k0 * g.plane(),
+                                 (k1 - k0) * g.plane() * sizeof(double), cudaMemcpyHostToDevice, sh2d));
+      }
+    LES_CUDA(cudaEventRecord(ev_in, sh2d));
+    LES_CUDA(cudaStreamWaitEvent(st, ev_in, 0));
+    if constexpr (!std::is_same<T, double>::value) {
+      Tag tag_(this, "io");
+      Convert3<T, double> a{{F[LES_U], F[LES_V], F[LES_W]}, {stage_in[0], stage_in[1], stage_in[2]}};
+      KL("k_convert3", 36.0 * g.field(), k_convert3<T, double><<<dim3(grid_for(g.field()), 3), 256, 0, st>>>(a, g.field()));
+    }
+    step(jt, jtt);  // ends with the diagnostics of the new state in dout
+    if constexpr (!std::is_same<T, double>::value) {
+      Tag tag_(this, "io");
+      Convert3<double, T> a{{stage_out[0], stage_out[1], stage_out[2]}, {F[LES_U], F[LES_V], F[LES_W]}};
+      KL("k_convert3", 36.0 * g.field(), k_convert3<double, T><<<dim3(grid_for(g.field()), 3), 256, 0, st>>>(a, g.field()));
+    }
+    LES_CUDA(cudaEventRecord(ev_done, st));
+    LES_CUDA(cudaStreamWaitEvent(sd2h, ev_done, 0));
+    if (diag4) LES_CUDA(cudaMemcpyAsync(diag4, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, sd2h));
+    for (int q = 0; q < 3; ++q)
+      for (int c = 0; c < nchunk; ++c) {
+        const int k0 = c * chunk_lev, k1 = std::min(g.L, k0 + chunk_lev);
+        LES_CUDA(cudaMemcpyAsync(h[q] + k0 * g.plane(), dev_out(q) + k0 * g.plane(),
+                                 (k1 - k0) * g.plane() * sizeof(double), cudaMemcpyDeviceToHost, sd2h));
+        LES_CUDA(cudaEventRecord(ev_out[q * nchunk + c], sd2h));
+      }
+    out_recorded = true;
+    LES_CUDA(cudaEventRecord(ev_copies, sd2h));
+    copies_pending = true;
   }
 
   void set_initial_conditions(const double* u, const double* v, const double* w) override {

@@ -133,6 +133,19 @@ struct SolverBase : LaunchHook {
   virtual void upload_async(int field, const double* pinned, int k0, int k1) = 0;
   virtual void download_async(int field, double* pinned, int k0, int k1) = 0;
   virtual void diagnostics_async(double* pinned4) = 0;
+  // One time step with u, v, w (levels 0..nz+1, FP64) in host memory: copies
+  // in, the step, copies back, on two copy streams around the state's stream
+  // (step_host in solver.cu).  The copies back of a call may still run when
+  // it returns; join_copies() orders the state's stream after them and runs
+  // at the start of every other entry point.
+  virtual void step_host(int jt, int jtt, double* u, double* v, double* w, double* diag4) = 0;
+  bool copies_pending = false;
+  cudaEvent_t ev_copies = nullptr;  // recorded after a call's last copy back
+  void join_copies() noexcept {
+    if (!copies_pending) return;
+    copies_pending = false;
+    (void)cudaStreamWaitEvent(st, ev_copies, 0);
+  }
   virtual void stat_init() = 0;
   virtual void stat_averages(int jt, int jtt, int start_stats, int running_period, const char* out_path) = 0;
   virtual void stat_sums(int index, double* out) = 0;

@@ -612,6 +612,29 @@ class LES:
     def diagnostics_async(self, pinned_ptr: int):
         check(self.lib.les_diagnostics_async(self._h, C.c_void_p(pinned_ptr)))
 
+    def step_host(self, u_ptr: int, v_ptr: int, w_ptr: int, diag_ptr: int | None = None, n: int = 1):
+        """Advance n time steps with u, v, w held in host memory (addresses of
+        FP64 arrays of shape (nz + 2, ny, nx), page-locked for the copies to
+        overlap): each step copies them in, steps, and copies the new state
+        and its diagnostics back (les_step_host).  Asynchronous like the
+        C entry point: sync() before touching the arrays.  The status check
+        and the statistics of step() follow at the same steps."""
+        p = self.params
+        d = C.c_void_p(diag_ptr) if diag_ptr else None
+        for _ in range(n):
+            self.jt += 1
+            self.jt_total += 1
+            check(self.lib.les_step_host(self._h, self.jt, self.jt_total, C.c_void_p(u_ptr), C.c_void_p(v_ptr),
+                                         C.c_void_p(w_ptr), d))
+            if p.nan_check > 0 and self.jt % p.nan_check == 0:
+                self.check_status()
+            if p.stat_flag and self.jt_total > p.start_stats:
+                self.stat_averages()
+            if p.spectra_flag:
+                self.stat_spectra()
+            if p.tke_flag and self.jt_total > p.start_tke:
+                self.tke_budget()
+
     # ------------------------------------------------------ learned closure
     def set_precision(self, precision: str):
         """Move the state to the other precision ("fp64" / "mixed"): fields,
