@@ -771,6 +771,13 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
   cplx<double> x = {r.x / bet, r.y / bet};
   xs[col] = x;
   bool bad = false;
+  // One FP64 reciprocal per level: the recurrence multiplies by 1/bet and
+  // 1/dz where the reference divides (compute_pressure.f90:473-478).  A
+  // division is a long dependent instruction sequence, and with one thread
+  // per system (~7 warps per SM) nothing hides its latency; the results
+  // differ from dividing by rounding only (an ulp per operation).
+  double ib = 1.0 / bet;
+  const double idz = 1.0 / dz;
   // The levels are loaded in batches of TB: the loads of the next batch are
   // issued before the recurrence runs through the current one, so that a
   // thread keeps 2 TB levels of reads in flight (the grid holds only one
@@ -802,7 +809,7 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
         const cplx<T> hx = cx[j], hy = cy[j], hzp = cz[j];
         const double sx = kxv * double(hx.x) + kyv * double(hy.x);
         const double sy = kxv * double(hx.y) + kyv * double(hy.y);
-        r = {-sy + (double(hzp.x) - double(hz.x)) / dz, sx + (double(hzp.y) - double(hz.y)) / dz};
+        r = {-sy + (double(hzp.x) - double(hz.x)) * idz, sx + (double(hzp.y) - double(hz.y)) * idz};
         if constexpr (INC) {
           r.x += double(cg[j].x);
           r.y += double(cg[j].y);
@@ -812,10 +819,11 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
           const double hkp = (k < nz) ? pm[k + 1] + pm_r21 * pm[pm_L + k + 1] : 0.0;
           r = {(hkp - hk) / dz + ((pm[2 * pm_L + k] + pm[3 * pm_L + k]) + pm[4 * pm_L + k]) * pm_idt, 0.0};
         }
-        const double g = cprev / bet;
+        const double g = cprev * ib;
         bet = b_in - a_in * g;
         bad |= (bet == 0.0);
-        x = {(r.x - a_in * x.x) / bet, (r.y - a_in * x.y) / bet};
+        ib = 1.0 / bet;
+        x = {(r.x - a_in * x.x) * ib, (r.y - a_in * x.y) * ib};
         gam[o] = g;
         xs[o] = x;
         cprev = a_in;
@@ -833,10 +841,11 @@ __global__ void k_tridiag(const cplx<T>* __restrict__ Hx, const cplx<T>* __restr
   {  // top row: -p(nz) + p(nz+1) = dz * top layer
     const long o = (long)(nz + 1) * sp + col;
     r = {double(top[icol].x) * dz, double(top[icol].y) * dz};
-    const double g = cprev / bet;
+    const double g = cprev * ib;
     bet = 1.0 - (-1.0) * g;
     bad |= (bet == 0.0);
-    x = {(r.x - (-1.0) * x.x) / bet, (r.y - (-1.0) * x.y) / bet};
+    ib = 1.0 / bet;
+    x = {(r.x - (-1.0) * x.x) * ib, (r.y - (-1.0) * x.y) * ib};
     gam[o] = g;
   }
   if (bad) atomicOr(status, ST_PIVOT);
