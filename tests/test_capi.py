@@ -51,6 +51,10 @@ def test_null_arguments_return_invalid(lib):
     assert lib.les_step(None, 1, 1) == capi.LES_ERR_INVALID
     assert b"null" in lib.les_last_error()
     assert lib.les_destroy(None) == capi.LES_OK
+    # the host-state step and the page-locking helpers check before any CUDA call
+    assert lib.les_step_host(None, 1, 1, None, None, None, None) == capi.LES_ERR_INVALID
+    assert lib.les_host_register(None, 8) == capi.LES_ERR_INVALID
+    assert lib.les_host_unregister(None) == capi.LES_ERR_INVALID
 
 
 def test_invalid_model_is_rejected_before_device_use(lib):
