@@ -308,8 +308,12 @@ def run_ours(args, dist, rank, local, ws):
     if train is not None:
         train.update(les.mlp_info())
         prof_chk = les.mlp_check_profile()
-        kmax = int(np.argmax(prof_chk))
-        train["check_profile_max"] = {"level": kmax + 1, "rms_log_error": round(float(prof_chk[kmax]), 4)}
+        nb = min(args.wall_levels, len(prof_chk) - 1)
+        kmax = nb + int(np.argmax(prof_chk[nb:]))
+        # levels 1..wall_levels run LASD: their entries are the closure's
+        # error where it is not used (why the band exists)
+        train["check_profile_max_above_wall_band"] = {"level": kmax + 1,
+                                                      "rms_log_error": round(float(prof_chk[kmax]), 4)}
         train["check_profile_levels_1_12"] = [round(float(x), 4) for x in prof_chk[:12]]
         train["check_after_steps"] = S
 
