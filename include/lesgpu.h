@@ -173,10 +173,14 @@ int les_press_from_increment(les_state* s, double tadv1, double tadv2);
  * default) is the single sweep.  Errors: 1 unless 1 <= nslabs <= 64 and nz
  * is a multiple of nslabs with at least two levels per slab. */
 int les_set_pressure_slabs(les_state* s, int nslabs);
-/* compute_wall_law.f90:198-254 obukhov(u_star_avg, wall_model) */
+/* compute_wall_law.f90:198-254 obukhov(u_star_avg, wl_type) */
 int les_obukhov(les_state* s);
-/* compute_wall_law.f90:107-185 wallstress(lbc_u, lbc_v, wall_model) */
+/* compute_wall_law.f90:107-185 wallstress(lbc_u, lbc_v, wl_type) */
 int les_wallstress(les_state* s);
+/* The wl_type argument of obukhov / wallstress: the wall model (LES_WALL_*)
+ * that they and les_step use from now on (les_params.wall_model at
+ * creation). */
+int les_set_wall_model(les_state* s, int wall_model);
 /* compute_sgs.f90:105-247 sgs_stress(jt, jtt) */
 int les_sgs_stress(les_state* s, int jt, int jtt);
 /* testfilter.f90:144-184 test_filter(f, G) on levels 1..nz+1;

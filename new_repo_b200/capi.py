@@ -107,6 +107,7 @@ PROTOTYPES = {
     "les_upload_async": [_P, _I, C.c_void_p, _I, _I],
     "les_download_async": [_P, _I, C.c_void_p, _I, _I],
     "les_diagnostics_async": [_P, C.c_void_p],
+    "les_set_wall_model": [_P, _I],
     "les_step_host": [_P, _I, _I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "les_host_register": [C.c_void_p, C.c_size_t],
     "les_host_unregister": [C.c_void_p],

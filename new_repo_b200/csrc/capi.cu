@@ -200,6 +200,13 @@ int les_press_from_increment(les_state* s, double tadv1, double tadv2) {
   if (!(tadv1 != 0.0)) return bad_arg("tadv1");
   return guard([&] { s->s->press_from_increment(tadv1, tadv2); });
 }
+int les_set_wall_model(les_state* s, int wall_model) {
+  STATE_OR_FAIL(s);
+  if (wall_model != LES_WALL_FILTER && wall_model != LES_WALL_INST && wall_model != LES_WALL_HOMOG)
+    return bad_arg("wall_model");
+  s->s->P.wall_model = wall_model;
+  return LES_OK;
+}
 int les_obukhov(les_state* s) {
   STATE_OR_FAIL(s);
   return guard([&] { s->s->obukhov(); });

@@ -446,10 +446,24 @@ class LES:
         tadv2 = 1.0 - float(tadv1) if tadv2 is None else float(tadv2)
         check(self.lib.les_press_from_increment(self._h, float(tadv1), tadv2))
 
-    def obukhov(self):
+    def set_wall_model(self, wl_type: str):
+        """The wl_type argument of obukhov / wallstress ('wall_filter',
+        'wall_inst', 'wall_homog'), kept for later calls and les_step."""
+        if wl_type not in capi.WALL_MODELS:
+            raise LesError(capi.LES_ERR_INVALID, f"Invalid wall model: {wl_type!r}")
+        check(self.lib.les_set_wall_model(self._h, capi.WALL_MODELS[wl_type]))
+        self.params = replace(self.params, wall_model=wl_type)
+
+    def obukhov(self, wl_type: str | None = None):
+        """compute_wall_law.f90:198-254 obukhov(u_star_avg, wl_type)."""
+        if wl_type is not None:
+            self.set_wall_model(wl_type)
         check(self.lib.les_obukhov(self._h))
 
-    def wallstress(self):
+    def wallstress(self, wl_type: str | None = None):
+        """compute_wall_law.f90:107-185 wallstress(lbc_u, lbc_v, wl_type)."""
+        if wl_type is not None:
+            self.set_wall_model(wl_type)
         check(self.lib.les_wallstress(self._h))
 
     def sgs_stress(self, jt: int, jtt: int):

@@ -83,6 +83,21 @@ def test_wall_law(gpu, model):
     _assert_close(les, st, TOL["fp64"], f"wall law {model}")
 
 
+@pytest.mark.parametrize("model", ["wall_inst", "wall_homog"])
+def test_wall_law_model_argument(gpu, model):
+    """obukhov(ustar_avg, wl_type) / wallstress(bc_u, bc_v, wl_type): the
+    model passed per call (a state created with wall_filter) equals the
+    oracle run with that model."""
+    p = O.Params(nx=32, ny=32, nz=16, wall_model=model)
+    ops, st, les = _pair(O.Params(nx=32, ny=32, nz=16, wall_model="wall_filter"))
+    ops = O.Ops(p)
+    O.obukhov(ops, st)
+    O.wallstress(ops, st)
+    les.obukhov(model)
+    les.wallstress(model)
+    _assert_close(les, st, TOL["fp64"], f"wall law {model} by argument")
+
+
 @pytest.mark.parametrize("alpha", [2, 4])
 def test_test_filter(gpu, alpha):
     from tests.helpers import rel_err
