@@ -315,6 +315,7 @@ def run_ours(args, dist, rank, local, ws):
         train["check_profile_max_above_wall_band"] = {"level": kmax + 1,
                                                       "rms_log_error": round(float(prof_chk[kmax]), 4)}
         train["check_profile_levels_1_12"] = [round(float(x), 4) for x in prof_chk[:12]]
+        train["check_profile_top_12"] = [round(float(x), 4) for x in prof_chk[-12:]]
         train["check_after_steps"] = S
 
     # ---- end to end through the public API with pinned host buffers ----
@@ -360,7 +361,8 @@ def run_ours(args, dist, rank, local, ws):
                 "velocity_rms_rel_error": float(math.sqrt(num / den)),
                 "mean_profile_drift": float(np.abs(prof_m - prof_r).max() / np.abs(prof_r).max()),
                 "after_steps": S,
-                "per_field_error_of_headline": field_errors(snap, snap64)}
+                "per_field_error_of_headline": field_errors(snap, snap64),
+                "velocity_error_by_level_band": level_band_errors(snap, snap64)}
         if snap_l is not None:
             lasd["per_field_error_vs_fp64"] = field_errors(snap_l, snap64)
             lasd["after_steps"] = S
@@ -416,6 +418,20 @@ def field_errors(a: dict, b: dict) -> dict:
         d = a[n] - b[n]
         out[n] = {"rms_rel": float(np.sqrt((d * d).mean() / max((b[n] * b[n]).mean(), 1e-300))),
                   "max_rel": float(np.abs(d).max() / max(np.abs(b[n]).max(), 1e-300))}
+    return out
+
+
+def level_band_errors(a: dict, b: dict, nbands: int = 8) -> dict:
+    """Where the velocity differs: RMS of a - b over each of nbands equal bands
+    of levels (1..nz, bottom to top), relative to the RMS of b over all
+    levels, for u, v, w."""
+    import numpy as np
+
+    out = {}
+    for n in ("u", "v", "w"):
+        ref = max(float((b[n] * b[n]).mean()), 1e-300)
+        bands = np.array_split(np.arange(b[n].shape[0]), nbands)
+        out[n] = [round(float(np.sqrt(((a[n][k] - b[n][k]) ** 2).mean() / ref)), 5) for k in bands]
     return out
 
 
