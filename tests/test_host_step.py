@@ -86,3 +86,35 @@ def test_host_step_equals_the_device_step(gpu, precision, grid, mem):
     del keep
     ref.close()
     hs.close()
+
+
+def test_entry_points_after_host_step_see_its_copies(gpu, tmp_path):
+    """Without les_sync, a checkpoint write and a precision switch right after
+    les_step_host order themselves after its copies back: the checkpoint is
+    byte-equal to the device-resident run's and the switched state holds the
+    stepped fields."""
+    grid = (64, 32, 24)
+    nx, ny, nz = grid
+    ref, hs = _les("fp64", *grid), _les("fp64", *grid)
+    (u, v, w), diag, keep = _host_arrays((nz + 2, ny, nx), "pinned")
+    for a, n in zip((u, v, w), "uvw"):
+        a[...] = hs.download(n)
+    hs.step_host(u.ctypes.data, v.ctypes.data, w.ctypes.data, diag.ctypes.data, n=3)
+    ref.step(3)
+    (tmp_path / "hs").mkdir()
+    (tmp_path / "ref").mkdir()
+    f_hs = hs.checkpoint_out(tmp_path / "hs")
+    f_ref = ref.checkpoint_out(tmp_path / "ref")
+    assert f_hs.read_bytes() == f_ref.read_bytes()
+    hs.step_host(u.ctypes.data, v.ctypes.data, w.ctypes.data, diag.ctypes.data, n=2)
+    ref.step(2)
+    hs.set_precision("mixed")
+    ref.set_precision("mixed")
+    for n in ("u", "v", "w", "rhsx", "cs_opt2"):
+        np.testing.assert_array_equal(hs.download(n), ref.download(n), err_msg=n)
+    hs.sync()
+    for a, n in zip((u, v, w), "uvw"):
+        np.testing.assert_array_equal(a.astype(np.float32).astype(np.float64), hs.download(n), err_msg=n)
+    del keep
+    ref.close()
+    hs.close()
