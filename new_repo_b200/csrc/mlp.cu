@@ -157,67 +157,142 @@ __device__ __forceinline__ unsigned hash32(unsigned x) {
 }
 
 // --------------------------------------------------------- collection ----
+// Two passes over the same grid (MLP_COLLECT_BLOCKS x 256 threads).  Pass 0
+// takes the feature range of every point and counts each block's sampled
+// slots (m.boff[2 b + v], v = 1 for validation); k_mlp_collect_scan turns
+// the counts into each block's first slot after the pairs collected so far;
+// pass 1 writes a block's pairs from there, each thread's in its own point
+// order after the slots of the threads before it.  The slot of every pair
+// depends on the state alone, not on the order in which the blocks run.
 template <typename T>
-__global__ void k_mlp_collect(const MlpFeatIn<T> a, const T* cs, MlpDevice m, int stride, int dense_levels,
-                              int wall_repeat, unsigned seed) {
+__global__ void __launch_bounds__(256) k_mlp_collect(const MlpFeatIn<T> a, const T* cs, MlpDevice m, int stride,
+                                                     int dense_levels, int wall_repeat, unsigned seed, int pass) {
   const long n = (long)(a.nz + 1) * a.plane;
-  float lmin[8], lmax[8];
+  // whether point q (level k) is sampled, into which set, and how many slots
+  // it takes: every point of the lowest levels, elsewhere one in `stride`
+  // (seeded hash); 10 % held out; the training pairs of the two levels next
+  // to the wall, where the SGS stress carries the momentum flux, repeated
+  auto sample = [&](long q, int k, int& val) -> int {
+    const unsigned h = hash32(unsigned(q) * 2654435761u ^ seed);
+    const unsigned st = k <= dense_levels ? 1u : unsigned(stride);
+    if (h % st != 0) return 0;
+    val = ((h / st) % 10u) == 0u;
+    return (k <= 2 && !val) ? wall_repeat : 1;
+  };
+  unsigned long long cnt[2] = {0, 0};
+  if (pass == 0) {
+    float lmin[8], lmax[8];
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    lmin[i] = 3.0e38f;
-    lmax[i] = -3.0e38f;
+    for (int i = 0; i < 8; ++i) {
+      lmin[i] = 3.0e38f;
+      lmax[i] = -3.0e38f;
+    }
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+      const long o = a.plane + q;
+      const int k = udiv32(o, a.plane);
+      float t[8];
+      raw_features(a, o, k, t);  // every point: the range covers the whole state
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        lmin[i] = fminf(lmin[i], t[i]);
+        lmax[i] = fmaxf(lmax[i], t[i]);
+      }
+      // the current coefficient is the next update's previous coefficient
+      const float lcur = logf(fmaxf(float(cs[o]), 1e-6f));
+      lmin[5] = fminf(lmin[5], lcur);
+      lmax[5] = fmaxf(lmax[5], lcur);
+      int val = 0;
+      const int rep = sample(q, k, val);
+      cnt[val] += rep;
+    }
+    // feature range of the state: warp reduction, one atomic per warp and
+    // bound (min and max do not depend on the order)
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      float a0 = lmin[i], b0 = lmax[i];
+      for (int off = 16; off > 0; off >>= 1) {
+        a0 = fminf(a0, __shfl_down_sync(0xffffffffu, a0, off));
+        b0 = fmaxf(b0, __shfl_down_sync(0xffffffffu, b0, off));
+      }
+      if ((threadIdx.x & 31) == 0) {
+        atomicMin(&m.range[i], ordered_int(a0));
+        atomicMax(&m.range[8 + i], ordered_int(b0));
+      }
+    }
+    // the block's slot counts (integers: exact in any order)
+    __shared__ unsigned long long wc[8][2];
+    for (int v = 0; v < 2; ++v) {
+      unsigned long long c = cnt[v];
+      for (int off = 16; off > 0; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
+      if ((threadIdx.x & 31) == 0) wc[threadIdx.x >> 5][v] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+      unsigned long long c = 0;
+      for (int w = 0; w < int(blockDim.x >> 5); ++w) c += wc[w][threadIdx.x];
+      m.boff[2 * blockIdx.x + threadIdx.x] = c;
+    }
+    return;
+  }
+  // pass 1: this thread's first slots are the block's plus the slots of the
+  // threads before it
+  __shared__ unsigned long long tcnt[256][2];
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    int val = 0;
+    const int rep = sample(q, udiv32(a.plane + q, a.plane), val);
+    cnt[val] += rep;
+  }
+  tcnt[threadIdx.x][0] = cnt[0];
+  tcnt[threadIdx.x][1] = cnt[1];
+  __syncthreads();
+  unsigned long long idx[2] = {m.boff[2 * blockIdx.x], m.boff[2 * blockIdx.x + 1]};
+  for (int t = 0; t < int(threadIdx.x); ++t) {
+    idx[0] += tcnt[t][0];
+    idx[1] += tcnt[t][1];
   }
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
     const long o = a.plane + q;
     const int k = udiv32(o, a.plane);
+    int val = 0;
+    const int rep = sample(q, k, val);
+    if (rep == 0) continue;
     float t[8];
-    raw_features(a, o, k, t);  // every point: the range covers the whole state
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      lmin[i] = fminf(lmin[i], t[i]);
-      lmax[i] = fmaxf(lmax[i], t[i]);
-    }
-    // the current coefficient is the next update's previous coefficient
-    const float lcur = logf(fmaxf(float(cs[o]), 1e-6f));
-    lmin[5] = fminf(lmin[5], lcur);
-    lmax[5] = fmaxf(lmax[5], lcur);
-    const unsigned h = hash32(unsigned(q) * 2654435761u ^ seed);
-    const unsigned st = k <= dense_levels ? 1u : unsigned(stride);  // every point of the lowest levels
-    if (h % st != 0) continue;
+    raw_features(a, o, k, t);
     // target: the change of log Cs^2 over the update (residual form: the
     // network's identity part is exact, it learns the relaxation)
     const float y = fmaxf(logf(fmaxf(float(cs[o]), 1e-30f)), MLP_LOG_CS_FLOOR) - t[5];
-    const int val = ((h / st) % 10u) == 0u;  // 10 % held out
-    // the two levels next to the wall, where the SGS stress carries the
-    // momentum flux, enter the training set wall_repeat times
-    const int rep = (k <= 2 && !val) ? wall_repeat : 1;
-    const unsigned long long idx = atomicAdd(&m.counts[val], (unsigned long long)rep);
     for (int r = 0; r < rep; ++r) {
-      if ((long)(idx + r) >= m.cap) break;
-      float* x = (val ? m.vx : m.dx) + (idx + r) * MLP_IN;
+      if ((long)(idx[val] + r) >= m.cap) break;
+      float* x = (val ? m.vx : m.dx) + (idx[val] + r) * MLP_IN;
 #pragma unroll
       for (int i = 0; i < MLP_IN; ++i) x[i] = t[i];
-      (val ? m.vt : m.dt)[idx + r] = y;
+      (val ? m.vt : m.dt)[idx[val] + r] = y;
     }
+    idx[val] += rep;
   }
-  // feature range of the state: warp reduction, one atomic per warp and bound
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    float a0 = lmin[i], b0 = lmax[i];
-    for (int off = 16; off > 0; off >>= 1) {
-      a0 = fminf(a0, __shfl_down_sync(0xffffffffu, a0, off));
-      b0 = fmaxf(b0, __shfl_down_sync(0xffffffffu, b0, off));
+}
+
+// one thread: the blocks' counts of pass 0 become their first slots, after
+// the pairs already collected; m.counts gets the new totals
+__global__ void k_mlp_collect_scan(MlpDevice m, int nblocks) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int v = 0; v < 2; ++v) {
+    unsigned long long run = m.counts[v];
+    for (int b = 0; b < nblocks; ++b) {
+      const unsigned long long c = m.boff[2 * b + v];
+      m.boff[2 * b + v] = run;
+      run += c;
     }
-    if ((threadIdx.x & 31) == 0) {
-      atomicMin(&m.range[i], ordered_int(a0));
-      atomicMax(&m.range[8 + i], ordered_int(b0));
-    }
+    m.counts[v] = run;
   }
 }
 
 // statistics (double accumulators): sum, sum of squares, min, max of the 8
 // raw features and the target, over train + validation
-__global__ void __launch_bounds__(128) k_mlp_stats(const float* x, const float* t, long n, double* acc) {
+// part[18 b + i]: block b's sums (added on the host in block order, so the
+// statistics do not depend on the order in which blocks finish)
+__global__ void __launch_bounds__(128) k_mlp_stats(const float* x, const float* t, long n, double* acc,
+                                                   double* part) {
   __shared__ double s[18][128];
   __shared__ float mn[9][128], mx[9][128];
   double loc[18] = {0};
@@ -244,7 +319,7 @@ __global__ void __launch_bounds__(128) k_mlp_stats(const float* x, const float* 
   if (threadIdx.x < 18) {
     double v = 0;
     for (int j = 0; j < 128; ++j) v += s[threadIdx.x][j];
-    atomicAdd(&acc[threadIdx.x], v);
+    part[18 * blockIdx.x + threadIdx.x] = v;
   } else if (threadIdx.x >= 32 && threadIdx.x < 41) {
     const int i = threadIdx.x - 32;
     float a = 3.0e38f, b = -3.0e38f;
@@ -739,29 +814,56 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(MlpDevice m, const float* X,
   }
   // the weight gradients: thread r reads TMEM lane r (D row r); every warp
   // runs the same loads (tcgen05.ld is warp-collective)
-  if (!first && S.ok) {
+  // This CTA's gradient goes to its own row of m.gpart (every entry written
+  // by one thread; zeros when the CTA had no tile), summed over the CTAs in
+  // a fixed order by k_mlp_grad_reduce.
+  float* gp = m.gpart + (size_t)blockIdx.x * MLP_NP;
+  const bool have = !first && S.ok;
+  {
     float v[64];
-    tmem_row64(S.tmem, TM_W, v);
+    if (have) tmem_row64(S.tmem, TM_W, v);
     if (tid < 64)
-      for (int i = 0; i < 64; ++i) atomicAdd(&m.grad[MLP_O_W2 + tid * MLP_H + i], v[i]);  // dW2[tid][.]
+      for (int i = 0; i < 64; ++i) gp[MLP_O_W2 + tid * MLP_H + i] = have ? v[i] : 0.0f;  // dW2[tid][.]
     else if (tid == 72)
-      for (int i = 0; i < 64; ++i) atomicAdd(&m.grad[MLP_O_B2 + i], v[i]);
-    tmem_row64(S.tmem, TM_W + 64, v);
+      for (int i = 0; i < 64; ++i) gp[MLP_O_B2 + i] = have ? v[i] : 0.0f;
+    if (have) tmem_row64(S.tmem, TM_W + 64, v);
     if (tid >= 64 && tid < 72)
-      for (int i = 0; i < 64; ++i) atomicAdd(&m.grad[MLP_O_W1 + (tid - 64) * MLP_H + i], v[i]);  // dW1
+      for (int i = 0; i < 64; ++i) gp[MLP_O_W1 + (tid - 64) * MLP_H + i] = have ? v[i] : 0.0f;  // dW1
     else if (tid == 72)
-      for (int i = 0; i < 64; ++i) atomicAdd(&m.grad[MLP_O_B1 + i], v[i]);
-    tmem_row64(S.tmem, TM_W + 128, v);
+      for (int i = 0; i < 64; ++i) gp[MLP_O_B1 + i] = have ? v[i] : 0.0f;
+    if (have) tmem_row64(S.tmem, TM_W + 128, v);
     if (tid == 73)
-      for (int i = 0; i < 64; ++i) atomicAdd(&m.grad[MLP_O_W3 + i], v[i]);
+      for (int i = 0; i < 64; ++i) gp[MLP_O_W3 + i] = have ? v[i] : 0.0f;
   }
   // a weight GEMM whose wait ran out may still be in flight: wait (bounded)
   // for it before the TMEM is freed
   if (tid == 0 && !S.ok && wfail) tc::mbar_wait(&TS.wbar, wphase ^ 1u);
   tc_teardown(S, 512, phase);
-  if (tid == 0) atomicAdd(&m.grad[MLP_O_B3], ab3);
+  if (tid == 0) gp[MLP_O_B3] = ab3;
   for (int off = 16; off > 0; off >>= 1) aloss += __shfl_down_sync(0xffffffffu, aloss, off);
-  if ((tid & 31) == 0 && loss) atomicAdd(loss, aloss);
+  __syncthreads();  // the last tile's reads of dsum (ab3) are done: reuse it for the warps' losses
+  if ((tid & 31) == 0) TS.dsum[tid >> 5] = aloss;
+  __syncthreads();
+  if (tid == 0) {
+    float l = 0.0f;
+    for (int w = 0; w < TILE / 32; ++w) l += TS.dsum[w];
+    m.lpart[blockIdx.x] = l;
+  }
+}
+
+// m.grad = the sum of the CTAs' gradient rows, CTA by CTA in index order;
+// *loss (when given) the same sum of their losses
+__global__ void k_mlp_grad_reduce(MlpDevice m, int nctas, float* loss) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < MLP_NP; i += gridDim.x * blockDim.x) {
+    float g = 0.0f;
+    for (int b = 0; b < nctas; ++b) g += m.gpart[(size_t)b * MLP_NP + i];
+    m.grad[i] = g;
+  }
+  if (loss && blockIdx.x == 0 && threadIdx.x == 0) {
+    float l = 0.0f;
+    for (int b = 0; b < nctas; ++b) l += m.lpart[b];
+    *loss = l;
+  }
 }
 
 __global__ void k_mlp_adam(float* p, const float* g, float* mm, float* vv, int step, float lr) {
@@ -805,9 +907,16 @@ __global__ void k_mlp_blend(T* cs, const T* cs_dyn, const int* flag, long plane,
     }
     if (flag[p]) cs[o] = cs_dyn[o];
   }
-  if (check) {
+  if (check) {  // the block's sum, warps in order: err2[k * gridDim.x + blockIdx.x]
+    __shared__ double we[8];
     for (int off = 16; off > 0; off >>= 1) e += __shfl_down_sync(0xffffffffu, e, off);
-    if ((threadIdx.x & 31) == 0) atomicAdd(&err2[k], e);
+    if ((threadIdx.x & 31) == 0) we[threadIdx.x >> 5] = e;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double b = 0.0;
+      for (int w = 0; w < int(blockDim.x >> 5); ++w) b += we[w];
+      err2[(long)k * gridDim.x + blockIdx.x] = b;
+    }
   }
 }
 
@@ -822,7 +931,15 @@ void mlp_collect(const MlpFeatIn<T>& in, const T* cs, MlpDevice& m, int stride, 
                  unsigned seed, cudaStream_t st) {
   const long n = (long)(in.nz + 1) * in.plane;
   hook_before("k_mlp_collect", double(n) * 11 * sizeof(T));
-  k_mlp_collect<T><<<148 * 8, 256, 0, st>>>(in, cs, m, stride, dense_levels, wall_repeat, seed);
+  k_mlp_collect<T><<<MLP_COLLECT_BLOCKS, 256, 0, st>>>(in, cs, m, stride, dense_levels, wall_repeat, seed, 0);
+  LES_CHECK_LAUNCH();
+  hook_after();
+  hook_before("k_mlp_collect_scan", 32.0 * MLP_COLLECT_BLOCKS);
+  k_mlp_collect_scan<<<1, 32, 0, st>>>(m, MLP_COLLECT_BLOCKS);
+  LES_CHECK_LAUNCH();
+  hook_after();
+  hook_before("k_mlp_collect", double(n) * 11 * sizeof(T));
+  k_mlp_collect<T><<<MLP_COLLECT_BLOCKS, 256, 0, st>>>(in, cs, m, stride, dense_levels, wall_repeat, seed, 1);
   LES_CHECK_LAUNCH();
   hook_after();
 }
@@ -867,12 +984,14 @@ void mlp_pack(MlpDevice& m, cudaStream_t st) {
 
 void mlp_grad(MlpDevice& m, const float* x, const float* t, long n, float* y_out, float* loss_dev, unsigned* status,
               cudaStream_t st, MlpPerm perm) {
-  LES_CUDA(cudaMemsetAsync(m.grad, 0, sizeof(float) * MLP_NP, st));
-  if (loss_dev) LES_CUDA(cudaMemsetAsync(loss_dev, 0, sizeof(float), st));
   const long ntiles = (n + TILE - 1) / TILE;
-  const int grid = int(std::max<long>(1, std::min<long>(ntiles, 148L)));
+  const int grid = int(std::max<long>(1, std::min<long>(ntiles, (long)MLP_TRAIN_CTAS)));
   hook_before("k_mlp_train", double(n) * 36.0);
   k_mlp_train<<<grid, TILE, train_smem(), st>>>(m, x, t, n, 1.0f / float(n), y_out, loss_dev, status, perm);
+  LES_CHECK_LAUNCH();
+  hook_after();
+  hook_before("k_mlp_grad_reduce", double(grid + 1) * MLP_NP * 4.0);
+  k_mlp_grad_reduce<<<19, 256, 0, st>>>(m, grid, loss_dev);
   LES_CHECK_LAUNCH();
   hook_after();
 }
@@ -891,8 +1010,9 @@ void mlp_fit_stats(MlpDevice& m, cudaStream_t st) {
   LES_CUDA(cudaStreamSynchronize(st));
   const long nt = std::min<long>((long)cnt[0], m.cap), nv = std::min<long>((long)cnt[1], m.cap);
   if (nt < 2) throw CudaError(1, "learned closure: no training data collected");
+  constexpr int SB = 148;  // blocks of k_mlp_stats
   double* acc = nullptr;
-  LES_CUDA(cudaMalloc(&acc, 36 * sizeof(double)));
+  LES_CUDA(cudaMalloc(&acc, (36 + 18 * SB) * sizeof(double)));
   std::vector<double> init(36, 0.0);
   // min slots start at +max, max slots at -max (order-preserving ints)
   for (int i = 0; i < 9; ++i) {
@@ -901,12 +1021,16 @@ void mlp_fit_stats(MlpDevice& m, cudaStream_t st) {
     std::memcpy(&init[27 + i], &neg, sizeof(int));
   }
   LES_CUDA(cudaMemcpyAsync(acc, init.data(), 36 * sizeof(double), cudaMemcpyHostToDevice, st));
-  k_mlp_stats<<<148, 128, 0, st>>>(m.dx, m.dt, nt, acc);
+  k_mlp_stats<<<SB, 128, 0, st>>>(m.dx, m.dt, nt, acc, acc + 36);
   LES_CHECK_LAUNCH();
-  std::vector<double> h(36);
-  LES_CUDA(cudaMemcpyAsync(h.data(), acc, 36 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  std::vector<double> h(36 + 18 * SB);
+  LES_CUDA(cudaMemcpyAsync(h.data(), acc, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
   LES_CUDA(cudaStreamSynchronize(st));
   cudaFree(acc);
+  for (int i = 0; i < 18; ++i) {
+    h[i] = 0.0;
+    for (int b = 0; b < SB; ++b) h[i] += h[36 + 18 * b + i];
+  }
   // feature range: the sampled pairs and every point of the collected states
   int rg[16];
   LES_CUDA(cudaMemcpyAsync(rg, m.range, sizeof(rg), cudaMemcpyDeviceToHost, st));
@@ -965,16 +1089,22 @@ int mlp_count_flags(MlpDevice& m, int* dcount, int* per_feature, cudaStream_t st
 template <typename T>
 void mlp_blend(T* cs, const T* cs_dyn, MlpDevice& m, int nz, bool check, double* derr, double* profile,
                cudaStream_t st) {
-  LES_CUDA(cudaMemsetAsync(derr, 0, sizeof(double) * (nz + 2), st));
+  constexpr int NB = MLP_BLEND_BLOCKS;
+  LES_CUDA(cudaMemsetAsync(derr, 0, sizeof(double) * NB * (nz + 2), st));
   const long n = (long)(nz + 1) * m.plane;
   hook_before("k_mlp_blend", double(n) * 3 * sizeof(T));
-  k_mlp_blend<T><<<dim3(4, nz + 1), 256, 0, st>>>(cs, cs_dyn, m.colflag, m.plane, derr, check ? 1 : 0);
+  k_mlp_blend<T><<<dim3(NB, nz + 1), 256, 0, st>>>(cs, cs_dyn, m.colflag, m.plane, derr, check ? 1 : 0);
   LES_CHECK_LAUNCH();
   hook_after();
   if (check) {
-    LES_CUDA(cudaMemcpyAsync(profile, derr, sizeof(double) * (nz + 2), cudaMemcpyDeviceToHost, st));
+    std::vector<double> h((size_t)NB * (nz + 2));
+    LES_CUDA(cudaMemcpyAsync(h.data(), derr, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
     LES_CUDA(cudaStreamSynchronize(st));
-    for (int k = 0; k <= nz + 1; ++k) profile[k] = std::sqrt(profile[k] / double(m.plane));
+    for (int k = 0; k <= nz + 1; ++k) {
+      double e = 0.0;
+      for (int b = 0; b < NB; ++b) e += h[(size_t)k * NB + b];  // blocks in order
+      profile[k] = std::sqrt(e / double(m.plane));
+    }
   }
 }
 template void mlp_blend<float>(float*, const float*, MlpDevice&, int, bool, double*, double*, cudaStream_t);

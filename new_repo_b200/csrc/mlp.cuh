@@ -43,6 +43,10 @@ struct MlpFeatIn {
   float cs_max = 1.0f;  // upper clip of the coefficient
 };
 
+constexpr int MLP_COLLECT_BLOCKS = 148 * 8;  // grid of both collection passes
+constexpr int MLP_TRAIN_CTAS = 148;          // most CTAs of a training launch
+constexpr int MLP_BLEND_BLOCKS = 4;          // blocks per level of the check's error sums
+
 struct MlpDevice {
   float* params = nullptr;     // MLP_NP master weights
   float* stats = nullptr;      // MLP_NS
@@ -56,6 +60,11 @@ struct MlpDevice {
   float* vt = nullptr;
   unsigned long long* counts = nullptr;  // [0] train, [1] validation
   long cap = 0;
+  // fixed-order reductions (training is deterministic: no floating-point
+  // atomics and no atomically assigned sample slots)
+  unsigned long long* boff = nullptr;  // collection: per block (train, validation) count, then first slot
+  float* gpart = nullptr;      // training: per CTA gradient [MLP_TRAIN_CTAS][MLP_NP]
+  float* lpart = nullptr;      // training: per CTA loss [MLP_TRAIN_CTAS]
   float* scratch = nullptr;    // forward outputs of the host-features path
   int* colflag = nullptr;      // per (i,j) column: bit i = feature i left the training range
   int* range = nullptr;        // raw feature min[8], max[8] of the collected states (order-preserving ints)
@@ -97,7 +106,7 @@ void mlp_adam(MlpDevice& m, int step, float lr, cudaStream_t st);
 int mlp_count_flags(MlpDevice& m, int* dcount, int* per_feature, cudaStream_t st);
 // replace flagged columns of cs by cs_dyn; with check, profile[k] (host,
 // nz + 2 values) gets the RMS over level k of log(cs) - log(cs_dyn), both
-// floored at 1e-6 (derr: nz + 2 device doubles)
+// floored at 1e-6 (derr: MLP_BLEND_BLOCKS * (nz + 2) device doubles)
 template <typename T>
 void mlp_blend(T* cs, const T* cs_dyn, MlpDevice& m, int nz, bool check, double* derr, double* profile,
                cudaStream_t st);

@@ -422,9 +422,12 @@ class Solver final : public SolverBase {
     md.colflag = track(dalloc<int>(g.plane()));
     md.range = track(dalloc<int>(16));
     md.counts = track(dalloc<unsigned long long>(2));
+    md.boff = track(dalloc<unsigned long long>(2 * MLP_COLLECT_BLOCKS));
+    md.gpart = track(dalloc<float>((size_t)MLP_TRAIN_CTAS * MLP_NP));
+    md.lpart = track(dalloc<float>(MLP_TRAIN_CTAS));
     md.plane = g.plane();
     dcount = track(dalloc<int>(9));
-    derr = track(dalloc<double>(g.L));
+    derr = track(dalloc<double>((size_t)MLP_BLEND_BLOCKS * g.L));
     mlp_profile.assign(g.L, -1.0);
     cs_prev = track(dalloc<T>(g.field()));
     init_mlp_attributes();

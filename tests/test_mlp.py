@@ -127,6 +127,44 @@ def test_mlp_gradient_matches_oracle(gpu, n):
     les.close()
 
 
+@pytest.mark.gpu
+def test_mlp_training_is_deterministic(gpu):
+    """The same state, collection and training give the same closure bit for
+    bit: collected pairs take slots fixed by the state (no atomic counter),
+    and the normalisation sums, the per-CTA weight gradients and the losses
+    are added in a fixed order (no floating-point atomics)."""
+    from new_repo_b200 import log_law_noise
+
+    def run():
+        les = _les(nx=64, ny=64, nz=32, sgs="dyn_LagScaleDep")
+        les.set_initial_conditions(*log_law_noise(les.params, seed=7))
+        les.mlp_init(0)
+        les.mlp_reset_data(1 << 20)
+        while les.jt_total < 30:
+            les.step(1)
+            if les.jt_total >= 5 and les.jt_total % 5 == 0:
+                les.mlp_collect(stride=3, seed=les.jt_total, dense_levels=4, wall_repeat=3)
+        counts = les.mlp_counts()
+        les.mlp_fit_stats()
+        losses, val = les.mlp_train(epochs=3, tiles_per_step=4, lr=2e-3)
+        params = les.mlp_params().copy()
+        # one gradient over fewer tiles than CTAs, twice
+        rng = np.random.default_rng(8)
+        x = rng.normal(size=(1000, 8)).astype(np.float32)
+        t = rng.normal(size=1000).astype(np.float32)
+        g1, l1 = les.mlp_grad(x, t)
+        g2, l2 = les.mlp_grad(x, t)
+        np.testing.assert_array_equal(g1, g2)
+        assert l1 == l2
+        les.close()
+        return counts, losses, val, params
+
+    a, b = run(), run()
+    assert a[0] == b[0] and a[0][0] > 10000
+    assert list(a[1]) == list(b[1]) and a[2] == b[2]
+    np.testing.assert_array_equal(a[3], b[3])
+
+
 def _fields(les):
     names = ("dudx", "dudy", "dudz", "dvdx", "dvdy", "dvdz", "dwdx", "dwdy", "dwdz")
     return {n: les.download(n) for n in names}
