@@ -716,11 +716,24 @@ __global__ void k_projection(T* u, T* v, T* w, T* rx, T* ry, T* rz, const T* dpd
 // p = fluctuation + FP64 mean profile (mixed precision only), p(nz+1) = BOGUS
 template <typename T>
 __global__ void k_p_finish(T* p, const double* pmean, long plane, int nz) {
-  const long n = (long)(nz + 2) * plane;
-  for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n; o += (long)gridDim.x * blockDim.x) {
-    const int k = udiv32(o, plane);
-    if (k == nz + 1) p[o] = T(BOGUS);
-    else if (pmean) p[o] = T(double(p[o]) + pmean[k]);
+  const long top = (long)(nz + 1) * plane;
+  const long t0 = blockIdx.x * (long)blockDim.x + threadIdx.x, ts = (long)gridDim.x * blockDim.x;
+  for (long q = t0; q < plane; q += ts) p[top + q] = T(BOGUS);
+  if (!pmean) return;
+  // levels 0..nz: the FP64 mean mode added back, four consecutive points of
+  // one level per thread and iteration where the plane allows
+  if (plane % 4 == 0) {
+    for (long q4 = t0; q4 < top / 4; q4 += ts) {
+      const long o = 4 * q4;
+      const double m = pmean[udiv32(o, plane)];
+      T a[4];
+      ld4(p + o, a);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = T(double(a[i]) + m);
+      st4(p + o, a);
+    }
+  } else {
+    for (long o = t0; o < top; o += ts) p[o] = T(double(p[o]) + pmean[udiv32(o, plane)]);
   }
 }
 
@@ -997,8 +1010,26 @@ __global__ void __launch_bounds__(256) k_diag_partial(const T* u, const T* v, co
       ld4(dudx + o, DX);
       ld4(dvdy + o, DY);
       ld4(dwdz + o, DZ);
+      // the four points' values summed in plain FP64, then one compensated
+      // addition per sum (the compensated sum is the cost, not the loads)
+      double su = 0.0, sv = 0.0, sw = 0.0, sd = 0.0;
 #pragma unroll
-      for (int i = 0; i < 4; ++i) point(U[i], V[i], W[i], WU[i], DX[i], DY[i], DZ[i]);
+      for (int i = 0; i < 4; ++i) {
+        const double uu = U[i], vv = V[i], ww = W[i];
+        nan |= (uu != uu) | (vv != vv) | (ww != ww);
+        a.mx[0] = fmax(a.mx[0], fabs(uu));
+        a.mx[1] = fmax(a.mx[1], fabs(vv));
+        a.mx[2] = fmax(a.mx[2], fabs(ww));
+        su += uu;
+        sv += vv;
+        sw += 0.5 * (ww + double(WU[i]));
+        const double dv = double(DX[i]) + double(DY[i]) + double(DZ[i]);
+        sd += dv * dv;
+      }
+      a.sum[0].add(su);
+      a.sum[1].add(sv);
+      a.sum[2].add(sw);
+      a.sum[3].add(sd);
     }
   } else {
     for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {

@@ -1468,7 +1468,7 @@ class Solver final : public SolverBase {
       launch_xinv<T>(g.nx, h, st);
       dpdz_only();
       KL("k_p_finish", 2.0 * g.field() * sizeof(T),
-         k_p_finish<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_P], pmean, g.plane(), nz));
+         k_p_finish<T><<<grid_for(g.field() / 4), 256, 0, st>>>(F[LES_P], pmean, g.plane(), nz));
       return;
     }
     if (pslabs > 1)
@@ -1499,7 +1499,7 @@ class Solver final : public SolverBase {
     launch_xinv<S>(g.nx, h, st);
     // dpdz (compute_pressure.f90:359-369), then p(nz+1) = BOGUS (:353-357)
     dpdz_only();
-    KL("k_p_finish", (mixed() ? 2.0 * g.field() : double(g.plane())) * sizeof(T), k_p_finish<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_P], mixed() ? pmean : nullptr, g.plane(), nz));
+    KL("k_p_finish", (mixed() ? 2.0 * g.field() : double(g.plane())) * sizeof(T), k_p_finish<T><<<grid_for(g.field() / 4), 256, 0, st>>>(F[LES_P], mixed() ? pmean : nullptr, g.plane(), nz));
   }
   double press_tadv1_ = 1.0;
   void dpdz_only();
@@ -1623,7 +1623,7 @@ class Solver final : public SolverBase {
     launch_xinv<T>(g.nx, h, st);
     dpdz_only();
     KL("k_p_finish", (mixed() ? 2.0 * g.field() : double(g.plane())) * sizeof(T),
-       k_p_finish<T><<<grid_for(g.field()), 256, 0, st>>>(F[LES_P], mixed() ? pmean : nullptr, g.plane(), nz));
+       k_p_finish<T><<<grid_for(g.field() / 4), 256, 0, st>>>(F[LES_P], mixed() ? pmean : nullptr, g.plane(), nz));
   }
 
 
@@ -2181,15 +2181,27 @@ class Solver final : public SolverBase {
 template <typename T>
 __global__ void k_dpdz(T* dpdz, const T* p, long plane, int nz, T rdz, const double* pmean) {
   const long n = (long)nz * plane;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
-    const long o = plane + q;
-    const int k = int(o / plane);
-    if (pmean) {
-      // p holds the fluctuation only (mean mode dropped from the FP32
-      // transform); the mean-mode difference is taken in FP64
-      dpdz[o] = T(double(rdz * (p[o] - p[o - plane])) + double(rdz) * (pmean[k] - pmean[k - 1]));
-    } else {
-      dpdz[o] = rdz * (p[o] - p[o - plane]);
+  const long t0 = blockIdx.x * (long)blockDim.x + threadIdx.x, ts = (long)gridDim.x * blockDim.x;
+  // p holds the fluctuation only in mixed precision (mean mode dropped from
+  // the FP32 transform); the mean-mode difference is taken in FP64
+  auto one = [&](T a, T b, double dm) -> T { return pmean ? T(double(rdz * (a - b)) + dm) : rdz * (a - b); };
+  if (plane % 4 == 0) {  // four consecutive points of one level per thread and iteration
+    for (long q4 = t0; q4 < n / 4; q4 += ts) {
+      const long o = plane + 4 * q4;
+      const int k = udiv32(o, plane);
+      const double dm = pmean ? double(rdz) * (pmean[k] - pmean[k - 1]) : 0.0;
+      T a[4], b[4], r[4];
+      ld4(p + o, a);
+      ld4(p + o - plane, b);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r[i] = one(a[i], b[i], dm);
+      st4(dpdz + o, r);
+    }
+  } else {
+    for (long q = t0; q < n; q += ts) {
+      const long o = plane + q;
+      const int k = udiv32(o, plane);
+      dpdz[o] = one(p[o], p[o - plane], pmean ? double(rdz) * (pmean[k] - pmean[k - 1]) : 0.0);
     }
   }
 }
@@ -2197,7 +2209,7 @@ __global__ void k_dpdz(T* dpdz, const T* p, long plane, int nz, T rdz, const dou
 template <typename T>
 void Solver<T>::dpdz_only() {
   const bool mixed = (P.precision == LES_MIXED);
-  KL("k_dpdz", 2.0 * g.nz * g.plane() * sizeof(T), k_dpdz<T><<<grid_for((long)g.nz * g.plane()), 256, 0, st>>>(F[LES_DPDZ], F[LES_P], g.plane(), g.nz,
+  KL("k_dpdz", 2.0 * g.nz * g.plane() * sizeof(T), k_dpdz<T><<<grid_for((long)g.nz * g.plane() / 4), 256, 0, st>>>(F[LES_DPDZ], F[LES_P], g.plane(), g.nz,
                                                              T(1.0 / dz()), mixed ? pmean : nullptr));
 }
 
