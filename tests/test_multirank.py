@@ -61,3 +61,25 @@ def test_max_over_ranks_gloo():
         assert p.exitcode == 0
     got = sorted(q.get(timeout=10) for _ in range(2))
     assert got == [(0, 20.0), (1, 20.0)]
+
+
+def test_bench_error_helpers():
+    """bench.py's precision comparison: per-field RMS / max relative errors
+    and the velocity error by bands of levels, on known arrays."""
+    import numpy as np
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    rng = np.random.default_rng(0)
+    b = {n: rng.normal(size=(16, 4, 4)) for n in bench.COMPARED}
+    a = {n: b[n].copy() for n in bench.COMPARED}
+    a["u"][12:] += 0.5  # levels 13..16 of 16: the top band of four
+    err = bench.field_errors(a, b)
+    assert err["v"] == {"rms_rel": 0.0, "max_rel": 0.0}
+    rms_b = np.sqrt((b["u"] ** 2).mean())
+    assert abs(err["u"]["rms_rel"] - np.sqrt(0.25 * 0.25) / rms_b) < 1e-12
+    bands = bench.level_band_errors(a, b, nbands=4)
+    assert bands["v"] == [0.0] * 4 and bands["w"] == [0.0] * 4
+    assert bands["u"][:3] == [0.0] * 3
+    assert abs(bands["u"][3] - round(0.5 / rms_b, 5)) < 1e-12
