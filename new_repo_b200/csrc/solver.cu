@@ -144,7 +144,8 @@ class Solver final : public SolverBase {
       if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : {ev_go, ev_in, ev_done, ev_copies})
       if (e) cudaEventDestroy(e);
-    for (auto e : ev_out) cudaEventDestroy(e);
+    for (auto* v : {&ev_out, &ev_inc, &ev_cvt})
+      for (auto e : *v) cudaEventDestroy(e);
     for (cudaStream_t s : {sh2d, sd2h})
       if (s) cudaStreamDestroy(s);
     if (st) cudaStreamDestroy(st);
@@ -960,10 +961,13 @@ class Solver final : public SolverBase {
   // device levels), so that one call's copies back and the next call's
   // copies in run at the same time, one in each direction of the link.
   // Mixed precision stages the FP64 values in device buffers (one set per
-  // direction) and converts on st.
+  // direction) and converts on st chunk by chunk: a chunk in as soon as it
+  // has arrived, a chunk out just before its copy back.
   cudaStream_t sh2d = nullptr, sd2h = nullptr;
   cudaEvent_t ev_go = nullptr, ev_in = nullptr, ev_done = nullptr;
   std::vector<cudaEvent_t> ev_out;  // per (field, chunk): copy back done
+  std::vector<cudaEvent_t> ev_inc;  // per (field, chunk): copy in done (mixed precision)
+  std::vector<cudaEvent_t> ev_cvt;  // per (field, chunk): converted for the copy back (mixed)
   bool out_recorded = false;
   double* stage_in[3] = {};
   double* stage_out[3] = {};
@@ -977,8 +981,10 @@ class Solver final : public SolverBase {
     const long pb = g.plane() * (long)sizeof(double);
     chunk_lev = int(std::max(1L, (16L << 20) / pb));
     nchunk = (g.L + chunk_lev - 1) / chunk_lev;
-    ev_out.assign(3 * nchunk, nullptr);
-    for (auto& e : ev_out) LES_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto* v : {&ev_out, &ev_inc, &ev_cvt}) {
+      v->assign(3 * nchunk, nullptr);
+      for (auto& e : *v) LES_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
     if (mixed())
       for (int q = 0; q < 3; ++q) {
         stage_in[q] = track(dalloc<double>(g.field()));
@@ -990,47 +996,78 @@ class Solver final : public SolverBase {
     if (!sh2d) setup_host_pipe();
     double* h[3] = {u, v, w};
     const int fid[3] = {LES_U, LES_V, LES_W};
-    auto dev = [&](int q) -> double* {
-      if constexpr (std::is_same<T, double>::value) return F[fid[q]];
+    constexpr bool f64 = std::is_same<T, double>::value;
+    auto dev_in = [&](int q) -> double* {
+      if constexpr (f64) return F[fid[q]];
       else return stage_in[q];
     };
     auto dev_out = [&](int q) -> const double* {
-      if constexpr (std::is_same<T, double>::value) return F[fid[q]];
+      if constexpr (f64) return F[fid[q]];
       else return stage_out[q];
+    };
+    auto chunk = [&](int c, int& k0, long& n) {
+      k0 = c * chunk_lev;
+      n = (long)(std::min(g.L, k0 + chunk_lev) - k0) * g.plane();
     };
     // the copies in follow everything queued on st before this call
     LES_CUDA(cudaEventRecord(ev_go, st));
     LES_CUDA(cudaStreamWaitEvent(sh2d, ev_go, 0));
     for (int q = 0; q < 3; ++q)
       for (int c = 0; c < nchunk; ++c) {
-        const int k0 = c * chunk_lev, k1 = std::min(g.L, k0 + chunk_lev);
+        int k0;
+        long n;
+        chunk(c, k0, n);
         if (out_recorded) LES_CUDA(cudaStreamWaitEvent(sh2d, ev_out[q * nchunk + c], 0));
-        LES_CUDA(cudaMemcpyAsync(dev(q) + k0 * g.plane(), h[q] + k0 * g.plane(),
-                                 (k1 - k0) * g.plane() * sizeof(double), cudaMemcpyHostToDevice, sh2d));
+        LES_CUDA(cudaMemcpyAsync(dev_in(q) + k0 * g.plane(), h[q] + k0 * g.plane(), n * sizeof(double),
+                                 cudaMemcpyHostToDevice, sh2d));
+        if constexpr (!f64) LES_CUDA(cudaEventRecord(ev_inc[q * nchunk + c], sh2d));
       }
-    LES_CUDA(cudaEventRecord(ev_in, sh2d));
-    LES_CUDA(cudaStreamWaitEvent(st, ev_in, 0));
-    if constexpr (!std::is_same<T, double>::value) {
+    if constexpr (f64) {
+      LES_CUDA(cudaEventRecord(ev_in, sh2d));
+      LES_CUDA(cudaStreamWaitEvent(st, ev_in, 0));
+    } else {
+      // each chunk converted as soon as it has arrived, while the rest copy
       Tag tag_(this, "io");
-      Convert3<T, double> a{{F[LES_U], F[LES_V], F[LES_W]}, {stage_in[0], stage_in[1], stage_in[2]}};
-      KL("k_convert3", 36.0 * g.field(), k_convert3<T, double><<<dim3(grid_for(g.field()), 3), 256, 0, st>>>(a, g.field()));
+      for (int q = 0; q < 3; ++q)
+        for (int c = 0; c < nchunk; ++c) {
+          int k0;
+          long n;
+          chunk(c, k0, n);
+          LES_CUDA(cudaStreamWaitEvent(st, ev_inc[q * nchunk + c], 0));
+          KL("k_convert", 12.0 * n, k_convert<T, double><<<grid_for(n), 256, 0, st>>>(
+                                        lev(F[fid[q]], k0), stage_in[q] + k0 * g.plane(), n));
+        }
     }
-    step(jt, jtt);  // ends with the diagnostics of the new state in dout
-    if constexpr (!std::is_same<T, double>::value) {
-      Tag tag_(this, "io");
-      Convert3<double, T> a{{stage_out[0], stage_out[1], stage_out[2]}, {F[LES_U], F[LES_V], F[LES_W]}};
-      KL("k_convert3", 36.0 * g.field(), k_convert3<double, T><<<dim3(grid_for(g.field()), 3), 256, 0, st>>>(a, g.field()));
+    step_body(jt, jtt, false);
+    if constexpr (f64) {
+      LES_CUDA(cudaEventRecord(ev_done, st));
+      LES_CUDA(cudaStreamWaitEvent(sd2h, ev_done, 0));
     }
-    LES_CUDA(cudaEventRecord(ev_done, st));
-    LES_CUDA(cudaStreamWaitEvent(sd2h, ev_done, 0));
-    if (diag4) LES_CUDA(cudaMemcpyAsync(diag4, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, sd2h));
     for (int q = 0; q < 3; ++q)
       for (int c = 0; c < nchunk; ++c) {
-        const int k0 = c * chunk_lev, k1 = std::min(g.L, k0 + chunk_lev);
-        LES_CUDA(cudaMemcpyAsync(h[q] + k0 * g.plane(), dev_out(q) + k0 * g.plane(),
-                                 (k1 - k0) * g.plane() * sizeof(double), cudaMemcpyDeviceToHost, sd2h));
+        int k0;
+        long n;
+        chunk(c, k0, n);
+        if constexpr (!f64) {  // the copy back of a chunk starts once that chunk is converted
+          Tag tag_(this, "io");
+          KL("k_convert", 12.0 * n, k_convert<double, T><<<grid_for(n), 256, 0, st>>>(
+                                        stage_out[q] + k0 * g.plane(), lev(F[fid[q]], k0), n));
+          LES_CUDA(cudaEventRecord(ev_cvt[q * nchunk + c], st));
+          LES_CUDA(cudaStreamWaitEvent(sd2h, ev_cvt[q * nchunk + c], 0));
+        }
+        LES_CUDA(cudaMemcpyAsync(h[q] + k0 * g.plane(), dev_out(q) + k0 * g.plane(), n * sizeof(double),
+                                 cudaMemcpyDeviceToHost, sd2h));
         LES_CUDA(cudaEventRecord(ev_out[q * nchunk + c], sd2h));
       }
+    // the step's diagnostics, on st while the copies back run; they rewrite
+    // dout, so they follow the previous call's copy of it (long done)
+    if (out_recorded) LES_CUDA(cudaStreamWaitEvent(st, ev_copies, 0));
+    diagnostics_launch();
+    if (diag4) {
+      LES_CUDA(cudaEventRecord(ev_done, st));
+      LES_CUDA(cudaStreamWaitEvent(sd2h, ev_done, 0));
+      LES_CUDA(cudaMemcpyAsync(diag4, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, sd2h));
+    }
     out_recorded = true;
     LES_CUDA(cudaEventRecord(ev_copies, sd2h));
     copies_pending = true;
@@ -2111,7 +2148,10 @@ class Solver final : public SolverBase {
                                                         g.plane(), g.nz, P.dt * tadv1));
   }
 
-  void step(int jt, int jtt) override {
+  void step(int jt, int jtt) override { step_body(jt, jtt, true); }
+  // with_diag false: the caller launches the diagnostics itself (step_host,
+  // after the copies back have started)
+  void step_body(int jt, int jtt, bool with_diag) {
     LES_CUDA(cudaEventRecord(ev[0], st));
     if (P.wall_law) wall_layer();  // obukhov + wallstress (same filtered layer)
     compute_vel_grad();
@@ -2137,7 +2177,7 @@ class Solver final : public SolverBase {
     LES_CUDA(cudaEventRecord(ev[4], st));
     projection(t1);
     set_bc();
-    diagnostics_launch();
+    if (with_diag) diagnostics_launch();
     LES_CUDA(cudaEventRecord(ev[5], st));
     timed = true;
   }
