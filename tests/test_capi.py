@@ -55,6 +55,7 @@ def test_null_arguments_return_invalid(lib):
     assert lib.les_step_host(None, 1, 1, None, None, None, None) == capi.LES_ERR_INVALID
     assert lib.les_host_register(None, 8) == capi.LES_ERR_INVALID
     assert lib.les_host_unregister(None) == capi.LES_ERR_INVALID
+    assert lib.les_set_wall_model(None, 0) == capi.LES_ERR_INVALID
 
 
 def test_invalid_model_is_rejected_before_device_use(lib):
