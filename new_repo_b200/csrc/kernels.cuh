@@ -457,26 +457,26 @@ struct LagGeom {
   int nlev;  // levels 1..nlev are interpolated (nz + 1: all)
 };
 
-// FF(i, j, k) of compute_interpolag_coeff (1-based i, j; level k in 0..nz+2)
-// as update_halo3 (decomp_2d_custom.f90:902-1024) and the overrides of
-// compute_LagScaleDep.f90:441-452 leave it.
-template <typename T>
-__device__ __forceinline__ T ff_at(const T* F, int i, int j, int k, const LagGeom& g) {
+// Offset of FF(i, j, k) of compute_interpolag_coeff (1-based i, j; level k
+// in 0..nz+2) as update_halo3 (decomp_2d_custom.f90:902-1024) and the
+// overrides of compute_LagScaleDep.f90:441-452 leave it.  The same for the
+// four averaged fields, so a point takes its eight neighbours' offsets once.
+__device__ __forceinline__ long ff_off(int i, int j, int k, const LagGeom& g) {
   if (k == 0) k = 1;
   const bool inner = (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny);
-  int ii = (i == 0) ? g.nx : ((i == g.nx + 1) ? 1 : i);
+  const int ii = (i == 0) ? g.nx : ((i == g.nx + 1) ? 1 : i);
   int jj;
   if (k >= g.nz + 1) {
-    if (inner) return F[(long)(g.nz + 1) * g.plane + (long)(j - 1) * g.nx + (i - 1)];
+    if (inner) return (long)(g.nz + 1) * g.plane + (long)(j - 1) * g.nx + (i - 1);
     if (g.mode == 1) {
       jj = (j == 0) ? g.ny : ((j == g.ny + 1) ? 1 : j);
-      return F[(long)(g.nz + 1) * g.plane + (long)(jj - 1) * g.nx + (ii - 1)];
+      return (long)(g.nz + 1) * g.plane + (long)(jj - 1) * g.nx + (ii - 1);
     }
     k -= 2;  // self-message halo: levels nz+1, nz+2 hold copies of nz-1, nz
   }
   if (g.mode == 1) jj = (j == 0) ? g.ny : ((j == g.ny + 1) ? 1 : j);
   else jj = (j == 0) ? 2 : ((j == g.ny + 1) ? g.ny - 1 : j);
-  return F[(long)k * g.plane + (long)(jj - 1) * g.nx + (ii - 1)];
+  return (long)k * g.plane + (long)(jj - 1) * g.nx + (ii - 1);
 }
 
 // compute_interpolag_weight (:309-411) + compute_interpolag_coeff (:427-474)
@@ -523,16 +523,30 @@ __global__ void k_lag_interp(const T* ul, const T* vl, const T* wl, const T* F0,
     const int az = k + (signbit(zp) ? -1 : 1);
     const T cx = fabs(xp), cy = fabs(yp), cz = fabs(zp);
     const T fx = T(1) - cx, fy = T(1) - cy, fz = T(1) - cz;
+    // the eight neighbours, then 32 independent loads
+    const long n000 = ff_off(i, j, k, g), n00z = ff_off(i, j, az, g);
+    const long n0y0 = ff_off(i, ay, k, g), n0yz = ff_off(i, ay, az, g);
+    const long nx00 = ff_off(ax, j, k, g), nx0z = ff_off(ax, j, az, g);
+    const long nxy0 = ff_off(ax, ay, k, g), nxyz = ff_off(ax, ay, az, g);
     const T* Fs[4] = {F0, F1, F2, F3};
     T* Ns[4] = {N0, N1, N2, N3};
+    T v[4][8];
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
-      const T* F = Fs[t];
-      Ns[t][o] = fx * fy * (ff_at(F, i, j, k, g) * fz + ff_at(F, i, j, az, g) * cz) +
-                 fx * cy * (ff_at(F, i, ay, k, g) * fz + ff_at(F, i, ay, az, g) * cz) +
-                 cx * fy * (ff_at(F, ax, j, k, g) * fz + ff_at(F, ax, j, az, g) * cz) +
-                 cx * cy * (ff_at(F, ax, ay, k, g) * fz + ff_at(F, ax, ay, az, g) * cz);
+      const T* __restrict__ F = Fs[t];
+      v[t][0] = F[n000];
+      v[t][1] = F[n00z];
+      v[t][2] = F[n0y0];
+      v[t][3] = F[n0yz];
+      v[t][4] = F[nx00];
+      v[t][5] = F[nx0z];
+      v[t][6] = F[nxy0];
+      v[t][7] = F[nxyz];
     }
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+      Ns[t][o] = fx * fy * (v[t][0] * fz + v[t][1] * cz) + fx * cy * (v[t][2] * fz + v[t][3] * cz) +
+                 cx * fy * (v[t][4] * fz + v[t][5] * cz) + cx * cy * (v[t][6] * fz + v[t][7] * cz);
   }
 }
 
