@@ -90,48 +90,61 @@ const Plan& plan_for(int n) {
   return *it->second;
 }
 
+// one Stockham pass of radix R (INV: exponent sign +, conjugate twiddles),
+// compiled per radix and direction so the butterfly loops carry no branches
+template <int R, bool INV>
+inline void fft_bfly(const cd* __restrict in, cd* __restrict out, int p, int q, int m, int s, const cd* tw) {
+  constexpr double sg = INV ? 1.0 : -1.0;
+  auto w = [&](int u) { return INV ? std::conj(tw[u]) : tw[u]; };
+  if constexpr (R == 2) {
+    const cd a = in[q + s * p], b = in[q + s * (p + m)];
+    out[q + s * (2 * p)] = a + b;
+    out[q + s * (2 * p + 1)] = (a - b) * w(0);
+  } else if constexpr (R == 4) {
+    const cd a0 = in[q + s * p], a1 = in[q + s * (p + m)], a2 = in[q + s * (p + 2 * m)],
+             a3 = in[q + s * (p + 3 * m)];
+    const cd t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, t3 = a1 - a3;
+    const cd jt3(-sg * t3.imag(), sg * t3.real());  // sg i t3
+    out[q + s * (4 * p)] = t0 + t2;
+    out[q + s * (4 * p + 1)] = (t1 + jt3) * w(0);
+    out[q + s * (4 * p + 2)] = (t0 - t2) * w(1);
+    out[q + s * (4 * p + 3)] = (t1 - jt3) * w(2);
+  } else {  // R == 3
+    constexpr double s3 = 0.86602540378443864676;  // sqrt(3) / 2
+    const cd a0 = in[q + s * p], a1 = in[q + s * (p + m)], a2 = in[q + s * (p + 2 * m)];
+    const cd t1 = a1 + a2, t2 = a1 - a2;
+    const cd mm = a0 - 0.5 * t1;
+    const cd st(-sg * s3 * t2.imag(), sg * s3 * t2.real());  // sg i sqrt(3)/2 t2
+    out[q + s * (3 * p)] = a0 + t1;
+    out[q + s * (3 * p + 1)] = (mm + st) * w(0);
+    out[q + s * (3 * p + 2)] = (mm - st) * w(1);
+  }
+}
+template <int R, bool INV>
+void fft_pass(const Plan::Stage& S, const cd* __restrict in, cd* __restrict out) {
+  const int m = S.m, s = S.s;
+  const cd* tw = S.tw.data();
+  if (s >= m) {  // the longer of the two loops innermost
+    for (int p = 0; p < m; ++p)
+      for (int q = 0; q < s; ++q) fft_bfly<R, INV>(in, out, p, q, m, s, tw + (size_t)p * (R - 1));
+  } else {
+    for (int q = 0; q < s; ++q)
+      for (int p = 0; p < m; ++p) fft_bfly<R, INV>(in, out, p, q, m, s, tw + (size_t)p * (R - 1));
+  }
+}
+
 // in-place complex transform of x (work: n values); inv: exponent sign +
 void cfft(const Plan& P, cd* x, cd* work, bool inv) {
   cd* in = x;
   cd* out = work;
-  const double sg = inv ? 1.0 : -1.0;
-  const double s3 = std::sqrt(3.0) / 2.0;
   for (const auto& S : P.st) {
-    const int r = S.r, m = S.m, s = S.s;
-    // one butterfly of block p, sub-sequence q (twiddles of block p)
-    auto bfly = [&](int p, int q, const cd* tw) {
-      if (r == 2) {
-        const cd a = in[q + s * p], b = in[q + s * (p + m)];
-        out[q + s * (2 * p)] = a + b;
-        out[q + s * (2 * p + 1)] = (a - b) * (inv ? std::conj(tw[0]) : tw[0]);
-      } else if (r == 4) {
-        const cd a0 = in[q + s * p], a1 = in[q + s * (p + m)], a2 = in[q + s * (p + 2 * m)],
-                 a3 = in[q + s * (p + 3 * m)];
-        const cd t0 = a0 + a2, t1 = a0 - a2, t2 = a1 + a3, t3 = a1 - a3;
-        const cd jt3(-sg * t3.imag(), sg * t3.real());  // sg i t3
-        out[q + s * (4 * p)] = t0 + t2;
-        out[q + s * (4 * p + 1)] = (t1 + jt3) * (inv ? std::conj(tw[0]) : tw[0]);
-        out[q + s * (4 * p + 2)] = (t0 - t2) * (inv ? std::conj(tw[1]) : tw[1]);
-        out[q + s * (4 * p + 3)] = (t1 - jt3) * (inv ? std::conj(tw[2]) : tw[2]);
-      } else {  // r == 3
-        const cd a0 = in[q + s * p], a1 = in[q + s * (p + m)], a2 = in[q + s * (p + 2 * m)];
-        const cd t1 = a1 + a2, t2 = a1 - a2;
-        const cd mm = a0 - 0.5 * t1;
-        const cd st(-sg * s3 * t2.imag(), sg * s3 * t2.real());  // sg i sqrt(3)/2 t2
-        out[q + s * (3 * p)] = a0 + t1;
-        out[q + s * (3 * p + 1)] = (mm + st) * (inv ? std::conj(tw[0]) : tw[0]);
-        out[q + s * (3 * p + 2)] = (mm - st) * (inv ? std::conj(tw[1]) : tw[1]);
-      }
-    };
-    // the longer of the two loops innermost
-    if (s >= m) {
-      for (int p = 0; p < m; ++p) {
-        const cd* tw = S.tw.data() + (size_t)p * (r - 1);
-        for (int q = 0; q < s; ++q) bfly(p, q, tw);
-      }
-    } else {
-      for (int q = 0; q < s; ++q)
-        for (int p = 0; p < m; ++p) bfly(p, q, S.tw.data() + (size_t)p * (r - 1));
+    switch (S.r * 2 + (inv ? 1 : 0)) {
+      case 4: fft_pass<2, false>(S, in, out); break;
+      case 5: fft_pass<2, true>(S, in, out); break;
+      case 6: fft_pass<3, false>(S, in, out); break;
+      case 7: fft_pass<3, true>(S, in, out); break;
+      case 8: fft_pass<4, false>(S, in, out); break;
+      default: fft_pass<4, true>(S, in, out); break;
     }
     std::swap(in, out);
   }
@@ -145,7 +158,7 @@ void r2c_pair(int n, const double* a, const double* b, cd* A, cd* B, cd* z, cd* 
   for (int i = 0; i < n; ++i) z[i] = cd(a[i], b ? b[i] : 0.0);
   cfft(P, z, work, false);
   for (int k = 0; k <= n / 2; ++k) {
-    const cd zk = z[k], zm = std::conj(z[(n - k) % n]);
+    const cd zk = z[k], zm = std::conj(z[k == 0 ? 0 : n - k]);
     A[k] = 0.5 * (zk + zm);
     if (B) B[k] = cd(0.0, -0.5) * (zk - zm);
   }
@@ -155,14 +168,13 @@ void r2c_pair(int n, const double* a, const double* b, cd* A, cd* B, cd* z, cd* 
 void c2r_pair(int n, const cd* A, const cd* B, double* a, double* b, cd* z, cd* work) {
   const Plan& P = plan_for(n);
   const int h = n / 2;
-  for (int k = 0; k <= h; ++k) {
-    cd x = A[k], y = B ? B[k] : cd(0.0, 0.0);
-    if (k == 0 || k == h) {
-      x = cd(x.real(), 0.0);
-      y = cd(y.real(), 0.0);
-    }
+  // bins 0 and n/2: real parts only
+  z[0] = cd(A[0].real(), B ? B[0].real() : 0.0);
+  z[h] = cd(A[h].real(), B ? B[h].real() : 0.0);
+  for (int k = 1; k < h; ++k) {
+    const cd x = A[k], y = B ? B[k] : cd(0.0, 0.0);
     z[k] = x + cd(0.0, 1.0) * y;
-    if (k > 0 && k < h) z[n - k] = std::conj(x) + cd(0.0, 1.0) * std::conj(y);
+    z[n - k] = std::conj(x) + cd(0.0, 1.0) * std::conj(y);
   }
   cfft(P, z, work, true);
   for (int i = 0; i < n; ++i) {
